@@ -1,0 +1,192 @@
+/*
+ * mgpcg_b200.h - C ABI of the B200-native MGPCG Poisson solver.
+ *
+ * This is the boundary a host binding (ctypes, cffi, a C/C++ simulator) links
+ * against.  Signatures use plain C types: integers, float/double scalars,
+ * void pointers to device memory and an opaque plan handle.  A cudaStream_t
+ * is passed as `void*`.  Nothing here allocates device memory: the caller
+ * allocates one workspace of mg_plan_workspace_bytes() and every field of the
+ * solver lives at a fixed offset inside it (mg_plan_field()).
+ *
+ * Each entry point names the reference interface it replaces
+ * (file:line in g1n0st/taichi-ferrofluid).
+ *
+ * Return value of every `int` function: MG_OK (0) or a negative MG_E* code.
+ */
+#ifndef MGPCG_B200_H
+#define MGPCG_B200_H
+
+#include <stdint.h>
+
+#if defined(__GNUC__)
+#define MG_API __attribute__((visibility("default")))
+#else
+#define MG_API
+#endif
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- labels: utils.py:4-6 --------------------------------------------- */
+#define MG_FLUID 0
+#define MG_AIR 1
+#define MG_SOLID 2
+
+/* ---- status codes -------------------------------------------------------- */
+#define MG_OK 0
+#define MG_E_BADARG (-1)    /* invalid size, level count, pointer or field id */
+#define MG_E_CUDA (-2)      /* a CUDA runtime call failed (see mg_last_error) */
+#define MG_E_UNBOUND (-3)   /* the plan has no workspace bound */
+#define MG_E_TOO_BIG (-4)   /* a size exceeds a fixed capacity of the call */
+
+/* solve outcome, written to mg_solve_stats_t.status */
+#define MG_SOLVE_CONVERGED 0
+#define MG_SOLVE_MAX_ITERS 1   /* stopped at max_iters (the reference is silent) */
+#define MG_SOLVE_NONFINITE 2   /* a reduction produced NaN/Inf (H3: zero Adiag) */
+
+/* V-cycle grid storage type */
+#define MG_STORE_F32 0
+#define MG_STORE_F16 1
+#define MG_STORE_BF16 2
+
+/* field ids for mg_plan_field() */
+#define MG_FIELD_B 0        /* level 0, f32: right-hand side       (mgpcg.py:21) */
+#define MG_FIELD_X 1        /* level 0, f32: solution              (mgpcg.py:39) */
+#define MG_FIELD_P 2        /* level 0, f32: CG direction          (mgpcg.py:40) */
+#define MG_FIELD_AP 3       /* level 0, f32: A p                   (mgpcg.py:41) */
+#define MG_FIELD_R 4        /* per level: residual r[l]; level 0 is f32, coarser
+                               levels use the storage type          (mgpcg.py:23) */
+#define MG_FIELD_Z 5        /* per level, storage type: z[l]        (mgpcg.py:25) */
+#define MG_FIELD_TYPE 6     /* per level, int8: grid_type[l]        (mgpcg.py:29) */
+#define MG_FIELD_ADIAG 7    /* per level, f32: Adiag[l]             (mgpcg.py:33) */
+#define MG_FIELD_AX 8       /* per level, f32, component k: Ax[l][k] stored as
+                               `dim` contiguous planes (SoA)        (mgpcg.py:35) */
+
+/* Problem description: MGPCGPoissonSolver.__init__ (mgpcg.py:6-44). */
+typedef struct mg_plan_desc {
+  int32_t dim;          /* 2 or 3 */
+  int32_t res[3];       /* level-0 shape; res[2] ignored when dim == 2 */
+  int32_t levels;       /* n_mg_levels (>= 1); every res[k] % 2^(levels-1) == 0 */
+  int32_t pre_post;     /* pre_and_post_smoothing */
+  int32_t bottom;       /* bottom_smoothing (half of it in each colour order) */
+  int32_t storage;      /* MG_STORE_*: type of the V-cycle grids */
+  int32_t refresh_every;/* recompute r = b - A x every N iterations (0: never) */
+  int32_t reserved;
+} mg_plan_desc_t;
+
+/* Solve parameters: MGPCGPoissonSolver.solve (mgpcg.py:150-155). */
+typedef struct mg_solve_params {
+  int32_t max_iters;    /* -1: no limit */
+  int32_t warm_start;   /* 0: x = 0, r = b (reference); 1: r = b - A x for the given x */
+  double rel_tol;       /* on squared norms: stop when r.r < max(abs_tol, rel_tol * b.b) */
+  double abs_tol;
+  double eps;           /* added to the denominators of alpha and beta */
+} mg_solve_params_t;
+
+/* Outcome of one solve (the reference returns nothing; see H5). */
+typedef struct mg_solve_stats {
+  int32_t status;       /* MG_SOLVE_* */
+  int32_t iters;        /* the reference's `iter` counter at exit */
+  double rTr0;          /* initial r.r */
+  double rTr;           /* final r.r (recursive residual) */
+  double bTb;           /* b.b; the tolerance is max(abs_tol, rel_tol * b.b),
+                           which equals the reference's r0.r0 for a cold start */
+} mg_solve_stats_t;
+
+typedef struct mg_plan mg_plan_t;
+
+/* ---- plan ----------------------------------------------------------------- */
+
+/* MGPCGPoissonSolver.__init__ (mgpcg.py:6-44): validates the description and
+ * lays out every field; allocates host memory only. */
+MG_API int mg_plan_create(const mg_plan_desc_t* desc, mg_plan_t** out);
+MG_API int mg_plan_destroy(mg_plan_t* plan);
+
+/* Bytes of device memory the caller must provide (256-byte aligned). */
+MG_API int64_t mg_plan_workspace_bytes(const mg_plan_t* plan);
+
+/* Offset and size in bytes of a field inside the workspace (mgpcg.py:21-44). */
+MG_API int mg_plan_field(const mg_plan_t* plan, int32_t field, int32_t level, int32_t component,
+                  int64_t* offset, int64_t* nbytes);
+
+/* Binds the workspace base pointer (device memory on the current device). */
+MG_API int mg_plan_bind(mg_plan_t* plan, void* workspace);
+
+/* ---- setup: MGPCGPoissonSolver.initialize / reinitialize ------------------ */
+
+/* initialize() (mgpcg.py:63-77): zeroes every field. */
+MG_API int mg_initialize(mg_plan_t* plan, void* stream);
+
+/* grid_type[0].copy_from(cell_type) (mgpcg.py:81): int32 labels -> int8. */
+MG_API int mg_set_cell_type(mg_plan_t* plan, const int32_t* cell_type, void* stream);
+
+/* init_gridtype(grid_type[l-1], grid_type[l]) (mgpcg.py:46-60, :86). */
+MG_API int mg_init_gridtype(mg_plan_t* plan, int32_t level, void* stream);
+
+/* grid_type[l].fill(FLUID) for every level (mgpcg.py:93). */
+MG_API int mg_fill_fluid(mg_plan_t* plan, void* stream);
+
+/* PressureProjectStrategy.build_b_kernel (pressure_project.py:15-39).
+ * vel[k] is the MAC face velocity of axis k, shape res + e_k (f32);
+ * phi is the level set at cell centres (f32).  ghost != 0 selects the ghost
+ * fluid method; gfm_clamp is the cap on (phi_i - phi_j) / phi_i (1e3 in the
+ * reference). */
+MG_API int mg_build_pressure_b(mg_plan_t* plan, const float* vel0, const float* vel1, const float* vel2,
+                        const float* phi, float p0, float scale_A, float scale_b, int32_t ghost,
+                        float gfm_clamp, void* stream);
+
+/* PressureProjectStrategy.build_A_kernel(level) (pressure_project.py:45-64). */
+MG_API int mg_build_pressure_A(mg_plan_t* plan, int32_t level, const float* phi, float scale_A,
+                        int32_t ghost, float gfm_clamp, void* stream);
+
+/* b[I] += c * src[I] (or += c when src is NULL) on level-0 FLUID cells:
+ * PressureProjectWithVolumeControlStrategy.add_c (volume_control.py:33-37),
+ * and the extra smooth source term of the precision workload. */
+MG_API int mg_add_rhs(mg_plan_t* plan, const float* src, float c, void* stream);
+
+/* Prepares the V-cycle operator after the Strategy has written A:
+ * detects whether every level's off-diagonals are the uniform label-derived
+ * value (the pressure Strategy's form) and, for 16-bit storage, writes the
+ * scaled 16-bit coefficient copies.  Called by mg_pcg_solve when A changed;
+ * callable explicitly to separate setup from solve time. */
+MG_API int mg_plan_prepare(mg_plan_t* plan, void* stream);
+/* Reports the operator form chosen per level: 1 = label-uniform, 0 = stored. */
+MG_API int mg_plan_operator_form(const mg_plan_t* plan, int32_t level, int32_t* form);
+
+/* ---- the reference's per-kernel operations (for parity tests) ------------ */
+
+MG_API int mg_smooth(mg_plan_t* plan, int32_t level, int32_t phase, void* stream);   /* mgpcg.py:104-109 */
+MG_API int mg_restrict(mg_plan_t* plan, int32_t level, void* stream);                /* mgpcg.py:111-118 */
+MG_API int mg_prolongate(mg_plan_t* plan, int32_t level, void* stream);              /* mgpcg.py:120-123 */
+MG_API int mg_v_cycle(mg_plan_t* plan, void* stream);                                /* mgpcg.py:125-148 */
+MG_API int mg_compute_Ap(mg_plan_t* plan, void* stream);                             /* mgpcg.py:218-224 */
+/* reduce(a, b) (mgpcg.py:211-216) over level-0 FLUID cells, FP64 sum, written
+ * to *out_host after a stream synchronize. a, b are MG_FIELD_* of level 0. */
+MG_API int mg_reduce(mg_plan_t* plan, int32_t field_a, int32_t field_b, double* out_host, void* stream);
+
+/* ---- solve ------------------------------------------------------------------ */
+
+/* solve(max_iters, verbose, rel_tol, abs_tol, eps) (mgpcg.py:150-209).
+ * The whole PCG loop runs on the device inside one CUDA graph (a while node);
+ * scalars alpha, beta and the norms are FP64 on the device.  Blocks until done
+ * and writes the outcome to *stats. */
+MG_API int mg_pcg_solve(mg_plan_t* plan, const mg_solve_params_t* params, mg_solve_stats_t* stats,
+                 void* stream);
+
+/* Same solve without the final synchronize: enqueue on `stream`; read the
+ * outcome later with mg_pcg_stats() after the stream has completed. */
+MG_API int mg_pcg_solve_async(mg_plan_t* plan, const mg_solve_params_t* params, void* stream);
+MG_API int mg_pcg_stats(mg_plan_t* plan, mg_solve_stats_t* stats, void* stream);
+
+/* Last CUDA error string recorded by this library (thread-local). */
+MG_API const char* mg_last_error(void);
+
+/* Library version (major * 10000 + minor * 100 + patch). */
+MG_API int32_t mg_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* MGPCG_B200_H */

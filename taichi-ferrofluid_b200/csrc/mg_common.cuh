@@ -1,0 +1,142 @@
+// Shared definitions of the B200 MGPCG library: grid geometry, the per-level
+// view passed to kernels, storage-type conversion and reduction helpers.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <cuda_fp16.h>
+#include <cuda_bf16.h>
+#include <stdint.h>
+
+#include "../../include/mgpcg_b200.h"
+
+namespace mg {
+
+constexpr int8_t FLUID = MG_FLUID;
+constexpr int8_t AIR = MG_AIR;
+constexpr int8_t SOLID = MG_SOLID;
+
+constexpr int kMaxLevels = 12;
+constexpr int kRedThreads = 256;      // threads of every reduction kernel
+constexpr int kMaxPartials = 2048;    // upper bound on reduction blocks
+
+// Row-major grid geometry, last axis fastest.  A 2D grid is stored as
+// (n0, n1, 1) and only axes < dim have neighbours, so one index formula serves
+// both dimensionalities: idx = (i0 * n1 + i1) * n2 + i2.
+struct Geom {
+  int dim;
+  int n[3];
+  long long count;
+  __host__ __device__ inline long long stride(int axis) const {
+    return axis == 0 ? (long long)n[1] * n[2] : (axis == 1 ? (long long)n[2] : 1LL);
+  }
+  __host__ __device__ inline void coords(long long idx, int c[3]) const {
+    c[2] = (int)(idx % n[2]);
+    long long t = idx / n[2];
+    c[1] = (int)(t % n[1]);
+    c[0] = (int)(t / n[1]);
+  }
+  __host__ __device__ inline long long index(int c0, int c1, int c2) const {
+    return ((long long)c0 * n[1] + c1) * n[2] + c2;
+  }
+};
+
+// Device pointers of one multigrid level (all inside the caller's workspace).
+struct Level {
+  Geom g;
+  int8_t* type;     // grid_type[l]
+  float* Adiag;     // public f32 coefficients written by the Strategy
+  float* Ax[3];     // SoA: Ax[k][idx] = A(idx, idx + e_k)
+  void* r;          // level 0: f32 CG residual; coarser: storage type
+  void* z;          // storage type
+  void* Adiag_s;    // storage-type copy of Adiag (aliases Adiag for f32)
+};
+
+// Scalars of the device-resident PCG loop (mgpcg.py:150-209).
+struct Control {
+  double rTr0, bTb, tol, old_zTr, pAp, rTr, new_zTr;
+  double rel_tol, abs_tol, eps;
+  float alpha, beta;          // the reference's f32 scalar fields (mgpcg.py:43-44)
+  int iter, status, max_iters, run;
+  int warm_start, refresh_every, since_refresh, pad0;
+  double scale_z;             // z (true) = scale_z * z (stored), 16-bit storage only
+  double scale_r;             // r (stored, level 0 input of the V-cycle) = scale_r * r
+  unsigned int counter[8];    // arrival counters of the last-block reductions
+  double scratch[8];          // single-value results of mg_reduce
+};
+
+template <typename T> __device__ __forceinline__ float to_f(T v);
+template <> __device__ __forceinline__ float to_f<float>(float v) { return v; }
+template <> __device__ __forceinline__ float to_f<__half>(__half v) { return __half2float(v); }
+template <> __device__ __forceinline__ float to_f<__nv_bfloat16>(__nv_bfloat16 v) { return __bfloat162float(v); }
+
+template <typename T> __device__ __forceinline__ T from_f(float v);
+template <> __device__ __forceinline__ float from_f<float>(float v) { return v; }
+template <> __device__ __forceinline__ __half from_f<__half>(float v) { return __float2half_rn(v); }
+template <> __device__ __forceinline__ __nv_bfloat16 from_f<__nv_bfloat16>(float v) { return __float2bfloat16_rn(v); }
+
+// Neighbour sum of mgpcg.py:96-102 in the reference's operation order:
+//   ret = 0; for each axis i: ret += (Ax[I-e_i][i] * v[I-e_i] + Ax[I][i] * v[I+e_i])
+// An index outside the level contributes 0 (out-of-range rule H1).
+__device__ __forceinline__ float nbr_sum_f32(const Level& L, const float* v, long long idx,
+                                             const int c[3]) {
+  float ret = 0.0f;
+#pragma unroll
+  for (int i = 0; i < 3; ++i) {
+    if (i >= L.g.dim) break;
+    long long s = L.g.stride(i);
+    float lo = 0.0f, hi = 0.0f;
+    if (c[i] > 0) lo = __fmul_rn(L.Ax[i][idx - s], v[idx - s]);
+    if (c[i] + 1 < L.g.n[i]) hi = __fmul_rn(L.Ax[i][idx], v[idx + s]);
+    ret = __fadd_rn(ret, __fadd_rn(lo, hi));
+  }
+  return ret;
+}
+
+// Block-wide FP64 sum; result valid in thread 0.  Fixed tree order.
+template <int NT>
+__device__ __forceinline__ double block_sum(double v, double* sh) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+  const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  if (lane == 0) sh[w] = v;
+  __syncthreads();
+  double t = 0.0;
+  if (w == 0) {
+    t = lane < NT / 32 ? sh[lane] : 0.0;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) t += __shfl_down_sync(0xffffffffu, t, o);
+  }
+  __syncthreads();
+  return t;
+}
+
+// Last-block reduction: every block stores its partial; the block that
+// arrives last sums all partials in index order (deterministic for a fixed
+// grid) and returns true with the total in *total (thread 0 only).
+template <int NT>
+__device__ __forceinline__ bool last_block_total(double partial, double* partials,
+                                                 unsigned int* counter, double* sh,
+                                                 double* total) {
+  __shared__ bool am_last;
+  double s = block_sum<NT>(partial, sh);
+  if (threadIdx.x == 0) {
+    partials[blockIdx.x] = s;
+    __threadfence();
+    unsigned int prev = atomicAdd(counter, 1u);
+    am_last = (prev == gridDim.x - 1);
+  }
+  __syncthreads();
+  if (!am_last) return false;
+  __threadfence();
+  double acc = 0.0;
+  for (unsigned int i = threadIdx.x; i < gridDim.x; i += NT)
+    acc += ((volatile double*)partials)[i];
+  double t = block_sum<NT>(acc, sh);
+  if (threadIdx.x == 0) {
+    *total = t;
+    *counter = 0u;  // ready for the next launch
+  }
+  return true;
+}
+
+}  // namespace mg

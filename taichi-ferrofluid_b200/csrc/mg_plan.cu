@@ -1,0 +1,566 @@
+// Plan, workspace layout, CUDA-graph PCG solve and the C ABI of the B200
+// MGPCG library (include/mgpcg_b200.h).
+//
+// Ownership: the caller allocates one device workspace of
+// mg_plan_workspace_bytes() bytes; every solver field (mgpcg.py:21-44) lives at
+// a fixed 256-byte aligned offset in it.  This file allocates host memory only
+// (the plan, a pinned parameter block) plus the CUDA graph objects.
+#include <cstdio>
+#include <cstring>
+#include <new>
+#include <vector>
+
+#include "mg_common.cuh"
+#include "mg_kernels.cuh"
+#include "mg_pcg.cuh"
+#include "mg_fused.cuh"
+
+using namespace mg;
+
+namespace {
+
+thread_local char g_err[512] = "";
+
+int set_err(const char* what, cudaError_t e) {
+  snprintf(g_err, sizeof(g_err), "%s: %s", what, cudaGetErrorString(e));
+  return MG_E_CUDA;
+}
+int bad(const char* what) {
+  snprintf(g_err, sizeof(g_err), "bad argument: %s", what);
+  return MG_E_BADARG;
+}
+
+#define CK(call)                                   \
+  do {                                             \
+    cudaError_t e_ = (call);                       \
+    if (e_ != cudaSuccess) return set_err(#call, e_); \
+  } while (0)
+
+#define CKL(what)                                  \
+  do {                                             \
+    cudaError_t e_ = cudaGetLastError();           \
+    if (e_ != cudaSuccess) return set_err(what, e_); \
+  } while (0)
+
+constexpr int kFields = 9;
+constexpr int kFieldAdiagS = 9;  // internal: storage copy of Adiag
+constexpr int kFieldCount = 10;
+
+struct Loc {
+  int64_t off = -1, bytes = 0;
+};
+
+int64_t align256(int64_t v) { return (v + 255) & ~int64_t(255); }
+
+int elem_bytes(int storage) { return storage == MG_STORE_F32 ? 4 : 2; }
+
+}  // namespace
+
+struct mg_plan {
+  mg_plan_desc_t d;
+  int L;
+  Geom geom[kMaxLevels];
+  Loc loc[kFieldCount][kMaxLevels][3];
+  int64_t off_partials, off_ctl, ws_bytes;
+  char* base = nullptr;
+  Level lv[kMaxLevels];
+  Control* ctl = nullptr;
+  double* partials = nullptr;
+  int red_blocks = 0;
+  int ew_blocks[kMaxLevels];
+  int op_form[kMaxLevels];
+  float offdiag[kMaxLevels];
+  bool prepared = false;
+  // graph state
+  cudaStream_t cap = nullptr;
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t exec = nullptr;
+  cudaGraphConditionalHandle cond = 0;
+  char* base_of_graph = nullptr;
+  // pinned parameter / stats staging
+  Control* host_ctl = nullptr;
+  int device = -1;
+  int num_sms = 148;
+};
+
+namespace {
+
+int64_t level_cells(const mg_plan* P, int l) { return P->geom[l].count; }
+
+void layout(mg_plan* P) {
+  int64_t off = 0;
+  auto put = [&](int f, int l, int comp, int64_t bytes) {
+    P->loc[f][l][comp].off = off;
+    P->loc[f][l][comp].bytes = bytes;
+    off = align256(off + bytes);
+  };
+  const int es = elem_bytes(P->d.storage);
+  const int dim = P->d.dim;
+  for (int l = 0; l < P->L; ++l) {
+    int64_t n = level_cells(P, l);
+    put(MG_FIELD_TYPE, l, 0, n);
+    put(MG_FIELD_ADIAG, l, 0, n * 4);
+    // the dim components back to back, so Ax[l] is one (dim, *shape) array
+    put(MG_FIELD_AX, l, 0, dim * n * 4);
+    for (int k = 0; k < dim; ++k) {
+      P->loc[MG_FIELD_AX][l][k].off = P->loc[MG_FIELD_AX][l][0].off + k * n * 4;
+      P->loc[MG_FIELD_AX][l][k].bytes = n * 4;
+    }
+    put(MG_FIELD_R, l, 0, n * (l == 0 ? 4 : es));
+    put(MG_FIELD_Z, l, 0, n * es);
+    if (P->d.storage != MG_STORE_F32) put(kFieldAdiagS, l, 0, n * es);
+    else P->loc[kFieldAdiagS][l][0] = P->loc[MG_FIELD_ADIAG][l][0];
+  }
+  int64_t n0 = level_cells(P, 0);
+  put(MG_FIELD_B, 0, 0, n0 * 4);
+  put(MG_FIELD_X, 0, 0, n0 * 4);
+  put(MG_FIELD_P, 0, 0, n0 * 4);
+  put(MG_FIELD_AP, 0, 0, n0 * 4);
+  P->off_partials = off;
+  off = align256(off + sizeof(double) * kMaxPartials);
+  P->off_ctl = off;
+  off = align256(off + sizeof(Control));
+  P->ws_bytes = off;
+}
+
+void bind_views(mg_plan* P) {
+  char* B = P->base;
+  for (int l = 0; l < P->L; ++l) {
+    Level& v = P->lv[l];
+    v.g = P->geom[l];
+    v.type = (int8_t*)(B + P->loc[MG_FIELD_TYPE][l][0].off);
+    v.Adiag = (float*)(B + P->loc[MG_FIELD_ADIAG][l][0].off);
+    for (int k = 0; k < 3; ++k)
+      v.Ax[k] = k < P->d.dim ? (float*)(B + P->loc[MG_FIELD_AX][l][k].off) : nullptr;
+    v.r = B + P->loc[MG_FIELD_R][l][0].off;
+    v.z = B + P->loc[MG_FIELD_Z][l][0].off;
+    v.Adiag_s = B + P->loc[kFieldAdiagS][l][0].off;
+  }
+  P->partials = (double*)(B + P->off_partials);
+  P->ctl = (Control*)(B + P->off_ctl);
+}
+
+inline cudaStream_t S(void* s) { return (cudaStream_t)s; }
+
+float* fptr(mg_plan* P, int f) { return (float*)(P->base + P->loc[f][0][0].off); }
+
+int grid_for(const mg_plan* P, int64_t n, int threads = 256) {
+  int64_t b = (n + threads - 1) / threads;
+  int64_t cap = (int64_t)P->num_sms * 16;
+  if (b > cap) b = cap;
+  if (b < 1) b = 1;
+  return (int)b;
+}
+
+// ---- launch sequences (shared by the direct calls and graph capture) -------
+
+constexpr int64_t kBottomBlockCells = 1 << 16;
+
+int launch_smooth(mg_plan* P, int l, int phase, cudaStream_t s) {
+  int64_t n = level_cells(P, l) / 2 + level_cells(P, l) / (P->d.dim == 3 ? P->geom[l].n[2] : P->geom[l].n[1]);
+  k_smooth<<<grid_for(P, n), 256, 0, s>>>(P->lv[l], phase);
+  CKL("k_smooth");
+  return MG_OK;
+}
+
+int launch_restrict(mg_plan* P, int l, cudaStream_t s) {
+  k_restrict<<<grid_for(P, level_cells(P, l + 1)), 256, 0, s>>>(P->lv[l], P->lv[l + 1]);
+  CKL("k_restrict");
+  return MG_OK;
+}
+
+int launch_prolongate(mg_plan* P, int l, cudaStream_t s) {
+  k_prolongate<<<grid_for(P, level_cells(P, l)), 256, 0, s>>>(P->lv[l], P->lv[l + 1]);
+  CKL("k_prolongate");
+  return MG_OK;
+}
+
+// v_cycle (mgpcg.py:125-148) with the stored-coefficient kernels.
+int launch_vcycle_generic(mg_plan* P, cudaStream_t s) {
+  const int L = P->L;
+  CK(cudaMemsetAsync(P->lv[0].z, 0, level_cells(P, 0) * sizeof(float), s));
+  for (int l = 0; l < L - 1; ++l) {
+    for (int i = 0; i < P->d.pre_post; ++i) {
+      if (int rc = launch_smooth(P, l, 0, s)) return rc;
+      if (int rc = launch_smooth(P, l, 1, s)) return rc;
+    }
+    if (int rc = launch_restrict(P, l, s)) return rc;
+  }
+  const int nh = P->d.bottom / 2;
+  if (level_cells(P, L - 1) <= kBottomBlockCells) {
+    if (nh > 0) {
+      k_bottom<<<1, 1024, 0, s>>>(P->lv[L - 1], nh);
+      CKL("k_bottom");
+    }
+  } else {
+    for (int i = 0; i < nh; ++i) {
+      if (int rc = launch_smooth(P, L - 1, 0, s)) return rc;
+      if (int rc = launch_smooth(P, L - 1, 1, s)) return rc;
+    }
+    for (int i = 0; i < nh; ++i) {
+      if (int rc = launch_smooth(P, L - 1, 1, s)) return rc;
+      if (int rc = launch_smooth(P, L - 1, 0, s)) return rc;
+    }
+  }
+  for (int l = L - 2; l >= 0; --l) {
+    if (int rc = launch_prolongate(P, l, s)) return rc;
+    for (int i = 0; i < P->d.pre_post; ++i) {
+      if (int rc = launch_smooth(P, l, 1, s)) return rc;
+      if (int rc = launch_smooth(P, l, 0, s)) return rc;
+    }
+  }
+  return MG_OK;
+}
+
+bool use_fused(const mg_plan* P) {
+  for (int l = 0; l < P->L; ++l)
+    if (P->op_form[l] != 1) return false;
+  return fused_supported(P->d.dim, P->geom, P->L, P->d.storage);
+}
+
+int launch_vcycle(mg_plan* P, cudaStream_t s) {
+  if (use_fused(P)) return launch_vcycle_fused(P->lv, P->L, P->d.dim, P->d.pre_post, P->d.bottom,
+                                               P->d.storage, P->num_sms, s);
+  return launch_vcycle_generic(P, s);
+}
+
+// The PCG loop as launches (mgpcg.py:150-209).  `prologue` selects the part
+// before the while node; otherwise the while-node body.
+int launch_pcg_part(mg_plan* P, bool prologue, cudaStream_t s) {
+  const Level& L0 = P->lv[0];
+  float* b = fptr(P, MG_FIELD_B);
+  float* x = fptr(P, MG_FIELD_X);
+  float* p = fptr(P, MG_FIELD_P);
+  float* Ap = fptr(P, MG_FIELD_AP);
+  const int RB = P->red_blocks;
+  const int EB = P->ew_blocks[0];
+  if (prologue) {
+    k_pcg_begin<<<RB, kRedThreads, 0, s>>>(L0, b, x, P->ctl, P->partials);
+    CKL("k_pcg_begin");
+    if (int rc = launch_vcycle(P, s)) return rc;
+    k_update_p<<<EB, 256, 0, s>>>(L0, p, P->ctl);
+    CKL("k_update_p");
+    k_zr<<<RB, kRedThreads, 0, s>>>(L0, P->ctl, P->partials, 0);
+    CKL("k_zr");
+  } else {
+    if (int rc = launch_vcycle(P, s)) return rc;
+    k_zr<<<RB, kRedThreads, 0, s>>>(L0, P->ctl, P->partials, 1);
+    CKL("k_zr");
+    k_update_p<<<EB, 256, 0, s>>>(L0, p, P->ctl);
+    CKL("k_update_p");
+  }
+  k_Ap_alpha<<<RB, kRedThreads, 0, s>>>(L0, p, Ap, P->ctl, P->partials);
+  CKL("k_Ap_alpha");
+  k_xr<<<RB, kRedThreads, 0, s>>>(L0, x, p, Ap, P->ctl, P->partials, P->cond, 1);
+  CKL("k_xr");
+  return MG_OK;
+}
+
+void destroy_graph(mg_plan* P) {
+  if (P->exec) cudaGraphExecDestroy(P->exec);
+  if (P->graph) cudaGraphDestroy(P->graph);
+  P->exec = nullptr;
+  P->graph = nullptr;
+  P->base_of_graph = nullptr;
+}
+
+// Builds graph = [prologue] -> while(cond) { body }.
+int build_graph(mg_plan* P) {
+  destroy_graph(P);
+  if (!P->cap) CK(cudaStreamCreateWithFlags(&P->cap, cudaStreamNonBlocking));
+  CK(cudaGraphCreate(&P->graph, 0));
+  CK(cudaGraphConditionalHandleCreate(&P->cond, P->graph, 0, cudaGraphCondAssignDefault));
+  CK(cudaStreamBeginCaptureToGraph(P->cap, P->graph, nullptr, nullptr, 0, cudaStreamCaptureModeRelaxed));
+  int rc = launch_pcg_part(P, true, P->cap);
+  if (rc) {
+    cudaGraph_t g;
+    cudaStreamEndCapture(P->cap, &g);
+    return rc;
+  }
+  cudaStreamCaptureStatus st;
+  const cudaGraphNode_t* deps = nullptr;
+  size_t ndeps = 0;
+  cudaGraph_t capg;
+  CK(cudaStreamGetCaptureInfo(P->cap, &st, nullptr, &capg, &deps, &ndeps));
+  cudaGraphNodeParams cp = {};
+  cp.type = cudaGraphNodeTypeConditional;
+  cp.conditional.handle = P->cond;
+  cp.conditional.type = cudaGraphCondTypeWhile;
+  cp.conditional.size = 1;
+  cudaGraphNode_t cnode;
+  CK(cudaGraphAddNode(&cnode, capg, deps, ndeps, &cp));
+  cudaGraph_t body = cp.conditional.phGraph_out[0];
+  CK(cudaStreamUpdateCaptureDependencies(P->cap, &cnode, 1, cudaStreamSetCaptureDependencies));
+  cudaGraph_t out;
+  CK(cudaStreamEndCapture(P->cap, &out));
+  CK(cudaStreamBeginCaptureToGraph(P->cap, body, nullptr, nullptr, 0, cudaStreamCaptureModeRelaxed));
+  rc = launch_pcg_part(P, false, P->cap);
+  {
+    cudaGraph_t g2;
+    cudaError_t e = cudaStreamEndCapture(P->cap, &g2);
+    if (rc) return rc;
+    if (e != cudaSuccess) return set_err("cudaStreamEndCapture(body)", e);
+  }
+  CK(cudaGraphInstantiate(&P->exec, P->graph, 0));
+  P->base_of_graph = P->base;
+  return MG_OK;
+}
+
+}  // namespace
+
+// ============================================================================
+// C ABI
+// ============================================================================
+extern "C" {
+
+const char* mg_last_error(void) { return g_err; }
+int32_t mg_version(void) { return 10000; }
+
+int mg_plan_create(const mg_plan_desc_t* desc, mg_plan_t** out) {
+  if (!desc || !out) return bad("null pointer");
+  const mg_plan_desc_t& d = *desc;
+  if (d.dim != 2 && d.dim != 3) return bad("dim must be 2 or 3");
+  if (d.levels < 1 || d.levels > kMaxLevels) return bad("levels out of range");
+  if (d.pre_post < 0 || d.bottom < 0) return bad("negative sweep count");
+  if (d.storage < MG_STORE_F32 || d.storage > MG_STORE_BF16) return bad("storage");
+  for (int k = 0; k < d.dim; ++k) {
+    if (d.res[k] < 2) return bad("res must be >= 2");
+    if (d.res[k] % (1 << (d.levels - 1)) != 0) return bad("res must be divisible by 2^(levels-1)");
+  }
+  mg_plan* P = new (std::nothrow) mg_plan();
+  if (!P) return bad("out of host memory");
+  P->d = d;
+  P->L = d.levels;
+  for (int l = 0; l < P->L; ++l) {
+    Geom& g = P->geom[l];
+    g.dim = d.dim;
+    g.n[0] = d.res[0] >> l;
+    g.n[1] = d.res[1] >> l;
+    g.n[2] = d.dim == 3 ? (d.res[2] >> l) : 1;
+    g.count = (long long)g.n[0] * g.n[1] * g.n[2];
+    P->op_form[l] = 0;
+  }
+  layout(P);
+  cudaGetDevice(&P->device);
+  int sms = 0;
+  if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, P->device) == cudaSuccess && sms > 0)
+    P->num_sms = sms;
+  cudaGetLastError();
+  int64_t n0 = P->geom[0].count;
+  int64_t rb = (n0 + kRedThreads * 8 - 1) / (kRedThreads * 8);
+  if (rb > P->num_sms * 4) rb = P->num_sms * 4;
+  if (rb > kMaxPartials / 2) rb = kMaxPartials / 2;  // two partial regions (b.b and r.r)
+  if (rb < 1) rb = 1;
+  P->red_blocks = (int)rb;
+  for (int l = 0; l < P->L; ++l) P->ew_blocks[l] = grid_for(P, P->geom[l].count);
+  *out = P;
+  return MG_OK;
+}
+
+int mg_plan_destroy(mg_plan_t* P) {
+  if (!P) return MG_OK;
+  destroy_graph(P);
+  if (P->cap) cudaStreamDestroy(P->cap);
+  if (P->host_ctl) cudaFreeHost(P->host_ctl);
+  delete P;
+  return MG_OK;
+}
+
+int64_t mg_plan_workspace_bytes(const mg_plan_t* P) { return P ? P->ws_bytes : -1; }
+
+int mg_plan_field(const mg_plan_t* P, int32_t field, int32_t level, int32_t comp, int64_t* offset,
+                  int64_t* nbytes) {
+  if (!P || !offset || !nbytes) return bad("null pointer");
+  if (field < 0 || field >= kFields) return bad("field id");
+  if (level < 0 || level >= P->L) return bad("level");
+  bool level0_only = field == MG_FIELD_B || field == MG_FIELD_X || field == MG_FIELD_P || field == MG_FIELD_AP;
+  if (level0_only && level != 0) return bad("field exists on level 0 only");
+  int ncomp = field == MG_FIELD_AX ? P->d.dim : 1;
+  if (comp < 0 || comp >= ncomp) return bad("component");
+  *offset = P->loc[field][level][comp].off;
+  *nbytes = P->loc[field][level][comp].bytes;
+  return MG_OK;
+}
+
+int mg_plan_bind(mg_plan_t* P, void* ws) {
+  if (!P || !ws) return bad("null pointer");
+  if (((uintptr_t)ws & 255u) != 0) return bad("workspace must be 256-byte aligned");
+  P->base = (char*)ws;
+  bind_views(P);
+  if (!P->host_ctl) CK(cudaMallocHost(&P->host_ctl, sizeof(Control)));
+  return MG_OK;
+}
+
+#define NEED_BOUND(P)                        \
+  do {                                       \
+    if (!(P)) return bad("null plan");       \
+    if (!(P)->base) {                        \
+      snprintf(g_err, sizeof(g_err), "plan has no workspace"); \
+      return MG_E_UNBOUND;                   \
+    }                                        \
+  } while (0)
+
+int mg_initialize(mg_plan_t* P, void* stream) {
+  NEED_BOUND(P);
+  // Every field, including the control block (counters, beta).
+  CK(cudaMemsetAsync(P->base, 0, P->ws_bytes, S(stream)));
+  P->prepared = false;
+  return MG_OK;
+}
+
+int mg_set_cell_type(mg_plan_t* P, const int32_t* ct, void* stream) {
+  NEED_BOUND(P);
+  if (!ct) return bad("cell_type");
+  k_set_cell_type<<<P->ew_blocks[0], 256, 0, S(stream)>>>(ct, P->lv[0].type, P->geom[0].count);
+  CKL("k_set_cell_type");
+  P->prepared = false;
+  return MG_OK;
+}
+
+int mg_init_gridtype(mg_plan_t* P, int32_t level, void* stream) {
+  NEED_BOUND(P);
+  if (level < 1 || level >= P->L) return bad("level");
+  k_init_gridtype<<<P->ew_blocks[level], 256, 0, S(stream)>>>(P->lv[level - 1], P->lv[level]);
+  CKL("k_init_gridtype");
+  P->prepared = false;
+  return MG_OK;
+}
+
+int mg_fill_fluid(mg_plan_t* P, void* stream) {
+  NEED_BOUND(P);
+  for (int l = 0; l < P->L; ++l) CK(cudaMemsetAsync(P->lv[l].type, MG_FLUID, P->geom[l].count, S(stream)));
+  P->prepared = false;
+  return MG_OK;
+}
+
+int mg_build_pressure_b(mg_plan_t* P, const float* v0, const float* v1, const float* v2, const float* phi,
+                        float p0, float sA, float sB, int32_t ghost, float clamp, void* stream) {
+  NEED_BOUND(P);
+  if (!v0 || !v1 || (P->d.dim == 3 && !v2)) return bad("velocity");
+  if (ghost && !phi) return bad("phi");
+  k_build_pressure_b<<<P->ew_blocks[0], 256, 0, S(stream)>>>(P->lv[0], v0, v1, v2, phi, p0, sA, sB, ghost,
+                                                             clamp, fptr(P, MG_FIELD_B));
+  CKL("k_build_pressure_b");
+  return MG_OK;
+}
+
+int mg_build_pressure_A(mg_plan_t* P, int32_t level, const float* phi, float sA, int32_t ghost, float clamp,
+                        void* stream) {
+  NEED_BOUND(P);
+  if (level < 0 || level >= P->L) return bad("level");
+  if (ghost && level == 0 && !phi) return bad("phi");
+  k_build_pressure_A<<<P->ew_blocks[level], 256, 0, S(stream)>>>(P->lv[level], level, phi, sA, ghost, clamp);
+  CKL("k_build_pressure_A");
+  P->prepared = false;
+  return MG_OK;
+}
+
+int mg_add_rhs(mg_plan_t* P, const float* src, float c, void* stream) {
+  NEED_BOUND(P);
+  k_add_rhs<<<P->ew_blocks[0], 256, 0, S(stream)>>>(P->lv[0], fptr(P, MG_FIELD_B), src, c);
+  CKL("k_add_rhs");
+  return MG_OK;
+}
+
+int mg_plan_prepare(mg_plan_t* P, void* stream) {
+  NEED_BOUND(P);
+  if (int rc = prepare_operator(P->lv, P->L, P->d.storage, P->ctl, P->partials, P->num_sms, P->op_form,
+                                P->offdiag, S(stream)))
+    return rc == MG_E_CUDA ? set_err("prepare_operator", cudaGetLastError()) : rc;
+  P->prepared = true;
+  return MG_OK;
+}
+
+int mg_plan_operator_form(const mg_plan_t* P, int32_t level, int32_t* form) {
+  if (!P || !form) return bad("null pointer");
+  if (level < 0 || level >= P->L) return bad("level");
+  *form = P->op_form[level];
+  return MG_OK;
+}
+
+int mg_smooth(mg_plan_t* P, int32_t level, int32_t phase, void* stream) {
+  NEED_BOUND(P);
+  if (level < 0 || level >= P->L || (phase != 0 && phase != 1)) return bad("level/phase");
+  if (P->d.storage != MG_STORE_F32) return bad("per-kernel entry points need f32 storage");
+  return launch_smooth(P, level, phase, S(stream));
+}
+
+int mg_restrict(mg_plan_t* P, int32_t level, void* stream) {
+  NEED_BOUND(P);
+  if (level < 0 || level >= P->L - 1) return bad("level");
+  if (P->d.storage != MG_STORE_F32) return bad("per-kernel entry points need f32 storage");
+  return launch_restrict(P, level, S(stream));
+}
+
+int mg_prolongate(mg_plan_t* P, int32_t level, void* stream) {
+  NEED_BOUND(P);
+  if (level < 0 || level >= P->L - 1) return bad("level");
+  if (P->d.storage != MG_STORE_F32) return bad("per-kernel entry points need f32 storage");
+  return launch_prolongate(P, level, S(stream));
+}
+
+int mg_v_cycle(mg_plan_t* P, void* stream) {
+  NEED_BOUND(P);
+  if (!P->prepared)
+    if (int rc = mg_plan_prepare(P, stream)) return rc;
+  return launch_vcycle(P, S(stream));
+}
+
+int mg_compute_Ap(mg_plan_t* P, void* stream) {
+  NEED_BOUND(P);
+  k_compute_Ap<<<P->ew_blocks[0], 256, 0, S(stream)>>>(P->lv[0], fptr(P, MG_FIELD_P), fptr(P, MG_FIELD_AP));
+  CKL("k_compute_Ap");
+  return MG_OK;
+}
+
+int mg_reduce(mg_plan_t* P, int32_t fa, int32_t fb, double* out, void* stream) {
+  NEED_BOUND(P);
+  auto ok = [](int f) { return f == MG_FIELD_B || f == MG_FIELD_X || f == MG_FIELD_P || f == MG_FIELD_AP ||
+                               f == MG_FIELD_R || f == MG_FIELD_Z; };
+  if (!ok(fa) || !ok(fb) || !out) return bad("reduce fields");
+  if (P->d.storage != MG_STORE_F32 && (fa == MG_FIELD_Z || fb == MG_FIELD_Z)) return bad("z is not f32");
+  const float* a = (const float*)(P->base + P->loc[fa][0][0].off);
+  const float* b = (const float*)(P->base + P->loc[fb][0][0].off);
+  k_dot<<<P->red_blocks, kRedThreads, 0, S(stream)>>>(P->lv[0], a, b, P->ctl, P->partials, 0);
+  CKL("k_dot");
+  CK(cudaMemcpyAsync(out, &P->ctl->scratch[0], sizeof(double), cudaMemcpyDeviceToHost, S(stream)));
+  CK(cudaStreamSynchronize(S(stream)));
+  return MG_OK;
+}
+
+int mg_pcg_solve_async(mg_plan_t* P, const mg_solve_params_t* prm, void* stream) {
+  NEED_BOUND(P);
+  if (!prm) return bad("params");
+  if (prm->max_iters < -1) return bad("max_iters");
+  if (!P->prepared)
+    if (int rc = mg_plan_prepare(P, stream)) return rc;
+  if (!P->exec || P->base_of_graph != P->base)
+    if (int rc = build_graph(P)) return rc;
+  // Parameters travel as kernel arguments (copied at launch, so back-to-back
+  // asynchronous solves cannot race on a host staging buffer); the previous
+  // solve's outputs and beta stay in place (mgpcg.py:44 persists beta).
+  k_set_params<<<1, 1, 0, S(stream)>>>(P->ctl, *prm, P->d.refresh_every);
+  CKL("k_set_params");
+  CK(cudaGraphLaunch(P->exec, S(stream)));
+  return MG_OK;
+}
+
+int mg_pcg_stats(mg_plan_t* P, mg_solve_stats_t* st, void* stream) {
+  NEED_BOUND(P);
+  if (!st) return bad("stats");
+  CK(cudaMemcpyAsync(P->host_ctl, P->ctl, sizeof(Control), cudaMemcpyDeviceToHost, S(stream)));
+  CK(cudaStreamSynchronize(S(stream)));
+  st->status = P->host_ctl->status;
+  st->iters = P->host_ctl->iter;
+  st->rTr0 = P->host_ctl->rTr0;
+  st->rTr = P->host_ctl->rTr;
+  st->bTb = P->host_ctl->bTb;
+  return MG_OK;
+}
+
+int mg_pcg_solve(mg_plan_t* P, const mg_solve_params_t* prm, mg_solve_stats_t* st, void* stream) {
+  if (int rc = mg_pcg_solve_async(P, prm, stream)) return rc;
+  return mg_pcg_stats(P, st, stream);
+}
+
+}  // extern "C"

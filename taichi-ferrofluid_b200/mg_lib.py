@@ -1,0 +1,141 @@
+"""ctypes binding of ``libmgpcg_b200.so`` (declared in include/mgpcg_b200.h).
+
+The library is the only compute path: importing this module raises if the
+shared object is missing or does not export every entry point of the header.
+There is no CPU or PyTorch fallback.
+"""
+import ctypes
+import os
+import re
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libmgpcg_b200.so")
+HEADER_PATH = os.path.join(HERE, "..", "include", "mgpcg_b200.h")
+
+FLUID, AIR, SOLID = 0, 1, 2
+
+MG_OK = 0
+MG_E_BADARG = -1
+MG_E_CUDA = -2
+MG_E_UNBOUND = -3
+MG_E_TOO_BIG = -4
+
+SOLVE_CONVERGED, SOLVE_MAX_ITERS, SOLVE_NONFINITE = 0, 1, 2
+STATUS_NAMES = {0: "converged", 1: "max_iters", 2: "nonfinite"}
+
+STORE = {"f32": 0, "fp32": 0, "float32": 0, "f16": 1, "fp16": 1, "float16": 1, "bf16": 2, "bfloat16": 2}
+STORE_BYTES = {0: 4, 1: 2, 2: 2}
+
+FIELD_B, FIELD_X, FIELD_P, FIELD_AP, FIELD_R, FIELD_Z, FIELD_TYPE, FIELD_ADIAG, FIELD_AX = range(9)
+
+
+class MGError(RuntimeError):
+    """A negative status from the C library, with its error string."""
+
+    def __init__(self, rc, where):
+        super().__init__(f"{where} failed with status {rc}: {last_error()}")
+        self.rc = rc
+
+
+class PlanDesc(ctypes.Structure):
+    _fields_ = [("dim", ctypes.c_int32), ("res", ctypes.c_int32 * 3), ("levels", ctypes.c_int32),
+                ("pre_post", ctypes.c_int32), ("bottom", ctypes.c_int32), ("storage", ctypes.c_int32),
+                ("refresh_every", ctypes.c_int32), ("reserved", ctypes.c_int32)]
+
+
+class SolveParams(ctypes.Structure):
+    _fields_ = [("max_iters", ctypes.c_int32), ("warm_start", ctypes.c_int32), ("rel_tol", ctypes.c_double),
+                ("abs_tol", ctypes.c_double), ("eps", ctypes.c_double)]
+
+
+class SolveStats(ctypes.Structure):
+    _fields_ = [("status", ctypes.c_int32), ("iters", ctypes.c_int32), ("rTr0", ctypes.c_double),
+                ("rTr", ctypes.c_double), ("bTb", ctypes.c_double)]
+
+
+_vp = ctypes.c_void_p
+_i32 = ctypes.c_int32
+_f32 = ctypes.c_float
+_SIGS = {
+    "mg_plan_create": (ctypes.c_int, [ctypes.POINTER(PlanDesc), ctypes.POINTER(_vp)]),
+    "mg_plan_destroy": (ctypes.c_int, [_vp]),
+    "mg_plan_workspace_bytes": (ctypes.c_int64, [_vp]),
+    "mg_plan_field": (ctypes.c_int, [_vp, _i32, _i32, _i32, ctypes.POINTER(ctypes.c_int64),
+                                     ctypes.POINTER(ctypes.c_int64)]),
+    "mg_plan_bind": (ctypes.c_int, [_vp, _vp]),
+    "mg_initialize": (ctypes.c_int, [_vp, _vp]),
+    "mg_set_cell_type": (ctypes.c_int, [_vp, _vp, _vp]),
+    "mg_init_gridtype": (ctypes.c_int, [_vp, _i32, _vp]),
+    "mg_fill_fluid": (ctypes.c_int, [_vp, _vp]),
+    "mg_build_pressure_b": (ctypes.c_int, [_vp, _vp, _vp, _vp, _vp, _f32, _f32, _f32, _i32, _f32, _vp]),
+    "mg_build_pressure_A": (ctypes.c_int, [_vp, _i32, _vp, _f32, _i32, _f32, _vp]),
+    "mg_add_rhs": (ctypes.c_int, [_vp, _vp, _f32, _vp]),
+    "mg_plan_prepare": (ctypes.c_int, [_vp, _vp]),
+    "mg_plan_operator_form": (ctypes.c_int, [_vp, _i32, ctypes.POINTER(_i32)]),
+    "mg_smooth": (ctypes.c_int, [_vp, _i32, _i32, _vp]),
+    "mg_restrict": (ctypes.c_int, [_vp, _i32, _vp]),
+    "mg_prolongate": (ctypes.c_int, [_vp, _i32, _vp]),
+    "mg_v_cycle": (ctypes.c_int, [_vp, _vp]),
+    "mg_compute_Ap": (ctypes.c_int, [_vp, _vp]),
+    "mg_reduce": (ctypes.c_int, [_vp, _i32, _i32, ctypes.POINTER(ctypes.c_double), _vp]),
+    "mg_pcg_solve": (ctypes.c_int, [_vp, ctypes.POINTER(SolveParams), ctypes.POINTER(SolveStats), _vp]),
+    "mg_pcg_solve_async": (ctypes.c_int, [_vp, ctypes.POINTER(SolveParams), _vp]),
+    "mg_pcg_stats": (ctypes.c_int, [_vp, ctypes.POINTER(SolveStats), _vp]),
+    "mg_last_error": (ctypes.c_char_p, []),
+    "mg_version": (ctypes.c_int32, []),
+}
+
+_lib = None
+
+
+def header_entry_points():
+    """Names of every function declared in include/mgpcg_b200.h."""
+    with open(HEADER_PATH) as f:
+        text = f.read()
+    return sorted(set(re.findall(r"MG_API\s+[\w\s\*]*?\b(mg_\w+)\s*\(", text)))
+
+
+def load():
+    """Loads the library once; raises if it is missing or incomplete."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIB_PATH):
+        raise ImportError(f"{LIB_PATH} is missing: build it with build_lib.py (no fallback exists)")
+    lib = ctypes.CDLL(LIB_PATH)
+    missing = [n for n in header_entry_points() if not hasattr(lib, n)]
+    if missing:
+        raise ImportError(f"{LIB_PATH} lacks entry points {missing}")
+    for name, (res, args) in _SIGS.items():
+        fn = getattr(lib, name)
+        fn.restype = res
+        fn.argtypes = args
+    _lib = lib
+    return lib
+
+
+def last_error() -> str:
+    if _lib is None:
+        return ""
+    s = _lib.mg_last_error()
+    return s.decode() if s else ""
+
+
+def check(rc, where=""):
+    if rc != MG_OK:
+        raise MGError(rc, where)
+    return rc
+
+
+def ptr(t):
+    """Device (or host) address of a tensor / array, or None."""
+    if t is None:
+        return None
+    if hasattr(t, "data_ptr"):
+        return t.data_ptr()
+    return t.ctypes.data
+
+
+def stream_ptr(device=None):
+    import torch
+    return torch.cuda.current_stream(device).cuda_stream

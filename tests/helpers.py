@@ -1,0 +1,54 @@
+"""Shared set-up for the parity tests: one scene fed to the CUDA solver and to
+the CPU oracle with identical inputs."""
+import numpy as np
+
+import mg_scenes
+
+
+def small_3d(n=32, seed=1, levels=3):
+    """The 3D drop/pool scene at a size the oracle finishes in well under a second."""
+    return mg_scenes.ferro_drop_3d(n=n, seed=seed, levels=levels)
+
+
+def oracle_for(scene, real=np.float32, bottom=50, pre_post=2, levels=None, clamp=None):
+    from oracle import OracleSolver
+    L = levels or scene.levels
+    o = OracleSolver(scene.dim, scene.res, L, pre_post, bottom, real=real)
+    o.reinitialize_pressure(scene.cell_type, scene.velocity, scene.phi, scene.p0, scene.scale_A, scene.scale_b,
+                            True, scene.gfm_clamp if clamp is None else clamp)
+    if scene.extra_rhs is not None:
+        b = o.get("b")
+        fl = o.get("grid_type") == 0
+        b[fl] = (b[fl].astype(real) + scene.extra_rhs[fl].astype(real)).astype(real)
+        o.set("b", b)
+    return o
+
+
+def gpu_for(scene, storage=None, bottom=50, pre_post=2, levels=None, clamp=None, refresh_every=None):
+    import torch
+    from mgpcg import MGPCGPoissonSolver
+    from pressure_project import PressureProjectStrategy
+    dev = torch.device("cuda", 0)
+    L = levels or scene.levels
+    s = MGPCGPoissonSolver(scene.dim, scene.res, L, pre_post, bottom, storage=storage, device=dev,
+                           refresh_every=refresh_every)
+    vel = [torch.from_numpy(v).to(dev) for v in scene.velocity]
+    phi = torch.from_numpy(scene.phi).to(dev)
+    st = PressureProjectStrategy(scene.dim, vel, True, phi, scene.p0,
+                                 gfm_clamp=scene.gfm_clamp if clamp is None else clamp)
+    st.scale_A = scene.scale_A
+    st.scale_b = scene.scale_b
+    s.reinitialize(torch.from_numpy(scene.cell_type).to(dev), st)
+    if scene.extra_rhs is not None:
+        src = torch.from_numpy(scene.extra_rhs).to(dev)
+        from mg_lib import check
+        check(s.lib.mg_add_rhs(s.plan, src.data_ptr(), 1.0, s._s()), "mg_add_rhs")
+        torch.cuda.synchronize()
+    return s, st
+
+
+def rel_l2(a, b):
+    a = np.asarray(a, np.float64)
+    b = np.asarray(b, np.float64)
+    d = np.linalg.norm(b)
+    return float(np.linalg.norm(a - b) / (d if d > 0 else 1.0))

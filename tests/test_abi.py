@@ -1,0 +1,89 @@
+"""The C-ABI library loads, exports every entry point of include/mgpcg_b200.h
+and validates plans on the host (no GPU needed)."""
+import ctypes
+
+import pytest
+
+import mg_lib
+
+
+def test_library_exports_every_header_symbol():
+    lib = mg_lib.load()
+    names = mg_lib.header_entry_points()
+    assert len(names) >= 20
+    for n in names:
+        assert hasattr(lib, n), n
+    assert lib.mg_version() >= 10000
+
+
+def _desc(dim=3, res=(64, 64, 64), levels=4, storage=0):
+    d = mg_lib.PlanDesc()
+    d.dim = dim
+    for k in range(3):
+        d.res[k] = res[k] if k < len(res) else 1
+    d.levels = levels
+    d.pre_post = 2
+    d.bottom = 50
+    d.storage = storage
+    return d
+
+
+def _create(d):
+    lib = mg_lib.load()
+    p = ctypes.c_void_p()
+    rc = lib.mg_plan_create(ctypes.byref(d), ctypes.byref(p))
+    return rc, p
+
+
+@pytest.mark.parametrize("dim,res,levels", [(2, (128, 128), 4), (3, (64, 64, 64), 5), (2, (96, 64), 4)])
+def test_plan_layout(dim, res, levels):
+    lib = mg_lib.load()
+    rc, p = _create(_desc(dim, res, levels))
+    assert rc == 0
+    try:
+        ws = lib.mg_plan_workspace_bytes(p)
+        spans = []
+        for f in range(9):
+            for l in range(levels):
+                ncomp = dim if f == mg_lib.FIELD_AX else 1
+                for c in range(ncomp):
+                    off, nb = ctypes.c_int64(), ctypes.c_int64()
+                    r = lib.mg_plan_field(p, f, l, c, ctypes.byref(off), ctypes.byref(nb))
+                    if f in (mg_lib.FIELD_B, mg_lib.FIELD_X, mg_lib.FIELD_P, mg_lib.FIELD_AP) and l > 0:
+                        assert r == mg_lib.MG_E_BADARG
+                        continue
+                    assert r == 0
+                    assert off.value % 16 == 0 and 0 <= off.value and off.value + nb.value <= ws
+                    cells = 1
+                    for v in res:
+                        cells *= v >> l
+                    esz = {mg_lib.FIELD_TYPE: 1}.get(f, 4)
+                    assert nb.value == cells * esz
+                    spans.append((off.value, off.value + nb.value))
+        spans.sort()
+        for a, b in zip(spans, spans[1:]):
+            assert a[1] <= b[0], "fields overlap"
+    finally:
+        lib.mg_plan_destroy(p)
+
+
+@pytest.mark.parametrize("kw", [dict(dim=4), dict(levels=0), dict(levels=13), dict(res=(100, 64, 64), levels=4),
+                                dict(storage=7)])
+def test_plan_rejects_bad_descriptions(kw):
+    args = dict(dim=3, res=(64, 64, 64), levels=4, storage=0)
+    args.update(kw)
+    rc, p = _create(_desc(**args))
+    assert rc == mg_lib.MG_E_BADARG
+    assert "bad argument" in mg_lib.last_error()
+
+
+def test_unbound_plan_is_refused():
+    lib = mg_lib.load()
+    rc, p = _create(_desc())
+    assert rc == 0
+    try:
+        assert lib.mg_initialize(p, None) == mg_lib.MG_E_UNBOUND
+        assert lib.mg_v_cycle(p, None) == mg_lib.MG_E_UNBOUND
+        assert lib.mg_plan_bind(p, ctypes.c_void_p(1234)) == mg_lib.MG_E_BADARG  # misaligned
+    finally:
+        lib.mg_plan_destroy(p)
