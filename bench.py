@@ -1,0 +1,421 @@
+"""Benchmark of the MGPCG Poisson path: solves/s and p50/p99 latency.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference]
+                    [--workload substep128|precision256|dam2d] [--storage f32|f16|bf16]
+
+A step is one substep's worth of Poisson solves of the workload, each solve
+= reinitialize(cell_type, strategy) + solve(500) at 1e-6 relative residual:
+
+* substep128 (default): the 3D ferrofluid substep at 128^3, 5 levels, pre/post
+  2, bottom 50: (a) the ghost-fluid pressure solve, (b) the magnetic potential
+  solve when available.
+* precision256: the 256^3 drop/pool scene with the smooth extra source, 6 levels.
+* dam2d: the 2D dam break at 128^2, 4 levels (the reference's CPU-runnable case).
+
+Inputs are seeded synthetic fields (mg_scenes); there is no dataset.
+`value` = solves/s with the inputs resident in HBM; `e2e` = the same through
+the public API with the inputs copied from pinned host memory and the pressure
+copied back inside each timed step.  L2 (126 MB) is flushed before every timed
+step.  Multi-GPU runs are independent replicas (the path shards by solve).
+`--impl reference` times the CPU oracle (C++/OpenMP restatement of the
+reference; the Taichi reference cannot be installed here) on the same workload.
+"""
+import argparse
+import json
+import os
+import subprocess
+import sys
+import tempfile
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+PKG = os.path.join(ROOT, "taichi-ferrofluid_b200")
+for _p in (PKG, ROOT):
+    if _p not in sys.path:
+        sys.path.insert(0, _p)
+
+import numpy as np  # noqa: E402
+
+import mg_scenes  # noqa: E402
+
+WORKLOADS = {
+    "substep128": dict(desc="3D ferrofluid substep 128^3 (pressure + potential solves), 5 levels",
+                       scenes=lambda: [mg_scenes.ferro_drop_3d(n=128, seed=1, levels=5)]),
+    "precision256": dict(desc="3D drop/pool 256^3 with smooth source, 6 levels",
+                         scenes=lambda: [mg_scenes.precision_3d(n=256, seed=2, levels=6)]),
+    "dam2d": dict(desc="2D dam break 128^2, 4 levels", scenes=lambda: [mg_scenes.dam_break_2d()]),
+}
+
+MAX_ITERS = 500
+REL_TOL = 1e-12  # squared: 1e-6 relative residual
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--workload", default="substep128", choices=list(WORKLOADS))
+    ap.add_argument("--storage", default="f32", choices=["f32", "f16", "bf16"])
+    ap.add_argument("--cpu-seconds", type=float, default=12.0, help="CPU baseline sample length")
+    return ap.parse_args()
+
+
+# ---------------------------------------------------------------- distributed
+def dist_init(n):
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        import torch
+        import torch.distributed as dist
+        import datetime
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    return rank, world, local
+
+
+def max_over_ranks(v, world):
+    if world == 1:
+        return v
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([float(v)], device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def barrier(world):
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+
+
+# ---------------------------------------------------------------- clocks
+class Clocks:
+    """nvidia-smi sampled every 200 ms while the timed region runs."""
+
+    def __init__(self, index):
+        self.index = index
+        self.proc = None
+        self.path = None
+
+    def __enter__(self):
+        fd, self.path = tempfile.mkstemp(suffix=".csv")
+        os.close(fd)
+        q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.index}", f"--query-gpu={q}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+        return self
+
+    def __exit__(self, *a):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self):
+        rows = []
+        try:
+            with open(self.path) as f:
+                for line in f:
+                    parts = [p.strip() for p in line.split(",")]
+                    if len(parts) >= 9 and parts[1].replace(".", "").isdigit():
+                        rows.append(parts)
+        except Exception:
+            pass
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"], "samples": 0}
+        sm = sorted(float(r[1]) for r in rows)
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in rows for i in range(4) if r[5 + i].lower().startswith("active")})
+        return {"sm_mhz": sm[len(sm) // 2], "sm_max_mhz": float(rows[0][2]), "reasons": reasons,
+                "samples": len(rows), "power_w_max": max(float(r[3]) for r in rows if r[3].replace(".", "").isdigit())
+                if any(r[3].replace(".", "").isdigit() for r in rows) else None}
+
+
+# ---------------------------------------------------------------- GPU arm
+class GpuCase:
+    """One solve of a scene through the drop-in API with device-resident inputs."""
+
+    def __init__(self, scene, storage, dev):
+        import torch
+        from mgpcg import MGPCGPoissonSolver
+        from pressure_project import PressureProjectStrategy
+        self.scene = scene
+        self.dev = dev
+        self.solver = MGPCGPoissonSolver(scene.dim, scene.res, scene.levels, 2, 50, storage=storage, device=dev)
+        self.vel = [torch.from_numpy(v).to(dev) for v in scene.velocity]
+        self.phi = torch.from_numpy(scene.phi).to(dev)
+        self.ct = torch.from_numpy(scene.cell_type).to(dev)
+        self.extra = torch.from_numpy(scene.extra_rhs).to(dev) if scene.extra_rhs is not None else None
+        self.strategy = PressureProjectStrategy(scene.dim, self.vel, True, self.phi, scene.p0,
+                                                gfm_clamp=scene.gfm_clamp)
+        self.strategy.scale_A = scene.scale_A
+        self.strategy.scale_b = scene.scale_b
+        # pinned host copies for the end-to-end path
+        self.h_vel = [torch.from_numpy(v).pin_memory() for v in scene.velocity]
+        self.h_phi = torch.from_numpy(scene.phi).pin_memory()
+        self.h_ct = torch.from_numpy(scene.cell_type).pin_memory()
+        self.h_x = torch.empty(scene.res, dtype=torch.float32).pin_memory()
+        self.h2d_bytes = sum(t.numel() * t.element_size() for t in self.h_vel) + \
+            self.h_phi.numel() * 4 + self.h_ct.numel() * 4
+        self.d2h_bytes = self.h_x.numel() * 4
+
+    def setup(self):
+        s = self.solver
+        s.reinitialize(self.ct, self.strategy)
+        if self.extra is not None:
+            from mg_lib import check
+            check(s.lib.mg_add_rhs(s.plan, self.extra.data_ptr(), 1.0, s._s()), "mg_add_rhs")
+
+    def run(self):
+        """reinitialize + solve, enqueued; returns nothing (stats read later)."""
+        self.setup()
+        self.solver.solve_async(MAX_ITERS, REL_TOL)
+
+    def run_e2e(self):
+        """The same through host buffers: H2D inputs, solve, D2H pressure."""
+        for d, h in zip(self.vel, self.h_vel):
+            d.copy_(h, non_blocking=True)
+        self.phi.copy_(self.h_phi, non_blocking=True)
+        self.ct.copy_(self.h_ct, non_blocking=True)
+        self.run()
+        self.h_x.copy_(self.solver.x, non_blocking=True)
+
+
+def stage_bytes(solver, storage):
+    """Algorithmic bytes per level-0 cell of each pipeline stage."""
+    sv = 4 if storage == "f32" else 2
+    d = solver.dim
+    coarse = 2 ** d
+    return {
+        "pre_l0": 4 + sv + 1 + sv + 2 * sv / coarse,          # r, Ad, label, z out, r_c + z_c out
+        "post_l0": sv + sv / coarse + 4 + sv + 1 + sv,         # z, z_c, r, Ad, label, z out
+        "Ap_alpha": 4 + 4 + 4 * d + 1 + 4,                     # p, Adiag, Ax, label, Ap out
+        "xr": 4 * 4 + 1 + 2 * 4,                               # x, p, r, Ap, label; x, r out
+    }
+
+
+def time_stages(case, storage, reps=20):
+    """CUDA-event time of each pipeline stage on the solver's stream."""
+    import torch
+    s = case.solver
+    stream = torch.cuda.current_stream(case.dev)
+    out = {}
+    stages = {"pre_l0": (0, 0), "post_l0": (1, 0), "coarse": (2, 0), "Ap_alpha": (3, 0), "xr": (4, 0),
+              "vcycle": (5, 0)}
+    for name, (st, lv) in stages.items():
+        try:
+            s.launch_stage(st, lv)
+        except Exception:
+            continue
+        torch.cuda.synchronize()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(reps):
+            s.launch_stage(st, lv)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        out[name] = e0.elapsed_time(e1) / reps
+    return out
+
+
+def gpu_arm(args, rank, world, local):
+    import torch
+    dev = torch.device("cuda", local)
+    torch.cuda.set_device(dev)
+    wl = WORKLOADS[args.workload]
+    scenes = wl["scenes"]()
+    cases = [GpuCase(sc, args.storage, dev) for sc in scenes]
+    flush = torch.empty(256 * 1024 * 1024, dtype=torch.uint8, device=dev)
+    stream = torch.cuda.current_stream(dev)
+
+    def step(e2e=False):
+        times = []
+        for c in cases:
+            flush.fill_(1)  # L2 flush, outside the timed region
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            if e2e:
+                c.run_e2e()
+            else:
+                c.run()
+            e1.record(stream)
+            times.append((e0, e1))
+        torch.cuda.synchronize()
+        return [a.elapsed_time(b) for a, b in times]
+
+    for _ in range(args.warmup):
+        step()
+        step(e2e=True)
+    torch.cuda.synchronize()
+    barrier(world)
+    with Clocks(local) as clk:
+        solve_ms = []
+        iters = []
+        for _ in range(args.steps):
+            solve_ms += step()
+            for c in cases:
+                st = c.solver.stats()
+                iters.append(st.iters)
+        torch.cuda.synchronize()
+    barrier(world)
+    e2e_ms = []
+    for _ in range(args.steps):
+        e2e_ms += step(e2e=True)
+    torch.cuda.synchronize()
+    total_ms = max_over_ranks(sum(solve_ms), world)
+    total_e2e = max_over_ranks(sum(e2e_ms), world)
+    n_solves = len(solve_ms) * world
+    # outcome of the last solve of each case, checked against the target
+    rel = [c.solver.last_rel_resid for c in cases]
+    status = [c.solver.last_status for c in cases]
+    # launches: setup + prologue + iterations * body
+    launches = 0
+    pro, body = cases[0].solver.launch_counts()
+    L = cases[0].solver.n_mg_levels
+    setup = 1 + 1 + L + (L - 1) + L + 1 + 1 + 1 + (L if args.storage != "f32" else 0)
+    for it in iters:
+        launches += setup + pro + it * body
+    stage_ms = time_stages(cases[0], args.storage)
+    sb = stage_bytes(cases[0].solver, args.storage)
+    cells = cases[0].scene.cells
+    kernels = {}
+    for k, ms in stage_ms.items():
+        kernels[k] = {"ms": round(ms, 5)}
+        if k in sb:
+            gbs = sb[k] * cells / (ms * 1e-3) / 1e9
+            kernels[k].update({"bytes_per_cell": sb[k], "GB_s": round(gbs, 1)})
+    dom = max((k for k in kernels if k in sb), key=lambda k: kernels[k]["ms"])
+    peaks = {}
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            peaks = json.load(f)
+    except Exception:
+        pass
+    peak = float(peaks.get("hbm_gbs", 6650.0))
+    lat = sorted(solve_ms)
+    res = {
+        "metric": "Poisson solves/s at 1e-6 relative residual (p50/p99 ms per solve)",
+        "value": round(n_solves / (total_ms * 1e-3), 3),
+        "unit": "solves/s",
+        "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": round(total_ms / args.steps, 4),
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f32" if args.storage == "f32" else f"{args.storage}-storage/f32-arith/f64-dots",
+        "data": "synthetic (seeded mg_scenes)",
+        "config": {"workload": args.workload, "desc": wl["desc"], "storage": args.storage,
+                   "solves_per_step": len(cases), "max_iters": MAX_ITERS, "rel_resid": 1e-6,
+                   "l2": "flushed before every timed solve", "parallelism": f"replicas x{world}"},
+        "p50_ms": round(lat[len(lat) // 2], 4), "p99_ms": round(lat[min(len(lat) - 1, int(0.99 * len(lat)))], 4),
+        "pcg_iters": {"min": min(iters), "max": max(iters)},
+        "last_rel_resid": rel, "last_status": status,
+        "cell_iters_per_s": round(sum(cells * (i + 1) for i in iters[: len(solve_ms)]) * world / (total_ms * 1e-3), 1),
+        "e2e": {"value": round(n_solves / (total_e2e * 1e-3), 3), "unit": "solves/s",
+                "h2d_bytes_per_step": sum(c.h2d_bytes for c in cases),
+                "d2h_bytes_per_step": sum(c.d2h_bytes for c in cases),
+                "p50_ms": round(sorted(e2e_ms)[len(e2e_ms) // 2], 4)},
+        "gpu_launches": launches * world,
+        "roofline": {"bound": "hbm", "kernel": dom,
+                     "achieved": kernels[dom]["GB_s"], "peak": peak, "unit": "GB/s",
+                     "frac": round(kernels[dom]["GB_s"] / peak, 4), "peak_source": "MEASURED_PEAKS.json hbm_gbs"
+                     if "hbm_gbs" in peaks else "fallback 6650 GB/s",
+                     "traffic": None},
+        "kernels": kernels,
+        "clocks": clk.summary(),
+    }
+    return res, cases
+
+
+# ---------------------------------------------------------------- CPU (oracle)
+def cpu_solve_rate(scenes, seconds, threads=None):
+    """Solves/s of the CPU oracle (float32, all host threads) on the workload."""
+    from oracle import OracleSolver
+    from oracle import oracle as omod
+    if threads:
+        omod.set_threads(threads)
+    n = 0
+    t0 = time.perf_counter()
+    iters = []
+    while True:
+        for sc in scenes:
+            o = OracleSolver(sc.dim, sc.res, sc.levels, 2, 50, real=np.float32)
+            o.reinitialize_pressure(sc.cell_type, sc.velocity, sc.phi, sc.p0, sc.scale_A, sc.scale_b, True,
+                                    sc.gfm_clamp)
+            if sc.extra_rhs is not None:
+                b = o.get("b")
+                fl = o.get("grid_type") == 0
+                b[fl] = b[fl] + sc.extra_rhs[fl]
+                o.set("b", b)
+            iters.append(o.solve(MAX_ITERS, REL_TOL))
+            n += 1
+        if time.perf_counter() - t0 >= seconds:
+            break
+    dt = time.perf_counter() - t0
+    return n / dt, n, dt, omod.max_threads(), iters
+
+
+def reference_arm(args, rank, world):
+    if rank != 0:
+        return None
+    wl = WORKLOADS[args.workload]
+    scenes = wl["scenes"]()
+    per_step = []
+    for i in range(args.warmup + args.steps):
+        rate, n, dt, cores, iters = cpu_solve_rate(scenes, 0.0)
+        if i >= args.warmup:
+            per_step.append(dt / n)
+    tot = sum(per_step)
+    v = len(per_step) / tot
+    lat = sorted(x * 1e3 for x in per_step)
+    return {
+        "impl": "reference",
+        "metric": "Poisson solves/s at 1e-6 relative residual (p50/p99 ms per solve)",
+        "value": round(v, 4), "unit": "solves/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": round(tot / args.steps * 1e3, 3), "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded mg_scenes)",
+        "config": {"workload": args.workload, "desc": wl["desc"], "storage": "f32"},
+        "p50_ms": round(lat[len(lat) // 2], 3), "p99_ms": round(lat[-1], 3),
+        "cpu_baseline": {"value": round(v, 4), "unit": "solves/s", "cores": cores, "kind": "port",
+                         "sample": f"{args.steps} timed solves of the workload by the C++/OpenMP oracle "
+                                   f"(the Taichi reference is not installable)"},
+        "e2e": {"value": round(v, 4), "unit": "solves/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+
+
+def main():
+    args = parse()
+    rank, world, local = dist_init(args.gpus)
+    if args.impl == "reference":
+        out = reference_arm(args, rank, world)
+        if out is not None:
+            print(json.dumps(out))
+        return
+    res, cases = gpu_arm(args, rank, world, local)
+    if rank == 0:
+        rate, n, dt, cores, iters = cpu_solve_rate([c.scene for c in cases], args.cpu_seconds) \
+            if world == 1 else (None, 0, 0, 0, [])
+        if world == 1:
+            res["cpu_baseline"] = {"value": round(rate, 4), "unit": "solves/s", "cores": cores, "kind": "port",
+                                   "sample": f"{n} solves of the workload in {dt:.1f} s by the C++/OpenMP oracle "
+                                             f"(float32, {cores} threads); CPU iterations {min(iters)}-{max(iters)}"}
+        print(json.dumps(res))
+    if world > 1:
+        import torch.distributed as dist
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -72,8 +72,12 @@ typedef struct mg_plan_desc {
   int32_t bottom;       /* bottom_smoothing (half of it in each colour order) */
   int32_t storage;      /* MG_STORE_*: type of the V-cycle grids */
   int32_t refresh_every;/* recompute r = b - A x every N iterations (0: never) */
-  int32_t reserved;
+  int32_t flags;        /* MG_PLAN_* bits */
 } mg_plan_desc_t;
+
+/* plan flags */
+#define MG_PLAN_STORED 1  /* always use the stored-coefficient kernels, one launch
+                             per reference kernel (no fused V-cycle) */
 
 /* Solve parameters: MGPCGPoissonSolver.solve (mgpcg.py:150-155). */
 typedef struct mg_solve_params {
@@ -178,6 +182,20 @@ MG_API int mg_pcg_solve(mg_plan_t* plan, const mg_solve_params_t* params, mg_sol
  * outcome later with mg_pcg_stats() after the stream has completed. */
 MG_API int mg_pcg_solve_async(mg_plan_t* plan, const mg_solve_params_t* params, void* stream);
 MG_API int mg_pcg_stats(mg_plan_t* plan, mg_solve_stats_t* stats, void* stream);
+
+/* ---- measurement --------------------------------------------------------------- */
+
+/* Kernel launches the solve graph makes: `prologue` once per solve, `body`
+ * once per PCG iteration after the first (no reference counterpart). */
+MG_API int mg_plan_launch_counts(mg_plan_t* plan, int32_t* prologue, int32_t* body);
+
+/* Launches one stage of the solve pipeline once on `stream`, on whatever the
+ * fields hold, so a caller can time it with events (no reference counterpart;
+ * the reference's closest tool is ti.kernel_profiler, fluid_simulator.py:16).
+ * stage: 0 = level-`level` pre-smoothing (+ restriction), 1 = level-`level`
+ * post-smoothing (+ prolongation), 2 = the coarse solve, 3 = the CG step
+ * p/Ap/alpha, 4 = the CG step x/r/r.r, 5 = one whole V-cycle. */
+MG_API int mg_launch_stage(mg_plan_t* plan, int32_t stage, int32_t level, void* stream);
 
 /* Last CUDA error string recorded by this library (thread-local). */
 MG_API const char* mg_last_error(void);

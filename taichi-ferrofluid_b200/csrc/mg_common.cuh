@@ -48,6 +48,7 @@ struct Level {
   float* Ax[3];     // SoA: Ax[k][idx] = A(idx, idx + e_k)
   void* r;          // level 0: f32 CG residual; coarser: storage type
   void* z;          // storage type
+  void* zt;         // storage type: the fused V-cycle's pre-smoothed z
   void* Adiag_s;    // storage-type copy of Adiag (aliases Adiag for f32)
 };
 
@@ -60,8 +61,11 @@ struct Control {
   int warm_start, refresh_every, since_refresh, pad0;
   double scale_z;             // z (true) = scale_z * z (stored), 16-bit storage only
   double scale_r;             // r (stored, level 0 input of the V-cycle) = scale_r * r
+  double kappa;               // coefficient scale of 16-bit grids
+  double n_fluid;             // FLUID cells of level 0
   unsigned int counter[8];    // arrival counters of the last-block reductions
   double scratch[8];          // single-value results of mg_reduce
+  double det[3 * 12];         // operator detection: min, max, mismatches per level
 };
 
 template <typename T> __device__ __forceinline__ float to_f(T v);

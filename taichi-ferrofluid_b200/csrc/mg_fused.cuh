@@ -2,20 +2,48 @@
 //
 // "Label-uniform" form: every off-diagonal of a level equals -s_l between two
 // FLUID cells and 0 elsewhere.  The pressure Strategy always produces it
-// (pressure_project.py:56-58).  The kernels then rebuild each coupling from the
-// labels instead of reading dim coefficient arrays: the same values, and so the
-// same arithmetic, with 3 to 4 times fewer coefficient bytes per cell.
+// (pressure_project.py:56-58).  The fused kernels rebuild each coupling from
+// the labels instead of reading dim coefficient arrays: the same values, and so
+// the same float32 operations in the same order as the stored-coefficient
+// kernels of mg_kernels.cuh (the tests check the two bit for bit).
+//
+// Kernels per V-cycle (mgpcg.py:125-148):
+//  * k_sweep<PRE>   level l: z = 0, 2*pre_post red-black half sweeps in colour
+//                   order 0,1,0,1,..., then r[l+1] = sum of the 2^d children's
+//                   (r - A z) (restrict, mgpcg.py:111-118) and z[l+1] = 0.
+//  * k_sweep<POST>  level l: z += z[l+1][I/2] (prolongate, mgpcg.py:120-123),
+//                   then 2*pre_post half sweeps in colour order 1,0,1,0,...
+//  * k_coarse       the levels from `lc` down, the bottom sweeps and back up,
+//                   in ONE thread block with every grid in shared memory.
+//
+// k_sweep streams a tile of (TY x TX) columns through the slowest axis plane by
+// plane.  A ring of NS+3 planes (tile + halo H = NS+1 per side) lives in shared
+// memory; after plane p is loaded, half sweep m (m = 1..NS) is applied to plane
+// p-m, so every half sweep sees its neighbours at the previous half sweep
+// (temporal blocking): each cell's r, A and labels come from memory once per
+// kernel instead of once per half sweep.  The in-plane region shrinks by one
+// cell per half sweep; a chunk of planes starts NS+1 planes early so its first
+// owned plane is exact.
+//
+// 16-bit storage keeps every grid scaled so that it stays inside the FP16
+// range: at level l, r~ = c_l r and z~ = (c_l / kappa) z with c_0 = sigma
+// (a power of two near 1/rms(r), set per V-cycle), c_{l+1} = c_l / 2^dim and
+// kappa a power of two near 1/s_0 applied to the coefficients.  All factors are
+// powers of two, so in float32 they change no bit; with float32 storage they
+// are 1.
 #pragma once
 #include "mg_common.cuh"
 
 namespace mg {
 
-// Per-level check of the label-uniform form.  partials[3*b + {0,1,2}] receive
-// the block's min and max of the nonzero off-diagonals and its count of cells
-// whose coupling pattern differs from the labels.
+// ---------------------------------------------------------------------------
+// Operator detection
+// ---------------------------------------------------------------------------
+
+// partials[3*b + {0,1,2}] receive the block's min and max of the nonzero
+// off-diagonals and its count of couplings that differ from the labels.
 __global__ void __launch_bounds__(kRedThreads) k_detect_uniform(Level L, double* partials,
                                                                 unsigned int* counter, double* out3) {
-  __shared__ double sh[32];
   __shared__ bool am_last;
   double vmin = 1e300, vmax = -1e300, bad = 0.0;
   for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < L.g.count;
@@ -35,7 +63,6 @@ __global__ void __launch_bounds__(kRedThreads) k_detect_uniform(Level L, double*
       }
     }
   }
-  // three block reductions (min, max, sum)
   for (int o = 16; o > 0; o >>= 1) {
     vmin = fmin(vmin, __shfl_down_sync(0xffffffffu, vmin, o));
     vmax = fmax(vmax, __shfl_down_sync(0xffffffffu, vmax, o));
@@ -77,38 +104,70 @@ __global__ void __launch_bounds__(kRedThreads) k_detect_uniform(Level L, double*
     out3[2] = c;
     *counter = 0u;
   }
-  (void)sh;
 }
 
-// Fills op_form[l] (1 label-uniform, 0 stored coefficients).  Synchronises
-// `s`: the choice decides which kernels the solve graph launches.
-inline int prepare_operator(Level* lv, int L, int storage, Control* ctl, double* partials, int num_sms,
-                            int* op_form, float* offdiag, cudaStream_t s) {
-  const int blocks = num_sms * 2 < kMaxPartials / 3 ? num_sms * 2 : kMaxPartials / 3;
-  for (int l = 0; l < L; ++l) {
-    k_detect_uniform<<<blocks, kRedThreads, 0, s>>>(lv[l], partials, &ctl->counter[5], &ctl->scratch[3 * 0 + 1]);
-    if (cudaGetLastError() != cudaSuccess) return MG_E_CUDA;
-    double h[3];
-    if (cudaMemcpyAsync(h, &ctl->scratch[1], sizeof(h), cudaMemcpyDeviceToHost, s) != cudaSuccess) return MG_E_CUDA;
-    if (cudaStreamSynchronize(s) != cudaSuccess) return MG_E_CUDA;
-    const bool none = h[0] > h[1];  // no nonzero off-diagonal at all
-    const bool uniform = h[2] == 0.0 && (none || (h[0] == h[1] && h[0] < 0.0));
-    op_form[l] = uniform ? 1 : 0;
-    offdiag[l] = uniform && !none ? (float)(-h[0]) : 0.0f;
+// Storage-type copy of kappa * Adiag (16-bit storage only).
+template <typename ST>
+__global__ void k_store_diag(const float* __restrict__ ad, ST* __restrict__ out, long long n, float kappa) {
+  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+    out[i] = from_f<ST>(__fmul_rn(kappa, ad[i]));
+}
+
+// FLUID cell count of a level into out[0] (for the per-V-cycle r scale).
+__global__ void __launch_bounds__(kRedThreads) k_count_fluid(Level L, double* partials, unsigned int* counter,
+                                                             double* out) {
+  __shared__ double sh[32];
+  double acc = 0.0;
+  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < L.g.count;
+       i += (long long)gridDim.x * blockDim.x)
+    acc += L.type[i] == FLUID ? 1.0 : 0.0;
+  double tot;
+  if (last_block_total<kRedThreads>(acc, partials, counter, sh, &tot) && threadIdx.x == 0) *out = tot;
+}
+
+// ---------------------------------------------------------------------------
+// Fused kernels
+// ---------------------------------------------------------------------------
+
+// One level as the fused kernels see it.
+template <typename ST>
+struct FLevel {
+  int n[3];             // n[2] == 1 in 2D
+  const int8_t* type;
+  const ST* Ad;         // kappa * Adiag in storage type (aliases Adiag for f32)
+  const void* r;        // float (level 0) or ST
+  ST* z;                // written: PRE's smoothed z (into the level's second
+                        // z buffer), POST's final z
+  const ST* zin;        // POST: PRE's smoothed z.  Separate buffers because a
+                        // block's halo cells belong to other blocks, which
+                        // write their own output while it reads.
+  float s;              // kappa * s_l, the coupling magnitude
+};
+
+template <typename ST>
+struct SweepArgs {
+  FLevel<ST> f;
+  ST* rc;               // PRE: coarse r (written); POST: unused
+  ST* zc;               // PRE: coarse z (zeroed); POST: coarse z (read)
+  int nc[3];
+  float rho;            // PRE: c_{l+1} / c_l
+  float pi;             // POST: c_l / c_{l+1}
+  const Control* ctl;   // sigma for level 0 (scale_r)
+  int r_f32;            // level 0: r is float and scaled by sigma on load
+  int chunk;            // planes per block along axis 0
+  int tiles_x, tiles_y; // tiles per plane
+};
+
+// r of a level: level 0 holds the float32 CG residual, scaled by sigma on
+// load when the grids are 16-bit; coarser levels hold storage-type values.
+template <typename ST>
+__device__ __forceinline__ float load_r(const void* r, long long i, int r_f32, float sigma) {
+  if (r_f32) {
+    const float v = ((const float*)r)[i];
+    if constexpr (sizeof(ST) == 4) return v;
+    else return __fmul_rn(sigma, v);
   }
-  (void)storage;
-  return MG_OK;
-}
-
-inline bool fused_supported(int dim, const Geom* geom, int L, int storage) {
-  (void)dim; (void)geom; (void)L; (void)storage;
-  return false;
-}
-
-inline int launch_vcycle_fused(Level* lv, int L, int dim, int pre_post, int bottom, int storage, int num_sms,
-                               cudaStream_t s) {
-  (void)lv; (void)L; (void)dim; (void)pre_post; (void)bottom; (void)storage; (void)num_sms; (void)s;
-  return MG_E_BADARG;
+  return to_f<ST>(((const ST*)r)[i]);
 }
 
 }  // namespace mg

@@ -1,0 +1,222 @@
+// Host side of the fused V-cycle: per-level launch shapes, the split between
+// streamed levels and the block-resident coarse levels, and the launches.
+#pragma once
+#include <cmath>
+
+#include "mg_sweep.cuh"
+
+namespace mg {
+
+// Shared memory one block may use (B200: 227 KB per block).
+constexpr size_t kSmemLimit = 227 * 1024;
+// Cells the block-resident coarse V-cycle may hold: 13 bytes each
+// (z, r, Adiag as float32 plus the label), under ~200 KB.
+constexpr int kCoarseMaxCells = 15360;
+
+struct TileShape {
+  int tx, ty, nt;
+};
+
+// Launch shape of the streamed levels: a tile of ty x tx columns per block.
+inline TileShape tile_for(int dim) { return dim == 3 ? TileShape{32, 8, 256} : TileShape{128, 1, 128}; }
+
+inline size_t sweep_smem(int dim, int ns, bool pre, TileShape t) {
+  const int H = pre ? ns + 1 : ns;
+  const int RX = t.tx + 2 * H;
+  const int RY = dim == 3 ? t.ty + 2 * H : 1;
+  const int W = pre ? ns + 3 : ns + 2;
+  return (size_t)W * RX * RY * 13;
+}
+
+struct FusedPlan {
+  bool valid = false;
+  int lc = 0;                      // first level of the block-resident coarse solve
+  int dim = 3, ns = 4, storage = 0;
+  int chunk[kMaxLevels], tiles_x[kMaxLevels], tiles_y[kMaxLevels], blocks[kMaxLevels];
+  TileShape tile;
+  CoarseArgs coarse;
+  size_t coarse_smem = 0;
+  float kappa = 1.0f, rho = 1.0f, pi = 1.0f;
+  float s[kMaxLevels];
+};
+
+// Chooses the launch shapes.  Needs every level in label-uniform form and
+// pre_post in 1..3; returns false (stored-coefficient kernels) otherwise.
+inline bool make_fused_plan(const Level* lv, int L, int dim, int pre_post, int bottom, int storage,
+                            const int* op_form, const float* offdiag, int num_sms, FusedPlan* F) {
+  F->valid = false;
+  for (int l = 0; l < L; ++l)
+    if (op_form[l] != 1) return false;
+  if (pre_post < 1 || pre_post > 3) return false;
+  F->dim = dim;
+  F->ns = 2 * pre_post;
+  F->storage = storage;
+  F->tile = tile_for(dim);
+  // first level whose sub-hierarchy fits one block
+  long long tot = 0;
+  int lc = L;
+  for (int l = L - 1; l >= 0; --l) {
+    tot += lv[l].g.count;
+    if (tot > kCoarseMaxCells) break;
+    lc = l;
+  }
+  if (lc == L) return false;  // even the bottom level is too big for one block
+  F->lc = lc;
+  // scale factors (powers of two): kappa ~ 1/s_0 for 16-bit grids
+  F->kappa = 1.0f;
+  F->rho = 1.0f;
+  F->pi = 1.0f;
+  if (storage != MG_STORE_F32) {
+    float s0 = 0.0f;
+    for (int l = 0; l < L && s0 == 0.0f; ++l) s0 = offdiag[l];
+    if (s0 > 0.0f && std::isfinite(s0)) F->kappa = std::ldexp(1.0f, -(int)std::lround(std::log2((double)s0)));
+    F->rho = std::ldexp(1.0f, -dim);
+    F->pi = std::ldexp(1.0f, dim);
+  }
+  for (int l = 0; l < L; ++l) F->s[l] = offdiag[l] * F->kappa;
+  // streamed levels
+  for (int l = 0; l < lc; ++l) {
+    const Geom& g = lv[l].g;
+    const int nx = dim == 3 ? g.n[2] : g.n[1];
+    const int ny = dim == 3 ? g.n[1] : 1;
+    F->tiles_x[l] = (nx + F->tile.tx - 1) / F->tile.tx;
+    F->tiles_y[l] = dim == 3 ? (ny + F->tile.ty - 1) / F->tile.ty : 1;
+    const long long tiles = (long long)F->tiles_x[l] * F->tiles_y[l];
+    // enough blocks for ~3 resident per SM (the 3D ring takes ~69 KB)
+    const long long target = 3LL * num_sms;
+    long long chunk = (long long)g.n[0] * tiles / target;
+    if (chunk < 8) chunk = 8;
+    chunk &= ~1LL;
+    if (chunk > g.n[0]) chunk = g.n[0];
+    if (chunk < 2) chunk = 2;
+    F->chunk[l] = (int)chunk;
+    F->blocks[l] = (int)(tiles * ((g.n[0] + chunk - 1) / chunk));
+  }
+  // block-resident coarse levels
+  CoarseArgs& C = F->coarse;
+  C.dim = dim;
+  C.nlev = L - lc;
+  C.pre_post = pre_post;
+  C.bottom = bottom;
+  int off = 0;
+  for (int i = 0; i < C.nlev; ++i) {
+    const Geom& g = lv[lc + i].g;
+    C.n[i][0] = g.n[0];
+    C.n[i][1] = g.n[1];
+    C.n[i][2] = g.n[2];
+    C.off[i] = off;
+    off += (int)g.count;
+    C.s[i] = F->s[lc + i];
+    C.type[i] = lv[lc + i].type;
+    C.Ad[i] = lv[lc + i].Adiag_s;
+  }
+  C.total = off;
+  C.r0 = lv[lc].r;
+  C.z0 = lv[lc].z;
+  C.r_f32 = lc == 0;
+  C.rho = F->rho;
+  C.pi = F->pi;
+  F->coarse_smem = (size_t)off * 13;
+  F->valid = true;
+  return true;
+}
+
+template <typename ST, bool PRE>
+inline SweepArgs<ST> sweep_args(const FusedPlan& F, const Level* lv, int l, const Control* ctl) {
+  SweepArgs<ST> a;
+  const Level& f = lv[l];
+  const Level& c = lv[l + 1];
+  for (int k = 0; k < 3; ++k) {
+    a.f.n[k] = f.g.n[k];
+    a.nc[k] = c.g.n[k];
+  }
+  a.f.type = f.type;
+  a.f.Ad = (const ST*)f.Adiag_s;
+  a.f.r = f.r;
+  a.f.z = PRE ? (ST*)f.zt : (ST*)f.z;
+  a.f.zin = (const ST*)f.zt;
+  a.f.s = F.s[l];
+  a.rc = (ST*)c.r;
+  a.zc = (ST*)c.z;
+  a.rho = F.rho;
+  a.pi = F.pi;
+  a.ctl = ctl;
+  a.r_f32 = l == 0;
+  a.chunk = F.chunk[l];
+  a.tiles_x = F.tiles_x[l];
+  a.tiles_y = F.tiles_y[l];
+  return a;
+}
+
+template <int DIM, typename ST, int NS, bool PRE>
+inline cudaError_t launch_sweep_t(const FusedPlan& F, const Level* lv, int l, const Control* ctl, cudaStream_t s) {
+  constexpr int TX = DIM == 3 ? 32 : 128;
+  constexpr int TY = DIM == 3 ? 8 : 1;
+  constexpr int NT = DIM == 3 ? 256 : 128;
+  auto kern = k_sweep<DIM, ST, NS, TX, TY, PRE, NT>;
+  const size_t smem = sweep_smem(DIM, NS, PRE, TileShape{TX, TY, NT});
+  cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (e != cudaSuccess) return e;
+  kern<<<F.blocks[l], NT, smem, s>>>(sweep_args<ST, PRE>(F, lv, l, ctl));
+  return cudaGetLastError();
+}
+
+template <typename ST, bool PRE>
+inline cudaError_t launch_sweep_st(const FusedPlan& F, const Level* lv, int l, const Control* ctl, cudaStream_t s) {
+  if (F.dim == 3) {
+    switch (F.ns) {
+      case 2: return launch_sweep_t<3, ST, 2, PRE>(F, lv, l, ctl, s);
+      case 4: return launch_sweep_t<3, ST, 4, PRE>(F, lv, l, ctl, s);
+      case 6: return launch_sweep_t<3, ST, 6, PRE>(F, lv, l, ctl, s);
+    }
+  } else {
+    switch (F.ns) {
+      case 2: return launch_sweep_t<2, ST, 2, PRE>(F, lv, l, ctl, s);
+      case 4: return launch_sweep_t<2, ST, 4, PRE>(F, lv, l, ctl, s);
+      case 6: return launch_sweep_t<2, ST, 6, PRE>(F, lv, l, ctl, s);
+    }
+  }
+  return cudaErrorInvalidValue;
+}
+
+template <bool PRE>
+inline cudaError_t launch_sweep(const FusedPlan& F, const Level* lv, int l, const Control* ctl, cudaStream_t s) {
+  switch (F.storage) {
+    case MG_STORE_F32: return launch_sweep_st<float, PRE>(F, lv, l, ctl, s);
+    case MG_STORE_F16: return launch_sweep_st<__half, PRE>(F, lv, l, ctl, s);
+    case MG_STORE_BF16: return launch_sweep_st<__nv_bfloat16, PRE>(F, lv, l, ctl, s);
+  }
+  return cudaErrorInvalidValue;
+}
+
+template <typename ST>
+inline cudaError_t launch_coarse_st(const FusedPlan& F, const Control* ctl, cudaStream_t s) {
+  CoarseArgs a = F.coarse;
+  a.ctl = ctl;
+  cudaError_t e = cudaFuncSetAttribute(k_coarse<ST>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       (int)F.coarse_smem);
+  if (e != cudaSuccess) return e;
+  k_coarse<ST><<<1, kCoarseThreads, F.coarse_smem, s>>>(a);
+  return cudaGetLastError();
+}
+
+inline cudaError_t launch_coarse(const FusedPlan& F, const Control* ctl, cudaStream_t s) {
+  switch (F.storage) {
+    case MG_STORE_F32: return launch_coarse_st<float>(F, ctl, s);
+    case MG_STORE_F16: return launch_coarse_st<__half>(F, ctl, s);
+    case MG_STORE_BF16: return launch_coarse_st<__nv_bfloat16>(F, ctl, s);
+  }
+  return cudaErrorInvalidValue;
+}
+
+// One V-cycle (mgpcg.py:125-148) with the fused kernels: 2 * lc + 1 launches.
+inline cudaError_t launch_vcycle_fused(const FusedPlan& F, const Level* lv, const Control* ctl, cudaStream_t s) {
+  for (int l = 0; l < F.lc; ++l)
+    if (cudaError_t e = launch_sweep<true>(F, lv, l, ctl, s)) return e;
+  if (cudaError_t e = launch_coarse(F, ctl, s)) return e;
+  for (int l = F.lc - 1; l >= 0; --l)
+    if (cudaError_t e = launch_sweep<false>(F, lv, l, ctl, s)) return e;
+  return cudaSuccess;
+}
+
+}  // namespace mg

@@ -10,6 +10,13 @@
 
 namespace mg {
 
+// Coefficient scale after mg_plan_prepare; sigma = 1 until a solve sets it.
+__global__ void k_set_kappa(Control* ctl, double kappa) {
+  ctl->kappa = kappa;
+  ctl->scale_r = 1.0;
+  ctl->scale_z = kappa;
+}
+
 // Copies one solve's parameters into the control block.
 __global__ void k_set_params(Control* ctl, mg_solve_params_t prm, int refresh_every) {
   ctl->rel_tol = prm.rel_tol;
@@ -19,6 +26,8 @@ __global__ void k_set_params(Control* ctl, mg_solve_params_t prm, int refresh_ev
   ctl->warm_start = prm.warm_start;
   ctl->refresh_every = refresh_every;
 }
+
+__device__ void set_scales(Control* ctl, double rTr);
 
 // r = b (reference), or r = b - A x (warm start); then r.r over FLUID cells.
 // Epilogue: rTr0, tol = max(abs_tol, rTr0 * rel_tol) (mgpcg.py:157-164).
@@ -58,30 +67,54 @@ __global__ void __launch_bounds__(kRedThreads) k_pcg_begin(Level L, const float*
     ctl->run = 1;
     ctl->since_refresh = 0;
     if (warm) ctl->beta = 0.0f;  // p is rebuilt from z only
+    set_scales(ctl, tot);
   }
 }
 
+// z of level 0 as float32: 16-bit grids hold z~ = z / scale_z (a power of two).
+template <typename ST>
+__device__ __forceinline__ float z_true(const ST* z, long long i, float scale_z) {
+  if constexpr (sizeof(ST) == 4) return z[i];
+  else return __fmul_rn(scale_z, to_f<ST>(z[i]));
+}
+
+// The per-V-cycle scale of 16-bit grids: sigma = 2^-round(log2(rms(r))), from
+// r.r over the FLUID cells, and scale_z = kappa / sigma.
+__device__ void set_scales(Control* ctl, double rTr) {
+  double sigma = 1.0;
+  if (ctl->n_fluid > 0.0 && rTr > 0.0 && isfinite(rTr)) {
+    const double rms = sqrt(rTr / ctl->n_fluid);
+    sigma = exp2(-rint(log2(rms)));
+  }
+  ctl->scale_r = sigma;
+  ctl->scale_z = ctl->kappa / sigma;
+}
+
 // update_p (mgpcg.py:234-238): p = z + beta p on FLUID cells.
+template <typename ST>
 __global__ void k_update_p(Level L, float* __restrict__ p, const Control* ctl) {
   const float beta = ctl->beta;
-  const float* z = (const float*)L.z;
+  const float sz = (float)ctl->scale_z;
+  const ST* z = (const ST*)L.z;
   for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < L.g.count;
        i += (long long)gridDim.x * blockDim.x)
-    if (L.type[i] == FLUID) p[i] = __fadd_rn(z[i], __fmul_rn(beta, p[i]));
+    if (L.type[i] == FLUID) p[i] = __fadd_rn(z_true<ST>(z, i, sz), __fmul_rn(beta, p[i]));
 }
 
 // reduce(z, r) (mgpcg.py:171, :201) with the scalar epilogue.
 //  mode 0 (before the loop): old_zTr = z.r; the loop runs iff max_iters != 0.
 //  mode 1 (end of an iteration): beta = new / (old + eps); old = new; iter++;
 //          stop at max_iters (mgpcg.py:176, :200-209).
+template <typename ST>
 __global__ void __launch_bounds__(kRedThreads) k_zr(Level L, Control* ctl, double* partials, int mode) {
   __shared__ double sh[32];
-  const float* z = (const float*)L.z;
+  const ST* z = (const ST*)L.z;
   const float* r = (const float*)L.r;
+  const float sz = (float)ctl->scale_z;
   double acc = 0.0;
   for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < L.g.count;
        i += (long long)gridDim.x * blockDim.x)
-    if (L.type[i] == FLUID) acc += (double)z[i] * (double)r[i];
+    if (L.type[i] == FLUID) acc += (double)z_true<ST>(z, i, sz) * (double)r[i];
   double tot;
   if (last_block_total<kRedThreads>(acc, partials, &ctl->counter[1], sh, &tot) && threadIdx.x == 0) {
     if (mode == 0) {
@@ -100,8 +133,8 @@ __global__ void __launch_bounds__(kRedThreads) k_zr(Level L, Control* ctl, doubl
 // compute_Ap (mgpcg.py:218-224) + reduce(p, Ap) + alpha = zTr / (pAp + eps).
 __global__ void __launch_bounds__(kRedThreads) k_Ap_alpha(Level L, const float* __restrict__ p,
                                                           float* __restrict__ Ap, Control* ctl,
-                                                          double* partials) {
-  if (!ctl->run) return;
+                                                          double* partials, int force = 0) {
+  if (!ctl->run && !force) return;
   __shared__ double sh[32];
   double acc = 0.0;
   for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < L.g.count;
@@ -127,9 +160,9 @@ __global__ void __launch_bounds__(kRedThreads) k_xr(Level L, float* __restrict__
                                                     const float* __restrict__ p,
                                                     const float* __restrict__ Ap, Control* ctl,
                                                     double* partials, cudaGraphConditionalHandle cond,
-                                                    int has_cond) {
+                                                    int has_cond, int force = 0) {
   __shared__ double sh[32];
-  if (!ctl->run) {
+  if (!ctl->run && !force) {
     if (has_cond && blockIdx.x == 0 && threadIdx.x == 0) cudaGraphSetConditional(cond, 0);
     return;
   }
@@ -154,6 +187,61 @@ __global__ void __launch_bounds__(kRedThreads) k_xr(Level L, float* __restrict__
       ctl->status = MG_SOLVE_CONVERGED;
       ctl->run = 0;
     }
+    ctl->since_refresh += 1;
+    set_scales(ctl, tot);
+    if (has_cond) cudaGraphSetConditional(cond, ctl->run ? 1u : 0u);
+  }
+}
+
+// True-residual refresh (the mixed form's iterative refinement): every
+// refresh_every iterations, and whenever the recursive residual claims
+// convergence, r = b - A x is recomputed in FP64 arithmetic from the stored
+// float32 x, and the convergence test is taken again on it.  The recursive
+// residual of the reference never does this (mgpcg.py:226-232).
+__global__ void __launch_bounds__(kRedThreads) k_refresh(Level L, const float* __restrict__ b,
+                                                         const float* __restrict__ x, Control* ctl,
+                                                         double* partials, cudaGraphConditionalHandle cond,
+                                                         int has_cond) {
+  __shared__ double sh[32];
+  const bool claimed = ctl->status == MG_SOLVE_CONVERGED && !ctl->run;
+  const bool due = ctl->run && ctl->refresh_every > 0 && ctl->since_refresh >= ctl->refresh_every;
+  if (!(claimed || due)) {
+    if (has_cond && blockIdx.x == 0 && threadIdx.x == 0) cudaGraphSetConditional(cond, ctl->run ? 1u : 0u);
+    return;
+  }
+  float* r = (float*)L.r;
+  double acc = 0.0;
+  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < L.g.count;
+       i += (long long)gridDim.x * blockDim.x) {
+    if (L.type[i] != FLUID) continue;
+    int c[3];
+    L.g.coords(i, c);
+    double ax = (double)L.Adiag[i] * (double)x[i];
+    for (int k = 0; k < L.g.dim; ++k) {
+      const long long s = L.g.stride(k);
+      if (c[k] > 0) ax += (double)L.Ax[k][i - s] * (double)x[i - s];
+      if (c[k] + 1 < L.g.n[k]) ax += (double)L.Ax[k][i] * (double)x[i + s];
+    }
+    const double rr = (double)b[i] - ax;
+    r[i] = (float)rr;
+    acc += rr * rr;
+  }
+  double tot;
+  if (last_block_total<kRedThreads>(acc, partials, &ctl->counter[7], sh, &tot) && threadIdx.x == 0) {
+    ctl->rTr = tot;
+    ctl->since_refresh = 0;
+    if (!isfinite(tot)) {
+      ctl->status = MG_SOLVE_NONFINITE;
+      ctl->run = 0;
+    } else if (tot < ctl->tol) {
+      ctl->status = MG_SOLVE_CONVERGED;
+      ctl->run = 0;
+    } else {
+      // the recursive residual was too optimistic: keep iterating
+      ctl->status = MG_SOLVE_MAX_ITERS;
+      ctl->run = ctl->max_iters == -1 || ctl->iter + 1 < ctl->max_iters;
+    }
+    set_scales(ctl, tot);
     if (has_cond) cudaGraphSetConditional(cond, ctl->run ? 1u : 0u);
   }
 }

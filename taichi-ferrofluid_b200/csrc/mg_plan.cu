@@ -13,7 +13,7 @@
 #include "mg_common.cuh"
 #include "mg_kernels.cuh"
 #include "mg_pcg.cuh"
-#include "mg_fused.cuh"
+#include "mg_fused_host.cuh"
 
 using namespace mg;
 
@@ -44,7 +44,8 @@ int bad(const char* what) {
 
 constexpr int kFields = 9;
 constexpr int kFieldAdiagS = 9;  // internal: storage copy of Adiag
-constexpr int kFieldCount = 10;
+constexpr int kFieldZT = 10;     // internal: second z buffer of the fused V-cycle
+constexpr int kFieldCount = 11;
 
 struct Loc {
   int64_t off = -1, bytes = 0;
@@ -71,6 +72,9 @@ struct mg_plan {
   int op_form[kMaxLevels];
   float offdiag[kMaxLevels];
   bool prepared = false;
+  FusedPlan fp;
+  int has_cond = 1;          // the graph body ends by setting the while condition
+  uint64_t graph_sig = 0;
   // graph state
   cudaStream_t cap = nullptr;
   cudaGraph_t graph = nullptr;
@@ -110,6 +114,7 @@ void layout(mg_plan* P) {
     put(MG_FIELD_Z, l, 0, n * es);
     if (P->d.storage != MG_STORE_F32) put(kFieldAdiagS, l, 0, n * es);
     else P->loc[kFieldAdiagS][l][0] = P->loc[MG_FIELD_ADIAG][l][0];
+    put(kFieldZT, l, 0, n * es);
   }
   int64_t n0 = level_cells(P, 0);
   put(MG_FIELD_B, 0, 0, n0 * 4);
@@ -135,6 +140,7 @@ void bind_views(mg_plan* P) {
     v.r = B + P->loc[MG_FIELD_R][l][0].off;
     v.z = B + P->loc[MG_FIELD_Z][l][0].off;
     v.Adiag_s = B + P->loc[kFieldAdiagS][l][0].off;
+    v.zt = B + P->loc[kFieldZT][l][0].off;
   }
   P->partials = (double*)(B + P->off_partials);
   P->ctl = (Control*)(B + P->off_ctl);
@@ -212,16 +218,63 @@ int launch_vcycle_generic(mg_plan* P, cudaStream_t s) {
   return MG_OK;
 }
 
-bool use_fused(const mg_plan* P) {
-  for (int l = 0; l < P->L; ++l)
-    if (P->op_form[l] != 1) return false;
-  return fused_supported(P->d.dim, P->geom, P->L, P->d.storage);
+int launch_vcycle(mg_plan* P, cudaStream_t s) {
+  if (P->fp.valid) {
+    cudaError_t e = launch_vcycle_fused(P->fp, P->lv, P->ctl, s);
+    return e == cudaSuccess ? MG_OK : set_err("launch_vcycle_fused", e);
+  }
+  return launch_vcycle_generic(P, s);
 }
 
-int launch_vcycle(mg_plan* P, cudaStream_t s) {
-  if (use_fused(P)) return launch_vcycle_fused(P->lv, P->L, P->d.dim, P->d.pre_post, P->d.bottom,
-                                               P->d.storage, P->num_sms, s);
-  return launch_vcycle_generic(P, s);
+template <typename ST>
+int launch_zr_p(mg_plan* P, bool prologue, cudaStream_t s) {
+  const Level& L0 = P->lv[0];
+  float* p = fptr(P, MG_FIELD_P);
+  if (prologue) {
+    k_update_p<ST><<<P->ew_blocks[0], 256, 0, s>>>(L0, p, P->ctl);
+    CKL("k_update_p");
+    k_zr<ST><<<P->red_blocks, kRedThreads, 0, s>>>(L0, P->ctl, P->partials, 0);
+    CKL("k_zr");
+  } else {
+    k_zr<ST><<<P->red_blocks, kRedThreads, 0, s>>>(L0, P->ctl, P->partials, 1);
+    CKL("k_zr");
+    k_update_p<ST><<<P->ew_blocks[0], 256, 0, s>>>(L0, p, P->ctl);
+    CKL("k_update_p");
+  }
+  return MG_OK;
+}
+
+int launch_zr_p_any(mg_plan* P, bool prologue, cudaStream_t s) {
+  switch (P->d.storage) {
+    case MG_STORE_F16: return launch_zr_p<__half>(P, prologue, s);
+    case MG_STORE_BF16: return launch_zr_p<__nv_bfloat16>(P, prologue, s);
+    default: return launch_zr_p<float>(P, prologue, s);
+  }
+}
+
+// The CG step after z is known: Ap, alpha, x/r update, r.r, the test, and
+// (mixed form) the true-residual refresh.  Stages 3 and 4 of mg_launch_stage.
+int launch_cg_tail(mg_plan* P, cudaStream_t s, int which) {
+  const Level& L0 = P->lv[0];
+  float* b = fptr(P, MG_FIELD_B);
+  float* x = fptr(P, MG_FIELD_X);
+  float* p = fptr(P, MG_FIELD_P);
+  float* Ap = fptr(P, MG_FIELD_AP);
+  const int RB = P->red_blocks;
+  const bool refresh = P->d.refresh_every > 0;
+  if (which & 1) {
+    k_Ap_alpha<<<RB, kRedThreads, 0, s>>>(L0, p, Ap, P->ctl, P->partials);
+    CKL("k_Ap_alpha");
+  }
+  if (which & 2) {
+    k_xr<<<RB, kRedThreads, 0, s>>>(L0, x, p, Ap, P->ctl, P->partials, P->cond, refresh ? 0 : P->has_cond);
+    CKL("k_xr");
+    if (refresh) {
+      k_refresh<<<RB, kRedThreads, 0, s>>>(L0, b, x, P->ctl, P->partials, P->cond, P->has_cond);
+      CKL("k_refresh");
+    }
+  }
+  return MG_OK;
 }
 
 // The PCG loop as launches (mgpcg.py:150-209).  `prologue` selects the part
@@ -230,30 +283,21 @@ int launch_pcg_part(mg_plan* P, bool prologue, cudaStream_t s) {
   const Level& L0 = P->lv[0];
   float* b = fptr(P, MG_FIELD_B);
   float* x = fptr(P, MG_FIELD_X);
-  float* p = fptr(P, MG_FIELD_P);
-  float* Ap = fptr(P, MG_FIELD_AP);
-  const int RB = P->red_blocks;
-  const int EB = P->ew_blocks[0];
   if (prologue) {
-    k_pcg_begin<<<RB, kRedThreads, 0, s>>>(L0, b, x, P->ctl, P->partials);
+    k_pcg_begin<<<P->red_blocks, kRedThreads, 0, s>>>(L0, b, x, P->ctl, P->partials);
     CKL("k_pcg_begin");
-    if (int rc = launch_vcycle(P, s)) return rc;
-    k_update_p<<<EB, 256, 0, s>>>(L0, p, P->ctl);
-    CKL("k_update_p");
-    k_zr<<<RB, kRedThreads, 0, s>>>(L0, P->ctl, P->partials, 0);
-    CKL("k_zr");
-  } else {
-    if (int rc = launch_vcycle(P, s)) return rc;
-    k_zr<<<RB, kRedThreads, 0, s>>>(L0, P->ctl, P->partials, 1);
-    CKL("k_zr");
-    k_update_p<<<EB, 256, 0, s>>>(L0, p, P->ctl);
-    CKL("k_update_p");
   }
-  k_Ap_alpha<<<RB, kRedThreads, 0, s>>>(L0, p, Ap, P->ctl, P->partials);
-  CKL("k_Ap_alpha");
-  k_xr<<<RB, kRedThreads, 0, s>>>(L0, x, p, Ap, P->ctl, P->partials, P->cond, 1);
-  CKL("k_xr");
-  return MG_OK;
+  if (int rc = launch_vcycle(P, s)) return rc;
+  if (int rc = launch_zr_p_any(P, prologue, s)) return rc;
+  return launch_cg_tail(P, s, 3);
+}
+
+// Kernels one launch_pcg_part enqueues (the graph's node count per part).
+int count_pcg_part(const mg_plan* P, bool prologue) {
+  int v = P->fp.valid ? 2 * P->fp.lc + 1
+                      : (P->L - 1) * (4 * P->d.pre_post + 2) +
+                            (P->geom[P->L - 1].count <= kBottomBlockCells ? (P->d.bottom / 2 > 0) : 2 * P->d.bottom);
+  return (prologue ? 1 : 0) + v + 2 + 2 + (P->d.refresh_every > 0 ? 1 : 0);
 }
 
 void destroy_graph(mg_plan* P) {
@@ -464,9 +508,67 @@ int mg_add_rhs(mg_plan_t* P, const float* src, float c, void* stream) {
 
 int mg_plan_prepare(mg_plan_t* P, void* stream) {
   NEED_BOUND(P);
-  if (int rc = prepare_operator(P->lv, P->L, P->d.storage, P->ctl, P->partials, P->num_sms, P->op_form,
-                                P->offdiag, S(stream)))
-    return rc == MG_E_CUDA ? set_err("prepare_operator", cudaGetLastError()) : rc;
+  cudaStream_t s = S(stream);
+  // 1. operator form of every level (one synchronisation for all levels)
+  const int blocks = P->num_sms * 2 < kMaxPartials / 3 ? P->num_sms * 2 : kMaxPartials / 3;
+  for (int l = 0; l < P->L; ++l) {
+    k_detect_uniform<<<blocks, kRedThreads, 0, s>>>(P->lv[l], P->partials, &P->ctl->counter[5],
+                                                    &P->ctl->det[3 * l]);
+    CKL("k_detect_uniform");
+  }
+  double det[3 * kMaxLevels];
+  CK(cudaMemcpyAsync(det, P->ctl->det, sizeof(double) * 3 * P->L, cudaMemcpyDeviceToHost, s));
+  CK(cudaStreamSynchronize(s));
+  for (int l = 0; l < P->L; ++l) {
+    const double* h = det + 3 * l;
+    const bool none = h[0] > h[1];  // no nonzero off-diagonal at all
+    const bool uniform = h[2] == 0.0 && (none || (h[0] == h[1] && h[0] < 0.0));
+    P->op_form[l] = uniform ? 1 : 0;
+    P->offdiag[l] = uniform && !none ? (float)(-h[0]) : 0.0f;
+  }
+  // 2. launch shapes of the fused V-cycle
+  P->fp.valid = false;
+  if (!(P->d.flags & MG_PLAN_STORED))
+    make_fused_plan(P->lv, P->L, P->d.dim, P->d.pre_post, P->d.bottom, P->d.storage, P->op_form, P->offdiag,
+                    P->num_sms, &P->fp);
+  if (P->d.storage != MG_STORE_F32 && !P->fp.valid)
+    return bad("16-bit storage needs the label-uniform operator on every level and pre_and_post_smoothing 1..3");
+  // 3. 16-bit coefficient copies, FLUID count, scale factors
+  if (P->d.storage == MG_STORE_F16 || P->d.storage == MG_STORE_BF16) {
+    for (int l = 0; l < P->L; ++l) {
+      if (P->d.storage == MG_STORE_F16)
+        k_store_diag<__half><<<P->ew_blocks[l], 256, 0, s>>>(P->lv[l].Adiag, (__half*)P->lv[l].Adiag_s,
+                                                             P->geom[l].count, P->fp.kappa);
+      else
+        k_store_diag<__nv_bfloat16><<<P->ew_blocks[l], 256, 0, s>>>(
+            P->lv[l].Adiag, (__nv_bfloat16*)P->lv[l].Adiag_s, P->geom[l].count, P->fp.kappa);
+      CKL("k_store_diag");
+    }
+  }
+  k_count_fluid<<<P->red_blocks, kRedThreads, 0, s>>>(P->lv[0], P->partials, &P->ctl->counter[4],
+                                                      &P->ctl->n_fluid);
+  CKL("k_count_fluid");
+  k_set_kappa<<<1, 1, 0, s>>>(P->ctl, (double)P->fp.kappa);
+  CKL("k_set_kappa");
+  // 4. the solve graph captured kernel arguments (shapes, s_l, kappa): rebuild
+  //    it only when they changed
+  uint64_t sig = 1469598103934665603ull;
+  auto mix = [&](uint64_t v) { sig = (sig ^ v) * 1099511628211ull; };
+  mix(P->fp.valid);
+  mix(P->fp.lc);
+  for (int l = 0; l < P->L; ++l) {
+    uint32_t bits;
+    std::memcpy(&bits, &P->fp.s[l], 4);
+    mix(bits);
+    mix(P->op_form[l]);
+  }
+  uint32_t kb;
+  std::memcpy(&kb, &P->fp.kappa, 4);
+  mix(kb);
+  if (sig != P->graph_sig) {
+    destroy_graph(P);
+    P->graph_sig = sig;
+  }
   P->prepared = true;
   return MG_OK;
 }
@@ -556,6 +658,66 @@ int mg_pcg_stats(mg_plan_t* P, mg_solve_stats_t* st, void* stream) {
   st->rTr = P->host_ctl->rTr;
   st->bTb = P->host_ctl->bTb;
   return MG_OK;
+}
+
+int mg_plan_launch_counts(mg_plan_t* P, int32_t* prologue, int32_t* body) {
+  NEED_BOUND(P);
+  if (!prologue || !body) return bad("null pointer");
+  if (!P->prepared) return bad("plan not prepared");
+  *prologue = count_pcg_part(P, true);
+  *body = count_pcg_part(P, false);
+  return MG_OK;
+}
+
+int mg_launch_stage(mg_plan_t* P, int32_t stage, int32_t level, void* stream) {
+  NEED_BOUND(P);
+  cudaStream_t s = S(stream);
+  if (!P->prepared)
+    if (int rc = mg_plan_prepare(P, stream)) return rc;
+  const Level& L0 = P->lv[0];
+  switch (stage) {
+    case 0:
+    case 1: {
+      if (P->fp.valid) {
+        if (level < 0 || level >= P->fp.lc) return bad("level is not a streamed level");
+        cudaError_t e = stage == 0 ? launch_sweep<true>(P->fp, P->lv, level, P->ctl, s)
+                                   : launch_sweep<false>(P->fp, P->lv, level, P->ctl, s);
+        return e == cudaSuccess ? MG_OK : set_err("launch_sweep", e);
+      }
+      if (level < 0 || level >= P->L - 1) return bad("level");
+      if (stage == 0) {
+        for (int i = 0; i < P->d.pre_post; ++i) {
+          if (int rc = launch_smooth(P, level, 0, s)) return rc;
+          if (int rc = launch_smooth(P, level, 1, s)) return rc;
+        }
+        return launch_restrict(P, level, s);
+      }
+      if (int rc = launch_prolongate(P, level, s)) return rc;
+      for (int i = 0; i < P->d.pre_post; ++i) {
+        if (int rc = launch_smooth(P, level, 1, s)) return rc;
+        if (int rc = launch_smooth(P, level, 0, s)) return rc;
+      }
+      return MG_OK;
+    }
+    case 2: {
+      if (!P->fp.valid) return bad("the coarse stage belongs to the fused V-cycle");
+      cudaError_t e = launch_coarse(P->fp, P->ctl, s);
+      return e == cudaSuccess ? MG_OK : set_err("launch_coarse", e);
+    }
+    case 3:
+      k_Ap_alpha<<<P->red_blocks, kRedThreads, 0, s>>>(L0, fptr(P, MG_FIELD_P), fptr(P, MG_FIELD_AP), P->ctl,
+                                                       P->partials, 1);
+      CKL("k_Ap_alpha");
+      return MG_OK;
+    case 4:
+      k_xr<<<P->red_blocks, kRedThreads, 0, s>>>(L0, fptr(P, MG_FIELD_X), fptr(P, MG_FIELD_P),
+                                                 fptr(P, MG_FIELD_AP), P->ctl, P->partials, P->cond, 0, 1);
+      CKL("k_xr");
+      return MG_OK;
+    case 5:
+      return launch_vcycle(P, s);
+  }
+  return bad("stage");
 }
 
 int mg_pcg_solve(mg_plan_t* P, const mg_solve_params_t* prm, mg_solve_stats_t* st, void* stream) {

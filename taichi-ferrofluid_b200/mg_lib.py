@@ -40,7 +40,7 @@ class MGError(RuntimeError):
 class PlanDesc(ctypes.Structure):
     _fields_ = [("dim", ctypes.c_int32), ("res", ctypes.c_int32 * 3), ("levels", ctypes.c_int32),
                 ("pre_post", ctypes.c_int32), ("bottom", ctypes.c_int32), ("storage", ctypes.c_int32),
-                ("refresh_every", ctypes.c_int32), ("reserved", ctypes.c_int32)]
+                ("refresh_every", ctypes.c_int32), ("flags", ctypes.c_int32)]
 
 
 class SolveParams(ctypes.Structure):
@@ -56,6 +56,8 @@ class SolveStats(ctypes.Structure):
 _vp = ctypes.c_void_p
 _i32 = ctypes.c_int32
 _f32 = ctypes.c_float
+PLAN_STORED = 1
+
 _SIGS = {
     "mg_plan_create": (ctypes.c_int, [ctypes.POINTER(PlanDesc), ctypes.POINTER(_vp)]),
     "mg_plan_destroy": (ctypes.c_int, [_vp]),
@@ -81,6 +83,8 @@ _SIGS = {
     "mg_pcg_solve": (ctypes.c_int, [_vp, ctypes.POINTER(SolveParams), ctypes.POINTER(SolveStats), _vp]),
     "mg_pcg_solve_async": (ctypes.c_int, [_vp, ctypes.POINTER(SolveParams), _vp]),
     "mg_pcg_stats": (ctypes.c_int, [_vp, ctypes.POINTER(SolveStats), _vp]),
+    "mg_plan_launch_counts": (ctypes.c_int, [_vp, ctypes.POINTER(_i32), ctypes.POINTER(_i32)]),
+    "mg_launch_stage": (ctypes.c_int, [_vp, _i32, _i32, _vp]),
     "mg_last_error": (ctypes.c_char_p, []),
     "mg_version": (ctypes.c_int32, []),
 }

@@ -61,7 +61,7 @@ class MGPCGPoissonSolver:
     """
 
     def __init__(self, dim, res, n_mg_levels=4, pre_and_post_smoothing=2, bottom_smoothing=50,
-                 real=float, *, storage=None, refresh_every=None, device=None):
+                 real=float, *, storage=None, refresh_every=None, device=None, stored_kernels=False):
         self.lib = mg_lib.load()
         self.FLUID = FLUID
         self.SOLID = SOLID
@@ -89,6 +89,7 @@ class MGPCGPoissonSolver:
         d.bottom = self.bottom_smoothing
         d.storage = self.storage
         d.refresh_every = self.refresh_every
+        d.flags = mg_lib.PLAN_STORED if stored_kernels else 0
         plan = mg_lib.ctypes.c_void_p()
         check(self.lib.mg_plan_create(mg_lib.ctypes.byref(d), mg_lib.ctypes.byref(plan)), "mg_plan_create")
         self.plan = plan
@@ -252,6 +253,17 @@ class MGPCGPoissonSolver:
             self.x.copy_(torch.as_tensor(x0, device=self.device, dtype=torch.float32).reshape(self.res))
             prm.warm_start = 1
         check(self.lib.mg_pcg_solve_async(self.plan, mg_lib.ctypes.byref(prm), self._s()), "mg_pcg_solve_async")
+
+    def launch_counts(self):
+        """(kernels before the PCG loop, kernels per further iteration)."""
+        a, b = mg_lib.ctypes.c_int32(), mg_lib.ctypes.c_int32()
+        check(self.lib.mg_plan_launch_counts(self.plan, mg_lib.ctypes.byref(a), mg_lib.ctypes.byref(b)),
+              "mg_plan_launch_counts")
+        return int(a.value), int(b.value)
+
+    def launch_stage(self, stage, level=0):
+        """Launches one pipeline stage once (for timing; see mg_launch_stage)."""
+        check(self.lib.mg_launch_stage(self.plan, int(stage), int(level), self._s()), "mg_launch_stage")
 
     def stats(self):
         """Waits for the stream and returns the last solve's outcome."""

@@ -24,14 +24,37 @@ def oracle_for(scene, real=np.float32, bottom=50, pre_post=2, levels=None, clamp
     return o
 
 
-def gpu_for(scene, storage=None, bottom=50, pre_post=2, levels=None, clamp=None, refresh_every=None):
+def true_rel_resid(solver):
+    """||b - A x|| / ||b|| over FLUID cells, in float64 from the solver's own
+    float32 A, b and x (independent of the solver's residual bookkeeping)."""
+    x = solver.x.double().cpu().numpy()
+    b = solver.b.double().cpu().numpy()
+    ad = solver.Adiag[0].double().cpu().numpy()
+    ax = np.moveaxis(solver.Ax[0].double().cpu().numpy(), -1, 0)
+    fl = solver.grid_type[0].cpu().numpy() == 0
+    Axv = ad * x
+    for k in range(solver.dim):
+        lo = [slice(None)] * solver.dim
+        hi = [slice(None)] * solver.dim
+        lo[k] = slice(0, -1)
+        hi[k] = slice(1, None)
+        lo, hi = tuple(lo), tuple(hi)
+        Axv[hi] += ax[k][lo] * x[lo]
+        Axv[lo] += ax[k][lo] * x[hi]
+    r = np.where(fl, b - Axv, 0.0)
+    nb = np.linalg.norm(np.where(fl, b, 0.0))
+    return float(np.linalg.norm(r) / nb)
+
+
+def gpu_for(scene, storage=None, bottom=50, pre_post=2, levels=None, clamp=None, refresh_every=None,
+            stored_kernels=False):
     import torch
     from mgpcg import MGPCGPoissonSolver
     from pressure_project import PressureProjectStrategy
     dev = torch.device("cuda", 0)
     L = levels or scene.levels
     s = MGPCGPoissonSolver(scene.dim, scene.res, L, pre_post, bottom, storage=storage, device=dev,
-                           refresh_every=refresh_every)
+                           refresh_every=refresh_every, stored_kernels=stored_kernels)
     vel = [torch.from_numpy(v).to(dev) for v in scene.velocity]
     phi = torch.from_numpy(scene.phi).to(dev)
     st = PressureProjectStrategy(scene.dim, vel, True, phi, scene.p0,
