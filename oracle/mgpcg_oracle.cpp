@@ -293,10 +293,20 @@ struct Solver {
         if (tt[i] == FLUID) s += a[i] * c[i];
       return (double)s;
     }
+    // fixed blocks of 4096 cells summed in index order: the same result for
+    // any number of threads
+    const int64_t B = 4096, nb = (gg.count + B - 1) / B;
+    std::vector<double> part(nb, 0.0);
+#pragma omp parallel for schedule(static)
+    for (int64_t k = 0; k < nb; ++k) {
+      double s = 0.0;
+      const int64_t e = std::min(gg.count, (k + 1) * B);
+      for (int64_t i = k * B; i < e; ++i)
+        if (tt[i] == FLUID) s += (double)a[i] * (double)c[i];
+      part[k] = s;
+    }
     double s = 0.0;
-#pragma omp parallel for schedule(static) reduction(+ : s)
-    for (int64_t i = 0; i < gg.count; ++i)
-      if (tt[i] == FLUID) s += (double)a[i] * (double)c[i];
+    for (int64_t k = 0; k < nb; ++k) s += part[k];
     return s;
   }
 
