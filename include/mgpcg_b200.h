@@ -197,6 +197,23 @@ MG_API int mg_plan_launch_counts(mg_plan_t* plan, int32_t* prologue, int32_t* bo
  * p/Ap/alpha, 4 = the CG step x/r/r.r, 5 = one whole V-cycle. */
 MG_API int mg_launch_stage(mg_plan_t* plan, int32_t stage, int32_t level, void* stream);
 
+/* ---- allocation-free variant ------------------------------------------------------ */
+
+/* Sum of a[i] * b[i] over the n cells with grid_type[i] == MG_FLUID, in FP64,
+ * written to the DEVICE location *out (enqueued on `stream`, no synchronize).
+ * No counterpart in the reference: it is the reference's reduce
+ * (mgpcg.py:211-216) for callers that cannot allocate device memory - a host
+ * whose engine owns every byte of device memory, a real-time step loop where
+ * cudaMalloc/cudaFree would synchronise the device, or code without a solver
+ * plan.  It allocates nothing: its scratch (64 KB of FP64 partial sums and a
+ * counter) is a static array inside the library, held by every GPU that loads
+ * it.  The first call on a device looks that array up (cudaGetSymbolAddress)
+ * and should come before any stream capture.  n must be at most 33,554,432
+ * (else MG_E_TOO_BIG).  Calls share the array: calls that overlap on the GPU
+ * race; order them on one stream. */
+MG_API int mg_reduce_static(const int8_t* grid_type, const float* a, const float* b, int64_t n, double* out,
+                            void* stream);
+
 /* Last CUDA error string recorded by this library (thread-local). */
 MG_API const char* mg_last_error(void);
 

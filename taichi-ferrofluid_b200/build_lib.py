@@ -26,7 +26,7 @@ FLAGS = [
 
 
 def sources():
-    return [os.path.join(CSRC, "mg_plan.cu")]
+    return [os.path.join(CSRC, "mg_plan.cu"), os.path.join(CSRC, "mg_static.cu")]
 
 
 def deps():

@@ -352,6 +352,9 @@ int build_graph(mg_plan* P) {
 
 }  // namespace
 
+// Lets the library's other translation units record an error message.
+void mg_internal_set_error(const char* msg) { snprintf(g_err, sizeof(g_err), "%s", msg); }
+
 // ============================================================================
 // C ABI
 // ============================================================================

@@ -85,6 +85,7 @@ _SIGS = {
     "mg_pcg_stats": (ctypes.c_int, [_vp, ctypes.POINTER(SolveStats), _vp]),
     "mg_plan_launch_counts": (ctypes.c_int, [_vp, ctypes.POINTER(_i32), ctypes.POINTER(_i32)]),
     "mg_launch_stage": (ctypes.c_int, [_vp, _i32, _i32, _vp]),
+    "mg_reduce_static": (ctypes.c_int, [_vp, _vp, _vp, ctypes.c_int64, _vp, _vp]),
     "mg_last_error": (ctypes.c_char_p, []),
     "mg_version": (ctypes.c_int32, []),
 }
