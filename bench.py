@@ -38,13 +38,31 @@ import numpy as np  # noqa: E402
 
 import mg_scenes  # noqa: E402
 
+def _substep128():
+    sc = mg_scenes.ferro_drop_3d(n=128, seed=1, levels=5)
+    return [("pressure", sc), ("psi", sc)]
+
+
+# each workload: a list of (kind, scene) solves per step; kind "pressure" is the
+# ghost-fluid pressure solve, "psi" the magnetic potential solve (chi = 1 in the fluid)
 WORKLOADS = {
-    "substep128": dict(desc="3D ferrofluid substep 128^3 (pressure + potential solves), 5 levels",
-                       scenes=lambda: [mg_scenes.ferro_drop_3d(n=128, seed=1, levels=5)]),
+    "substep128": dict(desc="3D ferrofluid substep 128^3, 5 levels: (a) ghost-fluid pressure solve + "
+                            "(b) magnetic potential solve", cases=_substep128),
+    "pressure128": dict(desc="3D ghost-fluid pressure solve 128^3, 5 levels",
+                        cases=lambda: [("pressure", mg_scenes.ferro_drop_3d(n=128, seed=1, levels=5))]),
     "precision256": dict(desc="3D drop/pool 256^3 with smooth source, 6 levels",
-                         scenes=lambda: [mg_scenes.precision_3d(n=256, seed=2, levels=6)]),
-    "dam2d": dict(desc="2D dam break 128^2, 4 levels", scenes=lambda: [mg_scenes.dam_break_2d()]),
+                         cases=lambda: [("pressure", mg_scenes.precision_3d(n=256, seed=2, levels=6))]),
+    "dam2d": dict(desc="2D dam break 128^2, 4 levels",
+                  cases=lambda: [("pressure", mg_scenes.dam_break_2d())]),
 }
+
+PSI_H = (0.0, 1.0, 0.0)
+PSI_PIN = (1, 1, 1)
+
+
+def psi_chi(scene):
+    """Susceptibility of the potential solve: 1 inside the fluid, 0 outside."""
+    return (scene.phi < 0).astype(np.float32)
 
 MAX_ITERS = 500
 REL_TOL = 1e-12  # squared: 1e-6 relative residual
@@ -144,8 +162,44 @@ class Clocks:
 
 
 # ---------------------------------------------------------------- GPU arm
+class PsiCase:
+    """The magnetic potential solve: full_reinitialize + solve (ferrofluid_simulator.py:77-87)."""
+
+    kind = "psi"
+
+    def __init__(self, scene, storage, dev):
+        import torch
+        from mgpcg import MGPCGPoissonSolver
+        from magnetic_potential import MagneticPotentialStrategy
+        self.scene = scene
+        self.dev = dev
+        # the potential operator has stored coefficients: always float32 grids
+        self.solver = MGPCGPoissonSolver(scene.dim, scene.res, scene.levels, 2, 50, device=dev)
+        self.chi = torch.from_numpy(psi_chi(scene)).to(dev)
+        self.strategy = MagneticPotentialStrategy(scene.dim, self.chi, PSI_H, scene.dx, PSI_PIN)
+        self.h_chi = torch.from_numpy(psi_chi(scene)).pin_memory()
+        self.h_x = torch.empty(scene.res, dtype=torch.float32).pin_memory()
+        self.h2d_bytes = self.h_chi.numel() * 4
+        self.d2h_bytes = self.h_x.numel() * 4
+
+    def run(self):
+        self.solver.full_reinitialize(self.strategy)
+        self.solver.solve_async(MAX_ITERS, REL_TOL)
+
+    def run_e2e(self):
+        self.chi.copy_(self.h_chi, non_blocking=True)
+        self.run()
+        self.h_x.copy_(self.solver.x, non_blocking=True)
+
+
+def make_case(kind, scene, storage, dev):
+    return PsiCase(scene, storage, dev) if kind == "psi" else GpuCase(scene, storage, dev)
+
+
 class GpuCase:
-    """One solve of a scene through the drop-in API with device-resident inputs."""
+    """One pressure solve of a scene through the drop-in API with device-resident inputs."""
+
+    kind = "pressure"
 
     def __init__(self, scene, storage, dev):
         import torch
@@ -236,8 +290,7 @@ def gpu_arm(args, rank, world, local):
     dev = torch.device("cuda", local)
     torch.cuda.set_device(dev)
     wl = WORKLOADS[args.workload]
-    scenes = wl["scenes"]()
-    cases = [GpuCase(sc, args.storage, dev) for sc in scenes]
+    cases = [make_case(kind, sc, args.storage, dev) for kind, sc in wl["cases"]()]
     flush = torch.empty(256 * 1024 * 1024, dtype=torch.uint8, device=dev)
     stream = torch.cuda.current_stream(dev)
 
@@ -265,11 +318,13 @@ def gpu_arm(args, rank, world, local):
     with Clocks(local) as clk:
         solve_ms = []
         iters = []
+        per_case_iters = {c.kind: [] for c in cases}
         for _ in range(args.steps):
             solve_ms += step()
             for c in cases:
                 st = c.solver.stats()
-                iters.append(st.iters)
+                iters.append((c, st.iters))
+                per_case_iters[c.kind].append(st.iters)
         torch.cuda.synchronize()
     barrier(world)
     e2e_ms = []
@@ -284,10 +339,13 @@ def gpu_arm(args, rank, world, local):
     status = [c.solver.last_status for c in cases]
     # launches: setup + prologue + iterations * body
     launches = 0
-    pro, body = cases[0].solver.launch_counts()
-    L = cases[0].solver.n_mg_levels
-    setup = 1 + 1 + L + (L - 1) + L + 1 + 1 + 1 + (L if args.storage != "f32" else 0)
-    for it in iters:
+    for c, it in iters:
+        pro, body = c.solver.launch_counts()
+        L = c.solver.n_mg_levels
+        if c.kind == "psi":   # build_b, build_A, L-1 Galerkin, prepare (L + 2), set_params
+            setup = 2 + (L - 1) + (L + 2) + 1
+        else:                 # cell_type, build_b, L build_A, L-1 coarsen, prepare, set_params
+            setup = 2 + L + (L - 1) + (L + 2) + (L if c.solver.storage != 0 else 0) + 1
         launches += setup + pro + it * body
     stage_ms = time_stages(cases[0], args.storage)
     sb = stage_bytes(cases[0].solver, args.storage)
@@ -320,9 +378,9 @@ def gpu_arm(args, rank, world, local):
                    "solves_per_step": len(cases), "max_iters": MAX_ITERS, "rel_resid": 1e-6,
                    "l2": "flushed before every timed solve", "parallelism": f"replicas x{world}"},
         "p50_ms": round(lat[len(lat) // 2], 4), "p99_ms": round(lat[min(len(lat) - 1, int(0.99 * len(lat)))], 4),
-        "pcg_iters": {"min": min(iters), "max": max(iters)},
+        "pcg_iters": {k: {"min": min(v), "max": max(v)} for k, v in per_case_iters.items()},
         "last_rel_resid": rel, "last_status": status,
-        "cell_iters_per_s": round(sum(cells * (i + 1) for i in iters[: len(solve_ms)]) * world / (total_ms * 1e-3), 1),
+        "cell_iters_per_s": round(sum(c.scene.cells * (i + 1) for c, i in iters) * world / (total_ms * 1e-3), 1),
         "e2e": {"value": round(n_solves / (total_e2e * 1e-3), 3), "unit": "solves/s",
                 "h2d_bytes_per_step": sum(c.h2d_bytes for c in cases),
                 "d2h_bytes_per_step": sum(c.d2h_bytes for c in cases),
@@ -340,8 +398,9 @@ def gpu_arm(args, rank, world, local):
 
 
 # ---------------------------------------------------------------- CPU (oracle)
-def cpu_solve_rate(scenes, seconds, threads=None):
-    """Solves/s of the CPU oracle (float32, all host threads) on the workload."""
+def cpu_solve_rate(cases, seconds, threads=None):
+    """Solves/s of the CPU oracle (float32, all host threads) on the workload's
+    (kind, scene) solves: setup + solve, like the GPU arm's step."""
     from oracle import OracleSolver
     from oracle import oracle as omod
     if threads:
@@ -350,15 +409,18 @@ def cpu_solve_rate(scenes, seconds, threads=None):
     t0 = time.perf_counter()
     iters = []
     while True:
-        for sc in scenes:
+        for kind, sc in cases:
             o = OracleSolver(sc.dim, sc.res, sc.levels, 2, 50, real=np.float32)
-            o.reinitialize_pressure(sc.cell_type, sc.velocity, sc.phi, sc.p0, sc.scale_A, sc.scale_b, True,
-                                    sc.gfm_clamp)
-            if sc.extra_rhs is not None:
-                b = o.get("b")
-                fl = o.get("grid_type") == 0
-                b[fl] = b[fl] + sc.extra_rhs[fl]
-                o.set("b", b)
+            if kind == "psi":
+                o.full_reinitialize_psi(psi_chi(sc), PSI_H, sc.dx, PSI_PIN)
+            else:
+                o.reinitialize_pressure(sc.cell_type, sc.velocity, sc.phi, sc.p0, sc.scale_A, sc.scale_b, True,
+                                        sc.gfm_clamp)
+                if sc.extra_rhs is not None:
+                    b = o.get("b")
+                    fl = o.get("grid_type") == 0
+                    b[fl] = b[fl] + sc.extra_rhs[fl]
+                    o.set("b", b)
             iters.append(o.solve(MAX_ITERS, REL_TOL))
             n += 1
         if time.perf_counter() - t0 >= seconds:
@@ -371,10 +433,10 @@ def reference_arm(args, rank, world):
     if rank != 0:
         return None
     wl = WORKLOADS[args.workload]
-    scenes = wl["scenes"]()
+    cases = wl["cases"]()
     per_step = []
     for i in range(args.warmup + args.steps):
-        rate, n, dt, cores, iters = cpu_solve_rate(scenes, 0.0)
+        rate, n, dt, cores, iters = cpu_solve_rate(cases, 0.0)
         if i >= args.warmup:
             per_step.append(dt / n)
     tot = sum(per_step)
@@ -405,9 +467,10 @@ def main():
         return
     res, cases = gpu_arm(args, rank, world, local)
     if rank == 0:
-        rate, n, dt, cores, iters = cpu_solve_rate([c.scene for c in cases], args.cpu_seconds) \
-            if world == 1 else (None, 0, 0, 0, [])
-        if world == 1:
+        with_cpu = world == 1 and args.cpu_seconds > 0
+        rate, n, dt, cores, iters = cpu_solve_rate([(c.kind, c.scene) for c in cases], args.cpu_seconds) \
+            if with_cpu else (None, 0, 0, 0, [])
+        if with_cpu:
             res["cpu_baseline"] = {"value": round(rate, 4), "unit": "solves/s", "cores": cores, "kind": "port",
                                    "sample": f"{n} solves of the workload in {dt:.1f} s by the C++/OpenMP oracle "
                                              f"(float32, {cores} threads); CPU iterations {min(iters)}-{max(iters)}"}

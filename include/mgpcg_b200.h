@@ -149,6 +149,25 @@ MG_API int mg_build_pressure_A(mg_plan_t* plan, int32_t level, const float* phi,
  * and the extra smooth source term of the precision workload. */
 MG_API int mg_add_rhs(mg_plan_t* plan, const float* src, float c, void* stream);
 
+/* Magnetic potential Strategy of the 3D ferrofluid substep: the solve of
+ * FerrofluidSimulator.update_potential_function (ferrofluid_simulator.py:77-87,
+ * potential_function.py:19-55) in the benchmark's form: permeability
+ * mu = 1 + chi (chi at cell centres), face coefficient = harmonic mean of mu
+ * over dx^2, rhs = -div(mu H) for a constant external field H, Neumann at the
+ * domain boundary, psi pinned to 0 at cell `pin`.  Use with
+ * full_reinitialize (every label FLUID).  mg_build_psi_A builds level 0. */
+MG_API int mg_build_psi_b(mg_plan_t* plan, const float* chi, float H0, float H1, float H2, float dx,
+                          int32_t pin0, int32_t pin1, int32_t pin2, void* stream);
+MG_API int mg_build_psi_A(mg_plan_t* plan, const float* chi, float dx, int32_t pin0, int32_t pin1,
+                          int32_t pin2, void* stream);
+
+/* Galerkin coarse operator of `level` from level-1: A_c = P^T A P for the
+ * reference's piecewise-constant prolongation and child-sum restriction
+ * (mgpcg.py:111-123).  The reference's whole-domain Strategies rebuild each
+ * level from the fine fields instead (potential_function.py:130-145); this is
+ * the coarse-level rule of the magnetic potential Strategy above. */
+MG_API int mg_galerkin_coarsen(mg_plan_t* plan, int32_t level, void* stream);
+
 /* Prepares the V-cycle operator after the Strategy has written A:
  * detects whether every level's off-diagonals are the uniform label-derived
  * value (the pressure Strategy's form) and, for 16-bit storage, writes the

@@ -486,6 +486,98 @@ struct Solver {
     }
   }
 
+  // ---- magnetic potential solve of the 3D substep benchmark --------------
+  // Not a reference Strategy: the benchmark's variant of
+  // potential_function.py:19-55 (see the CUDA kernels in mg_strategies.cuh).
+  static Real mu_face(Real ca, Real cb) {
+    Real ma = Real(1) + ca, mb = Real(1) + cb;
+    return (Real(2) * (ma * mb)) / (ma + mb);
+  }
+  bool is_pin(const int c[3], const int pin[3]) const {
+    return c[0] == pin[0] && c[1] == pin[1] && (dim == 2 || c[2] == pin[2]);
+  }
+  void build_psi_b(const Real* chi, const Real H[3], Real dx, const int pin[3]) {
+    const Grid& gg = g[0];
+    for (int64_t i = 0; i < gg.count; ++i) {
+      int c[3];
+      gg.coords(i, c);
+      if (is_pin(c, pin)) {
+        b[i] = Real(0);
+        continue;
+      }
+      Real acc = Real(0);
+      for (int k = 0; k < dim; ++k) {
+        const int64_t s = gg.stride[k];
+        if (c[k] + 1 < gg.n[k]) acc = acc + H[k] * mu_face(chi[i], chi[i + s]);
+        if (c[k] > 0) acc = acc - H[k] * mu_face(chi[i - s], chi[i]);
+      }
+      b[i] = -(acc / dx);
+    }
+  }
+  void build_psi_A0(const Real* chi, Real dx, const int pin[3]) {
+    const Grid& gg = g[0];
+    const Real dx2 = dx * dx;
+    Real* ad = Adiag[0].data();
+    Real* ax = Ax[0].data();
+    for (int64_t i = 0; i < gg.count; ++i) {
+      int c[3];
+      gg.coords(i, c);
+      if (is_pin(c, pin)) {
+        ad[i] = Real(1) / dx2;
+        for (int k = 0; k < dim; ++k) ax[k * gg.count + i] = Real(0);
+        continue;
+      }
+      Real d = Real(0);
+      for (int k = 0; k < dim; ++k) {
+        const int64_t s = gg.stride[k];
+        Real up = Real(0);
+        if (c[k] > 0) d = d + mu_face(chi[i - s], chi[i]) / dx2;
+        if (c[k] + 1 < gg.n[k]) {
+          const Real cf = mu_face(chi[i], chi[i + s]) / dx2;
+          d = d + cf;
+          int cn[3] = {c[0], c[1], c[2]};
+          cn[k] += 1;
+          up = is_pin(cn, pin) ? Real(0) : -cf;
+        }
+        ax[k * gg.count + i] = up;
+      }
+      ad[i] = d;
+    }
+  }
+  // A_c = P^T A P for piecewise-constant P and child-sum restriction
+  void galerkin(int l) {
+    const Grid& gf = g[l - 1];
+    const Grid& gc = g[l];
+    for (int64_t ic = 0; ic < gc.count; ++ic) {
+      int cc[3];
+      gc.coords(ic, cc);
+      Real d = Real(0), axc[3] = {Real(0), Real(0), Real(0)};
+      for (int o0 = 0; o0 < 2; ++o0)
+        for (int o1 = 0; o1 < 2; ++o1)
+          for (int o2 = 0; o2 < (dim == 3 ? 2 : 1); ++o2) {
+            const int o[3] = {o0, o1, o2};
+            const int64_t i = (int64_t)(2 * cc[0] + o0) * gf.stride[0] + (int64_t)(2 * cc[1] + o1) * gf.stride[1] +
+                              (dim == 3 ? 2 * cc[2] + o2 : 0);
+            d = d + Adiag[l - 1][i];
+            for (int k = 0; k < dim; ++k) {
+              const Real a = Ax[l - 1][k * gf.count + i];
+              if (o[k] == 0) d = d + Real(2) * a;
+              else axc[k] = axc[k] + a;
+            }
+          }
+      Adiag[l][ic] = d;
+      for (int k = 0; k < dim; ++k) Ax[l][k * gc.count + ic] = (cc[k] + 1 < gc.n[k]) ? axc[k] : Real(0);
+    }
+  }
+  // full_reinitialize(strategy) (mgpcg.py:89-94) with the potential Strategy
+  void full_reinitialize_psi(const Real* chi, const Real H[3], Real dx, const int pin[3]) {
+    initialize();
+    build_psi_b(chi, H, dx, pin);
+    for (auto& t : type) std::fill(t.begin(), t.end(), (int8_t)FLUID);
+    build_psi_A0(chi, dx, pin);
+    for (int l = 1; l < L; ++l) galerkin(l);
+  }
+
   // mgpcg.py:79-87 with the pressure Strategy
   void reinitialize_pressure(const int32_t* cell_type, const Real* const* vel, const Real* phi,
                              Real p0, Real scale_A, Real scale_b, int ghost, Real clamp) {
@@ -624,6 +716,20 @@ void orc_reinitialize_pressure(void* hh, const int32_t* cell_type, const void* c
     auto* s = S<double>(h);
     s->reinitialize_pressure(cell_type, (const double* const*)vel, (const double*)phi, p0,
                              scale_A, scale_b, ghost, clamp);
+  }
+}
+
+// full_reinitialize with the magnetic potential Strategy; chi in the solver's precision.
+void orc_full_reinitialize_psi(void* hh, const void* chi, double H0, double H1, double H2, double dx, int p0,
+                               int p1, int p2) {
+  Handle* h = (Handle*)hh;
+  const int pin[3] = {p0, p1, p2};
+  if (h->real_bytes == 4) {
+    const float H[3] = {(float)H0, (float)H1, (float)H2};
+    S<float>(h)->full_reinitialize_psi((const float*)chi, H, (float)dx, pin);
+  } else {
+    const double H[3] = {H0, H1, H2};
+    S<double>(h)->full_reinitialize_psi((const double*)chi, H, dx, pin);
   }
 }
 

@@ -51,6 +51,8 @@ __global__ void __launch_bounds__(kRedThreads) k_detect_uniform(Level L, double*
     int c[3];
     L.g.coords(i, c);
     const bool fl = L.type[i] == FLUID;
+    // the fused kernels tell FLUID cells by a nonzero diagonal
+    if (fl != (L.Adiag[i] != 0.0f)) bad += 1.0;
     for (int k = 0; k < L.g.dim; ++k) {
       float a = L.Ax[k][i];
       bool coupled = fl && (c[k] + 1 < L.g.n[k]) && L.type[i + L.g.stride(k)] == FLUID;

@@ -4,6 +4,7 @@
 #include <cmath>
 
 #include "mg_sweep.cuh"
+#include "mg_coarse.cuh"
 
 namespace mg {
 
@@ -14,18 +15,21 @@ constexpr size_t kSmemLimit = 227 * 1024;
 constexpr int kCoarseMaxCells = 15360;
 
 struct TileShape {
-  int tx, ty, nt;
+  int tx, ty, nt, k;  // tile columns (x, y), threads, planes per step
 };
 
-// Launch shape of the streamed levels: a tile of ty x tx columns per block.
-inline TileShape tile_for(int dim) { return dim == 3 ? TileShape{32, 8, 256} : TileShape{128, 1, 128}; }
+// Launch shape of the streamed levels: a tile of ty x tx columns per block,
+// k planes per pipeline step.
+constexpr TileShape kTile3 = {32, 16, 256, 2};
+constexpr TileShape kTile2 = {128, 1, 128, 4};
+inline TileShape tile_for(int dim) { return dim == 3 ? kTile3 : kTile2; }
 
-inline size_t sweep_smem(int dim, int ns, bool pre, TileShape t) {
-  const int H = pre ? ns + 1 : ns;
-  const int RX = t.tx + 2 * H;
-  const int RY = dim == 3 ? t.ty + 2 * H : 1;
-  const int W = pre ? ns + 3 : ns + 2;
-  return (size_t)W * RX * RY * 13;
+// z, r, Adiag as float32 for a ring of k + ns + 1 planes of tile + halo ns.
+inline size_t sweep_smem(int dim, int ns, TileShape t) {
+  const int RX = t.tx + 2 * ns;
+  const int RY = dim == 3 ? t.ty + 2 * ns : 1;
+  const int W = t.k + ns + 1;
+  return (size_t)W * RX * RY * 12;
 }
 
 struct FusedPlan {
@@ -74,18 +78,24 @@ inline bool make_fused_plan(const Level* lv, int L, int dim, int pre_post, int b
     F->pi = std::ldexp(1.0f, dim);
   }
   for (int l = 0; l < L; ++l) F->s[l] = offdiag[l] * F->kappa;
-  // streamed levels
+  // streamed levels: the 4-wide groups need the fastest extent to be a
+  // multiple of 4 (then a group is wholly inside or wholly outside the grid)
+  const size_t smem = sweep_smem(dim, F->ns, F->tile);
+  const int per_sm = (int)(kSmemLimit / (smem + 1024)) < 1 ? 1 : (int)(kSmemLimit / (smem + 1024));
   for (int l = 0; l < lc; ++l) {
     const Geom& g = lv[l].g;
     const int nx = dim == 3 ? g.n[2] : g.n[1];
     const int ny = dim == 3 ? g.n[1] : 1;
+    if (nx % 4 != 0) return false;
     F->tiles_x[l] = (nx + F->tile.tx - 1) / F->tile.tx;
     F->tiles_y[l] = dim == 3 ? (ny + F->tile.ty - 1) / F->tile.ty : 1;
     const long long tiles = (long long)F->tiles_x[l] * F->tiles_y[l];
-    // enough blocks for ~3 resident per SM (the 3D ring takes ~69 KB)
-    const long long target = 3LL * num_sms;
+    // enough blocks to fill every SM with the blocks that fit its shared memory
+    const long long target = (long long)per_sm * num_sms;
+    // small levels are latency-bound: short chunks (more blocks, shorter
+    // serial plane chains) beat the extra halo planes they load
     long long chunk = (long long)g.n[0] * tiles / target;
-    if (chunk < 8) chunk = 8;
+    if (chunk < 2) chunk = 2;
     chunk &= ~1LL;
     if (chunk > g.n[0]) chunk = g.n[0];
     if (chunk < 2) chunk = 2;
@@ -150,11 +160,10 @@ inline SweepArgs<ST> sweep_args(const FusedPlan& F, const Level* lv, int l, cons
 
 template <int DIM, typename ST, int NS, bool PRE>
 inline cudaError_t launch_sweep_t(const FusedPlan& F, const Level* lv, int l, const Control* ctl, cudaStream_t s) {
-  constexpr int TX = DIM == 3 ? 32 : 128;
-  constexpr int TY = DIM == 3 ? 8 : 1;
-  constexpr int NT = DIM == 3 ? 256 : 128;
-  auto kern = k_sweep<DIM, ST, NS, TX, TY, PRE, NT>;
-  const size_t smem = sweep_smem(DIM, NS, PRE, TileShape{TX, TY, NT});
+  constexpr TileShape T = DIM == 3 ? kTile3 : kTile2;
+  auto kern = k_sweep<DIM, ST, NS, T.tx, T.ty, PRE, T.nt, T.k>;
+  constexpr int NT = T.nt;
+  const size_t smem = sweep_smem(DIM, NS, T);
   cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (e != cudaSuccess) return e;
   kern<<<F.blocks[l], NT, smem, s>>>(sweep_args<ST, PRE>(F, lv, l, ctl));

@@ -14,6 +14,7 @@
 #include "mg_kernels.cuh"
 #include "mg_pcg.cuh"
 #include "mg_fused_host.cuh"
+#include "mg_strategies.cuh"
 
 using namespace mg;
 
@@ -498,6 +499,34 @@ int mg_build_pressure_A(mg_plan_t* P, int32_t level, const float* phi, float sA,
   if (ghost && level == 0 && !phi) return bad("phi");
   k_build_pressure_A<<<P->ew_blocks[level], 256, 0, S(stream)>>>(P->lv[level], level, phi, sA, ghost, clamp);
   CKL("k_build_pressure_A");
+  P->prepared = false;
+  return MG_OK;
+}
+
+int mg_build_psi_b(mg_plan_t* P, const float* chi, float H0, float H1, float H2, float dx, int32_t p0,
+                   int32_t p1, int32_t p2, void* stream) {
+  NEED_BOUND(P);
+  if (!chi || !(dx > 0.0f)) return bad("chi / dx");
+  k_build_psi_b<<<P->ew_blocks[0], 256, 0, S(stream)>>>(P->lv[0], fptr(P, MG_FIELD_B), chi, H0, H1, H2, dx, p0,
+                                                         p1, P->d.dim == 3 ? p2 : 0);
+  CKL("k_build_psi_b");
+  return MG_OK;
+}
+
+int mg_build_psi_A(mg_plan_t* P, const float* chi, float dx, int32_t p0, int32_t p1, int32_t p2, void* stream) {
+  NEED_BOUND(P);
+  if (!chi || !(dx > 0.0f)) return bad("chi / dx");
+  k_build_psi_A<<<P->ew_blocks[0], 256, 0, S(stream)>>>(P->lv[0], chi, dx, p0, p1, P->d.dim == 3 ? p2 : 0);
+  CKL("k_build_psi_A");
+  P->prepared = false;
+  return MG_OK;
+}
+
+int mg_galerkin_coarsen(mg_plan_t* P, int32_t level, void* stream) {
+  NEED_BOUND(P);
+  if (level < 1 || level >= P->L) return bad("level");
+  k_galerkin<<<P->ew_blocks[level], 256, 0, S(stream)>>>(P->lv[level - 1], P->lv[level]);
+  CKL("k_galerkin");
   P->prepared = false;
   return MG_OK;
 }

@@ -72,6 +72,9 @@ _SIGS = {
     "mg_build_pressure_b": (ctypes.c_int, [_vp, _vp, _vp, _vp, _vp, _f32, _f32, _f32, _i32, _f32, _vp]),
     "mg_build_pressure_A": (ctypes.c_int, [_vp, _i32, _vp, _f32, _i32, _f32, _vp]),
     "mg_add_rhs": (ctypes.c_int, [_vp, _vp, _f32, _vp]),
+    "mg_build_psi_b": (ctypes.c_int, [_vp, _vp, _f32, _f32, _f32, _f32, _i32, _i32, _i32, _vp]),
+    "mg_build_psi_A": (ctypes.c_int, [_vp, _vp, _f32, _i32, _i32, _i32, _vp]),
+    "mg_galerkin_coarsen": (ctypes.c_int, [_vp, _i32, _vp]),
     "mg_plan_prepare": (ctypes.c_int, [_vp, _vp]),
     "mg_plan_operator_form": (ctypes.c_int, [_vp, _i32, ctypes.POINTER(_i32)]),
     "mg_smooth": (ctypes.c_int, [_vp, _i32, _i32, _vp]),
