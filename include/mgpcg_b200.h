@@ -44,6 +44,7 @@ extern "C" {
 #define MG_SOLVE_CONVERGED 0
 #define MG_SOLVE_MAX_ITERS 1   /* stopped at max_iters (the reference is silent) */
 #define MG_SOLVE_NONFINITE 2   /* a reduction produced NaN/Inf (H3: zero Adiag) */
+#define MG_SOLVE_BAD_OPERATOR 3 /* mg_plan_prepare_declared's declaration was wrong */
 
 /* V-cycle grid storage type */
 #define MG_STORE_F32 0
@@ -174,6 +175,25 @@ MG_API int mg_galerkin_coarsen(mg_plan_t* plan, int32_t level, void* stream);
  * scaled 16-bit coefficient copies.  Called by mg_pcg_solve when A changed;
  * callable explicitly to separate setup from solve time. */
 MG_API int mg_plan_prepare(mg_plan_t* plan, void* stream);
+/* Prepare without synchronizing: the caller declares that every level is
+ * label-uniform with off-diagonal magnitude offdiag[l] (what the pressure
+ * Strategy builds, pressure_project.py:56-58).  A device kernel verifies the
+ * declaration during the solve; a wrong one ends the solve with status
+ * MG_SOLVE_BAD_OPERATOR.  No reference counterpart (the reference has no
+ * operator forms). */
+MG_API int mg_plan_prepare_declared(mg_plan_t* plan, const float* offdiag, void* stream);
+
+/* The whole per-request pressure path in one call, enqueued on `stream` with
+ * no host synchronization: initialize, cell_type, PressureProjectStrategy
+ * build_b / build_A on every level, declared prepare, then the solve
+ * (mgpcg.py:79-87 followed by :150-209).  With params->warm_start the x held
+ * in the workspace is the initial guess (initialize then keeps x).  Read the
+ * outcome with mg_pcg_stats after the stream completes. */
+MG_API int mg_pressure_solve_async(mg_plan_t* plan, const int32_t* cell_type, const float* vel0,
+                                   const float* vel1, const float* vel2, const float* phi, float p0,
+                                   float scale_A, float scale_b, int32_t ghost, float gfm_clamp,
+                                   const mg_solve_params_t* params, void* stream);
+
 /* Reports the operator form chosen per level: 1 = label-uniform, 0 = stored. */
 MG_API int mg_plan_operator_form(const mg_plan_t* plan, int32_t level, int32_t* form);
 

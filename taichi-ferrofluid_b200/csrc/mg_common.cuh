@@ -63,6 +63,8 @@ struct Control {
   double scale_r;             // r (stored, level 0 input of the V-cycle) = scale_r * r
   double kappa;               // coefficient scale of 16-bit grids
   double n_fluid;             // FLUID cells of level 0
+  int bad_operator;           // set when a declared label-uniform form is wrong
+  int pad1;
   unsigned int counter[8];    // arrival counters of the last-block reductions
   double scratch[8];          // single-value results of mg_reduce
   double det[3 * 12];         // operator detection: min, max, mismatches per level

@@ -15,6 +15,25 @@ __global__ void k_set_kappa(Control* ctl, double kappa) {
   ctl->kappa = kappa;
   ctl->scale_r = 1.0;
   ctl->scale_z = kappa;
+  ctl->bad_operator = 0;
+}
+
+// Checks a declared label-uniform level: Adiag != 0 exactly on FLUID cells
+// and Ax = -s between two FLUID cells, 0 elsewhere.  Flags a mismatch.
+__global__ void k_verify_uniform(Level L, float s, Control* ctl) {
+  bool bad = false;
+  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < L.g.count;
+       i += (long long)gridDim.x * blockDim.x) {
+    int c[3];
+    L.g.coords(i, c);
+    const bool fl = L.type[i] == FLUID;
+    if (fl != (L.Adiag[i] != 0.0f)) bad = true;
+    for (int k = 0; k < L.g.dim; ++k) {
+      const bool coupled = fl && (c[k] + 1 < L.g.n[k]) && L.type[i + L.g.stride(k)] == FLUID;
+      if (L.Ax[k][i] != (coupled ? -s : 0.0f)) bad = true;
+    }
+  }
+  if (__any_sync(0xffffffffu, bad) && (threadIdx.x & 31) == 0) atomicOr(&ctl->bad_operator, 1);
 }
 
 // Copies one solve's parameters into the control block.
@@ -32,7 +51,7 @@ __device__ void set_scales(Control* ctl, double rTr);
 // r = b (reference), or r = b - A x (warm start); then r.r over FLUID cells.
 // Epilogue: rTr0, tol = max(abs_tol, rTr0 * rel_tol) (mgpcg.py:157-164).
 __global__ void __launch_bounds__(kRedThreads) k_pcg_begin(Level L, const float* __restrict__ b,
-                                                           const float* __restrict__ x, Control* ctl,
+                                                           float* __restrict__ x, Control* ctl,
                                                            double* partials) {
   __shared__ double sh[32];
   float* r = (float*)L.r;
@@ -48,6 +67,10 @@ __global__ void __launch_bounds__(kRedThreads) k_pcg_begin(Level L, const float*
       float Ax_ = __fmul_rn(L.Adiag[i], x[i]);
       Ax_ = __fadd_rn(Ax_, nbr_sum_f32(L, x, i, c));
       ri = __fsub_rn(ri, Ax_);
+    } else if (warm) {
+      // a cell that is no longer FLUID holds no pressure (the reference's x
+      // is 0 there); its stale value never enters A x (its couplings are 0)
+      x[i] = 0.0f;
     }
     r[i] = ri;
     if (L.type[i] == FLUID) acc += (double)ri * (double)ri;
@@ -67,6 +90,10 @@ __global__ void __launch_bounds__(kRedThreads) k_pcg_begin(Level L, const float*
     ctl->run = 1;
     ctl->since_refresh = 0;
     if (warm) ctl->beta = 0.0f;  // p is rebuilt from z only
+    if (ctl->bad_operator) {     // the declared operator form did not hold
+      ctl->status = MG_SOLVE_BAD_OPERATOR;
+      ctl->run = 0;
+    }
     set_scales(ctl, tot);
   }
 }

@@ -356,6 +356,8 @@ int build_graph(mg_plan* P) {
 // Lets the library's other translation units record an error message.
 void mg_internal_set_error(const char* msg) { snprintf(g_err, sizeof(g_err), "%s", msg); }
 
+static int finish_prepare(mg_plan_t* P, cudaStream_t s, bool declared);
+
 // ============================================================================
 // C ABI
 // ============================================================================
@@ -558,6 +560,24 @@ int mg_plan_prepare(mg_plan_t* P, void* stream) {
     P->op_form[l] = uniform ? 1 : 0;
     P->offdiag[l] = uniform && !none ? (float)(-h[0]) : 0.0f;
   }
+  return finish_prepare(P, s, false);
+}
+
+int mg_plan_prepare_declared(mg_plan_t* P, const float* offdiag, void* stream) {
+  NEED_BOUND(P);
+  if (!offdiag) return bad("offdiag");
+  for (int l = 0; l < P->L; ++l) {
+    P->op_form[l] = 1;
+    P->offdiag[l] = offdiag[l];
+  }
+  return finish_prepare(P, S(stream), true);
+}
+
+}  // extern "C"
+
+// Launch shapes, 16-bit coefficient copies, FLUID count, scale factors and
+// (declared forms) the asynchronous verification; no host synchronization.
+static int finish_prepare(mg_plan_t* P, cudaStream_t s, bool declared) {
   // 2. launch shapes of the fused V-cycle
   P->fp.valid = false;
   if (!(P->d.flags & MG_PLAN_STORED))
@@ -582,6 +602,12 @@ int mg_plan_prepare(mg_plan_t* P, void* stream) {
   CKL("k_count_fluid");
   k_set_kappa<<<1, 1, 0, s>>>(P->ctl, (double)P->fp.kappa);
   CKL("k_set_kappa");
+  if (declared) {
+    for (int l = 0; l < P->L; ++l) {
+      k_verify_uniform<<<P->ew_blocks[l], 256, 0, s>>>(P->lv[l], P->offdiag[l], P->ctl);
+      CKL("k_verify_uniform");
+    }
+  }
   // 4. the solve graph captured kernel arguments (shapes, s_l, kappa): rebuild
   //    it only when they changed
   uint64_t sig = 1469598103934665603ull;
@@ -604,6 +630,8 @@ int mg_plan_prepare(mg_plan_t* P, void* stream) {
   P->prepared = true;
   return MG_OK;
 }
+
+extern "C" {
 
 int mg_plan_operator_form(const mg_plan_t* P, int32_t level, int32_t* form) {
   if (!P || !form) return bad("null pointer");
@@ -750,6 +778,34 @@ int mg_launch_stage(mg_plan_t* P, int32_t stage, int32_t level, void* stream) {
       return launch_vcycle(P, s);
   }
   return bad("stage");
+}
+
+int mg_pressure_solve_async(mg_plan_t* P, const int32_t* ct, const float* v0, const float* v1, const float* v2,
+                            const float* phi, float p0, float sA, float sB, int32_t ghost, float clamp,
+                            const mg_solve_params_t* prm, void* stream) {
+  NEED_BOUND(P);
+  if (!prm || !ct) return bad("params / cell_type");
+  cudaStream_t s = S(stream);
+  // initialize() (mgpcg.py:63-77); a warm start keeps x
+  if (prm->warm_start) {
+    const Loc& lx = P->loc[MG_FIELD_X][0][0];
+    CK(cudaMemsetAsync(P->base, 0, lx.off, s));
+    const int64_t after = lx.off + lx.bytes;
+    CK(cudaMemsetAsync(P->base + after, 0, P->ws_bytes - after, s));
+  } else {
+    CK(cudaMemsetAsync(P->base, 0, P->ws_bytes, s));
+  }
+  if (int rc = mg_set_cell_type(P, ct, stream)) return rc;
+  if (int rc = mg_build_pressure_b(P, v0, v1, v2, phi, p0, sA, sB, ghost, clamp, stream)) return rc;
+  if (int rc = mg_build_pressure_A(P, 0, phi, sA, ghost, clamp, stream)) return rc;
+  for (int l = 1; l < P->L; ++l) {
+    if (int rc = mg_init_gridtype(P, l, stream)) return rc;
+    if (int rc = mg_build_pressure_A(P, l, phi, sA, ghost, clamp, stream)) return rc;
+  }
+  float od[kMaxLevels];
+  for (int l = 0; l < P->L; ++l) od[l] = sA;  // Ax = -scale_A between FLUID cells
+  if (int rc = mg_plan_prepare_declared(P, od, stream)) return rc;
+  return mg_pcg_solve_async(P, prm, stream);
 }
 
 int mg_pcg_solve(mg_plan_t* P, const mg_solve_params_t* prm, mg_solve_stats_t* st, void* stream) {

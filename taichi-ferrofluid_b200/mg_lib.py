@@ -20,8 +20,8 @@ MG_E_CUDA = -2
 MG_E_UNBOUND = -3
 MG_E_TOO_BIG = -4
 
-SOLVE_CONVERGED, SOLVE_MAX_ITERS, SOLVE_NONFINITE = 0, 1, 2
-STATUS_NAMES = {0: "converged", 1: "max_iters", 2: "nonfinite"}
+SOLVE_CONVERGED, SOLVE_MAX_ITERS, SOLVE_NONFINITE, SOLVE_BAD_OPERATOR = 0, 1, 2, 3
+STATUS_NAMES = {0: "converged", 1: "max_iters", 2: "nonfinite", 3: "bad_operator"}
 
 STORE = {"f32": 0, "fp32": 0, "float32": 0, "f16": 1, "fp16": 1, "float16": 1, "bf16": 2, "bfloat16": 2}
 STORE_BYTES = {0: 4, 1: 2, 2: 2}
@@ -76,6 +76,9 @@ _SIGS = {
     "mg_build_psi_A": (ctypes.c_int, [_vp, _vp, _f32, _i32, _i32, _i32, _vp]),
     "mg_galerkin_coarsen": (ctypes.c_int, [_vp, _i32, _vp]),
     "mg_plan_prepare": (ctypes.c_int, [_vp, _vp]),
+    "mg_plan_prepare_declared": (ctypes.c_int, [_vp, ctypes.POINTER(_f32), _vp]),
+    "mg_pressure_solve_async": (ctypes.c_int, [_vp, _vp, _vp, _vp, _vp, _vp, _f32, _f32, _f32, _i32, _f32,
+                                               ctypes.c_void_p, _vp]),
     "mg_plan_operator_form": (ctypes.c_int, [_vp, _i32, ctypes.POINTER(_i32)]),
     "mg_smooth": (ctypes.c_int, [_vp, _i32, _i32, _vp]),
     "mg_restrict": (ctypes.c_int, [_vp, _i32, _vp]),

@@ -184,20 +184,31 @@ SIDES_2D = tuple(range(64, 513, 32))
 SIDES_3D = tuple(range(32, 161, 16))
 
 
-def random_domain_phi(rng, res, dx):
-    """Union of 1-3 boxes or spheres, size/radius U[0.1, 0.3], centre U[0.2, 0.8]."""
-    pts = cell_centres(res, dx)
-    dim = len(res)
-    phi = None
+def domain_shapes(rng, dim):
+    """1-3 boxes or spheres: ("box", centre, half sizes) or ("sphere", centre, radius),
+    size/radius U[0.1, 0.3], centre U[0.2, 0.8]."""
+    shapes = []
     for _ in range(int(rng.integers(1, 4))):
         centre = rng.uniform(0.2, 0.8, size=dim)
         if rng.random() < 0.5:
-            half = rng.uniform(0.1, 0.3, size=dim)
-            d = box_sdf(pts, centre - half, centre + half)
+            shapes.append(("box", centre, rng.uniform(0.1, 0.3, size=dim)))
         else:
-            d = sphere_sdf(pts, centre, rng.uniform(0.1, 0.3))
+            shapes.append(("sphere", centre, rng.uniform(0.1, 0.3)))
+    return shapes
+
+
+def shapes_phi(shapes, pts):
+    """Signed distance to the union of `shapes` at the points `pts`."""
+    phi = None
+    for kind, centre, size in shapes:
+        d = box_sdf(pts, centre - size, centre + size) if kind == "box" else sphere_sdf(pts, centre, size)
         phi = d if phi is None else np.minimum(phi, d)
     return phi
+
+
+def random_domain_phi(rng, res, dx):
+    """Union of 1-3 boxes or spheres, size/radius U[0.1, 0.3], centre U[0.2, 0.8]."""
+    return shapes_phi(domain_shapes(rng, len(res)), cell_centres(res, dx))
 
 
 def batch_scene_params(seed=3, n2d=64, n3d=32):
@@ -235,16 +246,15 @@ def instance_scene(dim, side, scene_seed, levels=4, shift=None, fluid_rule="lt",
 
 
 def _random_domain_phi_at(rng, pts, dim):
-    phi = None
-    for _ in range(int(rng.integers(1, 4))):
-        centre = rng.uniform(0.2, 0.8, size=dim)
-        if rng.random() < 0.5:
-            half = rng.uniform(0.1, 0.3, size=dim)
-            d = box_sdf(pts, centre - half, centre + half)
-        else:
-            d = sphere_sdf(pts, centre, rng.uniform(0.1, 0.3))
-        phi = d if phi is None else np.minimum(phi, d)
-    return phi
+    return shapes_phi(domain_shapes(rng, dim), pts)
+
+
+def instance_shapes(dim, scene_seed):
+    """The shapes and the velocity seed instance_scene draws for a scene seed."""
+    rng = np.random.default_rng(scene_seed)
+    geo_rng = np.random.default_rng(rng.integers(0, 2**31 - 1))
+    vel_seed = int(rng.integers(0, 2**31 - 1))
+    return domain_shapes(geo_rng, dim), vel_seed
 
 
 def batch_scenes(seed=3, n2d=64, n3d=32, levels=4):

@@ -254,6 +254,28 @@ class MGPCGPoissonSolver:
             prm.warm_start = 1
         check(self.lib.mg_pcg_solve_async(self.plan, mg_lib.ctypes.byref(prm), self._s()), "mg_pcg_solve_async")
 
+    def pressure_solve_async(self, cell_type, velocity, phi, p0, scale_A, scale_b, ghost_fluid_method=True,
+                             gfm_clamp=1e3, max_iters=500, rel_tol=1e-12, abs_tol=1e-14, eps=1e-12,
+                             warm_start=False, stream=None):
+        """reinitialize(cell_type, PressureProjectStrategy) + solve in ONE
+        library call with no host synchronization (mg_pressure_solve_async):
+        many of these can be in flight on different streams.  Inputs are
+        device tensors in the layouts of PressureProjectStrategy; with
+        ``warm_start`` the current ``x`` is the initial guess."""
+        prm = mg_lib.SolveParams()
+        prm.max_iters = int(max_iters)
+        prm.rel_tol = float(rel_tol)
+        prm.abs_tol = float(abs_tol)
+        prm.eps = float(eps)
+        prm.warm_start = 1 if warm_start else 0
+        self._prm = prm  # the call copies it, but keep it alive for clarity
+        v2 = velocity[2] if self.dim == 3 else None
+        s = stream.cuda_stream if stream is not None else self._s()
+        check(self.lib.mg_pressure_solve_async(
+            self.plan, cell_type.data_ptr(), velocity[0].data_ptr(), velocity[1].data_ptr(), mg_lib.ptr(v2),
+            mg_lib.ptr(phi), float(p0), float(scale_A), float(scale_b), int(bool(ghost_fluid_method)),
+            float(gfm_clamp), mg_lib.ctypes.byref(prm), s), "mg_pressure_solve_async")
+
     def launch_counts(self):
         """(kernels before the PCG loop, kernels per further iteration)."""
         a, b = mg_lib.ctypes.c_int32(), mg_lib.ctypes.c_int32()
@@ -265,10 +287,11 @@ class MGPCGPoissonSolver:
         """Launches one pipeline stage once (for timing; see mg_launch_stage)."""
         check(self.lib.mg_launch_stage(self.plan, int(stage), int(level), self._s()), "mg_launch_stage")
 
-    def stats(self):
+    def stats(self, stream=None):
         """Waits for the stream and returns the last solve's outcome."""
         st = mg_lib.SolveStats()
-        check(self.lib.mg_pcg_stats(self.plan, mg_lib.ctypes.byref(st), self._s()), "mg_pcg_stats")
+        s = stream.cuda_stream if stream is not None else self._s()
+        check(self.lib.mg_pcg_stats(self.plan, mg_lib.ctypes.byref(st), s), "mg_pcg_stats")
         self.last_stats = st
         self.last_iters = st.iters
         self.last_status = mg_lib.STATUS_NAMES.get(st.status, str(st.status))
