@@ -77,6 +77,7 @@ def parse():
     ap.add_argument("--workload", default="substep128", choices=list(WORKLOADS))
     ap.add_argument("--storage", default="f32", choices=["f32", "f16", "bf16"])
     ap.add_argument("--cpu-seconds", type=float, default=12.0, help="CPU baseline sample length")
+    ap.add_argument("--no-variants", action="store_true", help="skip the batched / served comparison")
     return ap.parse_args()
 
 
@@ -252,6 +253,15 @@ def stage_bytes(solver, storage):
     sv = 4 if storage == "f32" else 2
     d = solver.dim
     coarse = 2 ** d
+    cg = {
+        "Ap_alpha": 4 + 4 + 4 * d + 1 + 4,                     # p, Adiag, Ax, label, Ap out
+        "xr": 4 * 4 + 1 + 2 * 4,                               # x, p, r, Ap, label; x, r out
+    }
+    if solver.operator_form(0) == 1:  # fused V-cycle kernels of the label-uniform form
+        return dict(cg, **{
+            "pre_l0": 4 + sv + sv + 2 * sv / coarse,           # r, Ad; z out, r_c + z_c out
+            "post_l0": sv + sv / coarse + 4 + sv + sv,          # zt, z_c, r, Ad; z out
+        })
     return {
         "pre_l0": 4 + sv + 1 + sv + 2 * sv / coarse,          # r, Ad, label, z out, r_c + z_c out
         "post_l0": sv + sv / coarse + 4 + sv + 1 + sv,         # z, z_c, r, Ad, label, z out
@@ -397,6 +407,53 @@ def gpu_arm(args, rank, world, local):
     return res, cases
 
 
+# ---------------------------------------------------------------- batched / served forms
+def variants(dev, reps=3):
+    """The 96-instance uneven batch and the served session stream, each against
+    the plain FP32 one-at-a-time form on the same GPU (device-resident inputs;
+    the batch is timed with CUDA events, serving by wall clock per request)."""
+    import torch
+    import mg_batch
+    import mg_serve
+    out = {}
+    params = mg_scenes.batch_scene_params(seed=3)
+    scenes = [mg_scenes.instance_scene(d, s, ss, levels=mg_serve.levels_for(d, s)) for d, s, ss in params]
+    bt = {"instances": len(scenes), "cells": int(sum(s.cells for s in scenes))}
+    for storage in ("f32", "f16"):
+        b = mg_batch.BatchSolver(scenes, storage=storage, streams=32, device=dev)
+        b.solve()
+        ms = min(b.solve()[0] for _ in range(reps))
+        _, st = b.solve()
+        bt[f"batched_{storage}"] = {"solves_per_s": round(len(scenes) / (ms * 1e-3), 1), "batch_ms": round(ms, 3),
+                                    "converged": sum(s.status == 0 for s in st),
+                                    "iters_max": max(s.iters for s in st)}
+        if storage == "f32":
+            b.solve_one_at_a_time()
+            ms1 = min(b.solve_one_at_a_time()[0] for _ in range(2))
+            bt["plain_f32_one_at_a_time"] = {"solves_per_s": round(len(scenes) / (ms1 * 1e-3), 1),
+                                             "batch_ms": round(ms1, 3)}
+        del b
+        torch.cuda.empty_cache()
+    base = bt["plain_f32_one_at_a_time"]["solves_per_s"]
+    bt["speedup_vs_plain"] = {k: round(bt[k]["solves_per_s"] / base, 2) for k in ("batched_f32", "batched_f16")}
+    out["batched"] = bt
+    specs = mg_scenes.serving_sessions(seed=4, n_sessions=32, substeps=20, rate_hz=400)
+    sv = {"sessions": len(specs), "substeps": 20, "arrival_rate_hz": 400, "hbm_budget_gb": 120}
+    for storage in ("f32", "f16"):
+        srv = mg_serve.SolveServer(storage=storage, streams=32, device=dev)
+        srv.run(specs[:4])
+        recs, wall = srv.run(specs)
+        sv[f"served_{storage}"] = mg_serve.summarize(recs, wall)
+    srv = mg_serve.SolveServer(storage="f32", streams=1, device=dev)
+    srv.run_one_at_a_time(specs[:2])
+    recs, wall = srv.run_one_at_a_time(specs)
+    sv["plain_f32_one_at_a_time"] = mg_serve.summarize(recs, wall)
+    base = sv["plain_f32_one_at_a_time"]["solves_per_s"]
+    sv["speedup_vs_plain"] = {k: round(sv[k]["solves_per_s"] / base, 2) for k in ("served_f32", "served_f16")}
+    out["served"] = sv
+    return out
+
+
 # ---------------------------------------------------------------- CPU (oracle)
 def cpu_solve_rate(cases, seconds, threads=None):
     """Solves/s of the CPU oracle (float32, all host threads) on the workload's
@@ -474,6 +531,9 @@ def main():
             res["cpu_baseline"] = {"value": round(rate, 4), "unit": "solves/s", "cores": cores, "kind": "port",
                                    "sample": f"{n} solves of the workload in {dt:.1f} s by the C++/OpenMP oracle "
                                              f"(float32, {cores} threads); CPU iterations {min(iters)}-{max(iters)}"}
+        if world == 1 and not args.no_variants:
+            import torch
+            res["variants"] = variants(torch.device("cuda", local))
         print(json.dumps(res))
     if world > 1:
         import torch.distributed as dist

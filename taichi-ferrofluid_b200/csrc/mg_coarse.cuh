@@ -8,225 +8,248 @@ namespace mg {
 // ---------------------------------------------------------------------------
 // k_coarse: the coarse V-cycle in one thread block
 // ---------------------------------------------------------------------------
+//
+// Shared memory, per level, a PADDED grid (one ring of cells around it) of
+//   zm: z masked - the value on FLUID cells, 0 on every other cell and on the
+//       ring, so a neighbour term is (-s) * zm for every neighbour (the same
+//       float32 result as the reference's Ax * z, see k_sweep);
+//   sr: r on FLUID cells; on non-FLUID cells the UNMASKED z, which the
+//       smoother never touches but prolongation carries to the finer level
+//       (mgpcg.py:120-123 adds to every cell); their r is never read;
+//   sa: Adiag (nonzero exactly on FLUID cells; mg_plan_prepare checks it).
 
-constexpr int kCoarseThreads = 512;
 constexpr int kBottomPerThread = 4;  // cached bottom cells per colour and thread
 
 struct CoarseArgs {
   int dim, nlev, pre_post, bottom;
   int n[kMaxLevels][3];     // shapes of the levels handled (lc .. L-1); 2D: (n0, n1, 1)
-  int off[kMaxLevels];      // cell offset of each level inside the shared arrays
+  int off[kMaxLevels];      // offset of each PADDED level inside the shared arrays
   float s[kMaxLevels];      // kappa * s_l
-  const int8_t* type[kMaxLevels];
   const void* Ad[kMaxLevels];
   const void* r0;           // r of level lc (float if r_f32)
   void* z0;                 // z of level lc (written)
   int r_f32;
   float rho, pi;            // per-level restriction / prolongation factors
   const Control* ctl;
-  int total;                // total cells
+  int total;                // padded cells of all levels
 };
 
-// Cell of colour `phase` number j of a level (row-major rows, every other
-// cell along the last axis).  Returns false when j runs past a short row.
-__device__ __forceinline__ bool colour_cell(const int n[3], int dim, int j, int phase, int c[3]) {
-  const int nl = dim == 3 ? n[2] : n[1];
+// Padded geometry of one level: P = n + 2 per axis (2D: no padding along the
+// absent third axis).
+struct PGeom {
+  int n0, n1, n2, P1, P2, o;   // sizes, padded strides, level offset
+  int s0, s1, s2;              // neighbour strides in the padded grid
+  __device__ __forceinline__ int at(int c0, int c1, int c2) const {
+    return o + ((c0 + 1) * P1 + (c1 + 1)) * P2 + c2 + (P2 > 1 ? 1 : 0);
+  }
+};
+
+__device__ __forceinline__ PGeom pgeom(const CoarseArgs& A, int l) {
+  PGeom g;
+  g.n0 = A.n[l][0];
+  g.n1 = A.n[l][1];
+  g.n2 = A.n[l][2];
+  g.P1 = g.n1 + 2;
+  g.P2 = A.dim == 3 ? g.n2 + 2 : 1;
+  g.o = A.off[l];
+  g.s0 = g.P1 * g.P2;
+  g.s1 = g.P2;
+  g.s2 = 1;
+  return g;
+}
+
+// j-th cell of colour `phase` (rows of the last axis, every other cell);
+// exact small-integer division through float reciprocals.
+__device__ __forceinline__ bool colour_cell(const PGeom& g, int dim, int j, int phase, int& c0, int& c1, int& c2) {
+  const int nl = dim == 3 ? g.n2 : g.n1;
   const int half = (nl + 1) >> 1;
-  const int row = j / half, k = j - row * half;
+  const int row = (int)(((float)j + 0.5f) / (float)half);
+  const int k = j - row * half;
   if (dim == 3) {
-    c[0] = row / n[1];
-    c[1] = row - c[0] * n[1];
-    c[2] = 2 * k + ((phase - c[0] - c[1]) & 1);
-    return c[2] < n[2];
+    c0 = (int)(((float)row + 0.5f) / (float)g.n1);
+    c1 = row - c0 * g.n1;
+    c2 = 2 * k + ((phase - c0 - c1) & 1);
+    return c2 < g.n2;
   }
-  c[0] = row;
-  c[1] = 2 * k + ((phase - c[0]) & 1);
-  c[2] = 0;
-  return c[1] < n[1];
+  c0 = row;
+  c1 = 2 * k + ((phase - c0) & 1);
+  c2 = 0;
+  return c1 < g.n1;
 }
 
-__device__ __forceinline__ int colour_count(const int n[3], int dim) {
-  const int nl = dim == 3 ? n[2] : n[1];
-  return (n[0] * n[1] * n[2] / nl) * ((nl + 1) >> 1);
+__device__ __forceinline__ int colour_count(const PGeom& g, int dim) {
+  const int nl = dim == 3 ? g.n2 : g.n1;
+  return (g.n0 * g.n1 * g.n2 / nl) * ((nl + 1) >> 1);
 }
 
-// Neighbour sum of cell (c0,c1,c2) of level l with FLUID checks (the coarse
-// kernel keeps unmasked z: non-FLUID z reaches finer levels by prolongation).
-__device__ __forceinline__ float coarse_nsum(const CoarseArgs& A, int l, const int c[3], int g, const float* sz,
-                                             const int8_t* sl) {
-  const int n0 = A.n[l][0], n1 = A.n[l][1], n2 = A.n[l][2];
-  const float ms = -A.s[l];
-  const int s0 = n1 * n2, s1 = n2;
+// Neighbour sum (mgpcg.py:96-102) at padded index p, masked z.
+__device__ __forceinline__ float csum(const float* zm, int p, const PGeom& g, int dim, float ms) {
   float ret = 0.0f;
-  float l0 = (c[0] > 0 && sl[g - s0] == FLUID) ? __fmul_rn(ms, sz[g - s0]) : 0.0f;
-  float h0 = (c[0] + 1 < n0 && sl[g + s0] == FLUID) ? __fmul_rn(ms, sz[g + s0]) : 0.0f;
-  ret = __fadd_rn(ret, __fadd_rn(l0, h0));
-  float l1 = (c[1] > 0 && sl[g - s1] == FLUID) ? __fmul_rn(ms, sz[g - s1]) : 0.0f;
-  float h1 = (c[1] + 1 < n1 && sl[g + s1] == FLUID) ? __fmul_rn(ms, sz[g + s1]) : 0.0f;
-  ret = __fadd_rn(ret, __fadd_rn(l1, h1));
-  if (A.dim == 3) {
-    float l2 = (c[2] > 0 && sl[g - 1] == FLUID) ? __fmul_rn(ms, sz[g - 1]) : 0.0f;
-    float h2 = (c[2] + 1 < n2 && sl[g + 1] == FLUID) ? __fmul_rn(ms, sz[g + 1]) : 0.0f;
-    ret = __fadd_rn(ret, __fadd_rn(l2, h2));
-  }
+  ret = __fadd_rn(ret, __fadd_rn(__fmul_rn(ms, zm[p - g.s0]), __fmul_rn(ms, zm[p + g.s0])));
+  ret = __fadd_rn(ret, __fadd_rn(__fmul_rn(ms, zm[p - g.s1]), __fmul_rn(ms, zm[p + g.s1])));
+  if (dim == 3) ret = __fadd_rn(ret, __fadd_rn(__fmul_rn(ms, zm[p - 1]), __fmul_rn(ms, zm[p + 1])));
   return ret;
 }
 
-__device__ void coarse_smooth(const CoarseArgs& A, int l, int phase, float* sz, const float* sr, const float* sa,
-                              const int8_t* sl) {
-  const int cnt = colour_count(A.n[l], A.dim);
+__device__ void coarse_smooth(const CoarseArgs& A, int l, int phase, float* zm, const float* sr, const float* sa) {
+  const PGeom g = pgeom(A, l);
+  const float ms = -A.s[l];
+  const int cnt = colour_count(g, A.dim);
   for (int j = threadIdx.x; j < cnt; j += blockDim.x) {
-    int c[3];
-    if (!colour_cell(A.n[l], A.dim, j, phase, c)) continue;
-    const int g = A.off[l] + (c[0] * A.n[l][1] + c[1]) * A.n[l][2] + c[2];
-    if (sl[g] != FLUID) continue;
-    sz[g] = __fdiv_rn(__fsub_rn(sr[g], coarse_nsum(A, l, c, g, sz, sl)), sa[g]);
+    int c0, c1, c2;
+    if (!colour_cell(g, A.dim, j, phase, c0, c1, c2)) continue;
+    const int p = g.at(c0, c1, c2);
+    const float a = sa[p];
+    if (a == 0.0f) continue;
+    zm[p] = __fdiv_rn(__fsub_rn(sr[p], csum(zm, p, g, A.dim, ms)), a);
   }
 }
 
-// Shared layout: z[total] f32, r[total] f32, Ad[total] f32, type[total] i8.
 template <typename ST>
-__global__ void __launch_bounds__(kCoarseThreads) k_coarse(CoarseArgs A) {
+__global__ void __launch_bounds__(1024) k_coarse(CoarseArgs A) {
   extern __shared__ __align__(16) unsigned char smem[];
-  float* sz = (float*)smem;
-  float* sr = sz + A.total;
+  float* zm = (float*)smem;
+  float* sr = zm + A.total;
   float* sa = sr + A.total;
-  int8_t* sl = (int8_t*)(sa + A.total);
   const float sigma = A.r_f32 ? (float)A.ctl->scale_r : 1.0f;
+  const int dim = A.dim;
+  // zero everything (the rings stay 0), then load each level's Adiag and
+  // level lc's r (FLUID cells) - z starts at 0
+  for (int i = threadIdx.x; i < 3 * A.total; i += blockDim.x) zm[i] = 0.0f;
+  __syncthreads();
   for (int l = 0; l < A.nlev; ++l) {
-    const int cnt = A.n[l][0] * A.n[l][1] * A.n[l][2];
-    const int o = A.off[l];
+    const PGeom g = pgeom(A, l);
+    const int cnt = g.n0 * g.n1 * g.n2;
     for (int i = threadIdx.x; i < cnt; i += blockDim.x) {
-      sl[o + i] = A.type[l][i];
-      sa[o + i] = to_f<ST>(((const ST*)A.Ad[l])[i]);
-      sz[o + i] = 0.0f;
-      sr[o + i] = l == 0 ? load_r<ST>(A.r0, i, A.r_f32, sigma) : 0.0f;
+      const int c2 = dim == 3 ? i % g.n2 : 0;
+      const int t = dim == 3 ? i / g.n2 : i;
+      const int c1 = t % g.n1, c0 = t / g.n1;
+      const int p = g.at(c0, c1, c2);
+      const float a = to_f<ST>(((const ST*)A.Ad[l])[i]);
+      sa[p] = a;
+      if (l == 0 && a != 0.0f) sr[p] = load_r<ST>(A.r0, i, A.r_f32, sigma);
     }
   }
   __syncthreads();
   const int L = A.nlev;
   for (int l = 0; l < L - 1; ++l) {
     for (int i = 0; i < A.pre_post; ++i) {
-      coarse_smooth(A, l, 0, sz, sr, sa, sl);
+      coarse_smooth(A, l, 0, zm, sr, sa);
       __syncthreads();
-      coarse_smooth(A, l, 1, sz, sr, sa, sl);
+      coarse_smooth(A, l, 1, zm, sr, sa);
       __syncthreads();
     }
-    // restrict: coarse r = rho * sum over FLUID children (lexicographic order)
-    const int m1 = A.n[l + 1][1], m2 = A.n[l + 1][2];
-    const int cnt = A.n[l + 1][0] * m1 * m2;
+    // restrict: coarse r = rho * sum over FLUID children (lexicographic order);
+    // a non-FLUID coarse cell keeps sr = 0, its unmasked z
+    const PGeom gf = pgeom(A, l), gc = pgeom(A, l + 1);
+    const float ms = -A.s[l];
+    const int cnt = gc.n0 * gc.n1 * gc.n2;
     for (int i = threadIdx.x; i < cnt; i += blockDim.x) {
-      const int c2 = i % m2, t = i / m2, c1 = t % m1, c0 = t / m1;
+      const int c2 = dim == 3 ? i % gc.n2 : 0;
+      const int t = dim == 3 ? i / gc.n2 : i;
+      const int c1 = t % gc.n1, c0 = t / gc.n1;
+      const int pc = gc.at(c0, c1, c2);
+      if (sa[pc] == 0.0f) continue;
       float acc = 0.0f;
       for (int o0 = 0; o0 < 2; ++o0)
         for (int o1 = 0; o1 < 2; ++o1)
-          for (int o2 = 0; o2 < (A.dim == 3 ? 2 : 1); ++o2) {
-            const int f[3] = {2 * c0 + o0, 2 * c1 + o1, A.dim == 3 ? 2 * c2 + o2 : 0};
-            const int g = A.off[l] + (f[0] * A.n[l][1] + f[1]) * A.n[l][2] + f[2];
-            if (sl[g] == FLUID) {
-              const float Az = __fadd_rn(__fmul_rn(sa[g], sz[g]), coarse_nsum(A, l, f, g, sz, sl));
-              acc = __fadd_rn(acc, __fsub_rn(sr[g], Az));
+          for (int o2 = 0; o2 < (dim == 3 ? 2 : 1); ++o2) {
+            const int p = gf.at(2 * c0 + o0, 2 * c1 + o1, dim == 3 ? 2 * c2 + o2 : 0);
+            const float a = sa[p];
+            if (a != 0.0f) {
+              const float Az = __fadd_rn(__fmul_rn(a, zm[p]), csum(zm, p, gf, dim, ms));
+              acc = __fadd_rn(acc, __fsub_rn(sr[p], Az));
             }
           }
-      sr[A.off[l + 1] + i] = __fmul_rn(A.rho, acc);
+      sr[pc] = __fmul_rn(A.rho, acc);
     }
     __syncthreads();
   }
   // bottom sweeps (mgpcg.py:136-142)
   const int nh = A.bottom / 2;
-  const int lb = L - 1;
-  const int cntb = colour_count(A.n[lb], A.dim);
-  if (cntb <= kBottomPerThread * kCoarseThreads) {
-    // cache each owned cell's index, r, Adiag and neighbour-coupling mask in
-    // registers: the 2*bottom half sweeps then touch shared memory only for z
-    int gi[2][kBottomPerThread], mk[2][kBottomPerThread];
-    float rr[2][kBottomPerThread], aa[2][kBottomPerThread];
-    const int n0 = A.n[lb][0], n1 = A.n[lb][1], n2 = A.n[lb][2];
-    const int s0 = n1 * n2, s1 = n2;
+  {
+    const PGeom g = pgeom(A, L - 1);
+    const float ms = -A.s[L - 1];
+    const int cntb = colour_count(g, dim);
+    if (cntb <= kBottomPerThread * (int)blockDim.x) {
+      // each owned cell's padded index, r and Adiag in registers
+      int gi[2][kBottomPerThread];
+      float rr[2][kBottomPerThread], aa[2][kBottomPerThread];
 #pragma unroll
-    for (int ph = 0; ph < 2; ++ph) {
-#pragma unroll
-      for (int k = 0; k < kBottomPerThread; ++k) {
-        const int j = threadIdx.x + k * kCoarseThreads;
-        int c[3];
-        gi[ph][k] = -1;
-        mk[ph][k] = 0;
-        rr[ph][k] = 0.0f;
-        aa[ph][k] = 1.0f;
-        if (j < cntb && colour_cell(A.n[lb], A.dim, j, ph, c)) {
-          const int g = A.off[lb] + (c[0] * n1 + c[1]) * n2 + c[2];
-          if (sl[g] == FLUID) {
-            int m = 0;
-            if (c[0] > 0 && sl[g - s0] == FLUID) m |= 1;
-            if (c[0] + 1 < n0 && sl[g + s0] == FLUID) m |= 2;
-            if (c[1] > 0 && sl[g - s1] == FLUID) m |= 4;
-            if (c[1] + 1 < n1 && sl[g + s1] == FLUID) m |= 8;
-            if (A.dim == 3 && c[2] > 0 && sl[g - 1] == FLUID) m |= 16;
-            if (A.dim == 3 && c[2] + 1 < n2 && sl[g + 1] == FLUID) m |= 32;
-            gi[ph][k] = g;
-            mk[ph][k] = m;
-            rr[ph][k] = sr[g];
-            aa[ph][k] = sa[g];
-          }
-        }
-      }
-    }
-    const float ms = -A.s[lb];
-    for (int i = 0; i < 2 * nh; ++i) {
-#pragma unroll
-      for (int h = 0; h < 2; ++h) {
-        const int ph = i < nh ? h : 1 - h;
+      for (int ph = 0; ph < 2; ++ph) {
 #pragma unroll
         for (int k = 0; k < kBottomPerThread; ++k) {
-          const int g = ph ? gi[1][k] : gi[0][k];
-          const int m = ph ? mk[1][k] : mk[0][k];
-          if (g >= 0) {
-            float ret = 0.0f;
-            float l0 = (m & 1) ? __fmul_rn(ms, sz[g - s0]) : 0.0f;
-            float h0 = (m & 2) ? __fmul_rn(ms, sz[g + s0]) : 0.0f;
-            ret = __fadd_rn(ret, __fadd_rn(l0, h0));
-            float l1 = (m & 4) ? __fmul_rn(ms, sz[g - s1]) : 0.0f;
-            float h1 = (m & 8) ? __fmul_rn(ms, sz[g + s1]) : 0.0f;
-            ret = __fadd_rn(ret, __fadd_rn(l1, h1));
-            if (A.dim == 3) {
-              float l2 = (m & 16) ? __fmul_rn(ms, sz[g - 1]) : 0.0f;
-              float h2 = (m & 32) ? __fmul_rn(ms, sz[g + 1]) : 0.0f;
-              ret = __fadd_rn(ret, __fadd_rn(l2, h2));
+          const int j = threadIdx.x + k * blockDim.x;
+          int c0, c1, c2;
+          gi[ph][k] = -1;
+          rr[ph][k] = 0.0f;
+          aa[ph][k] = 1.0f;
+          if (j < cntb && colour_cell(g, dim, j, ph, c0, c1, c2)) {
+            const int p = g.at(c0, c1, c2);
+            if (sa[p] != 0.0f) {
+              gi[ph][k] = p;
+              rr[ph][k] = sr[p];
+              aa[ph][k] = sa[p];
             }
-            const float r_ = ph ? rr[1][k] : rr[0][k];
-            const float a_ = ph ? aa[1][k] : aa[0][k];
-            sz[g] = __fdiv_rn(__fsub_rn(r_, ret), a_);
           }
         }
-        __syncthreads();
       }
-    }
-  } else {
-    for (int i = 0; i < 2 * nh; ++i) {
-      for (int h = 0; h < 2; ++h) {
-        coarse_smooth(A, lb, i < nh ? h : 1 - h, sz, sr, sa, sl);
-        __syncthreads();
+      for (int i = 0; i < 2 * nh; ++i) {
+#pragma unroll
+        for (int h = 0; h < 2; ++h) {
+          const int ph = i < nh ? h : 1 - h;
+#pragma unroll
+          for (int k = 0; k < kBottomPerThread; ++k) {
+            const int p = ph ? gi[1][k] : gi[0][k];
+            if (p >= 0) {
+              const float r_ = ph ? rr[1][k] : rr[0][k];
+              const float a_ = ph ? aa[1][k] : aa[0][k];
+              zm[p] = __fdiv_rn(__fsub_rn(r_, csum(zm, p, g, dim, ms)), a_);
+            }
+          }
+          __syncthreads();
+        }
+      }
+    } else {
+      for (int i = 0; i < 2 * nh; ++i) {
+        for (int h = 0; h < 2; ++h) {
+          coarse_smooth(A, L - 1, i < nh ? h : 1 - h, zm, sr, sa);
+          __syncthreads();
+        }
       }
     }
   }
   for (int l = L - 2; l >= 0; --l) {
-    const int cnt = A.n[l][0] * A.n[l][1] * A.n[l][2];
-    const int n1 = A.n[l][1], n2 = A.n[l][2];
+    // prolongate: every cell += parent's unmasked z (FLUID: zm, else sr)
+    const PGeom gf = pgeom(A, l), gc = pgeom(A, l + 1);
+    const int cnt = gf.n0 * gf.n1 * gf.n2;
     for (int i = threadIdx.x; i < cnt; i += blockDim.x) {
-      const int c2 = i % n2, t = i / n2, c1 = t % n1, c0 = t / n1;
-      const int gc = A.off[l + 1] + ((c0 >> 1) * A.n[l + 1][1] + (c1 >> 1)) * A.n[l + 1][2] + (c2 >> 1);
-      sz[A.off[l] + i] = __fadd_rn(sz[A.off[l] + i], __fmul_rn(A.pi, sz[gc]));
+      const int c2 = dim == 3 ? i % gf.n2 : 0;
+      const int t = dim == 3 ? i / gf.n2 : i;
+      const int c1 = t % gf.n1, c0 = t / gf.n1;
+      const int pc = gc.at(c0 >> 1, c1 >> 1, dim == 3 ? c2 >> 1 : 0);
+      const float v = __fmul_rn(A.pi, sa[pc] != 0.0f ? zm[pc] : sr[pc]);
+      const int p = gf.at(c0, c1, c2);
+      if (sa[p] != 0.0f) zm[p] = __fadd_rn(zm[p], v);
+      else sr[p] = __fadd_rn(sr[p], v);
     }
     __syncthreads();
     for (int i = 0; i < A.pre_post; ++i) {
-      coarse_smooth(A, l, 1, sz, sr, sa, sl);
+      coarse_smooth(A, l, 1, zm, sr, sa);
       __syncthreads();
-      coarse_smooth(A, l, 0, sz, sr, sa, sl);
+      coarse_smooth(A, l, 0, zm, sr, sa);
       __syncthreads();
     }
   }
-  const int cnt0 = A.n[0][0] * A.n[0][1] * A.n[0][2];
-  for (int i = threadIdx.x; i < cnt0; i += blockDim.x) ((ST*)A.z0)[i] = from_f<ST>(sz[i]);
+  const PGeom g0 = pgeom(A, 0);
+  const int cnt0 = g0.n0 * g0.n1 * g0.n2;
+  for (int i = threadIdx.x; i < cnt0; i += blockDim.x) {
+    const int c2 = dim == 3 ? i % g0.n2 : 0;
+    const int t = dim == 3 ? i / g0.n2 : i;
+    const int c1 = t % g0.n1, c0 = t / g0.n1;
+    const int p = g0.at(c0, c1, c2);
+    ((ST*)A.z0)[i] = from_f<ST>(sa[p] != 0.0f ? zm[p] : sr[p]);
+  }
 }
 
 }  // namespace mg

@@ -10,9 +10,14 @@ namespace mg {
 
 // Shared memory one block may use (B200: 227 KB per block).
 constexpr size_t kSmemLimit = 227 * 1024;
-// Cells the block-resident coarse V-cycle may hold: 13 bytes each
-// (z, r, Adiag as float32 plus the label), under ~200 KB.
-constexpr int kCoarseMaxCells = 15360;
+// Padded cells the block-resident coarse V-cycle may hold: 12 bytes each
+// (masked z, r / unmasked z, Adiag as float32), under 200 KB.
+constexpr int kCoarseMaxCells = 16384;
+
+// Cells of a level padded by one ring (2D: no padding along the absent axis).
+inline long long padded_cells(const Geom& g) {
+  return (long long)(g.n[0] + 2) * (g.n[1] + 2) * (g.dim == 3 ? g.n[2] + 2 : 1);
+}
 
 struct TileShape {
   int tx, ty, nt, k;  // tile columns (x, y), threads, planes per step
@@ -20,15 +25,18 @@ struct TileShape {
 
 // Launch shape of the streamed levels: a tile of ty x tx columns per block,
 // k planes per pipeline step.
-constexpr TileShape kTile3 = {32, 16, 256, 2};
+constexpr TileShape kTile3 = {32, 16, 512, 2};
 constexpr TileShape kTile2 = {128, 1, 128, 4};
 inline TileShape tile_for(int dim) { return dim == 3 ? kTile3 : kTile2; }
 
-// z, r, Adiag as float32 for a ring of k + ns + 1 planes of tile + halo ns.
-inline size_t sweep_smem(int dim, int ns, TileShape t) {
-  const int RX = t.tx + 2 * ns;
+// z, r, Adiag as float32 for a ring of k + ns + 1 planes of tile + halo ns
+// (rounded up to 4 along the fastest axis, as k_sweep lays it out).
+// A one-step launch (k = the whole chunk of 2 planes + 2 ns halo planes)
+// needs no ring: k planes.
+inline size_t sweep_smem(int dim, int ns, TileShape t, bool one_step = false) {
+  const int RX = t.tx + 2 * ((ns + 3) & ~3);
   const int RY = dim == 3 ? t.ty + 2 * ns : 1;
-  const int W = t.k + ns + 1;
+  const int W = one_step ? t.k : t.k + ns + 1;
   return (size_t)W * RX * RY * 12;
 }
 
@@ -40,6 +48,7 @@ struct FusedPlan {
   TileShape tile;
   CoarseArgs coarse;
   size_t coarse_smem = 0;
+  int coarse_threads = 512;
   float kappa = 1.0f, rho = 1.0f, pi = 1.0f;
   float s[kMaxLevels];
 };
@@ -60,7 +69,7 @@ inline bool make_fused_plan(const Level* lv, int L, int dim, int pre_post, int b
   long long tot = 0;
   int lc = L;
   for (int l = L - 1; l >= 0; --l) {
-    tot += lv[l].g.count;
+    tot += padded_cells(lv[l].g);
     if (tot > kCoarseMaxCells) break;
     lc = l;
   }
@@ -115,9 +124,8 @@ inline bool make_fused_plan(const Level* lv, int L, int dim, int pre_post, int b
     C.n[i][1] = g.n[1];
     C.n[i][2] = g.n[2];
     C.off[i] = off;
-    off += (int)g.count;
+    off += (int)padded_cells(g);
     C.s[i] = F->s[lc + i];
-    C.type[i] = lv[lc + i].type;
     C.Ad[i] = lv[lc + i].Adiag_s;
   }
   C.total = off;
@@ -126,7 +134,10 @@ inline bool make_fused_plan(const Level* lv, int L, int dim, int pre_post, int b
   C.r_f32 = lc == 0;
   C.rho = F->rho;
   C.pi = F->pi;
-  F->coarse_smem = (size_t)off * 13;
+  F->coarse_smem = (size_t)off * 12;
+  // 1024 threads: the upper coarse levels' phases take 1-2 cells per thread;
+  // the bottom level's cells sit in the first threads' registers
+  F->coarse_threads = 1024;
   F->valid = true;
   return true;
 }
@@ -161,6 +172,16 @@ inline SweepArgs<ST> sweep_args(const FusedPlan& F, const Level* lv, int l, cons
 template <int DIM, typename ST, int NS, bool PRE>
 inline cudaError_t launch_sweep_t(const FusedPlan& F, const Level* lv, int l, const Control* ctl, cudaStream_t s) {
   constexpr TileShape T = DIM == 3 ? kTile3 : kTile2;
+  if (DIM == 3 && F.chunk[l] == 2) {
+    // small level: each block's 2 planes + halo planes in ONE pipeline step
+    constexpr TileShape T1 = {T.tx, T.ty, T.nt, 2 + 2 * NS};
+    auto kern = k_sweep<DIM, ST, NS, T1.tx, T1.ty, PRE, T1.nt, T1.k>;
+    const size_t smem = sweep_smem(DIM, NS, T1, true);
+    cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return e;
+    kern<<<F.blocks[l], T1.nt, smem, s>>>(sweep_args<ST, PRE>(F, lv, l, ctl));
+    return cudaGetLastError();
+  }
   auto kern = k_sweep<DIM, ST, NS, T.tx, T.ty, PRE, T.nt, T.k>;
   constexpr int NT = T.nt;
   const size_t smem = sweep_smem(DIM, NS, T);
@@ -205,7 +226,7 @@ inline cudaError_t launch_coarse_st(const FusedPlan& F, const Control* ctl, cuda
   cudaError_t e = cudaFuncSetAttribute(k_coarse<ST>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                        (int)F.coarse_smem);
   if (e != cudaSuccess) return e;
-  k_coarse<ST><<<1, kCoarseThreads, F.coarse_smem, s>>>(a);
+  k_coarse<ST><<<1, F.coarse_threads, F.coarse_smem, s>>>(a);
   return cudaGetLastError();
 }
 

@@ -295,10 +295,11 @@ int launch_pcg_part(mg_plan* P, bool prologue, cudaStream_t s) {
 
 // Kernels one launch_pcg_part enqueues (the graph's node count per part).
 int count_pcg_part(const mg_plan* P, bool prologue) {
-  int v = P->fp.valid ? 2 * P->fp.lc + 1
-                      : (P->L - 1) * (4 * P->d.pre_post + 2) +
-                            (P->geom[P->L - 1].count <= kBottomBlockCells ? (P->d.bottom / 2 > 0) : 2 * P->d.bottom);
-  return (prologue ? 1 : 0) + v + 2 + 2 + (P->d.refresh_every > 0 ? 1 : 0);
+  const int refresh = P->d.refresh_every > 0 ? 1 : 0;
+  if (P->fp.valid) return (prologue ? 1 : 0) + 2 * P->fp.lc + 1 + 4 + refresh;
+  int v = (P->L - 1) * (4 * P->d.pre_post + 2) +
+          (P->geom[P->L - 1].count <= kBottomBlockCells ? (P->d.bottom / 2 > 0) : 2 * P->d.bottom);
+  return (prologue ? 1 : 0) + v + 2 + 2 + refresh;
 }
 
 void destroy_graph(mg_plan* P) {

@@ -63,7 +63,7 @@ __device__ __forceinline__ void ld4_r(const void* r, long long i, int r_f32, flo
 //
 // A block owns a (TY x TX) tile of columns and a chunk [z0, z1) of planes
 // along axis 0.  Shared memory holds a ring of W planes of the tile plus a
-// halo of H = NS cells; per cell z, r and Adiag as float32.  Each step loads K
+// halo of NS cells (rounded up to 4 along x); per cell z, r and Adiag as float32.  Each step loads K
 // planes (4-wide vector loads from registers prefetched during the previous
 // step) and applies half sweep m to the planes m behind the newest ones, so
 // every half sweep sees its neighbours after the previous half sweep.
@@ -83,17 +83,25 @@ __device__ __forceinline__ void ld4_r(const void* r, long long i, int r_f32, flo
 // plane, which saves one ring of halo.
 template <int DIM, typename ST, int NS, int TX, int TY, bool PRE, int NT, int K>
 __global__ void __launch_bounds__(NT) k_sweep(SweepArgs<ST> A) {
-  constexpr int H = NS;                           // in-plane halo
-  constexpr int RX = TX + 2 * H;
-  constexpr int RY = DIM == 3 ? TY + 2 * H : 1;
+  // halos: NS cells are needed on each side; along the fastest axis the halo
+  // is rounded up to 4 so every 4-wide group starts 16-byte (float) / 8-byte
+  // (16-bit) aligned; the XS extra cells are loaded but never smoothed
+  constexpr int HY = DIM == 3 ? NS : 0;
+  constexpr int HX = (NS + 3) & ~3;
+  constexpr int XS = HX - NS;
+  constexpr int RX = TX + 2 * HX;
+  constexpr int RY = DIM == 3 ? TY + 2 * HY : 1;
   constexpr int PL = RX * RY;                     // cells per plane
-  constexpr int W = K + NS + 1;                   // ring depth
+  // ring depth; a launch whose single step holds the whole 2-plane chunk and
+  // its 2 NS halo planes (K = 2 + 2 NS, chunk 2) needs no ring
+  constexpr bool ONE = K == 2 + 2 * NS;
+  constexpr int W = ONE ? K : K + NS + 1;
   constexpr int Q = RX / 4;                       // 4-cell groups per row
   constexpr int PL4 = Q * RY;                     // groups per plane
-  constexpr int PF = (K * PL4 + NT - 1) / NT;     // groups per thread per step
+  constexpr int PF = ONE ? 1 : (K * PL4 + NT - 1) / NT;  // prefetched groups per thread
   constexpr int CX = TX / 2, CY = DIM == 3 ? TY / 2 : 1;
   constexpr int D = PRE ? NS - 1 : NS;            // delay of the last half sweep
-  static_assert(RX % 4 == 0 && TX % 4 == 0, "4-wide groups");
+  static_assert(RX % 4 == 0 && TX % 4 == 0 && HX % 4 == 0, "aligned 4-wide groups");
   static_assert(CX * CY <= NT, "coarse cells of a tile must not exceed the threads");
 
   extern __shared__ __align__(16) unsigned char smem[];
@@ -122,75 +130,88 @@ __global__ void __launch_bounds__(NT) k_sweep(SweepArgs<ST> A) {
 
   auto slot = [](int p) { return (p + W * 64) % W; };
 
-  // ---- register prefetch of K planes -------------------------------------------
+  // ---- loading planes ---------------------------------------------------------------
+  // group q of the K planes from P: global loads into r[4], a[4], z[4]
+  auto load_group = [&](int P, int q, float* r, float* a, float* z) {
+#pragma unroll
+    for (int e = 0; e < 4; ++e) {
+      r[e] = 0.0f;
+      a[e] = 0.0f;
+      z[e] = 0.0f;
+    }
+    const int kp = q / PL4, rem = q - kp * PL4;
+    const int ry = rem / Q, rx = (rem - ry * Q) * 4;
+    const int p = P + kp;
+    const int gx = tx0 - HX + rx, gy = ty0 - HY + ry;
+    if (p >= 0 && p < n0 && gx >= 0 && gx < nx && gy >= 0 && gy < ny) {
+      const long long gi = (long long)p * plane_stride + (long long)gy * nx + gx;
+      ld4_r<ST>(F.r, gi, A.r_f32, sigma, r);
+      ld4<ST>(F.Ad + gi, a);
+      if (!PRE) {
+        float zi[4];
+        ld4<ST>(F.zin + gi, zi);
+        const long long gc = DIM == 3
+            ? ((long long)(p >> 1) * A.nc[1] + (gy >> 1)) * A.nc[2] + (gx >> 1)
+            : (long long)(p >> 1) * A.nc[1] + (gx >> 1);
+        const float c0 = to_f<ST>(A.zc[gc]), c1 = to_f<ST>(A.zc[gc + 1]);
+        z[0] = __fadd_rn(zi[0], __fmul_rn(A.pi, c0));
+        z[1] = __fadd_rn(zi[1], __fmul_rn(A.pi, c0));
+        z[2] = __fadd_rn(zi[2], __fmul_rn(A.pi, c1));
+        z[3] = __fadd_rn(zi[3], __fmul_rn(A.pi, c1));
+      }
+    }
+  };
+  // store group q into shared memory; PRE applies its pointwise first half
+  // sweep, POST writes the final value of non-FLUID interior cells it owns
+  auto put_group = [&](int P, int q, const float* r, const float* a, const float* z) {
+    const int kp = q / PL4, rem = q - kp * PL4;
+    const int ry = rem / Q, rx = (rem - ry * Q) * 4;
+    const int p = P + kp;
+    const int gx = tx0 - HX + rx, gy = ty0 - HY + ry;
+    float zv[4];
+#pragma unroll
+    for (int e = 0; e < 4; ++e) {
+      if (PRE) {
+        const bool c0 = ((p + gy + gx + e) & 1) == 0;
+        zv[e] = (c0 && a[e] != 0.0f) ? __fdiv_rn(r[e], a[e]) : 0.0f;
+      } else {
+        zv[e] = a[e] != 0.0f ? z[e] : 0.0f;
+      }
+    }
+    const int o = slot(p) * PL + ry * RX + rx;
+    *reinterpret_cast<float4*>(sz + o) = make_float4(zv[0], zv[1], zv[2], zv[3]);
+    *reinterpret_cast<float4*>(sr + o) = make_float4(r[0], r[1], r[2], r[3]);
+    *reinterpret_cast<float4*>(sa + o) = make_float4(a[0], a[1], a[2], a[3]);
+    if (!PRE && p >= z0 && p < z1 && gx >= tx0 && gx < tx0 + TX && gx < nx &&
+        gy >= ty0 && gy < ty0 + (DIM == 3 ? TY : 1) && gy < ny) {
+      const long long gi = (long long)p * plane_stride + (long long)gy * nx + gx;
+#pragma unroll
+      for (int e = 0; e < 4; ++e)
+        if (a[e] == 0.0f) F.z[gi + e] = from_f<ST>(z[e]);
+    }
+  };
+  // streaming: the next K planes are prefetched into registers during the
+  // current step; one step (ONE): loaded straight into shared memory
   float fr[PF][4], fa[PF][4], fz[PF][4];
   auto fetch = [&](int P) {
 #pragma unroll
     for (int g = 0; g < PF; ++g) {
       const int q = threadIdx.x + g * NT;
-#pragma unroll
-      for (int e = 0; e < 4; ++e) {
-        fr[g][e] = 0.0f;
-        fa[g][e] = 0.0f;
-        fz[g][e] = 0.0f;
-      }
-      if (q < K * PL4) {
-        const int kp = q / PL4, rem = q - kp * PL4;
-        const int ry = rem / Q, rx = (rem - ry * Q) * 4;
-        const int p = P + kp;
-        const int gx = tx0 - H + rx, gy = ty0 - (DIM == 3 ? H : 0) + ry;
-        if (p >= 0 && p < n0 && gx >= 0 && gx < nx && gy >= 0 && gy < ny) {
-          const long long gi = (long long)p * plane_stride + (long long)gy * nx + gx;
-          ld4_r<ST>(F.r, gi, A.r_f32, sigma, fr[g]);
-          ld4<ST>(F.Ad + gi, fa[g]);
-          if (!PRE) {
-            float zi[4];
-            ld4<ST>(F.zin + gi, zi);
-            const long long gc = DIM == 3
-                ? ((long long)(p >> 1) * A.nc[1] + (gy >> 1)) * A.nc[2] + (gx >> 1)
-                : (long long)(p >> 1) * A.nc[1] + (gx >> 1);
-            const float c0 = to_f<ST>(A.zc[gc]), c1 = to_f<ST>(A.zc[gc + 1]);
-            fz[g][0] = __fadd_rn(zi[0], __fmul_rn(A.pi, c0));
-            fz[g][1] = __fadd_rn(zi[1], __fmul_rn(A.pi, c0));
-            fz[g][2] = __fadd_rn(zi[2], __fmul_rn(A.pi, c1));
-            fz[g][3] = __fadd_rn(zi[3], __fmul_rn(A.pi, c1));
-          }
-        }
-      }
+      if (q < K * PL4) load_group(P, q, fr[g], fa[g], fz[g]);
     }
   };
-  // store K prefetched planes; PRE applies its pointwise first half sweep,
-  // POST writes the final value of non-FLUID interior cells of owned planes
   auto store = [&](int P) {
+    if constexpr (ONE) {
+      for (int q = threadIdx.x; q < K * PL4; q += NT) {
+        float r[4], a[4], z[4];
+        load_group(P, q, r, a, z);
+        put_group(P, q, r, a, z);
+      }
+    } else {
 #pragma unroll
-    for (int g = 0; g < PF; ++g) {
-      const int q = threadIdx.x + g * NT;
-      if (q < K * PL4) {
-        const int kp = q / PL4, rem = q - kp * PL4;
-        const int ry = rem / Q, rx = (rem - ry * Q) * 4;
-        const int p = P + kp;
-        const int gx = tx0 - H + rx, gy = ty0 - (DIM == 3 ? H : 0) + ry;
-        float zv[4];
-#pragma unroll
-        for (int e = 0; e < 4; ++e) {
-          if (PRE) {
-            const bool c0 = ((p + gy + gx + e) & 1) == 0;
-            zv[e] = (c0 && fa[g][e] != 0.0f) ? __fdiv_rn(fr[g][e], fa[g][e]) : 0.0f;
-          } else {
-            zv[e] = fa[g][e] != 0.0f ? fz[g][e] : 0.0f;
-          }
-        }
-        const int o = slot(p) * PL + ry * RX + rx;
-        *reinterpret_cast<float4*>(sz + o) = make_float4(zv[0], zv[1], zv[2], zv[3]);
-        *reinterpret_cast<float4*>(sr + o) = make_float4(fr[g][0], fr[g][1], fr[g][2], fr[g][3]);
-        *reinterpret_cast<float4*>(sa + o) = make_float4(fa[g][0], fa[g][1], fa[g][2], fa[g][3]);
-        if (!PRE && p >= z0 && p < z1 && gx >= tx0 && gx < tx0 + TX && gx < nx &&
-            gy >= ty0 && gy < ty0 + (DIM == 3 ? TY : 1) && gy < ny) {
-          const long long gi = (long long)p * plane_stride + (long long)gy * nx + gx;
-#pragma unroll
-          for (int e = 0; e < 4; ++e)
-            if (fa[g][e] == 0.0f) F.z[gi + e] = from_f<ST>(fz[g][e]);
-        }
+      for (int g = 0; g < PF; ++g) {
+        const int q = threadIdx.x + g * NT;
+        if (q < K * PL4) put_group(P, q, fr[g], fa[g], fz[g]);
       }
     }
   };
@@ -209,11 +230,13 @@ __global__ void __launch_bounds__(NT) k_sweep(SweepArgs<ST> A) {
   const int ct = threadIdx.x;                     // coarse in-plane cell of this thread
   const int ccx = ct % CX, ccy = ct / CX;
 
-  fetch(p_first);
+  if constexpr (!ONE) fetch(p_first);
   for (int P = p_first; P <= p_last; P += K) {
     store(P);
     __syncthreads();
-    if (P + K <= p_last) fetch(P + K);  // in flight during the half sweeps
+    if constexpr (!ONE) {
+      if (P + K <= p_last) fetch(P + K);  // in flight during the half sweeps
+    }
 
     // ---- half sweeps -------------------------------------------------------
 #pragma unroll
@@ -222,22 +245,26 @@ __global__ void __launch_bounds__(NT) k_sweep(SweepArgs<ST> A) {
       const int colour = PRE ? ((m - 1) & 1) : (m & 1);
       const int lo = DIM == 3 ? shift : 0;         // region rows [lo, RY-lo)
       const int rows = RY - 2 * lo;
-      const int cols = RX - 2 * shift;             // region cols [shift, RX-shift)
+      const int x0 = XS + shift;                   // region cols [x0, RX-x0)
+      const int cols = RX - 2 * x0;
       const int hc = (cols + 1) >> 1;
-      for (int j = threadIdx.x; j < K * rows * hc; j += NT) {
-        const int kp = j / (rows * hc), rem = j - kp * (rows * hc);
-        const int row = rem / hc, k = rem - row * hc;
+#pragma unroll
+      for (int kp = 0; kp < K; ++kp) {
+        // per-plane values hoisted out of the cell loop (uniform per block)
         const int pm = P + kp - shift;
         if (pm - 1 < p_first || pm < 0 || pm >= n0) continue;
-        // parity of the region origin: global (pm, ty0-H+lo, tx0-H+shift)
-        const int org = pm + (DIM == 3 ? ty0 - H + lo : 0) + (tx0 - H + shift);
-        const int cx = 2 * k + ((colour - org - row) & 1);
-        if (cx >= cols) continue;
-        const int sc = slot(pm) * PL;
-        const int c = (lo + row) * RX + (shift + cx);
-        const float a = sa[sc + c];
-        if (a == 0.0f) continue;                   // not FLUID
-        sz[sc + c] = __fdiv_rn(__fsub_rn(sr[sc + c], nsum(slot(pm - 1) * PL, sc, slot(pm + 1) * PL, c)), a);
+        const int sc = slot(pm) * PL, sb = slot(pm - 1) * PL, sa_ = slot(pm + 1) * PL;
+        // parity of the region origin: global (pm, ty0-HY+lo, tx0-HX+x0)
+        const int org = pm + (DIM == 3 ? ty0 - HY + lo : 0) + (tx0 - HX + x0);
+        for (int j = threadIdx.x; j < rows * hc; j += NT) {
+          const int row = j / hc, k = j - row * hc;
+          const int cx = 2 * k + ((colour - org - row) & 1);
+          if (cx >= cols) continue;
+          const int c = (lo + row) * RX + (x0 + cx);
+          const float a = sa[sc + c];
+          if (a == 0.0f) continue;                 // not FLUID
+          sz[sc + c] = __fdiv_rn(__fsub_rn(sr[sc + c], nsum(sb, sc, sa_, c)), a);
+        }
       }
       __syncthreads();
     }
@@ -252,7 +279,7 @@ __global__ void __launch_bounds__(NT) k_sweep(SweepArgs<ST> A) {
         const int ix = (j % (TX / 4)) * 4, iy = j / (TX / 4);
         const int gx = tx0 + ix, gy = ty0 + iy;
         if (gx >= nx || gy >= ny) continue;
-        const int c = (iy + (DIM == 3 ? H : 0)) * RX + (ix + H);
+        const int c = (iy + HY) * RX + (ix + HX);
         const long long gi = (long long)pw * plane_stride + (long long)gy * nx + gx;
         float v[4] = {sz[so + c], sz[so + c + 1], sz[so + c + 2], sz[so + c + 3]};
         if (PRE) {
@@ -277,7 +304,7 @@ __global__ void __launch_bounds__(NT) k_sweep(SweepArgs<ST> A) {
         for (int o1 = 0; o1 < (DIM == 3 ? 2 : 1); ++o1) {
 #pragma unroll
           for (int o2 = 0; o2 < 2; ++o2) {
-            const int c = (DIM == 3 ? H + 2 * ccy + o1 : 0) * RX + (H + 2 * ccx + o2);
+            const int c = (DIM == 3 ? HY + 2 * ccy + o1 : 0) * RX + (HX + 2 * ccx + o2);
             const float a = sa[sc + c];
             if (a != 0.0f) {
               const float Az = __fadd_rn(__fmul_rn(a, sz[sc + c]), nsum(sb, sc, sa_, c));

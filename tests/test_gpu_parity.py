@@ -100,6 +100,27 @@ def test_fused_equals_stored_kernels(name):
     assert b1 < b2
 
 
+@pytest.mark.parametrize("pre_post", [1, 3])
+@pytest.mark.parametrize("name", ["dam2d_128", "drop3d_48"])
+def test_fused_sweep_counts(pre_post, name):
+    """Other pre/post sweep counts: fused V-cycle bit-exact with the oracle and
+    fused solve bit-exact with the stored-coefficient solve."""
+    import torch
+    sc = SCENES[name]()
+    g, _ = gpu_for(sc, pre_post=pre_post)
+    o = oracle_for(sc, pre_post=pre_post)
+    o.set("r", o.get("b"), 0)
+    g.r[0].copy_(g.b)
+    g.v_cycle()
+    o.v_cycle()
+    torch.cuda.synchronize()
+    np.testing.assert_array_equal(_np(g.z[0]), o.get("z", 0))
+    g1, _ = gpu_for(sc, pre_post=pre_post)
+    g2, _ = gpu_for(sc, pre_post=pre_post, stored_kernels=True)
+    assert g1.solve(500) == g2.solve(500)
+    np.testing.assert_array_equal(_np(g1.x), _np(g2.x))
+
+
 @pytest.mark.parametrize("storage", ["f16", "bf16"])
 @pytest.mark.parametrize("name", ["dam2d_128", "drop3d_48"])
 def test_mixed_precision_reaches_target(storage, name):
