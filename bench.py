@@ -259,6 +259,7 @@ def stage_bytes(solver, storage):
     }
     if solver.operator_form(0) == 1:  # fused V-cycle kernels of the label-uniform form
         return dict(cg, **{
+            "Ap_alpha": 4 + 4 + 4,                              # Adiag, p; Ap out (no Ax, no labels)
             "pre_l0": 4 + sv + sv + 2 * sv / coarse,           # r, Ad; z out, r_c + z_c out
             "post_l0": sv + sv / coarse + 4 + sv + sv,          # zt, z_c, r, Ad; z out
         })

@@ -18,7 +18,7 @@ namespace mg {
 //       (mgpcg.py:120-123 adds to every cell); their r is never read;
 //   sa: Adiag (nonzero exactly on FLUID cells; mg_plan_prepare checks it).
 
-constexpr int kBottomPerThread = 4;  // cached bottom cells per colour and thread
+constexpr int kBottomPerThread = 2;  // cached bottom cells per colour and thread
 
 struct CoarseArgs {
   int dim, nlev, pre_post, bottom;
@@ -171,45 +171,58 @@ __global__ void __launch_bounds__(1024) k_coarse(CoarseArgs A) {
     const PGeom g = pgeom(A, L - 1);
     const float ms = -A.s[L - 1];
     const int cntb = colour_count(g, dim);
-    if (cntb <= kBottomPerThread * (int)blockDim.x) {
-      // each owned cell's padded index, r and Adiag in registers
-      int gi[2][kBottomPerThread];
-      float rr[2][kBottomPerThread], aa[2][kBottomPerThread];
+    // participants: two cells of a colour per thread where that fits, in
+    // whole warps; they synchronise among themselves on barrier 1 while the
+    // other warps wait at the block barrier below
+    int pt = ((cntb + 1) / 2 + 31) & ~31;
+    if (pt > (int)blockDim.x || (cntb + pt - 1) / pt > kBottomPerThread) pt = blockDim.x;
+    if (cntb <= kBottomPerThread * pt) {
+      if ((int)threadIdx.x < pt) {
+        // each owned cell's padded index, r and Adiag in registers
+        int gi[2][kBottomPerThread];
+        float rr[2][kBottomPerThread], aa[2][kBottomPerThread];
 #pragma unroll
-      for (int ph = 0; ph < 2; ++ph) {
-#pragma unroll
-        for (int k = 0; k < kBottomPerThread; ++k) {
-          const int j = threadIdx.x + k * blockDim.x;
-          int c0, c1, c2;
-          gi[ph][k] = -1;
-          rr[ph][k] = 0.0f;
-          aa[ph][k] = 1.0f;
-          if (j < cntb && colour_cell(g, dim, j, ph, c0, c1, c2)) {
-            const int p = g.at(c0, c1, c2);
-            if (sa[p] != 0.0f) {
-              gi[ph][k] = p;
-              rr[ph][k] = sr[p];
-              aa[ph][k] = sa[p];
-            }
-          }
-        }
-      }
-      for (int i = 0; i < 2 * nh; ++i) {
-#pragma unroll
-        for (int h = 0; h < 2; ++h) {
-          const int ph = i < nh ? h : 1 - h;
+        for (int ph = 0; ph < 2; ++ph) {
 #pragma unroll
           for (int k = 0; k < kBottomPerThread; ++k) {
-            const int p = ph ? gi[1][k] : gi[0][k];
-            if (p >= 0) {
-              const float r_ = ph ? rr[1][k] : rr[0][k];
-              const float a_ = ph ? aa[1][k] : aa[0][k];
-              zm[p] = __fdiv_rn(__fsub_rn(r_, csum(zm, p, g, dim, ms)), a_);
+            const int j = threadIdx.x + k * pt;
+            int c0, c1, c2;
+            gi[ph][k] = -1;
+            rr[ph][k] = 0.0f;
+            aa[ph][k] = 1.0f;
+            if (j < cntb && colour_cell(g, dim, j, ph, c0, c1, c2)) {
+              const int p = g.at(c0, c1, c2);
+              if (sa[p] != 0.0f) {
+                gi[ph][k] = p;
+                rr[ph][k] = sr[p];
+                aa[ph][k] = sa[p];
+              }
             }
           }
-          __syncthreads();
+        }
+        for (int i = 0; i < 2 * nh; ++i) {
+#pragma unroll
+          for (int h = 0; h < 2; ++h) {
+            const int ph = i < nh ? h : 1 - h;
+            float v[kBottomPerThread];
+#pragma unroll
+            for (int k = 0; k < kBottomPerThread; ++k) {   // all loads first
+              const int p = ph ? gi[1][k] : gi[0][k];
+              const int ps = p >= 0 ? p : g.at(0, 0, 0);     // an in-range cell for empty slots
+              const float r_ = ph ? rr[1][k] : rr[0][k];
+              const float a_ = ph ? aa[1][k] : aa[0][k];
+              v[k] = __fdiv_rn(__fsub_rn(r_, csum(zm, ps, g, dim, ms)), a_);
+            }
+#pragma unroll
+            for (int k = 0; k < kBottomPerThread; ++k) {   // then the stores
+              const int p = ph ? gi[1][k] : gi[0][k];
+              if (p >= 0) zm[p] = v[k];
+            }
+            asm volatile("bar.sync 1, %0;" ::"r"(pt) : "memory");
+          }
         }
       }
+      __syncthreads();
     } else {
       for (int i = 0; i < 2 * nh; ++i) {
         for (int h = 0; h < 2; ++h) {

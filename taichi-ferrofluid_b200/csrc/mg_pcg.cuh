@@ -181,6 +181,46 @@ __global__ void __launch_bounds__(kRedThreads) k_Ap_alpha(Level L, const float* 
   }
 }
 
+// The same for a label-uniform level 0 (every coupling -s between FLUID
+// cells): Ap = Adiag p + sum over in-range neighbours of (-s) p.  p is 0 on
+// every non-FLUID cell (update_p writes FLUID cells only), so a neighbour term
+// equals the reference's Ax * p up to the sign of a zero product; FLUID is
+// Adiag != 0 (checked by mg_plan_prepare).  No Ax arrays, no labels: 12 bytes
+// per cell instead of 25, the same values and the same summation order.
+__global__ void __launch_bounds__(kRedThreads) k_Ap_alpha_uniform(Level L, const float* __restrict__ p,
+                                                                  float* __restrict__ Ap, float s, Control* ctl,
+                                                                  double* partials, int force = 0) {
+  if (!ctl->run && !force) return;
+  __shared__ double sh[32];
+  const float ms = -s;
+  double acc = 0.0;
+  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < L.g.count;
+       i += (long long)gridDim.x * blockDim.x) {
+    const float a = L.Adiag[i];
+    if (a == 0.0f) continue;
+    int c[3];
+    L.g.coords(i, c);
+    const float pi = p[i];
+    float ret = 0.0f;
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+      if (k >= L.g.dim) break;
+      const long long st = L.g.stride(k);
+      const float lo = c[k] > 0 ? __fmul_rn(ms, p[i - st]) : 0.0f;
+      const float hi = c[k] + 1 < L.g.n[k] ? __fmul_rn(ms, p[i + st]) : 0.0f;
+      ret = __fadd_rn(ret, __fadd_rn(lo, hi));
+    }
+    const float v = __fadd_rn(__fmul_rn(a, pi), ret);
+    Ap[i] = v;
+    acc += (double)pi * (double)v;
+  }
+  double tot;
+  if (last_block_total<kRedThreads>(acc, partials, &ctl->counter[2], sh, &tot) && threadIdx.x == 0) {
+    ctl->pAp = tot;
+    ctl->alpha = (float)(ctl->old_zTr / (tot + ctl->eps));
+  }
+}
+
 // update_xr (mgpcg.py:226-232) + reduce(r, r) + the convergence test
 // (mgpcg.py:188-195).  Sets the while-node condition to ctl->run.
 __global__ void __launch_bounds__(kRedThreads) k_xr(Level L, float* __restrict__ x,

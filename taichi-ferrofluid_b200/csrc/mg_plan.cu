@@ -264,7 +264,10 @@ int launch_cg_tail(mg_plan* P, cudaStream_t s, int which) {
   const int RB = P->red_blocks;
   const bool refresh = P->d.refresh_every > 0;
   if (which & 1) {
-    k_Ap_alpha<<<RB, kRedThreads, 0, s>>>(L0, p, Ap, P->ctl, P->partials);
+    if (P->fp.valid)  // label-uniform level 0
+      k_Ap_alpha_uniform<<<RB, kRedThreads, 0, s>>>(L0, p, Ap, P->offdiag[0], P->ctl, P->partials);
+    else
+      k_Ap_alpha<<<RB, kRedThreads, 0, s>>>(L0, p, Ap, P->ctl, P->partials);
     CKL("k_Ap_alpha");
   }
   if (which & 2) {
@@ -766,8 +769,12 @@ int mg_launch_stage(mg_plan_t* P, int32_t stage, int32_t level, void* stream) {
       return e == cudaSuccess ? MG_OK : set_err("launch_coarse", e);
     }
     case 3:
-      k_Ap_alpha<<<P->red_blocks, kRedThreads, 0, s>>>(L0, fptr(P, MG_FIELD_P), fptr(P, MG_FIELD_AP), P->ctl,
-                                                       P->partials, 1);
+      if (P->fp.valid)
+        k_Ap_alpha_uniform<<<P->red_blocks, kRedThreads, 0, s>>>(L0, fptr(P, MG_FIELD_P), fptr(P, MG_FIELD_AP),
+                                                                 P->offdiag[0], P->ctl, P->partials, 1);
+      else
+        k_Ap_alpha<<<P->red_blocks, kRedThreads, 0, s>>>(L0, fptr(P, MG_FIELD_P), fptr(P, MG_FIELD_AP), P->ctl,
+                                                         P->partials, 1);
       CKL("k_Ap_alpha");
       return MG_OK;
     case 4:

@@ -256,14 +256,28 @@ __global__ void __launch_bounds__(NT) k_sweep(SweepArgs<ST> A) {
         const int sc = slot(pm) * PL, sb = slot(pm - 1) * PL, sa_ = slot(pm + 1) * PL;
         // parity of the region origin: global (pm, ty0-HY+lo, tx0-HX+x0)
         const int org = pm + (DIM == 3 ? ty0 - HY + lo : 0) + (tx0 - HX + x0);
-        for (int j = threadIdx.x; j < rows * hc; j += NT) {
-          const int row = j / hc, k = j - row * hc;
-          const int cx = 2 * k + ((colour - org - row) & 1);
-          if (cx >= cols) continue;
-          const int c = (lo + row) * RX + (x0 + cx);
-          const float a = sa[sc + c];
-          if (a == 0.0f) continue;                 // not FLUID
-          sz[sc + c] = __fdiv_rn(__fsub_rn(sr[sc + c], nsum(sb, sc, sa_, c)), a);
+        // two cells per thread and iteration, both computed before either is
+        // stored: cells of one colour never read each other, and the two
+        // dependent add / divide chains overlap
+        for (int j0 = threadIdx.x; j0 < rows * hc; j0 += 2 * NT) {
+          int cc[2];
+          float val[2];
+          bool ok[2];
+#pragma unroll
+          for (int u = 0; u < 2; ++u) {
+            // past the end: clamp to the last item (in the region) and skip it
+            const int j = min(j0 + u * NT, rows * hc - 1);
+            const int row = j / hc, k = j - row * hc;
+            const int cx = min(2 * k + ((colour - org - row) & 1), cols - 1);
+            cc[u] = (lo + row) * RX + (x0 + cx);
+            ok[u] = j0 + u * NT < rows * hc && 2 * k + ((colour - org - row) & 1) < cols;
+            const float a = ok[u] ? sa[sc + cc[u]] : 0.0f;
+            ok[u] = ok[u] && a != 0.0f;              // FLUID
+            val[u] = ok[u] ? __fdiv_rn(__fsub_rn(sr[sc + cc[u]], nsum(sb, sc, sa_, cc[u])), a) : 0.0f;
+          }
+#pragma unroll
+          for (int u = 0; u < 2; ++u)
+            if (ok[u]) sz[sc + cc[u]] = val[u];
         }
       }
       __syncthreads();
