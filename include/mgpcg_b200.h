@@ -165,9 +165,96 @@ MG_API int mg_build_psi_A(mg_plan_t* plan, const float* chi, float dx, int32_t p
 /* Galerkin coarse operator of `level` from level-1: A_c = P^T A P for the
  * reference's piecewise-constant prolongation and child-sum restriction
  * (mgpcg.py:111-123).  The reference's whole-domain Strategies rebuild each
- * level from the fine fields instead (potential_function.py:130-145); this is
- * the coarse-level rule of the magnetic potential Strategy above. */
+ * level from the fine fields instead (mgpcg.py:89-94, potential_function.py:
+ * 41-55); this is the coarse-level rule of the magnetic potential Strategy
+ * above. */
 MG_API int mg_galerkin_coarsen(mg_plan_t* plan, int32_t level, void* stream);
+
+/* ---- the reference's other Strategies (all f32, all on `stream`) ----------
+ * Fields are dense row-major device arrays, last axis fastest: cell fields
+ * have the plan's level-0 shape res, MAC face fields of axis k have shape
+ * res + e_k.  Python-side constants the reference folds in double (1/dt,
+ * sigma dt / dx^2, 1/dx) are taken as double and folded here the same way. */
+
+/* MagneticForceStrategy.build_b_kernel (magnetic_force.py:17-38): the
+ * pressure right-hand side with the magnetic pressure on AIR faces,
+ * scale_A (p0 + coef |H|^2) with H interpolated from the MAC field H at the
+ * AIR cell centre (FerrofluidSimulator.H_interp, ferrofluid_simulator.py:
+ * 64-69) and coef = k mu0 / 2.  Use with mg_build_pressure_A (the Strategy
+ * inherits build_A from PressureProjectStrategy). */
+MG_API int mg_build_magnetic_b(mg_plan_t* plan, const float* vel0, const float* vel1, const float* vel2,
+                               const float* H0, const float* H1, const float* H2, float p0, float scale_A,
+                               float scale_b, float coef, void* stream);
+
+/* PotentialFunctionStrategy (potential_function.py:19-55), the reference's
+ * own form of the magnetic potential solve: whole domain, negative-definite A
+ * with face coefficients (1 + chi)/dx from chi sampled at the faces, the
+ * origin cell pinned (Adiag = 1/dx, b = 0), faces tested against the fine
+ * resolution on every level.  H_ext is the MAC external field.  Use with
+ * full_reinitialize; mg_build_potential_A builds one level. */
+MG_API int mg_build_potential_b(mg_plan_t* plan, const float* chi, const float* Hext0, const float* Hext1,
+                                const float* Hext2, void* stream);
+MG_API int mg_build_potential_A(mg_plan_t* plan, int32_t level, const float* chi, double dx, void* stream);
+
+/* The field updates around the potential solve of the ferrofluid substep:
+ * mg_update_susceptibility: update_magnetic_susceptibility
+ * (ferrofluid_simulator.py:71-75), chi = k (1 - theta(phi)), eps the level
+ * set's half width; mg_update_magnetic_field: update_magnetic_field
+ * (ferrofluid_simulator.py:89-97), H = H_ext - grad psi on the MAC faces
+ * (H = H_ext on the domain faces); psi NULL reads the plan's x. */
+MG_API int mg_update_susceptibility(mg_plan_t* plan, const float* phi, double k, float eps, float* chi,
+                                    void* stream);
+MG_API int mg_update_magnetic_field(mg_plan_t* plan, const float* psi, const float* Hext0, const float* Hext1,
+                                    const float* Hext2, float dx, float* H0, float* H1, float* H2, void* stream);
+
+/* PressureProjectWithVolumeControlStrategy (volume_control.py:7-51).
+ * mg_level_set_volume: calc_volume (volume_control.py:22-31), the smoothed
+ * fluid volume sum over cells of the mean of theta(-phi) over the 2^d cell
+ * corners, summed in FP64 into the device double *out.  eps is the level
+ * set's interface half width (level_set.py:22, 5 dx).
+ * mg_volume_control: one build_b step after mg_build_pressure_b: the volume,
+ * the PI controller on the device and b += c on FLUID cells, with no host
+ * synchronisation.  state is 8 device doubles: [0] step, [1] vol_0, [2] y,
+ * [3] last volume, [4] last c, [5] k_p, [6] k_i, [7] dt; the caller sets
+ * [0..4] = 0 and [5..7] (k_p = 2.3 / (25 dt), k_i = (k_p / 4)^2 in the
+ * reference). */
+MG_API int mg_level_set_volume(mg_plan_t* plan, const float* phi, float eps, double* out, void* stream);
+MG_API int mg_volume_control(mg_plan_t* plan, const float* phi, float eps, double* state, void* stream);
+
+/* SurfaceTension (surface_tension.py:98-153) and SurfaceTensionStrategy
+ * (surface_tension.py:10-95) for velocity axis d: mg_calc_surface_normal
+ * writes n (dim planes of the cell grid, n[k * cells + i]) = normalised
+ * gradient of phi at the cell shifted half a cell off axis d; mg_calc_curvature
+ * writes kappa = div n; the builders write b and one level of A of the
+ * implicit surface tension solve for u_d (whole domain, use with
+ * full_reinitialize).  eps is the level set's half width (5 dx). */
+MG_API int mg_calc_surface_normal(mg_plan_t* plan, int32_t d, const float* phi, float dx, float* n,
+                                  void* stream);
+MG_API int mg_calc_curvature(mg_plan_t* plan, const float* n, float dx, float* kappa, void* stream);
+MG_API int mg_build_surface_tension_b(mg_plan_t* plan, int32_t d, const float* u_d, const float* phi,
+                                      const float* n, const float* kappa, double sigma, double dt, double dx,
+                                      double eps, void* stream);
+MG_API int mg_build_surface_tension_A(mg_plan_t* plan, int32_t level, int32_t d, const float* phi,
+                                      double sigma, double dt, double dx, double eps, void* stream);
+
+/* ---- the step after the solve ---------------------------------------------
+ * FluidSimulator.apply_pressure (fluid_simulator.py:193-214): the ghost-fluid
+ * pressure-gradient update of the MAC velocity, u_k[I] -= scale (p[I] -
+ * p[I - e_k]) with p0 (times the clamped ghost-fluid factor) on AIR sides
+ * and u = 0 on faces touching SOLID or the domain edge.  pressure NULL reads
+ * the plan's x (the solution stays on the device); cell_type (int32, the
+ * simulator's labels) NULL reads the plan's level-0 labels.
+ * scale = dt / (rho dx).
+ * mg_apply_magnetic_force: FerrofluidSimulator.apply_magnetic_force
+ * (ferrofluid_simulator.py:115-137), the same update with the AIR-side
+ * pressure p0 + coef |H|^2 and no ghost-fluid factor. */
+MG_API int mg_apply_pressure(mg_plan_t* plan, float* vel0, float* vel1, float* vel2, const float* pressure,
+                             const int32_t* cell_type, const float* phi, float scale, float p0, int32_t ghost,
+                             float gfm_clamp, void* stream);
+MG_API int mg_apply_magnetic_force(mg_plan_t* plan, float* vel0, float* vel1, float* vel2,
+                                   const float* pressure, const int32_t* cell_type, const float* H0,
+                                   const float* H1, const float* H2, float scale, float p0, float coef,
+                                   void* stream);
 
 /* Prepares the V-cycle operator after the Strategy has written A:
  * detects whether every level's off-diagonals are the uniform label-derived

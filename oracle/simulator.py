@@ -1,0 +1,174 @@
+"""ctypes wrapper over ``simulator_oracle.cpp`` (test infrastructure only).
+
+The oracle of the reference's other Strategies and of the pressure update:
+``apply_pressure`` (fluid_simulator.py:193-214), ``apply_magnetic_force``
+(ferrofluid_simulator.py:115-137), ``MagneticForceStrategy`` (magnetic_force.py),
+``PotentialFunctionStrategy`` (potential_function.py),
+``PressureProjectWithVolumeControlStrategy`` (volume_control.py) and
+``SurfaceTension`` / ``SurfaceTensionStrategy`` (surface_tension.py).  Every
+function takes and returns numpy arrays; the f32 inputs are copied, never
+modified in place.  Parity against the reference itself is unpinned.
+"""
+import ctypes
+
+import numpy as np
+
+from .oracle import _load
+
+_c = None
+
+
+def _lib():
+    global _c
+    if _c is None:
+        lib = _load()
+        vp, dd, ff, ii = ctypes.c_void_p, ctypes.c_double, ctypes.c_float, ctypes.c_int
+        lib.ors_apply_pressure.argtypes = [ii, vp, vp, vp, vp, vp, ff, ff, ii, ff, vp, ff]
+        lib.ors_volume.restype = dd
+        lib.ors_volume.argtypes = [ii, vp, vp, dd]
+        lib.ors_volume_control.argtypes = [ii, vp, vp, dd, vp, vp, vp]
+        lib.ors_build_magnetic_b.argtypes = [ii, vp, vp, vp, vp, ff, ff, ff, ff, vp]
+        lib.ors_build_potential_b.argtypes = [ii, vp, vp, vp, vp]
+        lib.ors_build_potential_A.argtypes = [ii, vp, ii, vp, dd, vp, vp]
+        lib.ors_calc_n.argtypes = [ii, vp, ii, vp, ff, vp]
+        lib.ors_calc_kappa.argtypes = [ii, vp, vp, ff, vp]
+        lib.ors_build_st_b.argtypes = [ii, vp, ii, vp, vp, vp, vp, dd, dd, dd, dd, vp]
+        lib.ors_build_st_A.argtypes = [ii, vp, ii, ii, vp, dd, dd, dd, dd, vp, vp]
+        lib.ors_update_chi.argtypes = [ii, vp, vp, dd, dd, vp]
+        lib.ors_update_H.argtypes = [ii, vp, ii, vp, vp, ff, vp]
+        _c = lib
+    return _c
+
+
+def _f32(a):
+    return np.ascontiguousarray(a, dtype=np.float32).copy()
+
+
+def _res(shape):
+    r = list(shape) + [1] * (3 - len(shape))
+    return (ctypes.c_int * 3)(*r)
+
+
+def _ptrs(arrs):
+    return (ctypes.c_void_p * 3)(*([a.ctypes.data for a in arrs] + [None] * (3 - len(arrs))))
+
+
+def apply_pressure(velocity, pressure, cell_type, phi, scale, p0, ghost_fluid_method=True, gfm_clamp=1e3):
+    """FluidSimulator.apply_pressure; returns the updated face velocities."""
+    ct = np.ascontiguousarray(cell_type, dtype=np.int32)
+    u = [_f32(v) for v in velocity]
+    p, ph = _f32(pressure), _f32(phi if phi is not None else np.zeros(ct.shape))
+    _lib().ors_apply_pressure(ct.ndim, _res(ct.shape), _ptrs(u), p.ctypes.data, ct.ctypes.data, ph.ctypes.data,
+                              float(scale), float(p0), int(bool(ghost_fluid_method)), float(gfm_clamp), None,
+                              0.0)
+    return u
+
+
+def apply_magnetic_force(velocity, pressure, cell_type, H, scale, p0, coef):
+    """FerrofluidSimulator.apply_magnetic_force; H is the MAC field (one array per axis)."""
+    ct = np.ascontiguousarray(cell_type, dtype=np.int32)
+    u = [_f32(v) for v in velocity]
+    Hs = [_f32(h) for h in H]
+    p = _f32(pressure)
+    _lib().ors_apply_pressure(ct.ndim, _res(ct.shape), _ptrs(u), p.ctypes.data, ct.ctypes.data, None,
+                              float(scale), float(p0), 0, 0.0, _ptrs(Hs), float(coef))
+    return u
+
+
+def volume(phi, eps):
+    """PressureProjectWithVolumeControlStrategy.calc_volume (FP64 sum)."""
+    ph = _f32(phi)
+    return float(_lib().ors_volume(ph.ndim, _res(ph.shape), ph.ctypes.data, float(eps)))
+
+
+def volume_control(phi, eps, grid_type, b, state):
+    """One controller step plus add_c; returns (b, state) updated copies."""
+    ph, bb = _f32(phi), _f32(b)
+    t = np.ascontiguousarray(grid_type, dtype=np.int8)
+    st = np.ascontiguousarray(state, dtype=np.float64).copy()
+    _lib().ors_volume_control(ph.ndim, _res(ph.shape), ph.ctypes.data, float(eps), t.ctypes.data,
+                              bb.ctypes.data, st.ctypes.data)
+    return bb, st
+
+
+def build_magnetic_b(grid_type, velocity, H, p0, scale_A, scale_b, coef):
+    """MagneticForceStrategy.build_b_kernel on a zeroed b."""
+    t = np.ascontiguousarray(grid_type, dtype=np.int8)
+    v = [_f32(a) for a in velocity]
+    Hs = [_f32(h) for h in H]
+    b = np.zeros(t.shape, np.float32)
+    _lib().ors_build_magnetic_b(t.ndim, _res(t.shape), t.ctypes.data, _ptrs(v), _ptrs(Hs), float(p0),
+                                float(scale_A), float(scale_b), float(coef), b.ctypes.data)
+    return b
+
+
+def build_potential_b(chi, H_ext):
+    c = _f32(chi)
+    Hs = [_f32(h) for h in H_ext]
+    b = np.zeros(c.shape, np.float32)
+    _lib().ors_build_potential_b(c.ndim, _res(c.shape), c.ctypes.data, _ptrs(Hs), b.ctypes.data)
+    return b
+
+
+def build_potential_A(chi, level, dx):
+    """One level; returns (Adiag, Ax) with Ax of shape (dim, *level_shape)."""
+    c = _f32(chi)
+    shp = tuple(v >> level for v in c.shape)
+    Ad = np.zeros(shp, np.float32)
+    Ax = np.zeros((c.ndim,) + shp, np.float32)
+    _lib().ors_build_potential_A(c.ndim, _res(c.shape), int(level), c.ctypes.data, float(dx), Ad.ctypes.data,
+                                 Ax.ctypes.data)
+    return Ad, Ax
+
+
+def calc_n(phi, d, dx):
+    ph = _f32(phi)
+    n = np.zeros((ph.ndim,) + ph.shape, np.float32)
+    _lib().ors_calc_n(ph.ndim, _res(ph.shape), int(d), ph.ctypes.data, float(dx), n.ctypes.data)
+    return n
+
+
+def calc_kappa(n, dx):
+    nn = _f32(n)
+    shp = nn.shape[1:]
+    k = np.zeros(shp, np.float32)
+    _lib().ors_calc_kappa(len(shp), _res(shp), nn.ctypes.data, float(dx), k.ctypes.data)
+    return k
+
+
+def build_st_b(d, u_d, phi, n, kappa, sigma, dt, dx, eps):
+    ph, u, nn, ka = _f32(phi), _f32(u_d), _f32(n), _f32(kappa)
+    b = np.zeros(ph.shape, np.float32)
+    _lib().ors_build_st_b(ph.ndim, _res(ph.shape), int(d), u.ctypes.data, ph.ctypes.data, nn.ctypes.data,
+                          ka.ctypes.data, float(sigma), float(dt), float(dx), float(eps), b.ctypes.data)
+    return b
+
+
+def build_st_A(phi, level, d, sigma, dt, dx, eps):
+    ph = _f32(phi)
+    shp = tuple(v >> level for v in ph.shape)
+    Ad = np.zeros(shp, np.float32)
+    Ax = np.zeros((ph.ndim,) + shp, np.float32)
+    _lib().ors_build_st_A(ph.ndim, _res(ph.shape), int(level), int(d), ph.ctypes.data, float(sigma), float(dt),
+                          float(dx), float(eps), Ad.ctypes.data, Ax.ctypes.data)
+    return Ad, Ax
+
+
+def update_chi(phi, k, eps):
+    """FerrofluidSimulator.update_magnetic_susceptibility."""
+    ph = _f32(phi)
+    chi = np.zeros(ph.shape, np.float32)
+    _lib().ors_update_chi(ph.ndim, _res(ph.shape), ph.ctypes.data, float(k), float(eps), chi.ctypes.data)
+    return chi
+
+
+def update_H(psi, H_ext, dx):
+    """FerrofluidSimulator.update_magnetic_field; returns one face array per axis."""
+    ps = _f32(psi)
+    out = []
+    for k, he in enumerate(H_ext):
+        h = _f32(he)
+        H = np.zeros(h.shape, np.float32)
+        _lib().ors_update_H(ps.ndim, _res(ps.shape), k, ps.ctypes.data, h.ctypes.data, float(dx), H.ctypes.data)
+        out.append(H)
+    return out

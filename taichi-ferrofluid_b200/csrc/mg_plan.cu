@@ -544,6 +544,176 @@ int mg_add_rhs(mg_plan_t* P, const float* src, float c, void* stream) {
   return MG_OK;
 }
 
+// ---- the other Strategies and the pressure-gradient update -----------------
+
+namespace {
+ThetaK theta_consts(float eps) {
+  ThetaK t;
+  t.eps = eps;
+  t.two_eps = (float)(2.0 * (double)eps);
+  t.pi = (float)3.14159265358979323846;
+  t.inv_2pi = (float)(1.0 / (2.0 * 3.14159265358979323846));
+  return t;
+}
+}  // namespace
+
+int mg_apply_pressure(mg_plan_t* P, float* u0, float* u1, float* u2, const float* pressure,
+                      const int32_t* cell_type, const float* phi, float scale, float p0, int32_t ghost,
+                      float clamp, void* stream) {
+  NEED_BOUND(P);
+  float* u[3] = {u0, u1, u2};
+  for (int k = 0; k < P->d.dim; ++k)
+    if (!u[k]) return bad("velocity");
+  if (ghost && !phi) return bad("phi");
+  const float* pr = pressure ? pressure : fptr(P, MG_FIELD_X);
+  for (int k = 0; k < P->d.dim; ++k) {
+    k_apply_pressure<<<P->ew_blocks[0], 256, 0, S(stream)>>>(P->lv[0], k, u[k], pr, cell_type, phi, scale, p0,
+                                                             ghost, clamp, nullptr, nullptr, nullptr, 0.0f);
+    CKL("k_apply_pressure");
+  }
+  return MG_OK;
+}
+
+int mg_apply_magnetic_force(mg_plan_t* P, float* u0, float* u1, float* u2, const float* pressure,
+                            const int32_t* cell_type, const float* H0, const float* H1, const float* H2,
+                            float scale, float p0, float coef, void* stream) {
+  NEED_BOUND(P);
+  float* u[3] = {u0, u1, u2};
+  for (int k = 0; k < P->d.dim; ++k)
+    if (!u[k]) return bad("velocity");
+  if (!H0 || !H1 || (P->d.dim == 3 && !H2)) return bad("H");
+  const float* pr = pressure ? pressure : fptr(P, MG_FIELD_X);
+  for (int k = 0; k < P->d.dim; ++k) {
+    k_apply_pressure<<<P->ew_blocks[0], 256, 0, S(stream)>>>(P->lv[0], k, u[k], pr, cell_type, nullptr, scale,
+                                                             p0, 0, 0.0f, H0, H1, H2, coef);
+    CKL("k_apply_pressure");
+  }
+  return MG_OK;
+}
+
+int mg_level_set_volume(mg_plan_t* P, const float* phi, float eps, double* out, void* stream) {
+  NEED_BOUND(P);
+  if (!phi || !out || !(eps > 0.0f)) return bad("phi / eps / out");
+  k_volume<<<P->red_blocks, kRedThreads, 0, S(stream)>>>(P->geom[0], phi, theta_consts(eps), P->partials,
+                                                         &P->ctl->counter[4], out, nullptr);
+  CKL("k_volume");
+  return MG_OK;
+}
+
+int mg_volume_control(mg_plan_t* P, const float* phi, float eps, double* state, void* stream) {
+  NEED_BOUND(P);
+  if (!phi || !state || !(eps > 0.0f)) return bad("phi / eps / state");
+  k_volume<<<P->red_blocks, kRedThreads, 0, S(stream)>>>(P->geom[0], phi, theta_consts(eps), P->partials,
+                                                         &P->ctl->counter[4], &state[3], state);
+  CKL("k_volume");
+  k_add_c<<<P->ew_blocks[0], 256, 0, S(stream)>>>(P->lv[0], fptr(P, MG_FIELD_B), state);
+  CKL("k_add_c");
+  return MG_OK;
+}
+
+int mg_build_magnetic_b(mg_plan_t* P, const float* v0, const float* v1, const float* v2, const float* H0,
+                        const float* H1, const float* H2, float p0, float sA, float sB, float coef, void* stream) {
+  NEED_BOUND(P);
+  if (!v0 || !v1 || (P->d.dim == 3 && !v2)) return bad("velocity");
+  if (!H0 || !H1 || (P->d.dim == 3 && !H2)) return bad("H");
+  k_build_magnetic_b<<<P->ew_blocks[0], 256, 0, S(stream)>>>(P->lv[0], v0, v1, v2, H0, H1, H2, p0, sA, sB, coef,
+                                                             fptr(P, MG_FIELD_B));
+  CKL("k_build_magnetic_b");
+  return MG_OK;
+}
+
+int mg_build_potential_b(mg_plan_t* P, const float* chi, const float* Hx0, const float* Hx1, const float* Hx2,
+                         void* stream) {
+  NEED_BOUND(P);
+  if (!chi || !Hx0 || !Hx1 || (P->d.dim == 3 && !Hx2)) return bad("chi / H_ext");
+  const Geom& g = P->geom[0];
+  k_build_potential_b<<<P->ew_blocks[0], 256, 0, S(stream)>>>(P->lv[0], fptr(P, MG_FIELD_B), chi, Hx0, Hx1, Hx2,
+                                                              g.n[0], g.n[1], g.n[2]);
+  CKL("k_build_potential_b");
+  return MG_OK;
+}
+
+int mg_build_potential_A(mg_plan_t* P, int32_t level, const float* chi, double dx, void* stream) {
+  NEED_BOUND(P);
+  if (level < 0 || level >= P->L) return bad("level");
+  if (!chi || !(dx > 0.0)) return bad("chi / dx");
+  const Geom& g = P->geom[0];
+  const double dxl = dx * (double)(1 << level);
+  k_build_potential_A<<<P->ew_blocks[level], 256, 0, S(stream)>>>(P->lv[level], level, chi, g, (float)dxl,
+                                                                  (float)(1.0 / dxl), g.n[0], g.n[1], g.n[2]);
+  CKL("k_build_potential_A");
+  P->prepared = false;
+  return MG_OK;
+}
+
+int mg_update_susceptibility(mg_plan_t* P, const float* phi, double k, float eps, float* chi, void* stream) {
+  NEED_BOUND(P);
+  if (!phi || !chi || !(eps > 0.0f)) return bad("phi / chi / eps");
+  k_update_chi<<<P->ew_blocks[0], 256, 0, S(stream)>>>(P->geom[0], phi, (float)k, theta_consts(eps), chi);
+  CKL("k_update_chi");
+  return MG_OK;
+}
+
+int mg_update_magnetic_field(mg_plan_t* P, const float* psi, const float* Hext0, const float* Hext1,
+                             const float* Hext2, float dx, float* H0, float* H1, float* H2, void* stream) {
+  NEED_BOUND(P);
+  const float* he[3] = {Hext0, Hext1, Hext2};
+  float* h[3] = {H0, H1, H2};
+  if (!(dx > 0.0f)) return bad("dx");
+  for (int k = 0; k < P->d.dim; ++k)
+    if (!he[k] || !h[k]) return bad("H / H_ext");
+  const float* ps = psi ? psi : fptr(P, MG_FIELD_X);
+  for (int k = 0; k < P->d.dim; ++k) {
+    k_update_H<<<P->ew_blocks[0], 256, 0, S(stream)>>>(P->geom[0], k, ps, he[k], dx, h[k]);
+    CKL("k_update_H");
+  }
+  return MG_OK;
+}
+
+int mg_calc_surface_normal(mg_plan_t* P, int32_t d, const float* phi, float dx, float* n, void* stream) {
+  NEED_BOUND(P);
+  if (d < 0 || d >= P->d.dim) return bad("axis");
+  if (!phi || !n || !(dx > 0.0f)) return bad("phi / n / dx");
+  k_calc_n<<<P->ew_blocks[0], 256, 0, S(stream)>>>(P->geom[0], d, phi, dx, n);
+  CKL("k_calc_n");
+  return MG_OK;
+}
+
+int mg_calc_curvature(mg_plan_t* P, const float* n, float dx, float* kappa, void* stream) {
+  NEED_BOUND(P);
+  if (!n || !kappa || !(dx > 0.0f)) return bad("n / kappa / dx");
+  k_calc_kappa<<<P->ew_blocks[0], 256, 0, S(stream)>>>(P->geom[0], n, dx, kappa);
+  CKL("k_calc_kappa");
+  return MG_OK;
+}
+
+int mg_build_surface_tension_b(mg_plan_t* P, int32_t d, const float* u, const float* phi, const float* n,
+                               const float* kappa, double sigma, double dt, double dx, double eps, void* stream) {
+  NEED_BOUND(P);
+  if (d < 0 || d >= P->d.dim) return bad("axis");
+  if (!u || !phi || !n || !kappa || !(dt > 0.0) || !(dx > 0.0) || !(eps > 0.0)) return bad("inputs");
+  k_build_st_b<<<P->ew_blocks[0], 256, 0, S(stream)>>>(P->geom[0], d, u, phi, n, kappa, (float)sigma, (float)dt,
+                                                       (float)dx, (float)(dx * dx), theta_consts((float)eps),
+                                                       fptr(P, MG_FIELD_B));
+  CKL("k_build_st_b");
+  return MG_OK;
+}
+
+int mg_build_surface_tension_A(mg_plan_t* P, int32_t level, int32_t d, const float* phi, double sigma, double dt,
+                               double dx, double eps, void* stream) {
+  NEED_BOUND(P);
+  if (level < 0 || level >= P->L) return bad("level");
+  if (d < 0 || d >= P->d.dim) return bad("axis");
+  if (!phi || !(dt > 0.0) || !(dx > 0.0) || !(eps > 0.0)) return bad("inputs");
+  const double dxl = dx * (double)(1 << level);
+  const float scale = (float)(sigma * dt / (dxl * dxl));
+  k_build_st_A<<<P->ew_blocks[level], 256, 0, S(stream)>>>(P->lv[level], level, P->geom[0], d, phi,
+                                                           (float)(1.0 / dt), scale, theta_consts((float)eps));
+  CKL("k_build_st_A");
+  P->prepared = false;
+  return MG_OK;
+}
+
 int mg_plan_prepare(mg_plan_t* P, void* stream) {
   NEED_BOUND(P);
   cudaStream_t s = S(stream);

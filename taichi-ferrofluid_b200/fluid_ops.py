@@ -1,0 +1,112 @@
+"""The simulator steps around the Poisson solves, on the device.
+
+Free functions with the argument meaning of the reference's simulator
+methods (the reference binds them to its ``FluidSimulator`` /
+``FerrofluidSimulator`` objects):
+
+* ``apply_pressure`` - FluidSimulator.apply_pressure (fluid_simulator.py:193-214),
+  the ghost-fluid pressure-gradient update of the MAC velocity;
+* ``apply_magnetic_force`` - FerrofluidSimulator.apply_magnetic_force
+  (ferrofluid_simulator.py:115-137), the same update with the magnetic
+  pressure on AIR faces;
+* ``update_magnetic_susceptibility`` (ferrofluid_simulator.py:71-75) and
+  ``update_magnetic_field`` (ferrofluid_simulator.py:89-97), the fields
+  before and after the potential solve.
+
+Every function takes the ``MGPCGPoissonSolver`` whose geometry (and, by
+default, whose solution ``x`` and level-0 labels) it uses, so the pressure
+goes from the solve to the velocity update without leaving the device.
+Velocity and H lists are float32 CUDA tensors with shapes res + e_k and are
+updated in place.
+"""
+import numpy as np
+import torch
+
+import mg_lib
+from mg_lib import check
+from pressure_project import _f32
+
+
+def _faces(solver, fields, what):
+    out = []
+    for k in range(solver.dim):
+        f = fields[k]
+        exp = list(solver.res)
+        exp[k] += 1
+        if tuple(f.shape) != tuple(exp) or f.dtype != torch.float32 or not f.is_contiguous() \
+                or f.device != solver.device:
+            raise ValueError(f"{what}[{k}] must be a contiguous float32 tensor of shape {tuple(exp)} "
+                             f"on {solver.device}")
+        out.append(f)
+    return out
+
+
+def _labels(solver, cell_type):
+    if cell_type is None:
+        return None
+    ct = torch.as_tensor(cell_type, device=solver.device).to(torch.int32).contiguous()
+    if tuple(ct.shape) != solver.res:
+        raise ValueError(f"cell_type shape {tuple(ct.shape)} != {solver.res}")
+    return ct
+
+
+def pressure_scale(dt, rho, dx):
+    """scale = dt / (rho dx): dt is an f32 kernel argument, rho dx folded in double."""
+    return float(np.float32(dt) / np.float32(rho * dx))
+
+
+def apply_pressure(solver, velocity, dt, rho, dx, p0, phi=None, ghost_fluid_method=True, cell_type=None,
+                   pressure=None, gfm_clamp=1e3):
+    """fluid_simulator.py:193-214.  pressure None: the solver's x; cell_type
+    None: the solver's level-0 labels (the simulator's cell_type after
+    reinitialize)."""
+    u = _faces(solver, velocity, "velocity")
+    ct = _labels(solver, cell_type)
+    pr = _f32(pressure, solver.device) if pressure is not None else None
+    ph = _f32(phi, solver.device) if ghost_fluid_method else None
+    if ghost_fluid_method and ph is None:
+        raise ValueError("the ghost fluid method needs phi")
+    u2 = u[2] if solver.dim == 3 else None
+    check(solver.lib.mg_apply_pressure(solver.plan, u[0].data_ptr(), u[1].data_ptr(), mg_lib.ptr(u2),
+                                       mg_lib.ptr(pr), mg_lib.ptr(ct), mg_lib.ptr(ph), pressure_scale(dt, rho, dx),
+                                       float(p0), int(bool(ghost_fluid_method)), float(gfm_clamp), solver._s()),
+          "mg_apply_pressure")
+    solver._keep_apply = (ct, pr, ph)
+
+
+def apply_magnetic_force(solver, velocity, H, dt, rho, dx, p0, k, mu0, cell_type=None, pressure=None):
+    """ferrofluid_simulator.py:115-137."""
+    u = _faces(solver, velocity, "velocity")
+    Hs = [_f32(h, solver.device) for h in H]
+    ct = _labels(solver, cell_type)
+    pr = _f32(pressure, solver.device) if pressure is not None else None
+    u2 = u[2] if solver.dim == 3 else None
+    H2 = Hs[2] if solver.dim == 3 else None
+    check(solver.lib.mg_apply_magnetic_force(solver.plan, u[0].data_ptr(), u[1].data_ptr(), mg_lib.ptr(u2),
+                                             mg_lib.ptr(pr), mg_lib.ptr(ct), Hs[0].data_ptr(), Hs[1].data_ptr(),
+                                             mg_lib.ptr(H2), pressure_scale(dt, rho, dx), float(p0),
+                                             float(1 / 2 * k * mu0), solver._s()), "mg_apply_magnetic_force")
+    solver._keep_apply = (ct, pr, Hs)
+
+
+def update_magnetic_susceptibility(solver, phi, k, eps, chi):
+    """ferrofluid_simulator.py:71-75: chi = k (1 - theta(phi)), in place."""
+    ph = _f32(phi, solver.device)
+    if tuple(chi.shape) != solver.res or not chi.is_contiguous():
+        raise ValueError("chi must be a contiguous float32 tensor of shape res")
+    check(solver.lib.mg_update_susceptibility(solver.plan, ph.data_ptr(), float(k), float(eps), chi.data_ptr(),
+                                              solver._s()), "mg_update_susceptibility")
+    solver._keep_chi = ph
+
+
+def update_magnetic_field(solver, H_ext, dx, H, psi=None):
+    """ferrofluid_simulator.py:89-97: H = H_ext - grad psi (psi None: the solver's x)."""
+    He = [_f32(h, solver.device) for h in H_ext]
+    Hs = _faces(solver, H, "H")
+    ps = _f32(psi, solver.device) if psi is not None else None
+    h2 = He[2] if solver.dim == 3 else None
+    o2 = Hs[2] if solver.dim == 3 else None
+    check(solver.lib.mg_update_magnetic_field(solver.plan, mg_lib.ptr(ps), He[0].data_ptr(), He[1].data_ptr(),
+                                              mg_lib.ptr(h2), float(dx), Hs[0].data_ptr(), Hs[1].data_ptr(),
+                                              mg_lib.ptr(o2), solver._s()), "mg_update_magnetic_field")
+    solver._keep_H = (He, ps)

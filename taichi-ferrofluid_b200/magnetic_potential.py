@@ -1,7 +1,7 @@
 """Magnetic potential Strategy of the 3D ferrofluid substep benchmark.
 
 The reference solves for the magnetic potential psi with
-``PotentialFunctionStrategy`` (potential_function.py:5-60) through
+``PotentialFunctionStrategy`` (potential_function.py:6-60) through
 ``full_reinitialize`` + ``solve`` (ferrofluid_simulator.py:77-87).  The
 benchmark's form of that solve, implemented here on the CUDA library:
 
@@ -12,7 +12,9 @@ benchmark's form of that solve, implemented here on the CUDA library:
 * Neumann at the domain boundary, psi pinned to 0 at cell ``pin``
   (the reference pins cell 0, potential_function.py:24, :48);
 * coarse levels: the Galerkin operator P^T A P of the reference's transfer
-  pair (the reference re-samples chi per level, potential_function.py:144).
+  pair (the reference re-samples chi per level, potential_function.py:54-55).
+
+The reference's own form is ``potential_function.PotentialFunctionStrategy``.
 
 Use it with ``solver.full_reinitialize(strategy)`` as the reference does.
 """

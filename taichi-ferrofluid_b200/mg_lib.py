@@ -56,6 +56,7 @@ class SolveStats(ctypes.Structure):
 _vp = ctypes.c_void_p
 _i32 = ctypes.c_int32
 _f32 = ctypes.c_float
+_f64 = ctypes.c_double
 PLAN_STORED = 1
 
 _SIGS = {
@@ -75,6 +76,20 @@ _SIGS = {
     "mg_build_psi_b": (ctypes.c_int, [_vp, _vp, _f32, _f32, _f32, _f32, _i32, _i32, _i32, _vp]),
     "mg_build_psi_A": (ctypes.c_int, [_vp, _vp, _f32, _i32, _i32, _i32, _vp]),
     "mg_galerkin_coarsen": (ctypes.c_int, [_vp, _i32, _vp]),
+    "mg_build_magnetic_b": (ctypes.c_int, [_vp, _vp, _vp, _vp, _vp, _vp, _vp, _f32, _f32, _f32, _f32, _vp]),
+    "mg_build_potential_b": (ctypes.c_int, [_vp, _vp, _vp, _vp, _vp, _vp]),
+    "mg_build_potential_A": (ctypes.c_int, [_vp, _i32, _vp, _f64, _vp]),
+    "mg_update_susceptibility": (ctypes.c_int, [_vp, _vp, _f64, _f32, _vp, _vp]),
+    "mg_update_magnetic_field": (ctypes.c_int, [_vp, _vp, _vp, _vp, _vp, _f32, _vp, _vp, _vp, _vp]),
+    "mg_level_set_volume": (ctypes.c_int, [_vp, _vp, _f32, _vp, _vp]),
+    "mg_volume_control": (ctypes.c_int, [_vp, _vp, _f32, _vp, _vp]),
+    "mg_calc_surface_normal": (ctypes.c_int, [_vp, _i32, _vp, _f32, _vp, _vp]),
+    "mg_calc_curvature": (ctypes.c_int, [_vp, _vp, _f32, _vp, _vp]),
+    "mg_build_surface_tension_b": (ctypes.c_int, [_vp, _i32, _vp, _vp, _vp, _vp, _f64, _f64, _f64, _f64, _vp]),
+    "mg_build_surface_tension_A": (ctypes.c_int, [_vp, _i32, _i32, _vp, _f64, _f64, _f64, _f64, _vp]),
+    "mg_apply_pressure": (ctypes.c_int, [_vp, _vp, _vp, _vp, _vp, _vp, _vp, _f32, _f32, _i32, _f32, _vp]),
+    "mg_apply_magnetic_force": (ctypes.c_int, [_vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _f32, _f32, _f32,
+                                               _vp]),
     "mg_plan_prepare": (ctypes.c_int, [_vp, _vp]),
     "mg_plan_prepare_declared": (ctypes.c_int, [_vp, ctypes.POINTER(_f32), _vp]),
     "mg_pressure_solve_async": (ctypes.c_int, [_vp, _vp, _vp, _vp, _vp, _vp, _f32, _f32, _f32, _i32, _f32,
