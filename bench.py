@@ -66,6 +66,7 @@ def psi_chi(scene):
 
 MAX_ITERS = 500
 REL_TOL = 1e-12  # squared: 1e-6 relative residual
+DIRECT_LAUNCH = False  # set by --direct
 
 
 def parse():
@@ -78,6 +79,9 @@ def parse():
     ap.add_argument("--storage", default="f32", choices=["f32", "f16", "bf16"])
     ap.add_argument("--cpu-seconds", type=float, default=12.0, help="CPU baseline sample length")
     ap.add_argument("--no-variants", action="store_true", help="skip the batched / served comparison")
+    ap.add_argument("--direct", action="store_true",
+                    help="launch the PCG iterations from a host loop instead of the CUDA graph (the same "
+                         "kernels; for profilers that do not follow conditional graph nodes; slower)")
     return ap.parse_args()
 
 
@@ -175,7 +179,8 @@ class PsiCase:
         self.scene = scene
         self.dev = dev
         # the potential operator has stored coefficients: always float32 grids
-        self.solver = MGPCGPoissonSolver(scene.dim, scene.res, scene.levels, 2, 50, device=dev)
+        self.solver = MGPCGPoissonSolver(scene.dim, scene.res, scene.levels, 2, 50, device=dev,
+                                         direct_launch=DIRECT_LAUNCH)
         self.chi = torch.from_numpy(psi_chi(scene)).to(dev)
         self.strategy = MagneticPotentialStrategy(scene.dim, self.chi, PSI_H, scene.dx, PSI_PIN)
         self.h_chi = torch.from_numpy(psi_chi(scene)).pin_memory()
@@ -208,7 +213,8 @@ class GpuCase:
         from pressure_project import PressureProjectStrategy
         self.scene = scene
         self.dev = dev
-        self.solver = MGPCGPoissonSolver(scene.dim, scene.res, scene.levels, 2, 50, storage=storage, device=dev)
+        self.solver = MGPCGPoissonSolver(scene.dim, scene.res, scene.levels, 2, 50, storage=storage, device=dev,
+                                         direct_launch=DIRECT_LAUNCH)
         self.vel = [torch.from_numpy(v).to(dev) for v in scene.velocity]
         self.phi = torch.from_numpy(scene.phi).to(dev)
         self.ct = torch.from_numpy(scene.cell_type).to(dev)
@@ -387,7 +393,8 @@ def gpu_arm(args, rank, world, local):
         "data": "synthetic (seeded mg_scenes)",
         "config": {"workload": args.workload, "desc": wl["desc"], "storage": args.storage,
                    "solves_per_step": len(cases), "max_iters": MAX_ITERS, "rel_resid": 1e-6,
-                   "l2": "flushed before every timed solve", "parallelism": f"replicas x{world}"},
+                   "l2": "flushed before every timed solve", "parallelism": f"replicas x{world}",
+                   "launch": "direct host loop (profiling)" if DIRECT_LAUNCH else "CUDA graph, device-side while"},
         "p50_ms": round(lat[len(lat) // 2], 4), "p99_ms": round(lat[min(len(lat) - 1, int(0.99 * len(lat)))], 4),
         "pcg_iters": {k: {"min": min(v), "max": max(v)} for k, v in per_case_iters.items()},
         "last_rel_resid": rel, "last_status": status,
@@ -516,7 +523,9 @@ def reference_arm(args, rank, world):
 
 
 def main():
+    global DIRECT_LAUNCH
     args = parse()
+    DIRECT_LAUNCH = args.direct
     rank, world, local = dist_init(args.gpus)
     if args.impl == "reference":
         out = reference_arm(args, rank, world)

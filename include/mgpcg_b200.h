@@ -79,6 +79,13 @@ typedef struct mg_plan_desc {
 /* plan flags */
 #define MG_PLAN_STORED 1  /* always use the stored-coefficient kernels, one launch
                              per reference kernel (no fused V-cycle) */
+#define MG_PLAN_DIRECT 2  /* launch the PCG iterations from a host loop instead
+                             of the CUDA graph: the same kernels in the same
+                             order, one 4-byte device->host read and stream
+                             synchronisation per iteration, so mg_pcg_solve_async
+                             returns only when the solve has finished.  For
+                             profilers that do not follow conditional graph
+                             nodes; slower than the default. */
 
 /* Solve parameters: MGPCGPoissonSolver.solve (mgpcg.py:150-155). */
 typedef struct mg_solve_params {
@@ -162,13 +169,15 @@ MG_API int mg_build_psi_b(mg_plan_t* plan, const float* chi, float H0, float H1,
 MG_API int mg_build_psi_A(mg_plan_t* plan, const float* chi, float dx, int32_t pin0, int32_t pin1,
                           int32_t pin2, void* stream);
 
-/* Galerkin coarse operator of `level` from level-1: A_c = P^T A P for the
- * reference's piecewise-constant prolongation and child-sum restriction
- * (mgpcg.py:111-123).  The reference's whole-domain Strategies rebuild each
+/* Galerkin coarse operator of `level` from level-1: A_c = scale * P^T A P for
+ * the reference's piecewise-constant prolongation and child-sum restriction
+ * (mgpcg.py:111-123); scale must be a power of two (exact in f32).  scale 1/2
+ * over-corrects the piecewise-constant coarse correction by 2, which the
+ * magnetic potential Strategy uses (8 PCG iterations instead of 38 at 128^3).  The reference's whole-domain Strategies rebuild each
  * level from the fine fields instead (mgpcg.py:89-94, potential_function.py:
  * 41-55); this is the coarse-level rule of the magnetic potential Strategy
  * above. */
-MG_API int mg_galerkin_coarsen(mg_plan_t* plan, int32_t level, void* stream);
+MG_API int mg_galerkin_coarsen(mg_plan_t* plan, int32_t level, float scale, void* stream);
 
 /* ---- the reference's other Strategies (all f32, all on `stream`) ----------
  * Fields are dense row-major device arrays, last axis fastest: cell fields

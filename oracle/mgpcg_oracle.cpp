@@ -544,8 +544,8 @@ struct Solver {
       ad[i] = d;
     }
   }
-  // A_c = P^T A P for piecewise-constant P and child-sum restriction
-  void galerkin(int l) {
+  // A_c = scale * P^T A P for piecewise-constant P and child-sum restriction
+  void galerkin(int l, Real scale) {
     const Grid& gf = g[l - 1];
     const Grid& gc = g[l];
     for (int64_t ic = 0; ic < gc.count; ++ic) {
@@ -565,17 +565,17 @@ struct Solver {
               else axc[k] = axc[k] + a;
             }
           }
-      Adiag[l][ic] = d;
-      for (int k = 0; k < dim; ++k) Ax[l][k * gc.count + ic] = (cc[k] + 1 < gc.n[k]) ? axc[k] : Real(0);
+      Adiag[l][ic] = scale * d;
+      for (int k = 0; k < dim; ++k) Ax[l][k * gc.count + ic] = (cc[k] + 1 < gc.n[k]) ? scale * axc[k] : Real(0);
     }
   }
   // full_reinitialize(strategy) (mgpcg.py:89-94) with the potential Strategy
-  void full_reinitialize_psi(const Real* chi, const Real H[3], Real dx, const int pin[3]) {
+  void full_reinitialize_psi(const Real* chi, const Real H[3], Real dx, const int pin[3], Real coarse_scale) {
     initialize();
     build_psi_b(chi, H, dx, pin);
     for (auto& t : type) std::fill(t.begin(), t.end(), (int8_t)FLUID);
     build_psi_A0(chi, dx, pin);
-    for (int l = 1; l < L; ++l) galerkin(l);
+    for (int l = 1; l < L; ++l) galerkin(l, coarse_scale);
   }
 
   // mgpcg.py:79-87 with the pressure Strategy
@@ -721,15 +721,15 @@ void orc_reinitialize_pressure(void* hh, const int32_t* cell_type, const void* c
 
 // full_reinitialize with the magnetic potential Strategy; chi in the solver's precision.
 void orc_full_reinitialize_psi(void* hh, const void* chi, double H0, double H1, double H2, double dx, int p0,
-                               int p1, int p2) {
+                               int p1, int p2, double coarse_scale) {
   Handle* h = (Handle*)hh;
   const int pin[3] = {p0, p1, p2};
   if (h->real_bytes == 4) {
     const float H[3] = {(float)H0, (float)H1, (float)H2};
-    S<float>(h)->full_reinitialize_psi((const float*)chi, H, (float)dx, pin);
+    S<float>(h)->full_reinitialize_psi((const float*)chi, H, (float)dx, pin, (float)coarse_scale);
   } else {
     const double H[3] = {H0, H1, H2};
-    S<double>(h)->full_reinitialize_psi((const double*)chi, H, dx, pin);
+    S<double>(h)->full_reinitialize_psi((const double*)chi, H, dx, pin, coarse_scale);
   }
 }
 

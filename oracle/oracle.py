@@ -35,7 +35,8 @@ def _load():
         lib.orc_reinitialize_pressure.argtypes = [vp, ctypes.POINTER(ctypes.c_int32), ctypes.POINTER(vp), vp,
                                                   ctypes.c_double, ctypes.c_double, ctypes.c_double,
                                                   ctypes.c_int, ctypes.c_double]
-        lib.orc_full_reinitialize_psi.argtypes = [vp, vp] + [ctypes.c_double] * 4 + [ctypes.c_int] * 3
+        lib.orc_full_reinitialize_psi.argtypes = [vp, vp] + [ctypes.c_double] * 4 + [ctypes.c_int] * 3 + \
+            [ctypes.c_double]
         lib.orc_reduce.restype = ctypes.c_double
         lib.orc_reduce.argtypes = [vp, ctypes.c_int, ctypes.c_int, ctypes.c_int]
         lib.orc_solve.restype = ctypes.c_int
@@ -155,16 +156,16 @@ class OracleSolver:
                                            ptrs, ph.ctypes.data, float(p0), float(scale_A),
                                            float(scale_b), int(bool(ghost_fluid_method)), float(gfm_clamp))
 
-    def full_reinitialize_psi(self, chi, H=(0.0, 1.0, 0.0), dx=1.0, pin=(1, 1, 1)):
+    def full_reinitialize_psi(self, chi, H=(0.0, 1.0, 0.0), dx=1.0, pin=(1, 1, 1), coarse_scale=0.5):
         """full_reinitialize (mgpcg.py:89-94) with the magnetic potential Strategy
         of the 3D substep benchmark (harmonic-mean mu faces, pinned cell,
-        Galerkin coarse levels)."""
+        coarse levels coarse_scale * P^T A P)."""
         c = np.ascontiguousarray(chi, dtype=self.real)
         assert c.shape == self.res
         H = list(H) + [0.0] * (3 - len(H))
         pin = list(pin) + [0] * (3 - len(pin))
         self.lib.orc_full_reinitialize_psi(self.h, c.ctypes.data, float(H[0]), float(H[1]), float(H[2]),
-                                           float(dx), int(pin[0]), int(pin[1]), int(pin[2]))
+                                           float(dx), int(pin[0]), int(pin[1]), int(pin[2]), float(coarse_scale))
 
     def set_system(self, grid_type, Adiag, Ax, b):
         """Writes a caller-built system (the Strategy protocol, pressure_project.py:41-70)."""

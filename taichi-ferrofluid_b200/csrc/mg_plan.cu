@@ -5,6 +5,7 @@
 // mg_plan_workspace_bytes() bytes; every solver field (mgpcg.py:21-44) lives at
 // a fixed 256-byte aligned offset in it.  This file allocates host memory only
 // (the plan, a pinned parameter block) plus the CUDA graph objects.
+#include <cmath>
 #include <cstdio>
 #include <cstring>
 #include <new>
@@ -355,6 +356,31 @@ int build_graph(mg_plan* P) {
   return MG_OK;
 }
 
+// The graph's prologue and loop body launched from the host (MG_PLAN_DIRECT):
+// after each part the host reads Control::run, which the body's last kernel
+// sets exactly where the graph's while condition is set.
+constexpr int kDirectMaxParts = 1 << 20;
+
+int solve_direct(mg_plan* P, const mg_solve_params_t* prm, cudaStream_t s) {
+  k_set_params<<<1, 1, 0, s>>>(P->ctl, *prm, P->d.refresh_every);
+  CKL("k_set_params");
+  const int saved = P->has_cond;
+  P->has_cond = 0;
+  int rc = launch_pcg_part(P, true, s);
+  for (int part = 0; rc == MG_OK && part < kDirectMaxParts; ++part) {
+    cudaError_t e = cudaMemcpyAsync(&P->host_ctl->run, &P->ctl->run, sizeof(P->ctl->run), cudaMemcpyDeviceToHost, s);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+    if (e != cudaSuccess) {
+      rc = set_err("solve_direct", e);
+      break;
+    }
+    if (!P->host_ctl->run) break;
+    rc = launch_pcg_part(P, false, s);
+  }
+  P->has_cond = saved;
+  return rc;
+}
+
 }  // namespace
 
 // Lets the library's other translation units record an error message.
@@ -528,10 +554,12 @@ int mg_build_psi_A(mg_plan_t* P, const float* chi, float dx, int32_t p0, int32_t
   return MG_OK;
 }
 
-int mg_galerkin_coarsen(mg_plan_t* P, int32_t level, void* stream) {
+int mg_galerkin_coarsen(mg_plan_t* P, int32_t level, float scale, void* stream) {
   NEED_BOUND(P);
   if (level < 1 || level >= P->L) return bad("level");
-  k_galerkin<<<P->ew_blocks[level], 256, 0, S(stream)>>>(P->lv[level - 1], P->lv[level]);
+  int e2 = 0;
+  if (!(scale > 0.0f) || std::frexp(scale, &e2) != 0.5f) return bad("scale must be a power of two");
+  k_galerkin<<<P->ew_blocks[level], 256, 0, S(stream)>>>(P->lv[level - 1], P->lv[level], scale);
   CKL("k_galerkin");
   P->prepared = false;
   return MG_OK;
@@ -870,6 +898,7 @@ int mg_pcg_solve_async(mg_plan_t* P, const mg_solve_params_t* prm, void* stream)
   if (prm->max_iters < -1) return bad("max_iters");
   if (!P->prepared)
     if (int rc = mg_plan_prepare(P, stream)) return rc;
+  if (P->d.flags & MG_PLAN_DIRECT) return solve_direct(P, prm, S(stream));
   if (!P->exec || P->base_of_graph != P->base)
     if (int rc = build_graph(P)) return rc;
   // Parameters travel as kernel arguments (copied at launch, so back-to-back

@@ -82,8 +82,10 @@ __global__ void k_build_psi_A(Level L, const float* __restrict__ chi, float dx, 
 //   Ax_c[J][k] = sum of Ax[i][k] over the children i of J on its +k face
 //   Adiag_c[J] = sum of Adiag[i] over the children + 2 * sum of the Ax of the
 //                faces between two children of J
-// Children are visited in lexicographic order.
-__global__ void k_galerkin(Level F, Level C) {
+// Children are visited in lexicographic order.  Both sums are then multiplied
+// by `scale` (a power of two, so the product is exact): 1 gives P^T A P, 1/2
+// the over-corrected coarse operator of the magnetic potential Strategy.
+__global__ void k_galerkin(Level F, Level C, float scale) {
   for (long long ic = (long long)blockIdx.x * blockDim.x + threadIdx.x; ic < C.g.count;
        ic += (long long)gridDim.x * blockDim.x) {
     int cc[3];
@@ -102,8 +104,8 @@ __global__ void k_galerkin(Level F, Level C) {
             else ax[k] = __fadd_rn(ax[k], a);                       // face to the next block
           }
         }
-    C.Adiag[ic] = d;
-    for (int k = 0; k < dim; ++k) C.Ax[k][ic] = (cc[k] + 1 < C.g.n[k]) ? ax[k] : 0.0f;
+    C.Adiag[ic] = __fmul_rn(scale, d);
+    for (int k = 0; k < dim; ++k) C.Ax[k][ic] = (cc[k] + 1 < C.g.n[k]) ? __fmul_rn(scale, ax[k]) : 0.0f;
   }
 }
 

@@ -58,6 +58,7 @@ _i32 = ctypes.c_int32
 _f32 = ctypes.c_float
 _f64 = ctypes.c_double
 PLAN_STORED = 1
+PLAN_DIRECT = 2
 
 _SIGS = {
     "mg_plan_create": (ctypes.c_int, [ctypes.POINTER(PlanDesc), ctypes.POINTER(_vp)]),
@@ -75,7 +76,7 @@ _SIGS = {
     "mg_add_rhs": (ctypes.c_int, [_vp, _vp, _f32, _vp]),
     "mg_build_psi_b": (ctypes.c_int, [_vp, _vp, _f32, _f32, _f32, _f32, _i32, _i32, _i32, _vp]),
     "mg_build_psi_A": (ctypes.c_int, [_vp, _vp, _f32, _i32, _i32, _i32, _vp]),
-    "mg_galerkin_coarsen": (ctypes.c_int, [_vp, _i32, _vp]),
+    "mg_galerkin_coarsen": (ctypes.c_int, [_vp, _i32, _f32, _vp]),
     "mg_build_magnetic_b": (ctypes.c_int, [_vp, _vp, _vp, _vp, _vp, _vp, _vp, _f32, _f32, _f32, _f32, _vp]),
     "mg_build_potential_b": (ctypes.c_int, [_vp, _vp, _vp, _vp, _vp, _vp]),
     "mg_build_potential_A": (ctypes.c_int, [_vp, _i32, _vp, _f64, _vp]),

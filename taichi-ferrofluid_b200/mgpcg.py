@@ -61,7 +61,8 @@ class MGPCGPoissonSolver:
     """
 
     def __init__(self, dim, res, n_mg_levels=4, pre_and_post_smoothing=2, bottom_smoothing=50,
-                 real=float, *, storage=None, refresh_every=None, device=None, stored_kernels=False):
+                 real=float, *, storage=None, refresh_every=None, device=None, stored_kernels=False,
+                 direct_launch=False):
         self.lib = mg_lib.load()
         self.FLUID = FLUID
         self.SOLID = SOLID
@@ -89,7 +90,7 @@ class MGPCGPoissonSolver:
         d.bottom = self.bottom_smoothing
         d.storage = self.storage
         d.refresh_every = self.refresh_every
-        d.flags = mg_lib.PLAN_STORED if stored_kernels else 0
+        d.flags = (mg_lib.PLAN_STORED if stored_kernels else 0) | (mg_lib.PLAN_DIRECT if direct_launch else 0)
         plan = mg_lib.ctypes.c_void_p()
         check(self.lib.mg_plan_create(mg_lib.ctypes.byref(d), mg_lib.ctypes.byref(plan)), "mg_plan_create")
         self.plan = plan
