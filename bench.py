@@ -397,6 +397,9 @@ def gpu_arm(args, rank, world, local):
                    "launch": "direct host loop (profiling)" if DIRECT_LAUNCH else "CUDA graph, device-side while"},
         "p50_ms": round(lat[len(lat) // 2], 4), "p99_ms": round(lat[min(len(lat) - 1, int(0.99 * len(lat)))], 4),
         "pcg_iters": {k: {"min": min(v), "max": max(v)} for k, v in per_case_iters.items()},
+        "vcycle": {c.kind: {"operator_form": c.solver.operator_form(0),
+                            "split_levels_bits": c.solver.split_levels()[0],
+                            "streamed_levels": c.solver.split_levels()[1]} for c in cases},
         "last_rel_resid": rel, "last_status": status,
         "cell_iters_per_s": round(sum(c.scene.cells * (i + 1) for c, i in iters) * world / (total_ms * 1e-3), 1),
         "e2e": {"value": round(n_solves / (total_e2e * 1e-3), 3), "unit": "solves/s",

@@ -290,8 +290,20 @@ MG_API int mg_pressure_solve_async(mg_plan_t* plan, const int32_t* cell_type, co
                                    float scale_A, float scale_b, int32_t ghost, float gfm_clamp,
                                    const mg_solve_params_t* params, void* stream);
 
-/* Reports the operator form chosen per level: 1 = label-uniform, 0 = stored. */
+/* Reports the operator form chosen per level: 1 = label-uniform (fused
+ * V-cycle), 2 = whole-domain stored coefficients (every cell FLUID with a
+ * nonzero diagonal; fused V-cycle reading the stored couplings), 0 = stored
+ * coefficients with the per-kernel V-cycle. */
 MG_API int mg_plan_operator_form(const mg_plan_t* plan, int32_t level, int32_t* form);
+
+/* The autotuner's choice per streamed level of a fused V-cycle: bit l set =
+ * level l runs the per-kernel sweeps / restriction / prolongation, clear =
+ * the streamed kernel.  The whole-domain stored form is timed both ways when
+ * a shape is first prepared (the choice is cached per shape); the
+ * label-uniform form always streams.  set != 0 forces *bits (after the plan
+ * is prepared; valid until the next prepare); *bits returns the choice and
+ * *streamed (if not NULL) the number of streamed levels. */
+MG_API int mg_plan_split(mg_plan_t* plan, int32_t set, uint32_t* bits, int32_t* streamed);
 
 /* ---- the reference's per-kernel operations (for parity tests) ------------ */
 

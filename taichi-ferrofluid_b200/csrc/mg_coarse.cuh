@@ -16,7 +16,9 @@ namespace mg {
 //   sr: r on FLUID cells; on non-FLUID cells the UNMASKED z, which the
 //       smoother never touches but prolongation carries to the finer level
 //       (mgpcg.py:120-123 adds to every cell); their r is never read;
-//   sa: Adiag (nonzero exactly on FLUID cells; mg_plan_prepare checks it).
+//   sa: Adiag (nonzero exactly on FLUID cells; mg_plan_prepare checks it);
+//   sx: (STO, the whole-domain stored form) the dim coupling arrays Ax[k],
+//       0 on the ring, so a neighbour outside a level reads as z = 0, Ax = 0.
 
 constexpr int kBottomPerThread = 2;  // cached bottom cells per colour and thread
 
@@ -26,6 +28,7 @@ struct CoarseArgs {
   int off[kMaxLevels];      // offset of each PADDED level inside the shared arrays
   float s[kMaxLevels];      // kappa * s_l
   const void* Ad[kMaxLevels];
+  const float* Ax[kMaxLevels][3];  // STO: the stored couplings of each level
   const void* r0;           // r of level lc (float if r_f32)
   void* z0;                 // z of level lc (written)
   int r_f32;
@@ -91,7 +94,30 @@ __device__ __forceinline__ float csum(const float* zm, int p, const PGeom& g, in
   return ret;
 }
 
-__device__ void coarse_smooth(const CoarseArgs& A, int l, int phase, float* zm, const float* sr, const float* sa) {
+// The neighbour sum with the stored couplings sx (dim arrays of `total`
+// cells each): sum_k Ax[p-s_k][k] z[p-s_k] + Ax[p][k] z[p+s_k].
+template <bool STO>
+__device__ __forceinline__ float csum_t(const float* zm, const float* sx, int total, int p, const PGeom& g, int dim,
+                                        float ms) {
+  if constexpr (STO) {
+    const float* x0 = sx;
+    const float* x1 = sx + total;
+    float ret = 0.0f;
+    ret = __fadd_rn(ret, __fadd_rn(__fmul_rn(x0[p - g.s0], zm[p - g.s0]), __fmul_rn(x0[p], zm[p + g.s0])));
+    ret = __fadd_rn(ret, __fadd_rn(__fmul_rn(x1[p - g.s1], zm[p - g.s1]), __fmul_rn(x1[p], zm[p + g.s1])));
+    if (dim == 3) {
+      const float* x2 = sx + 2 * total;
+      ret = __fadd_rn(ret, __fadd_rn(__fmul_rn(x2[p - 1], zm[p - 1]), __fmul_rn(x2[p], zm[p + 1])));
+    }
+    return ret;
+  } else {
+    return csum(zm, p, g, dim, ms);
+  }
+}
+
+template <bool STO>
+__device__ void coarse_smooth(const CoarseArgs& A, int l, int phase, float* zm, const float* sr, const float* sa,
+                              const float* sx) {
   const PGeom g = pgeom(A, l);
   const float ms = -A.s[l];
   const int cnt = colour_count(g, A.dim);
@@ -101,21 +127,24 @@ __device__ void coarse_smooth(const CoarseArgs& A, int l, int phase, float* zm, 
     const int p = g.at(c0, c1, c2);
     const float a = sa[p];
     if (a == 0.0f) continue;
-    zm[p] = __fdiv_rn(__fsub_rn(sr[p], csum(zm, p, g, A.dim, ms)), a);
+    zm[p] = __fdiv_rn(__fsub_rn(sr[p], csum_t<STO>(zm, sx, A.total, p, g, A.dim, ms)), a);
   }
 }
 
-template <typename ST>
+template <typename ST, bool STO = false>
 __global__ void __launch_bounds__(1024) k_coarse(CoarseArgs A) {
+  static_assert(!STO || sizeof(ST) == 4, "the stored form runs on float32 grids");
   extern __shared__ __align__(16) unsigned char smem[];
   float* zm = (float*)smem;
   float* sr = zm + A.total;
   float* sa = sr + A.total;
+  float* sx = sa + A.total;  // STO: dim arrays
   const float sigma = A.r_f32 ? (float)A.ctl->scale_r : 1.0f;
   const int dim = A.dim;
-  // zero everything (the rings stay 0), then load each level's Adiag and
-  // level lc's r (FLUID cells) - z starts at 0
-  for (int i = threadIdx.x; i < 3 * A.total; i += blockDim.x) zm[i] = 0.0f;
+  const int narr = STO ? 3 + dim : 3;
+  // zero everything (the rings stay 0), then load each level's Adiag (and
+  // couplings) and level lc's r (FLUID cells) - z starts at 0
+  for (int i = threadIdx.x; i < narr * A.total; i += blockDim.x) zm[i] = 0.0f;
   __syncthreads();
   for (int l = 0; l < A.nlev; ++l) {
     const PGeom g = pgeom(A, l);
@@ -128,15 +157,18 @@ __global__ void __launch_bounds__(1024) k_coarse(CoarseArgs A) {
       const float a = to_f<ST>(((const ST*)A.Ad[l])[i]);
       sa[p] = a;
       if (l == 0 && a != 0.0f) sr[p] = load_r<ST>(A.r0, i, A.r_f32, sigma);
+      if constexpr (STO) {
+        for (int k = 0; k < dim; ++k) sx[k * A.total + p] = A.Ax[l][k][i];
+      }
     }
   }
   __syncthreads();
   const int L = A.nlev;
   for (int l = 0; l < L - 1; ++l) {
     for (int i = 0; i < A.pre_post; ++i) {
-      coarse_smooth(A, l, 0, zm, sr, sa);
+      coarse_smooth<STO>(A, l, 0, zm, sr, sa, sx);
       __syncthreads();
-      coarse_smooth(A, l, 1, zm, sr, sa);
+      coarse_smooth<STO>(A, l, 1, zm, sr, sa, sx);
       __syncthreads();
     }
     // restrict: coarse r = rho * sum over FLUID children (lexicographic order);
@@ -157,7 +189,7 @@ __global__ void __launch_bounds__(1024) k_coarse(CoarseArgs A) {
             const int p = gf.at(2 * c0 + o0, 2 * c1 + o1, dim == 3 ? 2 * c2 + o2 : 0);
             const float a = sa[p];
             if (a != 0.0f) {
-              const float Az = __fadd_rn(__fmul_rn(a, zm[p]), csum(zm, p, gf, dim, ms));
+              const float Az = __fadd_rn(__fmul_rn(a, zm[p]), csum_t<STO>(zm, sx, A.total, p, gf, dim, ms));
               acc = __fadd_rn(acc, __fsub_rn(sr[p], Az));
             }
           }
@@ -211,7 +243,7 @@ __global__ void __launch_bounds__(1024) k_coarse(CoarseArgs A) {
               const int ps = p >= 0 ? p : g.at(0, 0, 0);     // an in-range cell for empty slots
               const float r_ = ph ? rr[1][k] : rr[0][k];
               const float a_ = ph ? aa[1][k] : aa[0][k];
-              v[k] = __fdiv_rn(__fsub_rn(r_, csum(zm, ps, g, dim, ms)), a_);
+              v[k] = __fdiv_rn(__fsub_rn(r_, csum_t<STO>(zm, sx, A.total, ps, g, dim, ms)), a_);
             }
 #pragma unroll
             for (int k = 0; k < kBottomPerThread; ++k) {   // then the stores
@@ -226,7 +258,7 @@ __global__ void __launch_bounds__(1024) k_coarse(CoarseArgs A) {
     } else {
       for (int i = 0; i < 2 * nh; ++i) {
         for (int h = 0; h < 2; ++h) {
-          coarse_smooth(A, L - 1, i < nh ? h : 1 - h, zm, sr, sa);
+          coarse_smooth<STO>(A, L - 1, i < nh ? h : 1 - h, zm, sr, sa, sx);
           __syncthreads();
         }
       }
@@ -248,9 +280,9 @@ __global__ void __launch_bounds__(1024) k_coarse(CoarseArgs A) {
     }
     __syncthreads();
     for (int i = 0; i < A.pre_post; ++i) {
-      coarse_smooth(A, l, 1, zm, sr, sa);
+      coarse_smooth<STO>(A, l, 1, zm, sr, sa, sx);
       __syncthreads();
-      coarse_smooth(A, l, 0, zm, sr, sa);
+      coarse_smooth<STO>(A, l, 0, zm, sr, sa, sx);
       __syncthreads();
     }
   }

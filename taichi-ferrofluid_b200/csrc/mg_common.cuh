@@ -67,7 +67,7 @@ struct Control {
   int pad1;
   unsigned int counter[8];    // arrival counters of the last-block reductions
   double scratch[8];          // single-value results of mg_reduce
-  double det[3 * 12];         // operator detection: min, max, mismatches per level
+  double det[4 * 12];         // operator detection per level (k_detect_uniform)
 };
 
 template <typename T> __device__ __forceinline__ float to_f(T v);

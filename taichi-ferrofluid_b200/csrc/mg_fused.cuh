@@ -40,70 +40,80 @@ namespace mg {
 // Operator detection
 // ---------------------------------------------------------------------------
 
-// partials[3*b + {0,1,2}] receive the block's min and max of the nonzero
-// off-diagonals and its count of couplings that differ from the labels.
+// Per level, into out4: the min and max of the nonzero off-diagonals, the
+// count of couplings that differ from the labels (label-uniform test), and
+// the count of cells that are not FLUID or have a zero diagonal (0 for a
+// whole-domain level: every cell FLUID with a nonzero diagonal).
+// partials[4*b + {0..3}] hold the blocks' values; the last block combines them.
 __global__ void __launch_bounds__(kRedThreads) k_detect_uniform(Level L, double* partials,
-                                                                unsigned int* counter, double* out3) {
+                                                                unsigned int* counter, double* out4) {
   __shared__ bool am_last;
-  double vmin = 1e300, vmax = -1e300, bad = 0.0;
-  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < L.g.count;
-       i += (long long)gridDim.x * blockDim.x) {
-    int c[3];
-    L.g.coords(i, c);
+  __shared__ double s4[4][32];
+  double v[4] = {1e300, -1e300, 0.0, 0.0};
+  const int n1 = L.g.n[1], n2 = L.g.n[2], dim = L.g.dim;
+  const int cells = (int)L.g.count;  // levels hold fewer than 2^31 cells
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < cells; i += gridDim.x * blockDim.x) {
+    const int c2 = i % n2, t = i / n2;
+    const int c[3] = {t / n1, t % n1, c2};
     const bool fl = L.type[i] == FLUID;
+    const float ad = L.Adiag[i];
     // the fused kernels tell FLUID cells by a nonzero diagonal
-    if (fl != (L.Adiag[i] != 0.0f)) bad += 1.0;
-    for (int k = 0; k < L.g.dim; ++k) {
-      float a = L.Ax[k][i];
-      bool coupled = fl && (c[k] + 1 < L.g.n[k]) && L.type[i + L.g.stride(k)] == FLUID;
+    if (fl != (ad != 0.0f)) v[2] += 1.0;
+    if (!fl || ad == 0.0f) v[3] += 1.0;
+    for (int k = 0; k < dim; ++k) {
+      const float a = L.Ax[k][i];
+      const int st = k == 0 ? n1 * n2 : (k == 1 ? n2 : 1);
+      const bool coupled = fl && (c[k] + 1 < L.g.n[k]) && L.type[i + st] == FLUID;
       if (a != 0.0f) {
-        vmin = fmin(vmin, (double)a);
-        vmax = fmax(vmax, (double)a);
-        if (!coupled) bad += 1.0;
+        v[0] = fmin(v[0], (double)a);
+        v[1] = fmax(v[1], (double)a);
+        if (!coupled) v[2] += 1.0;
       } else if (coupled) {
-        bad += 1.0;
+        v[2] += 1.0;
       }
     }
   }
-  for (int o = 16; o > 0; o >>= 1) {
-    vmin = fmin(vmin, __shfl_down_sync(0xffffffffu, vmin, o));
-    vmax = fmax(vmax, __shfl_down_sync(0xffffffffu, vmax, o));
-    bad += __shfl_down_sync(0xffffffffu, bad, o);
-  }
-  __shared__ double s3[3][32];
-  const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  if (lane == 0) {
-    s3[0][w] = vmin;
-    s3[1][w] = vmax;
-    s3[2][w] = bad;
-  }
-  __syncthreads();
-  if (threadIdx.x == 0) {
-    double a = 1e300, b = -1e300, c = 0.0;
-    for (int j = 0; j < (int)(blockDim.x >> 5); ++j) {
-      a = fmin(a, s3[0][j]);
-      b = fmax(b, s3[1][j]);
-      c += s3[2][j];
+  auto combine = [&](double* x) {  // block-wide min / max / sum / sum into thread 0
+    for (int o = 16; o > 0; o >>= 1) {
+      x[0] = fmin(x[0], __shfl_down_sync(0xffffffffu, x[0], o));
+      x[1] = fmax(x[1], __shfl_down_sync(0xffffffffu, x[1], o));
+      x[2] += __shfl_down_sync(0xffffffffu, x[2], o);
+      x[3] += __shfl_down_sync(0xffffffffu, x[3], o);
     }
-    partials[3 * blockIdx.x + 0] = a;
-    partials[3 * blockIdx.x + 1] = b;
-    partials[3 * blockIdx.x + 2] = c;
+    const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    if (lane == 0)
+      for (int q = 0; q < 4; ++q) s4[q][w] = x[q];
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      for (int j = 1; j < (int)(blockDim.x >> 5); ++j) {
+        x[0] = fmin(x[0], s4[0][j]);
+        x[1] = fmax(x[1], s4[1][j]);
+        x[2] += s4[2][j];
+        x[3] += s4[3][j];
+      }
+    }
+    __syncthreads();
+  };
+  combine(v);
+  if (threadIdx.x == 0) {
+    for (int q = 0; q < 4; ++q) partials[4 * blockIdx.x + q] = v[q];
     __threadfence();
     am_last = atomicAdd(counter, 1u) == gridDim.x - 1;
   }
   __syncthreads();
-  if (am_last && threadIdx.x == 0) {
-    __threadfence();
-    double a = 1e300, b = -1e300, c = 0.0;
-    volatile double* vp = partials;
-    for (unsigned int j = 0; j < gridDim.x; ++j) {
-      a = fmin(a, vp[3 * j + 0]);
-      b = fmax(b, vp[3 * j + 1]);
-      c += vp[3 * j + 2];
-    }
-    out3[0] = a;
-    out3[1] = b;
-    out3[2] = c;
+  if (!am_last) return;
+  __threadfence();
+  double w[4] = {1e300, -1e300, 0.0, 0.0};
+  volatile double* vp = partials;
+  for (unsigned int j = threadIdx.x; j < gridDim.x; j += blockDim.x) {
+    w[0] = fmin(w[0], vp[4 * j + 0]);
+    w[1] = fmax(w[1], vp[4 * j + 1]);
+    w[2] += vp[4 * j + 2];
+    w[3] += vp[4 * j + 3];
+  }
+  combine(w);
+  if (threadIdx.x == 0) {
+    for (int q = 0; q < 4; ++q) out4[q] = w[q];
     *counter = 0u;
   }
 }
@@ -144,6 +154,7 @@ struct FLevel {
                         // block's halo cells belong to other blocks, which
                         // write their own output while it reads.
   float s;              // kappa * s_l, the coupling magnitude
+  const float* ax[3];   // whole-domain stored form: Ax[k] (float32)
 };
 
 template <typename ST>

@@ -13,6 +13,9 @@ constexpr size_t kSmemLimit = 227 * 1024;
 // Padded cells the block-resident coarse V-cycle may hold: 12 bytes each
 // (masked z, r / unmasked z, Adiag as float32), under 200 KB.
 constexpr int kCoarseMaxCells = 16384;
+// The whole-domain stored form adds the dim coupling arrays (24 bytes a cell
+// in 3D): 8192 cells, under 200 KB.
+constexpr int kCoarseMaxCellsSto = 8192;
 
 // Cells of a level padded by one ring (2D: no padding along the absent axis).
 inline long long padded_cells(const Geom& g) {
@@ -27,21 +30,29 @@ struct TileShape {
 // k planes per pipeline step.
 constexpr TileShape kTile3 = {32, 16, 512, 2};
 constexpr TileShape kTile2 = {128, 1, 128, 4};
-inline TileShape tile_for(int dim) { return dim == 3 ? kTile3 : kTile2; }
+// the whole-domain stored form stages twice the bytes per cell: a smaller
+// tile keeps two blocks per SM
+constexpr TileShape kTile3S = {32, 8, 256, 2};
+inline TileShape tile_for(int dim, bool sto = false) { return sto ? kTile3S : (dim == 3 ? kTile3 : kTile2); }
 
-// z, r, Adiag as float32 for a ring of k + ns + 1 planes of tile + halo ns
-// (rounded up to 4 along the fastest axis, as k_sweep lays it out).
-// A one-step launch (k = the whole chunk of 2 planes + 2 ns halo planes)
-// needs no ring: k planes.
-inline size_t sweep_smem(int dim, int ns, TileShape t, bool one_step = false) {
+// z, r, Adiag (and, stored form, the dim couplings) as float32 for a ring of
+// k + ns + 1 planes of tile + halo ns (rounded up to 4 along the fastest
+// axis, as k_sweep lays it out).  A one-step launch (k = the whole chunk of 2
+// planes + 2 ns halo planes) needs no ring: k planes.
+inline size_t sweep_smem(int dim, int ns, TileShape t, bool one_step = false, bool sto = false) {
   const int RX = t.tx + 2 * ((ns + 3) & ~3);
   const int RY = dim == 3 ? t.ty + 2 * ns : 1;
   const int W = one_step ? t.k : t.k + ns + 1;
-  return (size_t)W * RX * RY * 12;
+  return (size_t)W * RX * RY * (12 + (sto ? 4 * dim : 0));
 }
 
 struct FusedPlan {
   bool valid = false;
+  bool sto = false;                // whole-domain stored form (else label-uniform)
+  // per streamed level: run the reference's per-kernel sweeps, restriction and
+  // prolongation instead of the streamed kernel (chosen by measurement: on
+  // the large levels of the stored form the per-kernel passes are faster)
+  bool split[kMaxLevels] = {};
   int lc = 0;                      // first level of the block-resident coarse solve
   int dim = 3, ns = 4, storage = 0;
   int chunk[kMaxLevels], tiles_x[kMaxLevels], tiles_y[kMaxLevels], blocks[kMaxLevels];
@@ -53,24 +64,36 @@ struct FusedPlan {
   float s[kMaxLevels];
 };
 
-// Chooses the launch shapes.  Needs every level in label-uniform form and
-// pre_post in 1..3; returns false (stored-coefficient kernels) otherwise.
+// Chooses the launch shapes.  Needs pre_post in 1..3 and either every level
+// in label-uniform form, or (the whole-domain stored form: float32 grids, 3D,
+// pre_post 1..2) every level whole-domain - every cell FLUID with a nonzero
+// diagonal.  Returns false (stored-coefficient kernels) otherwise.
 inline bool make_fused_plan(const Level* lv, int L, int dim, int pre_post, int bottom, int storage,
-                            const int* op_form, const float* offdiag, int num_sms, FusedPlan* F) {
+                            const int* op_form, const int* whole, const float* offdiag, int num_sms, FusedPlan* F) {
   F->valid = false;
-  for (int l = 0; l < L; ++l)
-    if (op_form[l] != 1) return false;
+  F->sto = false;
+  for (int l = 0; l < kMaxLevels; ++l) F->split[l] = false;
+  bool uniform = true, all_whole = true;
+  for (int l = 0; l < L; ++l) {
+    uniform = uniform && op_form[l] == 1;
+    all_whole = all_whole && whole[l] == 1;
+  }
   if (pre_post < 1 || pre_post > 3) return false;
+  if (!uniform) {
+    if (!(all_whole && storage == MG_STORE_F32 && dim == 3 && pre_post <= 2)) return false;
+    F->sto = true;
+  }
   F->dim = dim;
   F->ns = 2 * pre_post;
   F->storage = storage;
-  F->tile = tile_for(dim);
+  F->tile = tile_for(dim, F->sto);
   // first level whose sub-hierarchy fits one block
+  const long long cap = F->sto ? kCoarseMaxCellsSto : kCoarseMaxCells;
   long long tot = 0;
   int lc = L;
   for (int l = L - 1; l >= 0; --l) {
     tot += padded_cells(lv[l].g);
-    if (tot > kCoarseMaxCells) break;
+    if (tot > cap) break;
     lc = l;
   }
   if (lc == L) return false;  // even the bottom level is too big for one block
@@ -89,7 +112,7 @@ inline bool make_fused_plan(const Level* lv, int L, int dim, int pre_post, int b
   for (int l = 0; l < L; ++l) F->s[l] = offdiag[l] * F->kappa;
   // streamed levels: the 4-wide groups need the fastest extent to be a
   // multiple of 4 (then a group is wholly inside or wholly outside the grid)
-  const size_t smem = sweep_smem(dim, F->ns, F->tile);
+  const size_t smem = sweep_smem(dim, F->ns, F->tile, false, F->sto);
   const int per_sm = (int)(kSmemLimit / (smem + 1024)) < 1 ? 1 : (int)(kSmemLimit / (smem + 1024));
   for (int l = 0; l < lc; ++l) {
     const Geom& g = lv[l].g;
@@ -127,6 +150,7 @@ inline bool make_fused_plan(const Level* lv, int L, int dim, int pre_post, int b
     off += (int)padded_cells(g);
     C.s[i] = F->s[lc + i];
     C.Ad[i] = lv[lc + i].Adiag_s;
+    for (int k = 0; k < 3; ++k) C.Ax[i][k] = k < dim ? lv[lc + i].Ax[k] : nullptr;
   }
   C.total = off;
   C.r0 = lv[lc].r;
@@ -134,7 +158,7 @@ inline bool make_fused_plan(const Level* lv, int L, int dim, int pre_post, int b
   C.r_f32 = lc == 0;
   C.rho = F->rho;
   C.pi = F->pi;
-  F->coarse_smem = (size_t)off * 12;
+  F->coarse_smem = (size_t)off * (12 + (F->sto ? 4 * dim : 0));
   // 1024 threads: the upper coarse levels' phases take 1-2 cells per thread;
   // the bottom level's cells sit in the first threads' registers
   F->coarse_threads = 1024;
@@ -157,6 +181,7 @@ inline SweepArgs<ST> sweep_args(const FusedPlan& F, const Level* lv, int l, cons
   a.f.z = PRE ? (ST*)f.zt : (ST*)f.z;
   a.f.zin = (const ST*)f.zt;
   a.f.s = F.s[l];
+  for (int k = 0; k < 3; ++k) a.f.ax[k] = k < f.g.dim ? f.Ax[k] : nullptr;
   a.rc = (ST*)c.r;
   a.zc = (ST*)c.z;
   a.rho = F.rho;
@@ -169,22 +194,22 @@ inline SweepArgs<ST> sweep_args(const FusedPlan& F, const Level* lv, int l, cons
   return a;
 }
 
-template <int DIM, typename ST, int NS, bool PRE>
+template <int DIM, typename ST, int NS, bool PRE, bool STO = false>
 inline cudaError_t launch_sweep_t(const FusedPlan& F, const Level* lv, int l, const Control* ctl, cudaStream_t s) {
-  constexpr TileShape T = DIM == 3 ? kTile3 : kTile2;
+  constexpr TileShape T = STO ? kTile3S : (DIM == 3 ? kTile3 : kTile2);
   if (DIM == 3 && F.chunk[l] == 2) {
     // small level: each block's 2 planes + halo planes in ONE pipeline step
     constexpr TileShape T1 = {T.tx, T.ty, T.nt, 2 + 2 * NS};
-    auto kern = k_sweep<DIM, ST, NS, T1.tx, T1.ty, PRE, T1.nt, T1.k>;
-    const size_t smem = sweep_smem(DIM, NS, T1, true);
+    auto kern = k_sweep<DIM, ST, NS, T1.tx, T1.ty, PRE, T1.nt, T1.k, STO>;
+    const size_t smem = sweep_smem(DIM, NS, T1, true, STO);
     cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
     kern<<<F.blocks[l], T1.nt, smem, s>>>(sweep_args<ST, PRE>(F, lv, l, ctl));
     return cudaGetLastError();
   }
-  auto kern = k_sweep<DIM, ST, NS, T.tx, T.ty, PRE, T.nt, T.k>;
+  auto kern = k_sweep<DIM, ST, NS, T.tx, T.ty, PRE, T.nt, T.k, STO>;
   constexpr int NT = T.nt;
-  const size_t smem = sweep_smem(DIM, NS, T);
+  const size_t smem = sweep_smem(DIM, NS, T, false, STO);
   cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (e != cudaSuccess) return e;
   kern<<<F.blocks[l], NT, smem, s>>>(sweep_args<ST, PRE>(F, lv, l, ctl));
@@ -211,6 +236,13 @@ inline cudaError_t launch_sweep_st(const FusedPlan& F, const Level* lv, int l, c
 
 template <bool PRE>
 inline cudaError_t launch_sweep(const FusedPlan& F, const Level* lv, int l, const Control* ctl, cudaStream_t s) {
+  if (F.sto) {
+    switch (F.ns) {
+      case 2: return launch_sweep_t<3, float, 2, PRE, true>(F, lv, l, ctl, s);
+      case 4: return launch_sweep_t<3, float, 4, PRE, true>(F, lv, l, ctl, s);
+    }
+    return cudaErrorInvalidValue;
+  }
   switch (F.storage) {
     case MG_STORE_F32: return launch_sweep_st<float, PRE>(F, lv, l, ctl, s);
     case MG_STORE_F16: return launch_sweep_st<__half, PRE>(F, lv, l, ctl, s);
@@ -219,18 +251,19 @@ inline cudaError_t launch_sweep(const FusedPlan& F, const Level* lv, int l, cons
   return cudaErrorInvalidValue;
 }
 
-template <typename ST>
+template <typename ST, bool STO = false>
 inline cudaError_t launch_coarse_st(const FusedPlan& F, const Control* ctl, cudaStream_t s) {
   CoarseArgs a = F.coarse;
   a.ctl = ctl;
-  cudaError_t e = cudaFuncSetAttribute(k_coarse<ST>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                       (int)F.coarse_smem);
+  auto kern = k_coarse<ST, STO>;
+  cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)F.coarse_smem);
   if (e != cudaSuccess) return e;
-  k_coarse<ST><<<1, F.coarse_threads, F.coarse_smem, s>>>(a);
+  kern<<<1, F.coarse_threads, F.coarse_smem, s>>>(a);
   return cudaGetLastError();
 }
 
 inline cudaError_t launch_coarse(const FusedPlan& F, const Control* ctl, cudaStream_t s) {
+  if (F.sto) return launch_coarse_st<float, true>(F, ctl, s);
   switch (F.storage) {
     case MG_STORE_F32: return launch_coarse_st<float>(F, ctl, s);
     case MG_STORE_F16: return launch_coarse_st<__half>(F, ctl, s);
@@ -239,14 +272,8 @@ inline cudaError_t launch_coarse(const FusedPlan& F, const Control* ctl, cudaStr
   return cudaErrorInvalidValue;
 }
 
-// One V-cycle (mgpcg.py:125-148) with the fused kernels: 2 * lc + 1 launches.
-inline cudaError_t launch_vcycle_fused(const FusedPlan& F, const Level* lv, const Control* ctl, cudaStream_t s) {
-  for (int l = 0; l < F.lc; ++l)
-    if (cudaError_t e = launch_sweep<true>(F, lv, l, ctl, s)) return e;
-  if (cudaError_t e = launch_coarse(F, ctl, s)) return e;
-  for (int l = F.lc - 1; l >= 0; --l)
-    if (cudaError_t e = launch_sweep<false>(F, lv, l, ctl, s)) return e;
-  return cudaSuccess;
-}
+// The V-cycle (mgpcg.py:125-148) of a fused plan is composed in mg_plan.cu:
+// per streamed level the streamed kernel or (split) the per-kernel passes,
+// then the coarse block.
 
 }  // namespace mg

@@ -5,9 +5,12 @@
 // mg_plan_workspace_bytes() bytes; every solver field (mgpcg.py:21-44) lives at
 // a fixed 256-byte aligned offset in it.  This file allocates host memory only
 // (the plan, a pinned parameter block) plus the CUDA graph objects.
+#include <array>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <map>
+#include <mutex>
 #include <new>
 #include <vector>
 
@@ -72,6 +75,7 @@ struct mg_plan {
   int red_blocks = 0;
   int ew_blocks[kMaxLevels];
   int op_form[kMaxLevels];
+  int whole[kMaxLevels];     // level is whole-domain: every cell FLUID, Adiag != 0
   float offdiag[kMaxLevels];
   bool prepared = false;
   FusedPlan fp;
@@ -220,12 +224,111 @@ int launch_vcycle_generic(mg_plan* P, cudaStream_t s) {
   return MG_OK;
 }
 
-int launch_vcycle(mg_plan* P, cudaStream_t s) {
-  if (P->fp.valid) {
-    cudaError_t e = launch_vcycle_fused(P->fp, P->lv, P->ctl, s);
-    return e == cudaSuccess ? MG_OK : set_err("launch_vcycle_fused", e);
+// Pre-smoothing and restriction of streamed level l of a fused plan (PRE),
+// or prolongation and post-smoothing (POST): the streamed kernel, or for a
+// split level the per-kernel passes on z[l] in place.  The two forms meet
+// only in r[l+1] and z[l+1] (restriction zeroes z[l+1]; the streamed PRE
+// writes it 0), so levels of either form mix.
+int launch_level(mg_plan* P, int l, bool pre, cudaStream_t s) {
+  if (!P->fp.split[l]) {
+    cudaError_t e = pre ? launch_sweep<true>(P->fp, P->lv, l, P->ctl, s)
+                        : launch_sweep<false>(P->fp, P->lv, l, P->ctl, s);
+    return e == cudaSuccess ? MG_OK : set_err("launch_sweep", e);
   }
+  if (pre) {
+    if (l == 0) CK(cudaMemsetAsync(P->lv[0].z, 0, level_cells(P, 0) * sizeof(float), s));
+    for (int i = 0; i < P->d.pre_post; ++i) {
+      if (int rc = launch_smooth(P, l, 0, s)) return rc;
+      if (int rc = launch_smooth(P, l, 1, s)) return rc;
+    }
+    return launch_restrict(P, l, s);
+  }
+  if (int rc = launch_prolongate(P, l, s)) return rc;
+  for (int i = 0; i < P->d.pre_post; ++i) {
+    if (int rc = launch_smooth(P, l, 1, s)) return rc;
+    if (int rc = launch_smooth(P, l, 0, s)) return rc;
+  }
+  return MG_OK;
+}
+
+// One V-cycle of a fused plan: the streamed levels down, the coarse block,
+// the streamed levels up.
+int launch_vcycle_fused(mg_plan* P, cudaStream_t s) {
+  for (int l = 0; l < P->fp.lc; ++l)
+    if (int rc = launch_level(P, l, true, s)) return rc;
+  cudaError_t e = launch_coarse(P->fp, P->ctl, s);
+  if (e != cudaSuccess) return set_err("launch_coarse", e);
+  for (int l = P->fp.lc - 1; l >= 0; --l)
+    if (int rc = launch_level(P, l, false, s)) return rc;
+  return MG_OK;
+}
+
+int launch_vcycle(mg_plan* P, cudaStream_t s) {
+  if (P->fp.valid) return launch_vcycle_fused(P, s);
   return launch_vcycle_generic(P, s);
+}
+
+// ---- autotuner: streamed kernel or per-kernel passes, per level ------------
+//
+// The streamed kernel trades halo recomputation for memory traffic.  For the
+// label-uniform form it wins on every level measured (B200, 128^3 and 256^3);
+// for the whole-domain stored form, which stages 24 bytes a cell, the
+// per-kernel passes win on the large levels and the streamed kernel on the
+// small ones.  So for the stored form each streamed level is timed both ways
+// (CUDA events on the plan's stream, after one warm-up) the first time a
+// shape is prepared, and the faster is kept; the choice is cached per shape
+// for the process.  Both variants compute the same float32 values.
+std::mutex g_tune_mu;
+std::map<std::array<int, 7>, uint32_t> g_tune;  // bit l: split level l
+
+int tune_split(mg_plan* P, cudaStream_t s) {
+  if (!P->fp.valid || !P->fp.sto) return MG_OK;
+  const Geom& g = P->geom[0];
+  const std::array<int, 7> key = {g.dim, g.n[0], g.n[1], g.n[2], P->L, P->d.pre_post, P->fp.lc};
+  {
+    std::lock_guard<std::mutex> lk(g_tune_mu);
+    auto it = g_tune.find(key);
+    if (it != g_tune.end()) {
+      for (int l = 0; l < P->fp.lc; ++l) P->fp.split[l] = (it->second >> l) & 1u;
+      return MG_OK;
+    }
+  }
+  cudaEvent_t e0 = nullptr, e1 = nullptr;
+  CK(cudaEventCreate(&e0));
+  cudaError_t ce = cudaEventCreate(&e1);
+  if (ce != cudaSuccess) {
+    cudaEventDestroy(e0);
+    return set_err("cudaEventCreate", ce);
+  }
+  uint32_t bits = 0;
+  int rc = MG_OK;
+  for (int l = 0; l < P->fp.lc && rc == MG_OK; ++l) {
+    float t[2] = {0.0f, 0.0f};
+    for (int mode = 0; mode < 2 && rc == MG_OK; ++mode) {
+      P->fp.split[l] = mode == 1;
+      for (int rep = 0; rep < 4 && rc == MG_OK; ++rep) {  // rep 0 warms up
+        if (rep == 1) cudaEventRecord(e0, s);
+        rc = launch_level(P, l, true, s);
+        if (rc == MG_OK) rc = launch_level(P, l, false, s);
+      }
+      if (rc != MG_OK) break;
+      cudaEventRecord(e1, s);
+      cudaError_t e = cudaEventSynchronize(e1);
+      if (e == cudaSuccess) e = cudaEventElapsedTime(&t[mode], e0, e1);
+      if (e != cudaSuccess) rc = set_err("tune_split", e);
+    }
+    P->fp.split[l] = rc == MG_OK && t[1] < t[0];
+    if (P->fp.split[l]) bits |= 1u << l;
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  if (rc != MG_OK) {
+    for (int l = 0; l < kMaxLevels; ++l) P->fp.split[l] = false;
+    return rc;
+  }
+  std::lock_guard<std::mutex> lk(g_tune_mu);
+  g_tune[key] = bits;
+  return MG_OK;
 }
 
 template <typename ST>
@@ -265,7 +368,7 @@ int launch_cg_tail(mg_plan* P, cudaStream_t s, int which) {
   const int RB = P->red_blocks;
   const bool refresh = P->d.refresh_every > 0;
   if (which & 1) {
-    if (P->fp.valid)  // label-uniform level 0
+    if (P->fp.valid && !P->fp.sto)  // label-uniform level 0
       k_Ap_alpha_uniform<<<RB, kRedThreads, 0, s>>>(L0, p, Ap, P->offdiag[0], P->ctl, P->partials);
     else
       k_Ap_alpha<<<RB, kRedThreads, 0, s>>>(L0, p, Ap, P->ctl, P->partials);
@@ -300,7 +403,11 @@ int launch_pcg_part(mg_plan* P, bool prologue, cudaStream_t s) {
 // Kernels one launch_pcg_part enqueues (the graph's node count per part).
 int count_pcg_part(const mg_plan* P, bool prologue) {
   const int refresh = P->d.refresh_every > 0 ? 1 : 0;
-  if (P->fp.valid) return (prologue ? 1 : 0) + 2 * P->fp.lc + 1 + 4 + refresh;
+  if (P->fp.valid) {
+    int v = 1;  // the coarse block
+    for (int l = 0; l < P->fp.lc; ++l) v += P->fp.split[l] ? 2 * (2 * P->d.pre_post + 1) : 2;
+    return (prologue ? 1 : 0) + v + 4 + refresh;
+  }
   int v = (P->L - 1) * (4 * P->d.pre_post + 2) +
           (P->geom[P->L - 1].count <= kBottomBlockCells ? (P->d.bottom / 2 > 0) : 2 * P->d.bottom);
   return (prologue ? 1 : 0) + v + 2 + 2 + refresh;
@@ -407,6 +514,10 @@ int mg_plan_create(const mg_plan_desc_t* desc, mg_plan_t** out) {
     if (d.res[k] < 2) return bad("res must be >= 2");
     if (d.res[k] % (1 << (d.levels - 1)) != 0) return bad("res must be divisible by 2^(levels-1)");
   }
+  if ((long long)d.res[0] * d.res[1] * (d.dim == 3 ? d.res[2] : 1) >= (1LL << 31)) {
+    snprintf(g_err, sizeof(g_err), "a level of 2^31 cells or more exceeds the 32-bit cell index of the kernels");
+    return MG_E_TOO_BIG;
+  }
   mg_plan* P = new (std::nothrow) mg_plan();
   if (!P) return bad("out of host memory");
   P->d = d;
@@ -419,6 +530,7 @@ int mg_plan_create(const mg_plan_desc_t* desc, mg_plan_t** out) {
     g.n[2] = d.dim == 3 ? (d.res[2] >> l) : 1;
     g.count = (long long)g.n[0] * g.n[1] * g.n[2];
     P->op_form[l] = 0;
+    P->whole[l] = 0;
   }
   layout(P);
   cudaGetDevice(&P->device);
@@ -746,21 +858,22 @@ int mg_plan_prepare(mg_plan_t* P, void* stream) {
   NEED_BOUND(P);
   cudaStream_t s = S(stream);
   // 1. operator form of every level (one synchronisation for all levels)
-  const int blocks = P->num_sms * 2 < kMaxPartials / 3 ? P->num_sms * 2 : kMaxPartials / 3;
+  const int blocks = P->num_sms * 2 < kMaxPartials / 4 ? P->num_sms * 2 : kMaxPartials / 4;
   for (int l = 0; l < P->L; ++l) {
-    k_detect_uniform<<<blocks, kRedThreads, 0, s>>>(P->lv[l], P->partials, &P->ctl->counter[5],
-                                                    &P->ctl->det[3 * l]);
+    const int nb = grid_for(P, P->geom[l].count) < blocks ? grid_for(P, P->geom[l].count) : blocks;
+    k_detect_uniform<<<nb, kRedThreads, 0, s>>>(P->lv[l], P->partials, &P->ctl->counter[5], &P->ctl->det[4 * l]);
     CKL("k_detect_uniform");
   }
-  double det[3 * kMaxLevels];
-  CK(cudaMemcpyAsync(det, P->ctl->det, sizeof(double) * 3 * P->L, cudaMemcpyDeviceToHost, s));
+  double det[4 * kMaxLevels];
+  CK(cudaMemcpyAsync(det, P->ctl->det, sizeof(double) * 4 * P->L, cudaMemcpyDeviceToHost, s));
   CK(cudaStreamSynchronize(s));
   for (int l = 0; l < P->L; ++l) {
-    const double* h = det + 3 * l;
+    const double* h = det + 4 * l;
     const bool none = h[0] > h[1];  // no nonzero off-diagonal at all
     const bool uniform = h[2] == 0.0 && (none || (h[0] == h[1] && h[0] < 0.0));
     P->op_form[l] = uniform ? 1 : 0;
     P->offdiag[l] = uniform && !none ? (float)(-h[0]) : 0.0f;
+    P->whole[l] = h[3] == 0.0 ? 1 : 0;  // every cell FLUID with a nonzero diagonal
   }
   return finish_prepare(P, s, false);
 }
@@ -771,6 +884,7 @@ int mg_plan_prepare_declared(mg_plan_t* P, const float* offdiag, void* stream) {
   for (int l = 0; l < P->L; ++l) {
     P->op_form[l] = 1;
     P->offdiag[l] = offdiag[l];
+    P->whole[l] = 0;
   }
   return finish_prepare(P, S(stream), true);
 }
@@ -783,8 +897,8 @@ static int finish_prepare(mg_plan_t* P, cudaStream_t s, bool declared) {
   // 2. launch shapes of the fused V-cycle
   P->fp.valid = false;
   if (!(P->d.flags & MG_PLAN_STORED))
-    make_fused_plan(P->lv, P->L, P->d.dim, P->d.pre_post, P->d.bottom, P->d.storage, P->op_form, P->offdiag,
-                    P->num_sms, &P->fp);
+    make_fused_plan(P->lv, P->L, P->d.dim, P->d.pre_post, P->d.bottom, P->d.storage, P->op_form, P->whole,
+                    P->offdiag, P->num_sms, &P->fp);
   if (P->d.storage != MG_STORE_F32 && !P->fp.valid)
     return bad("16-bit storage needs the label-uniform operator on every level and pre_and_post_smoothing 1..3");
   // 3. 16-bit coefficient copies, FLUID count, scale factors
@@ -804,6 +918,7 @@ static int finish_prepare(mg_plan_t* P, cudaStream_t s, bool declared) {
   CKL("k_count_fluid");
   k_set_kappa<<<1, 1, 0, s>>>(P->ctl, (double)P->fp.kappa);
   CKL("k_set_kappa");
+  if (int rc = tune_split(P, s)) return rc;
   if (declared) {
     for (int l = 0; l < P->L; ++l) {
       k_verify_uniform<<<P->ew_blocks[l], 256, 0, s>>>(P->lv[l], P->offdiag[l], P->ctl);
@@ -815,7 +930,9 @@ static int finish_prepare(mg_plan_t* P, cudaStream_t s, bool declared) {
   uint64_t sig = 1469598103934665603ull;
   auto mix = [&](uint64_t v) { sig = (sig ^ v) * 1099511628211ull; };
   mix(P->fp.valid);
+  mix(P->fp.sto);
   mix(P->fp.lc);
+  for (int l = 0; l < P->L; ++l) mix(P->fp.split[l]);
   for (int l = 0; l < P->L; ++l) {
     uint32_t bits;
     std::memcpy(&bits, &P->fp.s[l], 4);
@@ -835,10 +952,27 @@ static int finish_prepare(mg_plan_t* P, cudaStream_t s, bool declared) {
 
 extern "C" {
 
+int mg_plan_split(mg_plan_t* P, int32_t set, uint32_t* bits, int32_t* streamed) {
+  if (!P || !bits) return bad("null pointer");
+  if (streamed) *streamed = P->fp.valid ? P->fp.lc : 0;
+  if (set) {
+    if (!P->fp.valid) return bad("the plan has no fused V-cycle");
+    if (*bits >> P->fp.lc) return bad("split bits beyond the streamed levels");
+    for (int l = 0; l < P->fp.lc; ++l) P->fp.split[l] = (*bits >> l) & 1u;
+    destroy_graph(P);
+    P->graph_sig = 0;
+  }
+  uint32_t b = 0;
+  for (int l = 0; l < P->fp.lc; ++l)
+    if (P->fp.split[l]) b |= 1u << l;
+  *bits = b;
+  return MG_OK;
+}
+
 int mg_plan_operator_form(const mg_plan_t* P, int32_t level, int32_t* form) {
   if (!P || !form) return bad("null pointer");
   if (level < 0 || level >= P->L) return bad("level");
-  *form = P->op_form[level];
+  *form = P->op_form[level] == 1 ? 1 : (P->fp.valid && P->fp.sto ? 2 : 0);
   return MG_OK;
 }
 
@@ -943,9 +1077,7 @@ int mg_launch_stage(mg_plan_t* P, int32_t stage, int32_t level, void* stream) {
     case 1: {
       if (P->fp.valid) {
         if (level < 0 || level >= P->fp.lc) return bad("level is not a streamed level");
-        cudaError_t e = stage == 0 ? launch_sweep<true>(P->fp, P->lv, level, P->ctl, s)
-                                   : launch_sweep<false>(P->fp, P->lv, level, P->ctl, s);
-        return e == cudaSuccess ? MG_OK : set_err("launch_sweep", e);
+        return launch_level(P, level, stage == 0, s);
       }
       if (level < 0 || level >= P->L - 1) return bad("level");
       if (stage == 0) {
@@ -968,7 +1100,7 @@ int mg_launch_stage(mg_plan_t* P, int32_t stage, int32_t level, void* stream) {
       return e == cudaSuccess ? MG_OK : set_err("launch_coarse", e);
     }
     case 3:
-      if (P->fp.valid)
+      if (P->fp.valid && !P->fp.sto)
         k_Ap_alpha_uniform<<<P->red_blocks, kRedThreads, 0, s>>>(L0, fptr(P, MG_FIELD_P), fptr(P, MG_FIELD_AP),
                                                                  P->offdiag[0], P->ctl, P->partials, 1);
       else

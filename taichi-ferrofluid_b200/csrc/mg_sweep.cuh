@@ -81,8 +81,16 @@ __device__ __forceinline__ void ld4_r(const void* r, long long i, int r_f32, flo
 // PRE starts from z = 0, so its first half sweep is pointwise, z = r / Adiag
 // on colour-0 cells (the neighbour sum is +0): it is applied while storing a
 // plane, which saves one ring of halo.
-template <int DIM, typename ST, int NS, int TX, int TY, bool PRE, int NT, int K>
+//
+// STO (whole-domain stored form, float32 only): every cell is FLUID and the
+// couplings are the stored Ax of the level, staged in the ring beside z, r
+// and Adiag; the neighbour sum is the reference's
+//   sum_k Ax[I-e_k][k] z[I-e_k] + Ax[I][k] z[I+e_k]
+// with the same operation order, and a neighbour outside the grid is loaded
+// as z = 0, Ax = 0 (rule H1).
+template <int DIM, typename ST, int NS, int TX, int TY, bool PRE, int NT, int K, bool STO = false>
 __global__ void __launch_bounds__(NT) k_sweep(SweepArgs<ST> A) {
+  static_assert(!STO || sizeof(ST) == 4, "the stored form runs on float32 grids");
   // halos: NS cells are needed on each side; along the fastest axis the halo
   // is rounded up to 4 so every 4-wide group starts 16-byte (float) / 8-byte
   // (16-bit) aligned; the XS extra cells are loaded but never smoothed
@@ -108,6 +116,10 @@ __global__ void __launch_bounds__(NT) k_sweep(SweepArgs<ST> A) {
   float* sz = (float*)smem;                       // [W][PL]
   float* sr = sz + W * PL;
   float* sa = sr + W * PL;
+  float* sx0 = sa + W * PL;                       // STO: Ax[0] (plane axis)
+  float* sx1 = sx0 + W * PL;                      // STO, 3D: Ax[1] (rows)
+  float* sxx = DIM == 3 ? sx1 + W * PL : sx1;     // STO: Ax[dim-1] (fastest axis)
+  constexpr int NX = STO ? DIM : 1;               // coefficient arrays loaded per cell
 
   const FLevel<ST>& F = A.f;
   const int n0 = F.n[0], n1 = F.n[1], n2 = F.n[2];
@@ -131,13 +143,16 @@ __global__ void __launch_bounds__(NT) k_sweep(SweepArgs<ST> A) {
   auto slot = [](int p) { return (p + W * 64) % W; };
 
   // ---- loading planes ---------------------------------------------------------------
-  // group q of the K planes from P: global loads into r[4], a[4], z[4]
-  auto load_group = [&](int P, int q, float* r, float* a, float* z) {
+  // group q of the K planes from P: global loads into r[4], a[4], z[4] and
+  // (STO) the coefficients x[NX][4]
+  auto load_group = [&](int P, int q, float* r, float* a, float* z, float (*x)[4]) {
 #pragma unroll
     for (int e = 0; e < 4; ++e) {
       r[e] = 0.0f;
       a[e] = 0.0f;
       z[e] = 0.0f;
+#pragma unroll
+      for (int k = 0; k < NX; ++k) x[k][e] = 0.0f;
     }
     const int kp = q / PL4, rem = q - kp * PL4;
     const int ry = rem / Q, rx = (rem - ry * Q) * 4;
@@ -147,6 +162,10 @@ __global__ void __launch_bounds__(NT) k_sweep(SweepArgs<ST> A) {
       const long long gi = (long long)p * plane_stride + (long long)gy * nx + gx;
       ld4_r<ST>(F.r, gi, A.r_f32, sigma, r);
       ld4<ST>(F.Ad + gi, a);
+      if constexpr (STO) {
+#pragma unroll
+        for (int k = 0; k < NX; ++k) ld4<float>(F.ax[k] + gi, x[k]);
+      }
       if (!PRE) {
         float zi[4];
         ld4<ST>(F.zin + gi, zi);
@@ -163,7 +182,7 @@ __global__ void __launch_bounds__(NT) k_sweep(SweepArgs<ST> A) {
   };
   // store group q into shared memory; PRE applies its pointwise first half
   // sweep, POST writes the final value of non-FLUID interior cells it owns
-  auto put_group = [&](int P, int q, const float* r, const float* a, const float* z) {
+  auto put_group = [&](int P, int q, const float* r, const float* a, const float* z, const float (*x)[4]) {
     const int kp = q / PL4, rem = q - kp * PL4;
     const int ry = rem / Q, rx = (rem - ry * Q) * 4;
     const int p = P + kp;
@@ -182,6 +201,12 @@ __global__ void __launch_bounds__(NT) k_sweep(SweepArgs<ST> A) {
     *reinterpret_cast<float4*>(sz + o) = make_float4(zv[0], zv[1], zv[2], zv[3]);
     *reinterpret_cast<float4*>(sr + o) = make_float4(r[0], r[1], r[2], r[3]);
     *reinterpret_cast<float4*>(sa + o) = make_float4(a[0], a[1], a[2], a[3]);
+    if constexpr (STO) {
+      *reinterpret_cast<float4*>(sx0 + o) = make_float4(x[0][0], x[0][1], x[0][2], x[0][3]);
+      if (DIM == 3) *reinterpret_cast<float4*>(sx1 + o) = make_float4(x[1][0], x[1][1], x[1][2], x[1][3]);
+      *reinterpret_cast<float4*>(sxx + o) =
+          make_float4(x[NX - 1][0], x[NX - 1][1], x[NX - 1][2], x[NX - 1][3]);
+    }
     if (!PRE && p >= z0 && p < z1 && gx >= tx0 && gx < tx0 + TX && gx < nx &&
         gy >= ty0 && gy < ty0 + (DIM == 3 ? TY : 1) && gy < ny) {
       const long long gi = (long long)p * plane_stride + (long long)gy * nx + gx;
@@ -192,26 +217,26 @@ __global__ void __launch_bounds__(NT) k_sweep(SweepArgs<ST> A) {
   };
   // streaming: the next K planes are prefetched into registers during the
   // current step; one step (ONE): loaded straight into shared memory
-  float fr[PF][4], fa[PF][4], fz[PF][4];
+  float fr[PF][4], fa[PF][4], fz[PF][4], fx[PF][NX][4];
   auto fetch = [&](int P) {
 #pragma unroll
     for (int g = 0; g < PF; ++g) {
       const int q = threadIdx.x + g * NT;
-      if (q < K * PL4) load_group(P, q, fr[g], fa[g], fz[g]);
+      if (q < K * PL4) load_group(P, q, fr[g], fa[g], fz[g], fx[g]);
     }
   };
   auto store = [&](int P) {
     if constexpr (ONE) {
       for (int q = threadIdx.x; q < K * PL4; q += NT) {
-        float r[4], a[4], z[4];
-        load_group(P, q, r, a, z);
-        put_group(P, q, r, a, z);
+        float r[4], a[4], z[4], x[NX][4];
+        load_group(P, q, r, a, z, x);
+        put_group(P, q, r, a, z, x);
       }
     } else {
 #pragma unroll
       for (int g = 0; g < PF; ++g) {
         const int q = threadIdx.x + g * NT;
-        if (q < K * PL4) put_group(P, q, fr[g], fa[g], fz[g]);
+        if (q < K * PL4) put_group(P, q, fr[g], fa[g], fz[g], fx[g]);
       }
     }
   };
@@ -219,10 +244,19 @@ __global__ void __launch_bounds__(NT) k_sweep(SweepArgs<ST> A) {
   // neighbour sum (mgpcg.py:96-102) of cell c of the plane at slot offset sc
   auto nsum = [&](int sb, int sc, int sa_, int c) {
     float ret = 0.0f;
-    ret = __fadd_rn(ret, __fadd_rn(__fmul_rn(ms, sz[sb + c]), __fmul_rn(ms, sz[sa_ + c])));
-    if (DIM == 3)
-      ret = __fadd_rn(ret, __fadd_rn(__fmul_rn(ms, sz[sc + c - RX]), __fmul_rn(ms, sz[sc + c + RX])));
-    ret = __fadd_rn(ret, __fadd_rn(__fmul_rn(ms, sz[sc + c - 1]), __fmul_rn(ms, sz[sc + c + 1])));
+    if constexpr (STO) {
+      ret = __fadd_rn(ret, __fadd_rn(__fmul_rn(sx0[sb + c], sz[sb + c]), __fmul_rn(sx0[sc + c], sz[sa_ + c])));
+      if (DIM == 3)
+        ret = __fadd_rn(ret, __fadd_rn(__fmul_rn(sx1[sc + c - RX], sz[sc + c - RX]),
+                                       __fmul_rn(sx1[sc + c], sz[sc + c + RX])));
+      ret = __fadd_rn(ret, __fadd_rn(__fmul_rn(sxx[sc + c - 1], sz[sc + c - 1]),
+                                     __fmul_rn(sxx[sc + c], sz[sc + c + 1])));
+    } else {
+      ret = __fadd_rn(ret, __fadd_rn(__fmul_rn(ms, sz[sb + c]), __fmul_rn(ms, sz[sa_ + c])));
+      if (DIM == 3)
+        ret = __fadd_rn(ret, __fadd_rn(__fmul_rn(ms, sz[sc + c - RX]), __fmul_rn(ms, sz[sc + c + RX])));
+      ret = __fadd_rn(ret, __fadd_rn(__fmul_rn(ms, sz[sc + c - 1]), __fmul_rn(ms, sz[sc + c + 1])));
+    }
     return ret;
   };
 

@@ -96,6 +96,7 @@ _SIGS = {
     "mg_pressure_solve_async": (ctypes.c_int, [_vp, _vp, _vp, _vp, _vp, _vp, _f32, _f32, _f32, _i32, _f32,
                                                ctypes.c_void_p, _vp]),
     "mg_plan_operator_form": (ctypes.c_int, [_vp, _i32, ctypes.POINTER(_i32)]),
+    "mg_plan_split": (ctypes.c_int, [_vp, _i32, ctypes.POINTER(ctypes.c_uint32), ctypes.POINTER(_i32)]),
     "mg_smooth": (ctypes.c_int, [_vp, _i32, _i32, _vp]),
     "mg_restrict": (ctypes.c_int, [_vp, _i32, _vp]),
     "mg_prolongate": (ctypes.c_int, [_vp, _i32, _vp]),

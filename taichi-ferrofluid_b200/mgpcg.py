@@ -169,6 +169,16 @@ class MGPCGPoissonSolver:
         """Chooses the V-cycle operator form for the A just built."""
         check(self.lib.mg_plan_prepare(self.plan, self._s()), "mg_plan_prepare")
 
+    def split_levels(self, bits=None):
+        """(bits, streamed levels): the autotuner's per-level choice (bit l: level
+        l runs the per-kernel passes); ``bits`` forces a choice until the next
+        prepare."""
+        b = mg_lib.ctypes.c_uint32(0 if bits is None else int(bits))
+        n = mg_lib.ctypes.c_int32(0)
+        check(self.lib.mg_plan_split(self.plan, 0 if bits is None else 1, mg_lib.ctypes.byref(b),
+                                     mg_lib.ctypes.byref(n)), "mg_plan_split")
+        return int(b.value), int(n.value)
+
     def operator_form(self, level=0):
         f = mg_lib.ctypes.c_int32()
         check(self.lib.mg_plan_operator_form(self.plan, level, mg_lib.ctypes.byref(f)), "mg_plan_operator_form")

@@ -36,7 +36,7 @@ def test_potential_system_bit_exact(n, levels):
         np.testing.assert_array_equal(np.moveaxis(g.Ax[l].cpu().numpy(), -1, 0), o.get("Ax", l))
         assert int(g.grid_type[l].abs().max()) == 0  # every cell FLUID (full_reinitialize)
     np.testing.assert_array_equal(g.b.cpu().numpy(), o.get("b"))
-    assert g.operator_form(0) == 0  # stored coefficients
+    assert g.operator_form(0) == 2  # whole-domain stored coefficients, fused V-cycle
 
 
 @pytest.mark.parametrize("n,levels", [(32, 3), (64, 4)])
