@@ -68,6 +68,16 @@ MAX_ITERS = 500
 REL_TOL = 1e-12  # squared: 1e-6 relative residual
 DIRECT_LAUNCH = False  # set by --direct
 
+# DRAM bytes (read + write) per launch of the dominant kernels, from one ncu
+# capture each (profiles/dram_traffic_pressure128.md,
+# profiles/k_sweep_pre_l0_precision256.md); the bench line's roofline.traffic.
+NCU_DRAM_BYTES = {
+    ("substep128", "pre_l0"): 16.80e6, ("substep128", "post_l0"): 26.24e6,
+    ("pressure128", "pre_l0"): 16.80e6, ("pressure128", "post_l0"): 26.24e6,
+    ("substep128", "Ap_alpha"): 11.29e6, ("pressure128", "Ap_alpha"): 11.29e6,
+    ("precision256", "pre_l0"): 196.06e6, ("precision256", "Ap_alpha"): 98.40e6,
+}
+
 
 def parse():
     ap = argparse.ArgumentParser()
@@ -411,7 +421,8 @@ def gpu_arm(args, rank, world, local):
                      "achieved": kernels[dom]["GB_s"], "peak": peak, "unit": "GB/s",
                      "frac": round(kernels[dom]["GB_s"] / peak, 4), "peak_source": "MEASURED_PEAKS.json hbm_gbs"
                      if "hbm_gbs" in peaks else "fallback 6650 GB/s",
-                     "traffic": None},
+                     "traffic": NCU_DRAM_BYTES.get((args.workload, dom)) if args.storage == "f32" else None,
+                     "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum per launch, profiles/"},
         "kernels": kernels,
         "clocks": clk.summary(),
     }

@@ -302,7 +302,9 @@ MG_API int mg_plan_operator_form(const mg_plan_t* plan, int32_t level, int32_t* 
  * a shape is first prepared (the choice is cached per shape); the
  * label-uniform form always streams.  set != 0 forces *bits (after the plan
  * is prepared; valid until the next prepare); *bits returns the choice and
- * *streamed (if not NULL) the number of streamed levels. */
+ * *streamed (if not NULL) the number of streamed levels.  The environment
+ * variable MGPCG_SPLIT=<bits> replaces the timing for every plan (for
+ * profilers, which serialise the trial launches). */
 MG_API int mg_plan_split(mg_plan_t* plan, int32_t set, uint32_t* bits, int32_t* streamed);
 
 /* ---- the reference's per-kernel operations (for parity tests) ------------ */

@@ -8,6 +8,7 @@
 #include <array>
 #include <cmath>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <map>
 #include <mutex>
@@ -283,6 +284,13 @@ std::map<std::array<int, 7>, uint32_t> g_tune;  // bit l: split level l
 
 int tune_split(mg_plan* P, cudaStream_t s) {
   if (!P->fp.valid || !P->fp.sto) return MG_OK;
+  // MGPCG_SPLIT=<bits> replaces the timing (profilers serialise the trial
+  // launches and would skew the choice)
+  if (const char* ov = std::getenv("MGPCG_SPLIT")) {
+    const unsigned long v = std::strtoul(ov, nullptr, 0);
+    for (int l = 0; l < P->fp.lc; ++l) P->fp.split[l] = (v >> l) & 1ul;
+    return MG_OK;
+  }
   const Geom& g = P->geom[0];
   const std::array<int, 7> key = {g.dim, g.n[0], g.n[1], g.n[2], P->L, P->d.pre_post, P->fp.lc};
   {
