@@ -246,6 +246,24 @@ MG_API int mg_build_surface_tension_b(mg_plan_t* plan, int32_t d, const float* u
 MG_API int mg_build_surface_tension_A(mg_plan_t* plan, int32_t level, int32_t d, const float* phi,
                                       double sigma, double dt, double dx, double eps, void* stream);
 
+/* ---- the step before the solve: labels and level set ----------------------
+ * Plan-free: the grid is (dim, res).  phi and cell_type are dense row-major
+ * device arrays of shape res (float32 / int32, the simulator's fields).
+ * mg_level_set_shape: LevelSet.initialize_with_aabb (level_set.py:40-59;
+ * sphere = 0, box [a, b]) or initialize_with_sphere (level_set.py:61-64;
+ * sphere != 0, centre a, radius b[0]): phi = the shape's signed distance at
+ * the cell centres (I + 0.5) dx; combine != 0 keeps min(phi, distance)
+ * instead, the union of several shapes.
+ * mg_apply_markers: FluidSimulator.apply_markers (fluid_simulator.py:151-159),
+ * non-SOLID cells AIR, then FLUID where phi <= 0 (strict != 0: phi < 0).
+ * mg_init_boundary: FluidSimulator.init_boundary (fluid_simulator.py:337-341),
+ * SOLID on the outermost ring. */
+MG_API int mg_level_set_shape(int32_t dim, const int32_t* res, float* phi, float dx, int32_t sphere,
+                              const float* a, const float* b, int32_t combine, void* stream);
+MG_API int mg_apply_markers(int32_t dim, const int32_t* res, int32_t* cell_type, const float* phi, int32_t strict,
+                            void* stream);
+MG_API int mg_init_boundary(int32_t dim, const int32_t* res, int32_t* cell_type, void* stream);
+
 /* ---- the step after the solve ---------------------------------------------
  * FluidSimulator.apply_pressure (fluid_simulator.py:193-214): the ghost-fluid
  * pressure-gradient update of the MAC velocity, u_k[I] -= scale (p[I] -

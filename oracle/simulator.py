@@ -36,6 +36,9 @@ def _lib():
         lib.ors_build_st_A.argtypes = [ii, vp, ii, ii, vp, dd, dd, dd, dd, vp, vp]
         lib.ors_update_chi.argtypes = [ii, vp, vp, dd, dd, vp]
         lib.ors_update_H.argtypes = [ii, vp, ii, vp, vp, ff, vp]
+        lib.ors_level_set_shape.argtypes = [ii, vp, vp, ff, ii, vp, vp, ii]
+        lib.ors_apply_markers.argtypes = [ii, vp, vp, vp, ii]
+        lib.ors_init_boundary.argtypes = [ii, vp, vp]
         _c = lib
     return _c
 
@@ -172,3 +175,28 @@ def update_H(psi, H_ext, dx):
         _lib().ors_update_H(ps.ndim, _res(ps.shape), k, ps.ctypes.data, h.ctypes.data, float(dx), H.ctypes.data)
         out.append(H)
     return out
+
+
+def level_set_shape(shape, dx, sphere, a, b, phi=None):
+    """LevelSet.initialize_with_aabb (sphere False: box [a, b]) or
+    initialize_with_sphere (centre a, radius b); with phi: union (min)."""
+    out = np.zeros(shape, np.float32) if phi is None else _f32(phi)
+    A = (ctypes.c_float * 3)(*(list(a) + [0.0] * (3 - len(a))))
+    bb = [b] if sphere else list(b)
+    B = (ctypes.c_float * 3)(*(bb + [0.0] * (3 - len(bb))))
+    _lib().ors_level_set_shape(len(shape), _res(shape), out.ctypes.data, float(dx), int(bool(sphere)), A, B,
+                               int(phi is not None))
+    return out
+
+
+def apply_markers(cell_type, phi, strict=False):
+    ct = np.ascontiguousarray(cell_type, dtype=np.int32).copy()
+    ph = _f32(phi)
+    _lib().ors_apply_markers(ct.ndim, _res(ct.shape), ct.ctypes.data, ph.ctypes.data, int(bool(strict)))
+    return ct
+
+
+def init_boundary(cell_type):
+    ct = np.ascontiguousarray(cell_type, dtype=np.int32).copy()
+    _lib().ors_init_boundary(ct.ndim, _res(ct.shape), ct.ctypes.data)
+    return ct

@@ -325,6 +325,65 @@ void ors_build_potential_A(int dim, const int* res, int level, const float* chi,
   }
 }
 
+// LevelSet.initialize_with_aabb / initialize_with_sphere (level_set.py:40-64)
+// at cell centres (I + 0.5) dx; combine: min with the existing phi.
+void ors_level_set_shape(int dim, const int* res, float* phi, float dx, int sphere, const float* a, const float* b,
+                         int combine) {
+  const G g = make(dim, res);
+  for (int64_t i = 0; i < g.cells(); ++i) {
+    int c[3];
+    coords(g, i, c);
+    float x[3];
+    for (int k = 0; k < dim; ++k) x[k] = ((float)c[k] + 0.5f) * dx;
+    float v;
+    if (sphere) {
+      float s = 0.0f;
+      for (int k = 0; k < dim; ++k) {
+        const float d = x[k] - a[k];
+        s = k == 0 ? d * d : s + d * d;
+      }
+      v = std::sqrt(s) - b[0];
+    } else {
+      bool inside = true;
+      for (int k = 0; k < dim; ++k) inside = inside && x[k] > a[k] && x[k] < b[k];
+      if (inside) {
+        v = std::fmax(a[0] - x[0], x[0] - b[0]);
+        for (int k = 1; k < dim; ++k) v = std::fmax(v, std::fmax(a[k] - x[k], x[k] - b[k]));
+      } else {
+        float s = 0.0f;
+        for (int k = 0; k < dim; ++k) {
+          const float p = x[k] < a[k] ? a[k] : (x[k] > b[k] ? b[k] : x[k]);
+          const float d = x[k] - p;
+          s = k == 0 ? d * d : s + d * d;
+        }
+        v = std::sqrt(s);
+      }
+    }
+    phi[i] = combine ? std::fmin(phi[i], v) : v;
+  }
+}
+
+// FluidSimulator.apply_markers (fluid_simulator.py:151-159).
+void ors_apply_markers(int dim, const int* res, int32_t* ct, const float* phi, int strict) {
+  const G g = make(dim, res);
+  for (int64_t i = 0; i < g.cells(); ++i)
+    if (ct[i] != SOLID) ct[i] = AIR;
+  for (int64_t i = 0; i < g.cells(); ++i)
+    if (ct[i] != SOLID && (strict ? phi[i] < 0.0f : phi[i] <= 0.0f)) ct[i] = FLUID;
+}
+
+// FluidSimulator.init_boundary (fluid_simulator.py:337-341).
+void ors_init_boundary(int dim, const int* res, int32_t* ct) {
+  const G g = make(dim, res);
+  for (int64_t i = 0; i < g.cells(); ++i) {
+    int c[3];
+    coords(g, i, c);
+    bool edge = false;
+    for (int k = 0; k < dim; ++k) edge = edge || c[k] == 0 || c[k] + 1 == g.n[k];
+    if (edge) ct[i] = SOLID;
+  }
+}
+
 // update_magnetic_susceptibility: chi = k (1 - theta(phi)).
 void ors_update_chi(int dim, const int* res, const float* phi, double k, double eps, float* chi) {
   const G g = make(dim, res);

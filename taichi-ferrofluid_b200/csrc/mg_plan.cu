@@ -20,6 +20,7 @@
 #include "mg_pcg.cuh"
 #include "mg_fused_host.cuh"
 #include "mg_strategies.cuh"
+#include "mg_levelset.cuh"
 
 using namespace mg;
 
@@ -791,6 +792,59 @@ int mg_build_potential_A(mg_plan_t* P, int32_t level, const float* chi, double d
                                                                   (float)(1.0 / dxl), g.n[0], g.n[1], g.n[2]);
   CKL("k_build_potential_A");
   P->prepared = false;
+  return MG_OK;
+}
+
+// ---- labels and level set from shapes (no plan: a grid shape suffices) ------
+
+namespace {
+int grid_of(int32_t dim, const int32_t* res, Geom* g) {
+  if ((dim != 2 && dim != 3) || !res) return bad("dim / res");
+  g->dim = dim;
+  for (int k = 0; k < 3; ++k) g->n[k] = k < dim ? res[k] : 1;
+  for (int k = 0; k < dim; ++k)
+    if (g->n[k] < 1) return bad("res");
+  g->count = (long long)g->n[0] * g->n[1] * g->n[2];
+  return MG_OK;
+}
+int blocks_of(long long n) {
+  long long b = (n + 255) / 256;
+  return (int)(b < 1 ? 1 : (b > 148 * 16 ? 148 * 16 : b));
+}
+}  // namespace
+
+int mg_level_set_shape(int32_t dim, const int32_t* res, float* phi, float dx, int32_t sphere, const float* a,
+                       const float* b, int32_t combine, void* stream) {
+  Geom g;
+  if (int rc = grid_of(dim, res, &g)) return rc;
+  if (!phi || !a || !b || !(dx > 0.0f)) return bad("phi / shape / dx");
+  float A[3] = {0.0f, 0.0f, 0.0f}, B[3] = {0.0f, 0.0f, 0.0f};
+  for (int k = 0; k < dim; ++k) A[k] = a[k];
+  if (sphere) B[0] = b[0];
+  else
+    for (int k = 0; k < dim; ++k) B[k] = b[k];
+  k_ls_shape<<<blocks_of(g.count), 256, 0, S(stream)>>>(g, phi, dx, sphere ? 1 : 0, A[0], A[1], A[2], B[0], B[1],
+                                                          B[2], combine);
+  CKL("k_ls_shape");
+  return MG_OK;
+}
+
+int mg_apply_markers(int32_t dim, const int32_t* res, int32_t* cell_type, const float* phi, int32_t strict,
+                     void* stream) {
+  Geom g;
+  if (int rc = grid_of(dim, res, &g)) return rc;
+  if (!cell_type || !phi) return bad("cell_type / phi");
+  k_apply_markers<<<blocks_of(g.count), 256, 0, S(stream)>>>(g, cell_type, phi, strict);
+  CKL("k_apply_markers");
+  return MG_OK;
+}
+
+int mg_init_boundary(int32_t dim, const int32_t* res, int32_t* cell_type, void* stream) {
+  Geom g;
+  if (int rc = grid_of(dim, res, &g)) return rc;
+  if (!cell_type) return bad("cell_type");
+  k_init_boundary<<<blocks_of(g.count), 256, 0, S(stream)>>>(g, cell_type);
+  CKL("k_init_boundary");
   return MG_OK;
 }
 

@@ -110,3 +110,35 @@ def update_magnetic_field(solver, H_ext, dx, H, psi=None):
                                               mg_lib.ptr(h2), float(dx), Hs[0].data_ptr(), Hs[1].data_ptr(),
                                               mg_lib.ptr(o2), solver._s()), "mg_update_magnetic_field")
     solver._keep_H = (He, ps)
+
+
+def _grid(cell_type):
+    dim = cell_type.dim()
+    return dim, (mg_lib.ctypes.c_int32 * 3)(*(list(cell_type.shape) + [1] * (3 - dim)))
+
+
+def _i32(t, what):
+    if t.dtype != torch.int32 or not t.is_contiguous() or not t.is_cuda:
+        raise ValueError(f"{what} must be a contiguous int32 CUDA tensor (the simulator's labels)")
+    return t
+
+
+def apply_markers(cell_type, phi, strict=False):
+    """fluid_simulator.py:151-159, in place: non-SOLID cells AIR, then FLUID
+    where phi <= 0 (strict: phi < 0, the benchmark scenes' rule)."""
+    ct = _i32(cell_type, "cell_type")
+    ph = _f32(phi, ct.device)
+    if ph.shape != ct.shape:
+        raise ValueError("phi and cell_type shapes differ")
+    dim, res = _grid(ct)
+    lib = mg_lib.load()
+    check(lib.mg_apply_markers(dim, res, ct.data_ptr(), ph.data_ptr(), int(bool(strict)),
+                               mg_lib.stream_ptr(ct.device)), "mg_apply_markers")
+
+
+def init_boundary(cell_type):
+    """fluid_simulator.py:337-341, in place: SOLID on the outermost ring."""
+    ct = _i32(cell_type, "cell_type")
+    dim, res = _grid(ct)
+    lib = mg_lib.load()
+    check(lib.mg_init_boundary(dim, res, ct.data_ptr(), mg_lib.stream_ptr(ct.device)), "mg_init_boundary")

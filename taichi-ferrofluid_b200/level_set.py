@@ -1,0 +1,44 @@
+"""Drop-in ``LevelSet`` (level_set.py:10-64): the signed-distance field phi
+of the fluid at cell centres, with the reference's initialisers.
+
+``phi`` is a float32 CUDA tensor of shape res; ``eps`` = 5 dx is the
+interface half width of the smoothed Heaviside / delta (level_set.py:22),
+used by the volume-control, magnetic and surface-tension Strategies.
+``initialize_with_aabb`` / ``initialize_with_sphere`` write phi on the device
+(``mg_level_set_shape``); ``union=True`` takes the minimum with the current
+phi instead of overwriting it (several shapes).
+"""
+import torch
+
+import mg_lib
+from mg_lib import check
+
+
+class LevelSet:
+    def __init__(self, dim, res, dx, real=float, device=None):
+        if real not in (float, torch.float32, "f32", "float32"):
+            raise ValueError("the level set is float32 (real=float)")
+        self.dim = int(dim)
+        self.res = tuple(int(v) for v in res)[: self.dim]
+        self.dx = float(dx)
+        self.real = real
+        self.device = torch.device(device) if device is not None else torch.device("cuda", torch.cuda.current_device())
+        self.phi = torch.zeros(self.res, dtype=torch.float32, device=self.device)
+        self.eps = 5 * self.dx  # the "thickness" of the interface
+        self.lib = mg_lib.load()
+        self._res = (mg_lib.ctypes.c_int32 * 3)(*(list(self.res) + [1] * (3 - self.dim)))
+
+    def _shape(self, sphere, a, b, union):
+        f3 = mg_lib.ctypes.c_float * 3
+        A = f3(*([float(v) for v in a][: self.dim] + [0.0] * (3 - self.dim)))
+        B = f3(float(b), 0.0, 0.0) if sphere else f3(*([float(v) for v in b][: self.dim] + [0.0] * (3 - self.dim)))
+        check(self.lib.mg_level_set_shape(self.dim, self._res, self.phi.data_ptr(), self.dx, int(sphere), A, B,
+                                          int(bool(union)), mg_lib.stream_ptr(self.device)), "mg_level_set_shape")
+
+    def initialize_with_aabb(self, x0, x1, union=False):
+        """level_set.py:56-59: signed distance to the box [x0, x1]."""
+        self._shape(False, x0, x1, union)
+
+    def initialize_with_sphere(self, x0, r, union=False):
+        """level_set.py:61-64: signed distance to the sphere of centre x0, radius r."""
+        self._shape(True, x0, r, union)

@@ -1,0 +1,72 @@
+"""Labels and the level set from shapes on the CUDA path (LevelSet
+initialisers, apply_markers, init_boundary) against the oracle, bit-exact,
+and the serving scene rebuilt from them."""
+import numpy as np
+import pytest
+
+from test_oracle_strategies import FLUID, AIR, SOLID
+
+pytestmark = pytest.mark.gpu
+
+
+def _bits(t):
+    return t.detach().cpu().numpy().view(np.uint32)
+
+
+@pytest.mark.parametrize("dim,n", [(2, 96), (3, 40)])
+def test_level_set_shapes_bit_exact(dim, n):
+    from level_set import LevelSet
+    from oracle import simulator as S
+    ls = LevelSet(dim, (n,) * dim, 1.0 / n)
+    lo, hi = [0.2, 0.1, 0.3][:dim], [0.6, 0.7, 0.55][:dim]
+    c = [0.5, 0.45, 0.5][:dim]
+    ls.initialize_with_aabb(lo, hi)
+    ref = S.level_set_shape((n,) * dim, 1.0 / n, False, lo, hi)
+    np.testing.assert_array_equal(_bits(ls.phi), ref.view(np.uint32))
+    ls.initialize_with_sphere(c, 0.23, union=True)
+    ref = S.level_set_shape((n,) * dim, 1.0 / n, True, c, 0.23, phi=ref)
+    np.testing.assert_array_equal(_bits(ls.phi), ref.view(np.uint32))
+    ls.initialize_with_sphere(c, 0.23)
+    np.testing.assert_array_equal(_bits(ls.phi), S.level_set_shape((n,) * dim, 1.0 / n, True, c, 0.23).view(np.uint32))
+
+
+@pytest.mark.parametrize("strict", [False, True])
+def test_labels_bit_exact(strict):
+    import torch
+    import fluid_ops
+    from oracle import simulator as S
+    rng = np.random.default_rng(8)
+    phi = rng.uniform(-1, 1, (24, 20, 16)).astype(np.float32)
+    phi[rng.random(phi.shape) < 0.05] = 0.0
+    ct0 = rng.integers(0, 3, phi.shape).astype(np.int32)
+    ct = torch.from_numpy(ct0).cuda()
+    fluid_ops.init_boundary(ct)
+    fluid_ops.apply_markers(ct, torch.from_numpy(phi).cuda(), strict=strict)
+    ref = S.apply_markers(S.init_boundary(ct0), phi, strict=strict)
+    np.testing.assert_array_equal(ct.cpu().numpy(), ref)
+
+
+def test_serving_scene_matches_oracle():
+    """mg_serve.DeviceScene: the session's shapes moved by the substep shift."""
+    import torch
+    import mg_scenes
+    from mg_serve import DeviceScene
+    from oracle import simulator as S
+    for spec in mg_scenes.serving_sessions(seed=4, n_sessions=4, substeps=5):
+        if spec["side"] > 160:
+            continue
+        sc = DeviceScene(spec, torch.device("cuda"))
+        for step in (0, 3):
+            sc.build(step)
+            shift = 0.5 * step * sc.dx * sc.direction
+            phi = None
+            for kind, centre, size in sc.shapes:
+                c = [float(centre[k] + shift[k]) for k in range(sc.dim)]
+                if kind == "box":
+                    phi = S.level_set_shape(sc.res, sc.dx, False, [c[k] - float(size[k]) for k in range(sc.dim)],
+                                            [c[k] + float(size[k]) for k in range(sc.dim)], phi=phi)
+                else:
+                    phi = S.level_set_shape(sc.res, sc.dx, True, c, float(size), phi=phi)
+            np.testing.assert_array_equal(_bits(sc.phi), phi.view(np.uint32))
+            ct = S.apply_markers(S.init_boundary(np.full(sc.res, AIR, np.int32)), phi, strict=True)
+            np.testing.assert_array_equal(sc.ct.cpu().numpy(), ct)

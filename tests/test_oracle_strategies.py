@@ -302,3 +302,39 @@ def test_update_H_and_chi():
     phi = np.array([[-1.0, -0.1, 0.0, 0.1, 1.0]], np.float32)
     chi = S.update_chi(phi, 5.0, eps)
     np.testing.assert_allclose(chi, [[5.0, 5.0, 2.5, 0.0, 0.0]], atol=1e-6)
+
+
+# ---------------------------------------------------------------- labels, phi
+def test_level_set_shapes_match_float64_sdf():
+    """LevelSet.initialize_with_aabb / _sphere (level_set.py:40-64) against the
+    float64 signed distances of mg_scenes, and the union rule."""
+    import mg_scenes
+    for dim, n in ((2, 48), (3, 20)):
+        dx = 1.0 / n
+        g = (np.arange(n) + 0.5) * dx
+        pts = np.meshgrid(*([g] * dim), indexing="ij")
+        lo, hi = np.array([0.2, 0.1, 0.3][:dim]), np.array([0.6, 0.7, 0.55][:dim])
+        box = S.level_set_shape((n,) * dim, dx, False, lo, hi)
+        np.testing.assert_allclose(box, mg_scenes.box_sdf(pts, lo, hi), atol=1e-6)
+        c = np.array([0.5, 0.45, 0.5][:dim])
+        sph = S.level_set_shape((n,) * dim, dx, True, c, 0.23)
+        np.testing.assert_allclose(sph, mg_scenes.sphere_sdf(pts, c, 0.23), atol=1e-6)
+        both = S.level_set_shape((n,) * dim, dx, True, c, 0.23, phi=box)
+        np.testing.assert_array_equal(both, np.minimum(box, sph))
+
+
+def test_apply_markers_and_boundary():
+    n = 10
+    phi = np.linspace(-1, 1, n * n, dtype=np.float32).reshape(n, n)
+    phi[3, 3] = 0.0
+    ct = S.init_boundary(np.full((n, n), AIR, np.int32))
+    assert (ct[0] == SOLID).all() and (ct[:, -1] == SOLID).all() and (ct[1:-1, 1:-1] == AIR).all()
+    le = S.apply_markers(ct, phi)
+    lt = S.apply_markers(ct, phi, strict=True)
+    inner = ct != SOLID
+    np.testing.assert_array_equal(le[inner], np.where(phi[inner] <= 0, FLUID, AIR))
+    np.testing.assert_array_equal(lt[inner], np.where(phi[inner] < 0, FLUID, AIR))
+    assert le[3, 3] == FLUID and lt[3, 3] == AIR
+    np.testing.assert_array_equal(le[~inner], SOLID)
+    again = S.apply_markers(np.where(inner, FLUID, ct).astype(np.int32), phi)  # stale labels are reset
+    np.testing.assert_array_equal(again, le)
