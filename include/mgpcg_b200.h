@@ -264,6 +264,19 @@ MG_API int mg_apply_markers(int32_t dim, const int32_t* res, int32_t* cell_type,
                             void* stream);
 MG_API int mg_init_boundary(int32_t dim, const int32_t* res, int32_t* cell_type, void* stream);
 
+/* FastSweepingLevelSet.redistance (level_set.py:260-334): valid = -1 and
+ * target_surface (level_set.py:66-86: cells beside a sign change get the
+ * interpolated distance to it, valid 0), then repeat_times rounds of the fast
+ * sweeping propagation (each round: forward and backward sweeps along the
+ * last axis, then along each slower axis; upwind Eikonal update of
+ * level_set.py:88-112), then phi = phi_temp.  phi_temp (float32) and valid
+ * (int32) are caller scratch of shape res.  The lines of a sweep run in
+ * parallel and read each other's cells while they change, as the
+ * reference's do, so the propagated values can differ in the last bits from
+ * run to run.  Every axis needs at least 2 cells. */
+MG_API int mg_level_set_redistance(int32_t dim, const int32_t* res, float* phi, float* phi_temp, int32_t* valid,
+                                   double dx, int32_t repeat_times, void* stream);
+
 /* ---- the step after the solve ---------------------------------------------
  * FluidSimulator.apply_pressure (fluid_simulator.py:193-214): the ghost-fluid
  * pressure-gradient update of the MAC velocity, u_k[I] -= scale (p[I] -

@@ -39,6 +39,7 @@ def _lib():
         lib.ors_level_set_shape.argtypes = [ii, vp, vp, ff, ii, vp, vp, ii]
         lib.ors_apply_markers.argtypes = [ii, vp, vp, vp, ii]
         lib.ors_init_boundary.argtypes = [ii, vp, vp]
+        lib.ors_redistance.argtypes = [ii, vp, vp, dd, ii, vp, vp]
         _c = lib
     return _c
 
@@ -200,3 +201,13 @@ def init_boundary(cell_type):
     ct = np.ascontiguousarray(cell_type, dtype=np.int32).copy()
     _lib().ors_init_boundary(ct.ndim, _res(ct.shape), ct.ctypes.data)
     return ct
+
+
+def redistance(phi, dx, repeat_times=2):
+    """FastSweepingLevelSet.redistance, lines swept one after another;
+    returns (phi, valid)."""
+    ph = _f32(phi)
+    valid = np.zeros(ph.shape, np.int32)
+    _lib().ors_redistance(ph.ndim, _res(ph.shape), ph.ctypes.data, float(dx), int(repeat_times), None,
+                          valid.ctypes.data)
+    return ph, valid

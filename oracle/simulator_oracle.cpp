@@ -30,6 +30,8 @@
 
 #include <cmath>
 #include <cstdint>
+#include <utility>
+#include <vector>
 
 namespace {
 
@@ -381,6 +383,95 @@ void ors_init_boundary(int dim, const int* res, int32_t* ct) {
     bool edge = false;
     for (int k = 0; k < dim; ++k) edge = edge || c[k] == 0 || c[k] + 1 == g.n[k];
     if (edge) ct[i] = SOLID;
+  }
+}
+
+// FastSweepingLevelSet.redistance (level_set.py:260-334) with target_surface
+// (:66-86) and update_from_neighbor (:88-112).  ts.sign is GLSL's sign
+// (-1, 0, +1) as in taichi_glsl (a dependency absent here, version
+// unpinned).  The reference runs the lines of a sweep in parallel; this runs
+// them one after another in index order, which is one of its schedules.
+// The reference bounds the forward axis-0 sweeps by res[1]
+// (level_set.py:303, 322); here res[0] (the same on square / cubic grids).
+static float gsign(float x) { return x > 0.0f ? 1.0f : (x < 0.0f ? -1.0f : 0.0f); }
+
+void ors_redistance(int dim, const int* res, float* phi, double dx, int repeat, float* temp_out, int32_t* valid_out) {
+  const G g = make(dim, res);
+  const int64_t n = g.cells();
+  std::vector<float> t(n);
+  std::vector<int32_t> valid(n, -1);
+  const float fdx = (float)dx, two_dx2 = (float)(2.0 * dx * dx), dx2 = (float)(dx * dx), third = (float)(1.0 / 3.0);
+  auto stride = [&](int k) -> int64_t { return k == 0 ? (int64_t)g.n[1] * g.n[2] : (k == 1 ? g.n[2] : 1); };
+  for (int64_t i = 0; i < n; ++i) {  // target_surface
+    int c[3];
+    coords(g, i, c);
+    const float p = phi[i], sp = gsign(p);
+    bool change = false;
+    float est = 1e20f;
+    for (int k = 0; k < dim; ++k)
+      for (int s = -1; s <= 1; s += 2) {
+        const int v = c[k] + s;
+        if (v < 0 || v >= g.n[k]) continue;
+        const float q = phi[i + s * stride(k)];
+        if (sp != gsign(q)) {
+          const float theta = p / (p - q);
+          const float est0 = sp * theta * fdx;
+          est = std::fabs(est0) < std::fabs(est) ? est0 : est;
+          change = true;
+        }
+      }
+    t[i] = change ? est : 1e20f;
+    if (change) valid[i] = 0;
+  }
+  auto update = [&](int64_t i, const int c[3]) {
+    float nb[3];
+    for (int k = 0; k < dim; ++k) {
+      const int64_t st = stride(k);
+      if (c[k] == 0 || (c[k] < g.n[k] - 1 && std::fabs(t[i + st]) < std::fabs(t[i - st]))) nb[k] = std::fabs(t[i + st]);
+      else nb[k] = std::fabs(t[i - st]);
+    }
+    for (int a = 0; a < dim - 1; ++a)
+      for (int b = 0; b < dim - 1 - a; ++b)
+        if (nb[b] > nb[b + 1]) std::swap(nb[b], nb[b + 1]);
+    float d = nb[0] + fdx;
+    if (d > nb[1]) {
+      const float e = nb[1] - nb[0];
+      d = 0.5f * (nb[0] + nb[1] + std::sqrt(two_dx2 - e * e));
+      if (dim == 3 && d > nb[2]) {
+        const float s = nb[0] + nb[1] + nb[2];
+        const float q = nb[0] * nb[0] + nb[1] * nb[1] + nb[2] * nb[2] - dx2;
+        d = third * (s + std::sqrt(std::fmax(0.0f, s * s - 3.0f * q)));
+      }
+    }
+    if (std::fabs(d) < std::fabs(t[i])) t[i] = d * gsign(phi[i]);
+  };
+  for (int r = 0; r < repeat; ++r)
+    for (int axis = dim - 1; axis >= 0; --axis)
+      for (int dir = 1; dir >= -1; dir -= 2) {
+        int oa[2], no = 0;
+        for (int k = 0; k < dim; ++k)
+          if (k != axis) oa[no++] = k;
+        const int64_t lines = n / g.n[axis];
+        const int nfast = no == 2 ? g.n[oa[1]] : 1;
+        for (int64_t l = 0; l < lines; ++l) {
+          int c[3] = {0, 0, 0};
+          if (no == 2) {
+            c[oa[0]] = (int)(l / nfast);
+            c[oa[1]] = (int)(l % nfast);
+          } else {
+            c[oa[0]] = (int)l;
+          }
+          for (int step = 0; step < g.n[axis]; ++step) {
+            c[axis] = dir > 0 ? step : g.n[axis] - 1 - step;
+            const int64_t i = g.at(c[0], c[1], c[2]);
+            if (valid[i] == -1) update(i, c);
+          }
+        }
+      }
+  for (int64_t i = 0; i < n; ++i) {
+    phi[i] = t[i];
+    if (temp_out) temp_out[i] = t[i];
+    if (valid_out) valid_out[i] = valid[i];
   }
 }
 

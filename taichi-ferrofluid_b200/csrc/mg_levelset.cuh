@@ -84,4 +84,107 @@ __global__ void k_init_boundary(Geom g, int32_t* __restrict__ ct) {
   }
 }
 
+// ---------------------------------------------------------------------------
+// FastSweepingLevelSet.redistance (level_set.py:260-334)
+// ---------------------------------------------------------------------------
+
+// GLSL sign (taichi_glsl's ts.sign): -1, 0 or +1.
+__device__ __forceinline__ float gsign(float x) { return x > 0.0f ? 1.0f : (x < 0.0f ? -1.0f : 0.0f); }
+
+// valid.fill(-1) and LevelSet.target_surface (level_set.py:66-86): cells with
+// a neighbour of the other sign get phi_temp = the signed distance to the
+// linearly interpolated crossing nearest to them (valid 0); the others 1e20.
+__global__ void k_target_surface(Geom g, const float* __restrict__ phi, float* __restrict__ phi_temp,
+                                 int32_t* __restrict__ valid, float dx) {
+  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < g.count;
+       i += (long long)gridDim.x * blockDim.x) {
+    int c[3];
+    g.coords(i, c);
+    const float p = phi[i], sp = gsign(p);
+    bool change = false;
+    float est = 1e20f;
+    for (int k = 0; k < g.dim; ++k)
+      for (int s = -1; s <= 1; s += 2) {
+        const int v = c[k] + s;
+        if (v < 0 || v >= g.n[k]) continue;
+        const float q = phi[i + s * g.stride(k)];
+        if (sp != gsign(q)) {
+          const float theta = __fdiv_rn(p, __fsub_rn(p, q));
+          const float est0 = __fmul_rn(__fmul_rn(sp, theta), dx);
+          est = fabsf(est0) < fabsf(est) ? est0 : est;
+          change = true;
+        }
+      }
+    phi_temp[i] = change ? est : 1e20f;
+    valid[i] = change ? 0 : -1;
+  }
+}
+
+// LevelSet.update_from_neighbor (level_set.py:88-112): the upwind Eikonal
+// update of cell i from the smaller |phi_temp| neighbour per axis, sorted;
+// dx1 = dx, two_dx2 = 2 dx^2, dx2 = dx^2, third = 1/3 folded on the host.
+__device__ __forceinline__ float eikonal(const Geom& g, const float* t, long long i, const int c[3], float dx1,
+                                         float two_dx2, float dx2, float third) {
+  float nb[3];
+  for (int k = 0; k < g.dim; ++k) {
+    const long long st = g.stride(k);
+    const float up = c[k] + 1 < g.n[k] ? fabsf(t[i + st]) : 0.0f;
+    if (c[k] == 0 || (c[k] < g.n[k] - 1 && up < fabsf(t[i - st]))) nb[k] = fabsf(t[i + st]);
+    else nb[k] = fabsf(t[i - st]);
+  }
+  for (int a = 0; a < g.dim - 1; ++a)  // the reference's bubble sort
+    for (int b = 0; b < g.dim - 1 - a; ++b)
+      if (nb[b] > nb[b + 1]) {
+        const float tmp = nb[b];
+        nb[b] = nb[b + 1];
+        nb[b + 1] = tmp;
+      }
+  float d = __fadd_rn(nb[0], dx1);
+  if (d > nb[1]) {
+    const float e = __fsub_rn(nb[1], nb[0]);
+    d = __fmul_rn(0.5f, __fadd_rn(__fadd_rn(nb[0], nb[1]), __fsqrt_rn(__fsub_rn(two_dx2, __fmul_rn(e, e)))));
+    if (g.dim == 3 && d > nb[2]) {
+      const float s = __fadd_rn(__fadd_rn(nb[0], nb[1]), nb[2]);
+      const float q = __fsub_rn(
+          __fadd_rn(__fadd_rn(__fmul_rn(nb[0], nb[0]), __fmul_rn(nb[1], nb[1])), __fmul_rn(nb[2], nb[2])), dx2);
+      const float inner = fmaxf(0.0f, __fsub_rn(__fmul_rn(s, s), __fmul_rn(3.0f, q)));
+      d = __fmul_rn(third, __fadd_rn(s, __fsqrt_rn(inner)));
+    }
+  }
+  return d;
+}
+
+// One sweep of FastSweepingLevelSet.propagate (level_set.py:284-327): every
+// line along `axis` is walked by one thread, forward (dir > 0) or backward,
+// applying propagate_update (level_set.py:267-271) to its cells in order.
+// As in the reference, the lines run in parallel and read each other's cells
+// while they change.  Consecutive threads take consecutive cells of the
+// fastest other axis.
+__global__ void k_fs_sweep(Geom g, int axis, int dir, float* phi_temp, const float* __restrict__ phi,
+                           const int32_t* __restrict__ valid, float dx1, float two_dx2, float dx2, float third) {
+  int oa[2], no = 0;
+  for (int k = 0; k < g.dim; ++k)
+    if (k != axis) oa[no++] = k;
+  const long long lines = g.count / g.n[axis];
+  const int nfast = no == 2 ? g.n[oa[1]] : 1;
+  for (long long l = (long long)blockIdx.x * blockDim.x + threadIdx.x; l < lines;
+       l += (long long)gridDim.x * blockDim.x) {
+    int c[3] = {0, 0, 0};
+    if (no == 2) {
+      c[oa[0]] = (int)(l / nfast);
+      c[oa[1]] = (int)(l % nfast);
+    } else {
+      c[oa[0]] = (int)l;
+    }
+    const int n = g.n[axis];
+    for (int step = 0; step < n; ++step) {
+      c[axis] = dir > 0 ? step : n - 1 - step;
+      const long long i = g.index(c[0], c[1], c[2]);
+      if (valid[i] != -1) continue;
+      const float d = eikonal(g, phi_temp, i, c, dx1, two_dx2, dx2, third);
+      if (fabsf(d) < fabsf(phi_temp[i])) phi_temp[i] = __fmul_rn(d, gsign(phi[i]));
+    }
+  }
+}
+
 }  // namespace mg

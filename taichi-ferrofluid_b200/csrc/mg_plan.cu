@@ -848,6 +848,29 @@ int mg_init_boundary(int32_t dim, const int32_t* res, int32_t* cell_type, void* 
   return MG_OK;
 }
 
+int mg_level_set_redistance(int32_t dim, const int32_t* res, float* phi, float* phi_temp, int32_t* valid,
+                            double dx, int32_t repeat_times, void* stream) {
+  Geom g;
+  if (int rc = grid_of(dim, res, &g)) return rc;
+  for (int k = 0; k < dim; ++k)
+    if (g.n[k] < 2) return bad("every axis needs at least 2 cells");
+  if (!phi || !phi_temp || !valid || !(dx > 0.0) || repeat_times < 0) return bad("inputs");
+  cudaStream_t s = S(stream);
+  k_target_surface<<<blocks_of(g.count), 256, 0, s>>>(g, phi, phi_temp, valid, (float)dx);
+  CKL("k_target_surface");
+  const float dx1 = (float)dx, two_dx2 = (float)(2.0 * dx * dx), dx2 = (float)(dx * dx), third = (float)(1.0 / 3.0);
+  for (int t = 0; t < repeat_times; ++t)
+    for (int axis = dim - 1; axis >= 0; --axis)
+      for (int dir = 1; dir >= -1; dir -= 2) {
+        const long long lines = g.count / g.n[axis];
+        const int blocks = (int)((lines + 127) / 128);
+        k_fs_sweep<<<blocks, 128, 0, s>>>(g, axis, dir, phi_temp, phi, valid, dx1, two_dx2, dx2, third);
+        CKL("k_fs_sweep");
+      }
+  CK(cudaMemcpyAsync(phi, phi_temp, g.count * sizeof(float), cudaMemcpyDeviceToDevice, s));
+  return MG_OK;
+}
+
 int mg_update_susceptibility(mg_plan_t* P, const float* phi, double k, float eps, float* chi, void* stream) {
   NEED_BOUND(P);
   if (!phi || !chi || !(eps > 0.0f)) return bad("phi / chi / eps");

@@ -42,3 +42,23 @@ class LevelSet:
     def initialize_with_sphere(self, x0, r, union=False):
         """level_set.py:61-64: signed distance to the sphere of centre x0, radius r."""
         self._shape(True, x0, r, union)
+
+
+class FastSweepingLevelSet(LevelSet):
+    """FastSweepingLevelSet (level_set.py:258-334): ``redistance()`` turns phi
+    into a signed distance with the same zero set - the crossing distances of
+    the cells beside the interface (target_surface), then ``repeat_times``
+    rounds of fast sweeping (H. Zhao, Math. Comp. 74:603-627, 2005) along each
+    axis; ``valid`` and ``phi_temp`` are the reference's scratch fields."""
+
+    def __init__(self, dim, res, dx, real=float, device=None):
+        super().__init__(dim, res, dx, real, device)
+        self.repeat_times = 2
+        self.valid = torch.full(self.res, -1, dtype=torch.int32, device=self.device)
+        self.phi_temp = torch.empty(self.res, dtype=torch.float32, device=self.device)
+
+    def redistance(self):
+        """level_set.py:329-333."""
+        check(self.lib.mg_level_set_redistance(self.dim, self._res, self.phi.data_ptr(), self.phi_temp.data_ptr(),
+                                               self.valid.data_ptr(), self.dx, int(self.repeat_times),
+                                               mg_lib.stream_ptr(self.device)), "mg_level_set_redistance")

@@ -91,6 +91,7 @@ _SIGS = {
     "mg_level_set_shape": (ctypes.c_int, [_i32, _vp, _vp, _f32, _i32, _vp, _vp, _i32, _vp]),
     "mg_apply_markers": (ctypes.c_int, [_i32, _vp, _vp, _vp, _i32, _vp]),
     "mg_init_boundary": (ctypes.c_int, [_i32, _vp, _vp, _vp]),
+    "mg_level_set_redistance": (ctypes.c_int, [_i32, _vp, _vp, _vp, _vp, _f64, _i32, _vp]),
     "mg_apply_pressure": (ctypes.c_int, [_vp, _vp, _vp, _vp, _vp, _vp, _vp, _f32, _f32, _i32, _f32, _vp]),
     "mg_apply_magnetic_force": (ctypes.c_int, [_vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _f32, _f32, _f32,
                                                _vp]),
