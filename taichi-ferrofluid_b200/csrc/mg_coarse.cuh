@@ -20,7 +20,16 @@ namespace mg {
 //   sx: (STO, the whole-domain stored form) the dim coupling arrays Ax[k],
 //       0 on the ring, so a neighbour outside a level reads as z = 0, Ax = 0.
 
-constexpr int kBottomPerThread = 2;  // cached bottom cells per colour and thread
+// Cached bottom cells per colour and thread, and the block size (compile-time
+// tuning constants).
+#ifndef MG_BOTTOM_CELLS_PER_THREAD
+#define MG_BOTTOM_CELLS_PER_THREAD 1  // 8 warps for 8^3: 37 vs 48 us a V-cycle at 128^3 (2 cells)
+#endif
+#ifndef MG_COARSE_THREADS
+#define MG_COARSE_THREADS 1024
+#endif
+constexpr int kBottomPerThread = MG_BOTTOM_CELLS_PER_THREAD;
+constexpr int kCoarseThreads = MG_COARSE_THREADS;
 
 struct CoarseArgs {
   int dim, nlev, pre_post, bottom;
@@ -132,7 +141,7 @@ __device__ void coarse_smooth(const CoarseArgs& A, int l, int phase, float* zm, 
 }
 
 template <typename ST, bool STO = false>
-__global__ void __launch_bounds__(1024) k_coarse(CoarseArgs A) {
+__global__ void __launch_bounds__(kCoarseThreads) k_coarse(CoarseArgs A) {
   static_assert(!STO || sizeof(ST) == 4, "the stored form runs on float32 grids");
   extern __shared__ __align__(16) unsigned char smem[];
   float* zm = (float*)smem;
@@ -203,10 +212,10 @@ __global__ void __launch_bounds__(1024) k_coarse(CoarseArgs A) {
     const PGeom g = pgeom(A, L - 1);
     const float ms = -A.s[L - 1];
     const int cntb = colour_count(g, dim);
-    // participants: two cells of a colour per thread where that fits, in
-    // whole warps; they synchronise among themselves on barrier 1 while the
+    // participants: kBottomPerThread cells of a colour per thread where that
+    // fits, in whole warps; they synchronise among themselves on barrier 1 while the
     // other warps wait at the block barrier below
-    int pt = ((cntb + 1) / 2 + 31) & ~31;
+    int pt = ((cntb + kBottomPerThread - 1) / kBottomPerThread + 31) & ~31;
     if (pt > (int)blockDim.x || (cntb + pt - 1) / pt > kBottomPerThread) pt = blockDim.x;
     if (cntb <= kBottomPerThread * pt) {
       if ((int)threadIdx.x < pt) {

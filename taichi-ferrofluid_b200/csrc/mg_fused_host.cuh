@@ -28,7 +28,10 @@ struct TileShape {
 
 // Launch shape of the streamed levels: a tile of ty x tx columns per block,
 // k planes per pipeline step.
-constexpr TileShape kTile3 = {32, 16, 512, 2};
+#ifndef MG_TILE3_K
+#define MG_TILE3_K 2
+#endif
+constexpr TileShape kTile3 = {32, 16, 512, MG_TILE3_K};
 constexpr TileShape kTile2 = {128, 1, 128, 4};
 // the whole-domain stored form stages twice the bytes per cell: a smaller
 // tile keeps two blocks per SM
@@ -161,7 +164,7 @@ inline bool make_fused_plan(const Level* lv, int L, int dim, int pre_post, int b
   F->coarse_smem = (size_t)off * (12 + (F->sto ? 4 * dim : 0));
   // 1024 threads: the upper coarse levels' phases take 1-2 cells per thread;
   // the bottom level's cells sit in the first threads' registers
-  F->coarse_threads = 1024;
+  F->coarse_threads = kCoarseThreads;
   F->valid = true;
   return true;
 }

@@ -157,6 +157,56 @@ __global__ void __launch_bounds__(kRedThreads) k_zr(Level L, Control* ctl, doubl
   }
 }
 
+// float32 grids whose cell count is a multiple of 4: the same two kernels
+// over 4-cell groups (16-byte loads of z, r, p; 4 labels in one load).
+__device__ __forceinline__ bool fluid_lane(uint32_t t4, int e) { return ((t4 >> (8 * e)) & 0xffu) == (uint32_t)FLUID; }
+
+__global__ void k_update_p4(Level L, float* __restrict__ p, const Control* ctl) {
+  const float beta = ctl->beta;
+  const int groups = (int)(L.g.count >> 2);
+  for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < groups; q += gridDim.x * blockDim.x) {
+    const uint32_t t4 = __ldg(reinterpret_cast<const uint32_t*>(L.type) + q);
+    if (t4 == 0x02020202u || t4 == 0x01010101u) continue;  // no FLUID lane (all SOLID / all AIR)
+    const float4 z = __ldg(reinterpret_cast<const float4*>((const float*)L.z) + q);
+    float4 pv = reinterpret_cast<float4*>(p)[q];
+    const float zv[4] = {z.x, z.y, z.z, z.w};
+    float* pp = reinterpret_cast<float*>(&pv);
+#pragma unroll
+    for (int e = 0; e < 4; ++e)
+      if (fluid_lane(t4, e)) pp[e] = __fadd_rn(zv[e], __fmul_rn(beta, pp[e]));
+    reinterpret_cast<float4*>(p)[q] = pv;
+  }
+}
+
+__global__ void __launch_bounds__(kRedThreads) k_zr4(Level L, Control* ctl, double* partials, int mode) {
+  __shared__ double sh[32];
+  const int groups = (int)(L.g.count >> 2);
+  double acc = 0.0;
+  for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < groups; q += gridDim.x * blockDim.x) {
+    const uint32_t t4 = __ldg(reinterpret_cast<const uint32_t*>(L.type) + q);
+    if (t4 == 0x02020202u || t4 == 0x01010101u) continue;
+    const float4 z = __ldg(reinterpret_cast<const float4*>((const float*)L.z) + q);
+    const float4 r = __ldg(reinterpret_cast<const float4*>((const float*)L.r) + q);
+    if (fluid_lane(t4, 0)) acc += (double)z.x * (double)r.x;
+    if (fluid_lane(t4, 1)) acc += (double)z.y * (double)r.y;
+    if (fluid_lane(t4, 2)) acc += (double)z.z * (double)r.z;
+    if (fluid_lane(t4, 3)) acc += (double)z.w * (double)r.w;
+  }
+  double tot;
+  if (last_block_total<kRedThreads>(acc, partials, &ctl->counter[1], sh, &tot) && threadIdx.x == 0) {
+    if (mode == 0) {
+      ctl->old_zTr = tot;
+      if (ctl->max_iters == 0) ctl->run = 0;
+    } else {
+      ctl->new_zTr = tot;
+      ctl->beta = (float)(tot / (ctl->old_zTr + ctl->eps));
+      ctl->old_zTr = tot;
+      ctl->iter += 1;
+      if (ctl->max_iters != -1 && ctl->iter >= ctl->max_iters) ctl->run = 0;
+    }
+  }
+}
+
 // compute_Ap (mgpcg.py:218-224) + reduce(p, Ap) + alpha = zTr / (pAp + eps).
 __global__ void __launch_bounds__(kRedThreads) k_Ap_alpha(Level L, const float* __restrict__ p,
                                                           float* __restrict__ Ap, Control* ctl,
@@ -173,6 +223,79 @@ __global__ void __launch_bounds__(kRedThreads) k_Ap_alpha(Level L, const float* 
     v = __fadd_rn(v, nbr_sum_f32(L, p, i, c));
     Ap[i] = v;
     acc += (double)p[i] * (double)v;
+  }
+  double tot;
+  if (last_block_total<kRedThreads>(acc, partials, &ctl->counter[2], sh, &tot) && threadIdx.x == 0) {
+    ctl->pAp = tot;
+    ctl->alpha = (float)(ctl->old_zTr / (tot + ctl->eps));
+  }
+}
+
+// k_Ap_alpha over groups of 4 consecutive cells along the fastest axis (its
+// extent a multiple of 4): 16-byte loads of labels, Adiag, p, the stored
+// couplings and the neighbour rows; the neighbour sum of nbr_sum_f32 per
+// cell in the same order.  Ap written on FLUID cells only.
+__global__ void __launch_bounds__(kRedThreads) k_Ap_alpha4(Level L, const float* __restrict__ p,
+                                                           float* __restrict__ Ap, Control* ctl, double* partials,
+                                                           int force = 0) {
+  if (!ctl->run && !force) return;
+  __shared__ double sh[32];
+  const int dim = L.g.dim;
+  const int nx = L.g.n[dim - 1];
+  const int groups = (int)(L.g.count >> 2);
+  const float4 z4 = make_float4(0.f, 0.f, 0.f, 0.f);
+  double acc = 0.0;
+  for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < groups; q += gridDim.x * blockDim.x) {
+    const int i = q << 2;
+    const uint32_t t4 = __ldg(reinterpret_cast<const uint32_t*>(L.type) + q);
+    if (t4 == 0x02020202u || t4 == 0x01010101u) continue;
+    const int x = i % nx, t = i / nx;
+    int c[2];
+    if (dim == 3) {
+      c[0] = t / L.g.n[1];
+      c[1] = t - c[0] * L.g.n[1];
+    } else {
+      c[0] = t;
+    }
+    const float4 pc = __ldg(reinterpret_cast<const float4*>(p + i));
+    const float4 ad = __ldg(reinterpret_cast<const float4*>(L.Adiag + i));
+    const float* axx = L.Ax[dim - 1];
+    const float4 xc = __ldg(reinterpret_cast<const float4*>(axx + i));
+    const float pxl = x > 0 ? __ldg(p + i - 1) : 0.0f, axl = x > 0 ? __ldg(axx + i - 1) : 0.0f;
+    const float pxr = x + 4 < nx ? __ldg(p + i + 4) : 0.0f;
+    float4 plo[2], phi_[2], alo[2], ahi[2];
+    bool has_lo[2], has_hi[2];
+    for (int k = 0; k < dim - 1; ++k) {
+      const int st = k == 0 ? (dim == 3 ? L.g.n[1] * nx : nx) : nx;
+      has_lo[k] = c[k] > 0;
+      has_hi[k] = c[k] + 1 < L.g.n[k];
+      plo[k] = has_lo[k] ? __ldg(reinterpret_cast<const float4*>(p + i - st)) : z4;
+      alo[k] = has_lo[k] ? __ldg(reinterpret_cast<const float4*>(L.Ax[k] + i - st)) : z4;
+      phi_[k] = has_hi[k] ? __ldg(reinterpret_cast<const float4*>(p + i + st)) : z4;
+      ahi[k] = __ldg(reinterpret_cast<const float4*>(L.Ax[k] + i));
+    }
+    const float pv[4] = {pc.x, pc.y, pc.z, pc.w}, av[4] = {ad.x, ad.y, ad.z, ad.w};
+    const float xv[4] = {xc.x, xc.y, xc.z, xc.w};
+#pragma unroll
+    for (int e = 0; e < 4; ++e) {
+      if (!fluid_lane(t4, e)) continue;
+      float ret = 0.0f;
+      for (int k = 0; k < dim - 1; ++k) {
+        const float* pl4 = reinterpret_cast<const float*>(&plo[k]);
+        const float* ph4 = reinterpret_cast<const float*>(&phi_[k]);
+        const float* al4 = reinterpret_cast<const float*>(&alo[k]);
+        const float* ah4 = reinterpret_cast<const float*>(&ahi[k]);
+        const float lo = has_lo[k] ? __fmul_rn(al4[e], pl4[e]) : 0.0f;
+        const float hi = has_hi[k] ? __fmul_rn(ah4[e], ph4[e]) : 0.0f;
+        ret = __fadd_rn(ret, __fadd_rn(lo, hi));
+      }
+      const float lo = x + e > 0 ? __fmul_rn(e == 0 ? axl : xv[e - 1], e == 0 ? pxl : pv[e - 1]) : 0.0f;
+      const float hi = x + e + 1 < nx ? __fmul_rn(xv[e], e == 3 ? pxr : pv[e + 1]) : 0.0f;
+      ret = __fadd_rn(ret, __fadd_rn(lo, hi));
+      const float v = __fadd_rn(__fmul_rn(av[e], pv[e]), ret);
+      Ap[i + e] = v;
+      acc += (double)pv[e] * (double)v;
+    }
   }
   double tot;
   if (last_block_total<kRedThreads>(acc, partials, &ctl->counter[2], sh, &tot) && threadIdx.x == 0) {
@@ -213,6 +336,82 @@ __global__ void __launch_bounds__(kRedThreads) k_Ap_alpha_uniform(Level L, const
     const float v = __fadd_rn(__fmul_rn(a, pi), ret);
     Ap[i] = v;
     acc += (double)pi * (double)v;
+  }
+  double tot;
+  if (last_block_total<kRedThreads>(acc, partials, &ctl->counter[2], sh, &tot) && threadIdx.x == 0) {
+    ctl->pAp = tot;
+    ctl->alpha = (float)(ctl->old_zTr / (tot + ctl->eps));
+  }
+}
+
+// k_Ap_alpha_uniform over groups of 4 consecutive cells along the fastest
+// axis (its extent a multiple of 4, as every fused plan has): 16-byte loads of
+// Adiag, p and the p rows of the other axes' neighbours, two scalar loads for
+// the x neighbours, 32-bit indices, several groups in flight per thread.  The
+// same float32 operations per cell in the same axis order; non-FLUID cells
+// keep their Ap (written only where Adiag != 0).
+__global__ void __launch_bounds__(kRedThreads) k_Ap_alpha_uniform4(Level L, const float* __restrict__ p,
+                                                                   float* __restrict__ Ap, float s, Control* ctl,
+                                                                   double* partials, int force = 0) {
+  if (!ctl->run && !force) return;
+  __shared__ double sh[32];
+  const float ms = -s;
+  const int dim = L.g.dim;
+  const int nx = L.g.n[dim - 1];
+  const int groups = (int)(L.g.count >> 2);
+  double acc = 0.0;
+  for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < groups; q += gridDim.x * blockDim.x) {
+    const int i = q << 2;
+    const float4 a = __ldg(reinterpret_cast<const float4*>(L.Adiag + i));
+    if (a.x == 0.0f && a.y == 0.0f && a.z == 0.0f && a.w == 0.0f) continue;
+    const int x = i % nx, t = i / nx;
+    int c[2];  // coordinates of the slower axes
+    if (dim == 3) {
+      c[0] = t / L.g.n[1];
+      c[1] = t - c[0] * L.g.n[1];
+    } else {
+      c[0] = t;
+    }
+    const float4 pc = __ldg(reinterpret_cast<const float4*>(p + i));
+    const float pxl = x > 0 ? __ldg(p + i - 1) : 0.0f;
+    const float pxr = x + 4 < nx ? __ldg(p + i + 4) : 0.0f;
+    float4 lo4[2], hi4[2];
+    bool has_lo[2], has_hi[2];
+    for (int k = 0; k < dim - 1; ++k) {
+      const int st = k == 0 ? (dim == 3 ? L.g.n[1] * nx : nx) : nx;
+      has_lo[k] = c[k] > 0;
+      has_hi[k] = c[k] + 1 < L.g.n[k];
+      lo4[k] = has_lo[k] ? __ldg(reinterpret_cast<const float4*>(p + i - st)) : make_float4(0.f, 0.f, 0.f, 0.f);
+      hi4[k] = has_hi[k] ? __ldg(reinterpret_cast<const float4*>(p + i + st)) : make_float4(0.f, 0.f, 0.f, 0.f);
+    }
+    const float av[4] = {a.x, a.y, a.z, a.w};
+    const float pv[4] = {pc.x, pc.y, pc.z, pc.w};
+    float out[4];
+#pragma unroll
+    for (int e = 0; e < 4; ++e) {
+      float ret = 0.0f;
+      for (int k = 0; k < dim - 1; ++k) {
+        const float* l4 = reinterpret_cast<const float*>(&lo4[k]);
+        const float* h4 = reinterpret_cast<const float*>(&hi4[k]);
+        const float lo = has_lo[k] ? __fmul_rn(ms, l4[e]) : 0.0f;
+        const float hi = has_hi[k] ? __fmul_rn(ms, h4[e]) : 0.0f;
+        ret = __fadd_rn(ret, __fadd_rn(lo, hi));
+      }
+      const float pl = e == 0 ? pxl : pv[e - 1];
+      const float pr = e == 3 ? pxr : pv[e + 1];
+      const float lo = x + e > 0 ? __fmul_rn(ms, pl) : 0.0f;
+      const float hi = x + e + 1 < nx ? __fmul_rn(ms, pr) : 0.0f;
+      ret = __fadd_rn(ret, __fadd_rn(lo, hi));
+      out[e] = __fadd_rn(__fmul_rn(av[e], pv[e]), ret);
+      if (av[e] != 0.0f) acc += (double)pv[e] * (double)out[e];
+    }
+    if (a.x != 0.0f && a.y != 0.0f && a.z != 0.0f && a.w != 0.0f) {
+      *reinterpret_cast<float4*>(Ap + i) = make_float4(out[0], out[1], out[2], out[3]);
+    } else {
+#pragma unroll
+      for (int e = 0; e < 4; ++e)
+        if (av[e] != 0.0f) Ap[i + e] = out[e];
+    }
   }
   double tot;
   if (last_block_total<kRedThreads>(acc, partials, &ctl->counter[2], sh, &tot) && threadIdx.x == 0) {

@@ -344,6 +344,21 @@ template <typename ST>
 int launch_zr_p(mg_plan* P, bool prologue, cudaStream_t s) {
   const Level& L0 = P->lv[0];
   float* p = fptr(P, MG_FIELD_P);
+  if (sizeof(ST) == 4 && P->geom[0].count % 4 == 0) {  // float32: 4-cell groups
+    const int eb = grid_for(P, P->geom[0].count / 4);
+    if (prologue) {
+      k_update_p4<<<eb, 256, 0, s>>>(L0, p, P->ctl);
+      CKL("k_update_p4");
+      k_zr4<<<P->red_blocks, kRedThreads, 0, s>>>(L0, P->ctl, P->partials, 0);
+      CKL("k_zr4");
+    } else {
+      k_zr4<<<P->red_blocks, kRedThreads, 0, s>>>(L0, P->ctl, P->partials, 1);
+      CKL("k_zr4");
+      k_update_p4<<<eb, 256, 0, s>>>(L0, p, P->ctl);
+      CKL("k_update_p4");
+    }
+    return MG_OK;
+  }
   if (prologue) {
     k_update_p<ST><<<P->ew_blocks[0], 256, 0, s>>>(L0, p, P->ctl);
     CKL("k_update_p");
@@ -368,6 +383,9 @@ int launch_zr_p_any(mg_plan* P, bool prologue, cudaStream_t s) {
 
 // The CG step after z is known: Ap, alpha, x/r update, r.r, the test, and
 // (mixed form) the true-residual refresh.  Stages 3 and 4 of mg_launch_stage.
+// The fastest axis of level 0 holds whole 4-cell groups (16-byte vectors).
+bool x_by4(const mg_plan* P) { return P->geom[0].n[P->d.dim - 1] % 4 == 0; }
+
 int launch_cg_tail(mg_plan* P, cudaStream_t s, int which) {
   const Level& L0 = P->lv[0];
   float* b = fptr(P, MG_FIELD_B);
@@ -377,8 +395,12 @@ int launch_cg_tail(mg_plan* P, cudaStream_t s, int which) {
   const int RB = P->red_blocks;
   const bool refresh = P->d.refresh_every > 0;
   if (which & 1) {
-    if (P->fp.valid && !P->fp.sto)  // label-uniform level 0
+    if (P->fp.valid && !P->fp.sto && x_by4(P))  // label-uniform level 0, 4-cell groups
+      k_Ap_alpha_uniform4<<<RB, kRedThreads, 0, s>>>(L0, p, Ap, P->offdiag[0], P->ctl, P->partials);
+    else if (P->fp.valid && !P->fp.sto)
       k_Ap_alpha_uniform<<<RB, kRedThreads, 0, s>>>(L0, p, Ap, P->offdiag[0], P->ctl, P->partials);
+    else if (x_by4(P))
+      k_Ap_alpha4<<<RB, kRedThreads, 0, s>>>(L0, p, Ap, P->ctl, P->partials);
     else
       k_Ap_alpha<<<RB, kRedThreads, 0, s>>>(L0, p, Ap, P->ctl, P->partials);
     CKL("k_Ap_alpha");
@@ -1185,9 +1207,15 @@ int mg_launch_stage(mg_plan_t* P, int32_t stage, int32_t level, void* stream) {
       return e == cudaSuccess ? MG_OK : set_err("launch_coarse", e);
     }
     case 3:
-      if (P->fp.valid && !P->fp.sto)
+      if (P->fp.valid && !P->fp.sto && x_by4(P))
+        k_Ap_alpha_uniform4<<<P->red_blocks, kRedThreads, 0, s>>>(L0, fptr(P, MG_FIELD_P), fptr(P, MG_FIELD_AP),
+                                                                  P->offdiag[0], P->ctl, P->partials, 1);
+      else if (P->fp.valid && !P->fp.sto)
         k_Ap_alpha_uniform<<<P->red_blocks, kRedThreads, 0, s>>>(L0, fptr(P, MG_FIELD_P), fptr(P, MG_FIELD_AP),
                                                                  P->offdiag[0], P->ctl, P->partials, 1);
+      else if (x_by4(P))
+        k_Ap_alpha4<<<P->red_blocks, kRedThreads, 0, s>>>(L0, fptr(P, MG_FIELD_P), fptr(P, MG_FIELD_AP), P->ctl,
+                                                          P->partials, 1);
       else
         k_Ap_alpha<<<P->red_blocks, kRedThreads, 0, s>>>(L0, fptr(P, MG_FIELD_P), fptr(P, MG_FIELD_AP), P->ctl,
                                                          P->partials, 1);
