@@ -277,6 +277,34 @@ MG_API int mg_init_boundary(int32_t dim, const int32_t* res, int32_t* cell_type,
 MG_API int mg_level_set_redistance(int32_t dim, const int32_t* res, float* phi, float* phi_temp, int32_t* valid,
                                    double dx, int32_t repeat_times, void* stream);
 
+/* ---- the velocity steps around the projection (plan-free) ----------------
+ * Velocity components vel0..2 are MAC face arrays of shape res + e_k; cell
+ * arrays have shape res.
+ * mg_advect_quantity: FluidSimulator.advect_quantity (fluid_simulator.py:
+ * 216-236): every face of every component (and, if phi_out is not NULL, the
+ * level set) is traced back through the velocity with the midpoint rule and
+ * sampled from its source (utils.sample) into the *_out arrays, which must not
+ * alias the inputs; update_quantity is the caller's copy back.
+ * mg_extrapolate_velocity: FluidSimulator.extrap_velocity for one axis
+ * (fluid_simulator.py:244-272): faces beside a FLUID cell are valid, then
+ * `iterations` rounds (10 in the reference) give each invalid face with valid
+ * neighbours in its 3^d box their mean.  u_tmp, valid, valid_tmp are caller
+ * scratch of the face shape; a neighbour outside the face array is invalid.
+ * mg_enforce_boundary: FluidSimulator.enforce_boundary (fluid_simulator.py:
+ * 168-174): zero velocity on both faces of every SOLID cell.
+ * mg_add_gravity: FluidSimulator.add_gravity (fluid_simulator.py:160-166):
+ * u_k += g_k dt for every nonzero component g_k. */
+MG_API int mg_advect_quantity(int32_t dim, const int32_t* res, const float* vel0, const float* vel1,
+                              const float* vel2, const float* phi, float* phi_out, float* vel0_out, float* vel1_out,
+                              float* vel2_out, float dx, float dt, void* stream);
+MG_API int mg_extrapolate_velocity(int32_t dim, const int32_t* res, int32_t axis, float* vel, float* vel_tmp,
+                                   int32_t* valid, int32_t* valid_tmp, const int32_t* cell_type, int32_t iterations,
+                                   void* stream);
+MG_API int mg_enforce_boundary(int32_t dim, const int32_t* res, float* vel0, float* vel1, float* vel2,
+                               const int32_t* cell_type, void* stream);
+MG_API int mg_add_gravity(int32_t dim, const int32_t* res, float* vel0, float* vel1, float* vel2, double g0,
+                          double g1, double g2, float dt, void* stream);
+
 /* ---- the step after the solve ---------------------------------------------
  * FluidSimulator.apply_pressure (fluid_simulator.py:193-214): the ghost-fluid
  * pressure-gradient update of the MAC velocity, u_k[I] -= scale (p[I] -

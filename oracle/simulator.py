@@ -40,6 +40,10 @@ def _lib():
         lib.ors_apply_markers.argtypes = [ii, vp, vp, vp, ii]
         lib.ors_init_boundary.argtypes = [ii, vp, vp]
         lib.ors_redistance.argtypes = [ii, vp, vp, dd, ii, vp, vp]
+        lib.ors_advect.argtypes = [ii, vp, vp, ii, vp, vp, ff, ff]
+        lib.ors_extrapolate.argtypes = [ii, vp, ii, vp, vp, ii, vp]
+        lib.ors_enforce_boundary.argtypes = [ii, vp, vp, vp]
+        lib.ors_add_gravity.argtypes = [ii, vp, vp, vp, ff]
         _c = lib
     return _c
 
@@ -211,3 +215,39 @@ def redistance(phi, dx, repeat_times=2):
     _lib().ors_redistance(ph.ndim, _res(ph.shape), ph.ctypes.data, float(dx), int(repeat_times), None,
                           valid.ctypes.data)
     return ph, valid
+
+
+def advect(velocity, src, field, dx, dt):
+    """FluidSimulator.advect of one field (field -1: cell field, k: faces of axis k)."""
+    u = [_f32(v) for v in velocity]
+    sr = _f32(src)
+    shape = tuple(s - (k == field) for k, s in enumerate(sr.shape)) if field >= 0 else sr.shape
+    out = np.zeros(sr.shape, np.float32)
+    _lib().ors_advect(len(shape), _res(shape), _ptrs(u), int(field), sr.ctypes.data, out.ctypes.data, float(dx),
+                      float(dt))
+    return out
+
+
+def extrapolate(u_k, k, cell_type, iterations=10):
+    """FluidSimulator.extrap_velocity for axis k; returns (u_k, valid)."""
+    ct = np.ascontiguousarray(cell_type, dtype=np.int32)
+    u = _f32(u_k)
+    valid = np.zeros(u.shape, np.int32)
+    _lib().ors_extrapolate(ct.ndim, _res(ct.shape), int(k), u.ctypes.data, ct.ctypes.data, int(iterations),
+                           valid.ctypes.data)
+    return u, valid
+
+
+def enforce_boundary(velocity, cell_type):
+    ct = np.ascontiguousarray(cell_type, dtype=np.int32)
+    u = [_f32(v) for v in velocity]
+    _lib().ors_enforce_boundary(ct.ndim, _res(ct.shape), _ptrs(u), ct.ctypes.data)
+    return u
+
+
+def add_gravity(velocity, gravity, dt):
+    u = [_f32(v) for v in velocity]
+    shape = tuple(s - (k == 0) for k, s in enumerate(u[0].shape))
+    g = (ctypes.c_double * 3)(*(list(gravity) + [0.0] * (3 - len(gravity))))
+    _lib().ors_add_gravity(len(shape), _res(shape), _ptrs(u), g, float(dt))
+    return u

@@ -475,6 +475,122 @@ void ors_redistance(int dim, const int* res, float* phi, double dx, int repeat, 
   }
 }
 
+// FluidSimulator.vel_interp (fluid_simulator.py:138-143).
+static void vel_interp(const float* const* u, const G& g, float dx, const float* pos, float* v) {
+  for (int q = 0; q < g.dim; ++q) {
+    float s[3] = {0.0f, 0.0f, 0.0f};
+    for (int a = 0; a < g.dim; ++a) s[a] = pos[a] / dx - (a == q ? 0.0f : 0.5f);
+    v[q] = sample(u[q], faces(g, q), s);
+  }
+}
+
+// FluidSimulator.advect (fluid_simulator.py:216-221) of one field: field -1
+// the cell field (offset 0.5), field k the faces of axis k (0.5 (1 - e_k)).
+void ors_advect(int dim, const int* res, const float* const* u, int field, const float* src, float* dst, float dx,
+                float dt) {
+  const G g = make(dim, res);
+  const G f = field < 0 ? g : faces(g, field);
+  const float half_dt = 0.5f * dt;
+  for (int64_t i = 0; i < f.cells(); ++i) {
+    int c[3];
+    coords(f, i, c);
+    float off[3], pos[3], v[3], mid[3], p0[3], s[3] = {0.0f, 0.0f, 0.0f};
+    for (int a = 0; a < 3; ++a) off[a] = (a >= dim || (field >= 0 && a == field)) ? 0.0f : 0.5f;
+    for (int a = 0; a < dim; ++a) pos[a] = ((float)c[a] + off[a]) * dx;
+    vel_interp(u, g, dx, pos, v);
+    for (int a = 0; a < dim; ++a) mid[a] = pos[a] - v[a] * half_dt;
+    vel_interp(u, g, dx, mid, v);
+    for (int a = 0; a < dim; ++a) p0[a] = pos[a] - v[a] * dt;
+    for (int a = 0; a < dim; ++a) s[a] = p0[a] / dx - off[a];
+    dst[i] = sample(src, f, s);
+  }
+}
+
+// FluidSimulator.extrap_velocity for axis k (fluid_simulator.py:244-272): the
+// valid faces, then `iterations` rounds of diffuse_quantity (a neighbour
+// outside the face array is invalid).
+void ors_extrapolate(int dim, const int* res, int k, float* u, const int32_t* ct, int iterations, int32_t* valid_out) {
+  const G g = make(dim, res);
+  const G f = faces(g, k);
+  const int64_t n = f.cells();
+  std::vector<int32_t> valid(n), vt(n);
+  std::vector<float> backup(n);
+  for (int64_t i = 0; i < n; ++i) {
+    int c[3];
+    coords(f, i, c);
+    int c1[3] = {c[0], c[1], c[2]};
+    c1[k] -= 1;
+    const bool fl1 = c1[k] >= 0 && ct[g.at(c1[0], c1[1], c1[2])] == FLUID;
+    const bool fl0 = c[k] < g.n[k] && ct[g.at(c[0], c[1], c[2])] == FLUID;
+    valid[i] = (fl1 || fl0) ? 1 : 0;
+  }
+  const int span = dim == 3 ? 27 : 9;
+  for (int it = 0; it < iterations; ++it) {
+    for (int64_t i = 0; i < n; ++i) {
+      backup[i] = u[i];
+      vt[i] = valid[i];
+    }
+    for (int64_t i = 0; i < n; ++i) {
+      if (vt[i] != 0) continue;
+      int c[3];
+      coords(f, i, c);
+      float tot = 0.0f;
+      int cnt = 0;
+      for (int o = 0; o < span; ++o) {
+        int m[3] = {c[0], c[1], c[2]};
+        if (dim == 3) {
+          m[0] += o / 9 - 1;
+          m[1] += (o / 3) % 3 - 1;
+          m[2] += o % 3 - 1;
+        } else {
+          m[0] += o / 3 - 1;
+          m[1] += o % 3 - 1;
+        }
+        bool in = true;
+        for (int a = 0; a < dim; ++a) in = in && m[a] >= 0 && m[a] < f.n[a];
+        if (!in) continue;
+        const int64_t j = f.at(m[0], m[1], m[2]);
+        if (vt[j] == 1) {
+          tot += backup[j];
+          ++cnt;
+        }
+      }
+      if (cnt > 0) {
+        u[i] = tot / (float)cnt;
+        valid[i] = 1;
+      }
+    }
+  }
+  if (valid_out)
+    for (int64_t i = 0; i < n; ++i) valid_out[i] = valid[i];
+}
+
+// FluidSimulator.enforce_boundary (fluid_simulator.py:168-174).
+void ors_enforce_boundary(int dim, const int* res, float* const* u, const int32_t* ct) {
+  const G g = make(dim, res);
+  for (int64_t i = 0; i < g.cells(); ++i) {
+    if (ct[i] != SOLID) continue;
+    int c[3];
+    coords(g, i, c);
+    for (int k = 0; k < dim; ++k) {
+      const G f = faces(g, k);
+      u[k][f.at(c[0], c[1], c[2])] = 0.0f;
+      u[k][f.at(c[0] + (k == 0), c[1] + (k == 1), c[2] + (k == 2))] = 0.0f;
+    }
+  }
+}
+
+// FluidSimulator.add_gravity (fluid_simulator.py:160-166).
+void ors_add_gravity(int dim, const int* res, float* const* u, const double* grav, float dt) {
+  const G g = make(dim, res);
+  for (int k = 0; k < dim; ++k) {
+    if (grav[k] == 0.0) continue;
+    const G f = faces(g, k);
+    const float gdt = (float)grav[k] * dt;
+    for (int64_t i = 0; i < f.cells(); ++i) u[k][i] = u[k][i] + gdt;
+  }
+}
+
 // update_magnetic_susceptibility: chi = k (1 - theta(phi)).
 void ors_update_chi(int dim, const int* res, const float* phi, double k, double eps, float* chi) {
   const G g = make(dim, res);

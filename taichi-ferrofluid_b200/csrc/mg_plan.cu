@@ -13,6 +13,7 @@
 #include <map>
 #include <mutex>
 #include <new>
+#include <utility>
 #include <vector>
 
 #include "mg_common.cuh"
@@ -21,6 +22,7 @@
 #include "mg_fused_host.cuh"
 #include "mg_strategies.cuh"
 #include "mg_levelset.cuh"
+#include "mg_advect.cuh"
 
 using namespace mg;
 
@@ -890,6 +892,91 @@ int mg_level_set_redistance(int32_t dim, const int32_t* res, float* phi, float* 
         CKL("k_fs_sweep");
       }
   CK(cudaMemcpyAsync(phi, phi_temp, g.count * sizeof(float), cudaMemcpyDeviceToDevice, s));
+  return MG_OK;
+}
+
+// ---- advection, extrapolation, gravity, solid boundary (plan-free) --------
+
+int mg_advect_quantity(int32_t dim, const int32_t* res, const float* u0, const float* u1, const float* u2,
+                       const float* phi, float* phi_out, float* u0_out, float* u1_out, float* u2_out, float dx,
+                       float dt, void* stream) {
+  Geom g;
+  if (int rc = grid_of(dim, res, &g)) return rc;
+  const float* u[3] = {u0, u1, u2};
+  float* uo[3] = {u0_out, u1_out, u2_out};
+  for (int k = 0; k < dim; ++k)
+    if (!u[k] || !uo[k]) return bad("velocity");
+  if (phi_out && !phi) return bad("phi");
+  if (!(dx > 0.0f)) return bad("dx");
+  Vel V;
+  for (int k = 0; k < 3; ++k) V.u[k] = k < dim ? u[k] : nullptr;
+  if (phi_out) {
+    k_advect<<<blocks_of(g.count), 256, 0, S(stream)>>>(g, -1, V, phi, phi_out, dx, dt);
+    CKL("k_advect");
+  }
+  for (int k = 0; k < dim; ++k) {
+    const long long nf = g.count / g.n[k] * (g.n[k] + 1);
+    k_advect<<<blocks_of(nf), 256, 0, S(stream)>>>(g, k, V, u[k], uo[k], dx, dt);
+    CKL("k_advect");
+  }
+  return MG_OK;
+}
+
+int mg_extrapolate_velocity(int32_t dim, const int32_t* res, int32_t k, float* u, float* u_tmp, int32_t* valid,
+                            int32_t* valid_tmp, const int32_t* cell_type, int32_t iterations, void* stream) {
+  Geom g;
+  if (int rc = grid_of(dim, res, &g)) return rc;
+  if (k < 0 || k >= dim) return bad("axis");
+  if (!u || !u_tmp || !valid || !valid_tmp || !cell_type || iterations < 0) return bad("inputs");
+  cudaStream_t s = S(stream);
+  const long long nf = g.count / g.n[k] * (g.n[k] + 1);
+  k_mark_valid<<<blocks_of(nf), 256, 0, s>>>(g, k, cell_type, valid);
+  CKL("k_mark_valid");
+  float* a = u;
+  float* b = u_tmp;
+  int32_t* va = valid;
+  int32_t* vb = valid_tmp;
+  for (int it = 0; it < iterations; ++it) {
+    k_diffuse<<<blocks_of(nf), 256, 0, s>>>(g, k, a, b, va, vb);
+    CKL("k_diffuse");
+    std::swap(a, b);
+    std::swap(va, vb);
+  }
+  if (a != u) {  // an odd round count ends in the scratch buffers
+    CK(cudaMemcpyAsync(u, a, nf * sizeof(float), cudaMemcpyDeviceToDevice, s));
+    CK(cudaMemcpyAsync(valid, va, nf * sizeof(int32_t), cudaMemcpyDeviceToDevice, s));
+  }
+  return MG_OK;
+}
+
+int mg_enforce_boundary(int32_t dim, const int32_t* res, float* u0, float* u1, float* u2, const int32_t* cell_type,
+                        void* stream) {
+  Geom g;
+  if (int rc = grid_of(dim, res, &g)) return rc;
+  float* u[3] = {u0, u1, u2};
+  for (int k = 0; k < dim; ++k)
+    if (!u[k]) return bad("velocity");
+  if (!cell_type) return bad("cell_type");
+  Vel V;
+  for (int k = 0; k < 3; ++k) V.u[k] = k < dim ? u[k] : nullptr;
+  k_enforce_boundary<<<blocks_of(g.count), 256, 0, S(stream)>>>(g, V, cell_type);
+  CKL("k_enforce_boundary");
+  return MG_OK;
+}
+
+int mg_add_gravity(int32_t dim, const int32_t* res, float* u0, float* u1, float* u2, double g0, double g1, double g2,
+                   float dt, void* stream) {
+  Geom g;
+  if (int rc = grid_of(dim, res, &g)) return rc;
+  float* u[3] = {u0, u1, u2};
+  const double gv[3] = {g0, g1, g2};
+  for (int k = 0; k < dim; ++k) {
+    if (gv[k] == 0.0) continue;  // the reference skips zero components (ti.static)
+    if (!u[k]) return bad("velocity");
+    const long long nf = g.count / g.n[k] * (g.n[k] + 1);
+    k_add_gravity<<<blocks_of(nf), 256, 0, S(stream)>>>(g, k, u[k], (float)gv[k], dt);
+    CKL("k_add_gravity");
+  }
   return MG_OK;
 }
 

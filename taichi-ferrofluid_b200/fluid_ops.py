@@ -142,3 +142,83 @@ def init_boundary(cell_type):
     dim, res = _grid(ct)
     lib = mg_lib.load()
     check(lib.mg_init_boundary(dim, res, ct.data_ptr(), mg_lib.stream_ptr(ct.device)), "mg_init_boundary")
+
+
+# ---- the velocity steps around the projection ----------------------------------
+def _vel_grid(velocity):
+    dim = len(velocity)
+    shape = [int(s) - (k == 0) for k, s in enumerate(velocity[0].shape)]
+    return dim, shape, (mg_lib.ctypes.c_int32 * 3)(*(shape + [1] * (3 - dim)))
+
+
+def _check_faces(fields, shape, what):
+    for k, f in enumerate(fields):
+        exp = list(shape)
+        exp[k] += 1
+        if tuple(f.shape) != tuple(exp) or f.dtype != torch.float32 or not f.is_contiguous() or not f.is_cuda:
+            raise ValueError(f"{what}[{k}] must be a contiguous float32 CUDA tensor of shape {tuple(exp)}")
+
+
+def advect_quantity(velocity, velocity_backup, dx, dt, phi=None, phi_temp=None):
+    """fluid_simulator.py:223-231: velocity_backup[k] (and phi_temp, when phi
+    is given) = the semi-Lagrangian (midpoint) advection of velocity[k] (phi)
+    through velocity."""
+    dim, shape, res = _vel_grid(velocity)
+    _check_faces(velocity, shape, "velocity")
+    _check_faces(velocity_backup, shape, "velocity_backup")
+    if (phi is None) != (phi_temp is None):
+        raise ValueError("phi and phi_temp go together")
+    u = [velocity[k].data_ptr() for k in range(dim)] + [None] * (3 - dim)
+    o = [velocity_backup[k].data_ptr() for k in range(dim)] + [None] * (3 - dim)
+    lib = mg_lib.load()
+    check(lib.mg_advect_quantity(dim, res, u[0], u[1], u[2], mg_lib.ptr(phi), mg_lib.ptr(phi_temp), o[0], o[1], o[2],
+                                 float(dx), float(dt), mg_lib.stream_ptr(velocity[0].device)), "mg_advect_quantity")
+
+
+def update_quantity(velocity, velocity_backup, phi=None, phi_temp=None):
+    """fluid_simulator.py:233-237: copy the advected fields back."""
+    if phi is not None:
+        phi.copy_(phi_temp)
+    for v, b in zip(velocity, velocity_backup):
+        v.copy_(b)
+
+
+def extrap_velocity(velocity, cell_type, iterations=10):
+    """fluid_simulator.py:268-272: per axis, faces beside a FLUID cell are
+    valid and `iterations` rounds extend the velocity into the invalid faces
+    (the mean of the valid faces of the 3^d box)."""
+    dim, shape, res = _vel_grid(velocity)
+    _check_faces(velocity, shape, "velocity")
+    ct = _i32(cell_type, "cell_type")
+    lib = mg_lib.load()
+    st = mg_lib.stream_ptr(velocity[0].device)
+    for k in range(dim):
+        u = velocity[k]
+        tmp = torch.empty_like(u)
+        valid = torch.empty(u.shape, dtype=torch.int32, device=u.device)
+        valid_tmp = torch.empty_like(valid)
+        check(lib.mg_extrapolate_velocity(dim, res, k, u.data_ptr(), tmp.data_ptr(), valid.data_ptr(),
+                                          valid_tmp.data_ptr(), ct.data_ptr(), int(iterations), st),
+              "mg_extrapolate_velocity")
+
+
+def enforce_boundary(velocity, cell_type):
+    """fluid_simulator.py:168-174: zero velocity on the faces of SOLID cells."""
+    dim, shape, res = _vel_grid(velocity)
+    _check_faces(velocity, shape, "velocity")
+    ct = _i32(cell_type, "cell_type")
+    u = [velocity[k].data_ptr() for k in range(dim)] + [None] * (3 - dim)
+    lib = mg_lib.load()
+    check(lib.mg_enforce_boundary(dim, res, u[0], u[1], u[2], ct.data_ptr(), mg_lib.stream_ptr(ct.device)),
+          "mg_enforce_boundary")
+
+
+def add_gravity(velocity, gravity, dt):
+    """fluid_simulator.py:160-166: velocity[k] += gravity[k] dt (nonzero k)."""
+    dim, shape, res = _vel_grid(velocity)
+    _check_faces(velocity, shape, "velocity")
+    g = [float(v) for v in gravity] + [0.0] * (3 - len(gravity))
+    u = [velocity[k].data_ptr() for k in range(dim)] + [None] * (3 - dim)
+    lib = mg_lib.load()
+    check(lib.mg_add_gravity(dim, res, u[0], u[1], u[2], g[0], g[1], g[2], float(dt),
+                             mg_lib.stream_ptr(velocity[0].device)), "mg_add_gravity")

@@ -380,3 +380,85 @@ def test_redistance_restores_distance(dim, n):
             change |= sc
     np.testing.assert_array_equal(valid == 0, change)
     np.testing.assert_array_equal(out[change].view(np.uint32), est[change].astype(np.float32).view(np.uint32))
+
+
+# ---------------------------------------------------- advection, extrapolation
+def test_advect_identity_and_translation():
+    """advect (fluid_simulator.py:216-221): zero velocity leaves a field
+    unchanged (up to the f32 round trip (I + 0.5) dx / dx - 0.5, an ulp off I,
+    which mixes in neighbours with weights ~1e-7); a uniform velocity
+    translates a linear field."""
+    n, dx, dt = 24, 1.0 / 24, 0.01
+    rng = np.random.default_rng(1)
+    zero = [np.zeros((n + (k == 0), n + (k == 1)), np.float32) for k in range(2)]
+    f = rng.standard_normal((n, n)).astype(np.float32)
+    np.testing.assert_allclose(S.advect(zero, f, -1, dx, dt), f, rtol=0, atol=1e-5)
+    u0 = rng.standard_normal((n + 1, n)).astype(np.float32)
+    np.testing.assert_allclose(S.advect(zero, u0, 0, dx, dt), u0, rtol=0, atol=1e-5)
+    c = (0.7, -0.4)
+    vel = [np.full((n + (k == 0), n + (k == 1)), c[k], np.float32) for k in range(2)]
+    x, y = np.meshgrid((np.arange(n) + 0.5) * dx, (np.arange(n) + 0.5) * dx, indexing="ij")
+    lin = (2 * x + 3 * y).astype(np.float32)
+    out = S.advect(vel, lin, -1, dx, dt)
+    exact = 2 * (x - c[0] * dt) + 3 * (y - c[1] * dt)
+    np.testing.assert_allclose(out[2:-2, 2:-2], exact[2:-2, 2:-2], atol=1e-5)
+
+
+def test_extrapolate_matches_numpy():
+    """extrap_velocity (fluid_simulator.py:244-272) against a vectorised numpy
+    restatement of mark_valid and diffuse_quantity."""
+    rng = np.random.default_rng(3)
+    for dim, n in ((2, 20), (3, 10)):
+        ct = np.full((n,) * dim, AIR, np.int32)
+        ct[tuple(slice(n // 4, n // 2) for _ in range(dim))] = FLUID
+        for k in range(dim):
+            shp = tuple(n + (a == k) for a in range(dim))
+            u = rng.standard_normal(shp).astype(np.float32)
+            got, gvalid = S.extrapolate(u, k, ct, 10)
+            # numpy: faces beside FLUID are valid
+            pad = np.full(tuple(s + 2 for s in shp), False)
+            fl = ct == FLUID
+            lo = [slice(1, -1)] * dim
+            hi = [slice(1, -1)] * dim
+            valid = np.zeros(shp, bool)
+            sl_hi = tuple(slice(0, n) if a == k else slice(None) for a in range(dim))
+            sl_lo = tuple(slice(1, n + 1) if a == k else slice(None) for a in range(dim))
+            valid[sl_hi] |= fl
+            valid[sl_lo] |= fl
+            uu = u.copy()
+            for _ in range(10):
+                src, vs = uu.copy(), valid.copy()
+                ps = np.pad(src, 1)
+                pv = np.pad(vs, 1)
+                tot = np.zeros(shp, np.float32)
+                cnt = np.zeros(shp, np.int32)
+                for off in np.ndindex(*(3,) * dim):
+                    sl = tuple(slice(o, o + s) for o, s in zip(off, shp))
+                    tot = (tot + np.where(pv[sl], ps[sl], np.float32(0))).astype(np.float32)
+                    cnt += pv[sl]
+                fill = (~vs) & (cnt > 0)
+                with np.errstate(divide="ignore", invalid="ignore"):
+                    uu = np.where(fill, (tot / cnt.astype(np.float32)).astype(np.float32), uu)
+                valid = vs | fill
+            np.testing.assert_array_equal(gvalid.astype(bool), valid)
+            np.testing.assert_array_equal(got.view(np.uint32), uu.view(np.uint32))
+
+
+def test_boundary_and_gravity():
+    n = 8
+    rng = np.random.default_rng(4)
+    ct = S.init_boundary(np.full((n, n), AIR, np.int32))
+    vel = [rng.standard_normal((n + (k == 0), n + (k == 1))).astype(np.float32) for k in range(2)]
+    out = S.enforce_boundary(vel, ct)
+    solid = ct == SOLID
+    for k in range(2):
+        lo = tuple(slice(0, n) if a == k else slice(None) for a in range(2))
+        hi = tuple(slice(1, n + 1) if a == k else slice(None) for a in range(2))
+        touched = np.zeros(out[k].shape, bool)
+        touched[lo] |= solid
+        touched[hi] |= solid
+        np.testing.assert_array_equal(out[k][touched], 0.0)
+        np.testing.assert_array_equal(out[k][~touched], vel[k][~touched])
+    g = S.add_gravity(vel, (0.0, -9.8), np.float32(1 / 60))
+    np.testing.assert_array_equal(g[0], vel[0])
+    np.testing.assert_array_equal(g[1], vel[1] + np.float32(-9.8) * np.float32(1 / 60))
