@@ -142,6 +142,7 @@ __device__ void coarse_smooth(const CoarseArgs& A, int l, int phase, float* zm, 
 
 template <typename ST, bool STO = false>
 __global__ void __launch_bounds__(kCoarseThreads) k_coarse(CoarseArgs A) {
+  pdl_enter();
   static_assert(!STO || sizeof(ST) == 4, "the stored form runs on float32 grids");
   extern __shared__ __align__(16) unsigned char smem[];
   float* zm = (float*)smem;

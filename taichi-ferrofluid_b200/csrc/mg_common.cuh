@@ -98,6 +98,54 @@ __device__ __forceinline__ float nbr_sum_f32(const Level& L, const float* v, lon
   return ret;
 }
 
+// Programmatic dependent launch between the kernels of the PCG loop: each is
+// launched with programmatic stream serialisation, so its launch overlaps the
+// end of the kernel before it, and it first waits (griddepcontrol.wait; a
+// no-op without a programmatic dependency) until that kernel has completed
+// and its writes are visible.  Every memory access follows the wait, so the
+// overlap changes no result.  An explicit early trigger
+// (griddepcontrol.launch_dependents, MG_PDL_TRIGGER=1) lets the next grid's
+// CTAs become resident while this one runs; measured on B200 it speeds up
+// host-launched V-cycles but slows the graph-launched solve (128^3: 4.84 ->
+// 5.07 ms; 256^3: 27.1 -> 29.4 ms), so by default the dependents launch at
+// the implicit trigger, this grid's completion (128^3 solve 4.80 ms, V-cycle
+// from a host loop 187 -> 173 us).
+#ifndef MG_PDL
+#define MG_PDL 1
+#endif
+#ifndef MG_PDL_TRIGGER
+#define MG_PDL_TRIGGER 0
+#endif
+__device__ __forceinline__ void pdl_enter() {
+#if MG_PDL
+  asm volatile("griddepcontrol.wait;" ::: "memory");
+#if MG_PDL_TRIGGER
+  asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+#endif
+#endif
+}
+
+// Launch with the programmatic-serialisation attribute (see pdl_enter).
+template <typename... P, typename... A>
+inline cudaError_t launch_k(void (*kern)(P...), dim3 grid, dim3 block, size_t smem, cudaStream_t s, A... args) {
+#if MG_PDL
+  cudaLaunchAttribute at[1];
+  at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  at[0].val.programmaticStreamSerializationAllowed = 1;
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = grid;
+  cfg.blockDim = block;
+  cfg.dynamicSmemBytes = smem;
+  cfg.stream = s;
+  cfg.attrs = at;
+  cfg.numAttrs = 1;
+  return cudaLaunchKernelEx(&cfg, kern, args...);
+#else
+  kern<<<grid, block, smem, s>>>(args...);
+  return cudaGetLastError();
+#endif
+}
+
 // Block-wide FP64 sum; result valid in thread 0.  Fixed tree order.
 template <int NT>
 __device__ __forceinline__ double block_sum(double v, double* sh) {

@@ -31,7 +31,16 @@ struct TileShape {
 #ifndef MG_TILE3_K
 #define MG_TILE3_K 2
 #endif
-constexpr TileShape kTile3 = {32, 16, 512, MG_TILE3_K};
+#ifndef MG_TILE3_TX
+#define MG_TILE3_TX 32
+#endif
+#ifndef MG_TILE3_TY
+#define MG_TILE3_TY 16
+#endif
+#ifndef MG_TILE3_NT
+#define MG_TILE3_NT 512
+#endif
+constexpr TileShape kTile3 = {MG_TILE3_TX, MG_TILE3_TY, MG_TILE3_NT, MG_TILE3_K};
 constexpr TileShape kTile2 = {128, 1, 128, 4};
 // the whole-domain stored form stages twice the bytes per cell: a smaller
 // tile keeps two blocks per SM
@@ -207,16 +216,14 @@ inline cudaError_t launch_sweep_t(const FusedPlan& F, const Level* lv, int l, co
     const size_t smem = sweep_smem(DIM, NS, T1, true, STO);
     cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
-    kern<<<F.blocks[l], T1.nt, smem, s>>>(sweep_args<ST, PRE>(F, lv, l, ctl));
-    return cudaGetLastError();
+    return launch_k(kern, F.blocks[l], T1.nt, smem, s, sweep_args<ST, PRE>(F, lv, l, ctl));
   }
   auto kern = k_sweep<DIM, ST, NS, T.tx, T.ty, PRE, T.nt, T.k, STO>;
   constexpr int NT = T.nt;
   const size_t smem = sweep_smem(DIM, NS, T, false, STO);
   cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (e != cudaSuccess) return e;
-  kern<<<F.blocks[l], NT, smem, s>>>(sweep_args<ST, PRE>(F, lv, l, ctl));
-  return cudaGetLastError();
+  return launch_k(kern, F.blocks[l], NT, smem, s, sweep_args<ST, PRE>(F, lv, l, ctl));
 }
 
 template <typename ST, bool PRE>
@@ -261,8 +268,7 @@ inline cudaError_t launch_coarse_st(const FusedPlan& F, const Control* ctl, cuda
   auto kern = k_coarse<ST, STO>;
   cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)F.coarse_smem);
   if (e != cudaSuccess) return e;
-  kern<<<1, F.coarse_threads, F.coarse_smem, s>>>(a);
-  return cudaGetLastError();
+  return launch_k(kern, 1, F.coarse_threads, F.coarse_smem, s, a);
 }
 
 inline cudaError_t launch_coarse(const FusedPlan& F, const Control* ctl, cudaStream_t s) {

@@ -170,6 +170,7 @@ __device__ __forceinline__ long long colour_cells(const Geom& g) {
 }
 
 __global__ void k_smooth(Level L, int phase) {
+  pdl_enter();
   const long long n = colour_cells(L.g);
   for (long long j = gtid(); j < n; j += gstride()) smooth_cell(L, j, phase);
 }
@@ -178,6 +179,7 @@ __global__ void k_smooth(Level L, int phase) {
 // children's (r - (Adiag z + nbr_sum)) in lexicographic child order.  Also
 // zeroes the coarse z (the r[l+1].fill(0), z[l+1].fill(0) of mgpcg.py:132-133).
 __global__ void k_restrict(Level F, Level C) {
+  pdl_enter();
   const float* zf = (const float*)F.z;
   const float* rf = (const float*)F.r;
   for (long long ic = gtid(); ic < C.g.count; ic += gstride()) {
@@ -203,6 +205,7 @@ __global__ void k_restrict(Level F, Level C) {
 
 // prolongate(l) (mgpcg.py:120-123): z[l][I] += z[l+1][I // 2], every cell.
 __global__ void k_prolongate(Level F, Level C) {
+  pdl_enter();
   float* zf = (float*)F.z;
   const float* zc = (const float*)C.z;
   for (long long i = gtid(); i < F.g.count; i += gstride()) {
@@ -216,6 +219,7 @@ __global__ void k_prolongate(Level F, Level C) {
 // sweeps in colour order (0, 1) then nhalf in order (1, 0), block-synchronised
 // between half sweeps.  Used for levels small enough for one block.
 __global__ void k_bottom(Level L, int nhalf) {
+  pdl_enter();
   const long long n = colour_cells(L.g);
   for (int it = 0; it < 2 * nhalf; ++it) {
     for (int h = 0; h < 2; ++h) {

@@ -53,6 +53,7 @@ __device__ void set_scales(Control* ctl, double rTr);
 __global__ void __launch_bounds__(kRedThreads) k_pcg_begin(Level L, const float* __restrict__ b,
                                                            float* __restrict__ x, Control* ctl,
                                                            double* partials) {
+  pdl_enter();
   __shared__ double sh[32];
   float* r = (float*)L.r;
   const int warm = ctl->warm_start;
@@ -120,6 +121,7 @@ __device__ void set_scales(Control* ctl, double rTr) {
 // update_p (mgpcg.py:234-238): p = z + beta p on FLUID cells.
 template <typename ST>
 __global__ void k_update_p(Level L, float* __restrict__ p, const Control* ctl) {
+  pdl_enter();
   const float beta = ctl->beta;
   const float sz = (float)ctl->scale_z;
   const ST* z = (const ST*)L.z;
@@ -134,6 +136,7 @@ __global__ void k_update_p(Level L, float* __restrict__ p, const Control* ctl) {
 //          stop at max_iters (mgpcg.py:176, :200-209).
 template <typename ST>
 __global__ void __launch_bounds__(kRedThreads) k_zr(Level L, Control* ctl, double* partials, int mode) {
+  pdl_enter();
   __shared__ double sh[32];
   const ST* z = (const ST*)L.z;
   const float* r = (const float*)L.r;
@@ -162,6 +165,7 @@ __global__ void __launch_bounds__(kRedThreads) k_zr(Level L, Control* ctl, doubl
 __device__ __forceinline__ bool fluid_lane(uint32_t t4, int e) { return ((t4 >> (8 * e)) & 0xffu) == (uint32_t)FLUID; }
 
 __global__ void k_update_p4(Level L, float* __restrict__ p, const Control* ctl) {
+  pdl_enter();
   const float beta = ctl->beta;
   const int groups = (int)(L.g.count >> 2);
   for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < groups; q += gridDim.x * blockDim.x) {
@@ -179,6 +183,7 @@ __global__ void k_update_p4(Level L, float* __restrict__ p, const Control* ctl) 
 }
 
 __global__ void __launch_bounds__(kRedThreads) k_zr4(Level L, Control* ctl, double* partials, int mode) {
+  pdl_enter();
   __shared__ double sh[32];
   const int groups = (int)(L.g.count >> 2);
   double acc = 0.0;
@@ -211,6 +216,7 @@ __global__ void __launch_bounds__(kRedThreads) k_zr4(Level L, Control* ctl, doub
 __global__ void __launch_bounds__(kRedThreads) k_Ap_alpha(Level L, const float* __restrict__ p,
                                                           float* __restrict__ Ap, Control* ctl,
                                                           double* partials, int force = 0) {
+  pdl_enter();
   if (!ctl->run && !force) return;
   __shared__ double sh[32];
   double acc = 0.0;
@@ -238,6 +244,7 @@ __global__ void __launch_bounds__(kRedThreads) k_Ap_alpha(Level L, const float* 
 __global__ void __launch_bounds__(kRedThreads) k_Ap_alpha4(Level L, const float* __restrict__ p,
                                                            float* __restrict__ Ap, Control* ctl, double* partials,
                                                            int force = 0) {
+  pdl_enter();
   if (!ctl->run && !force) return;
   __shared__ double sh[32];
   const int dim = L.g.dim;
@@ -313,6 +320,7 @@ __global__ void __launch_bounds__(kRedThreads) k_Ap_alpha4(Level L, const float*
 __global__ void __launch_bounds__(kRedThreads) k_Ap_alpha_uniform(Level L, const float* __restrict__ p,
                                                                   float* __restrict__ Ap, float s, Control* ctl,
                                                                   double* partials, int force = 0) {
+  pdl_enter();
   if (!ctl->run && !force) return;
   __shared__ double sh[32];
   const float ms = -s;
@@ -353,6 +361,7 @@ __global__ void __launch_bounds__(kRedThreads) k_Ap_alpha_uniform(Level L, const
 __global__ void __launch_bounds__(kRedThreads) k_Ap_alpha_uniform4(Level L, const float* __restrict__ p,
                                                                    float* __restrict__ Ap, float s, Control* ctl,
                                                                    double* partials, int force = 0) {
+  pdl_enter();
   if (!ctl->run && !force) return;
   __shared__ double sh[32];
   const float ms = -s;
@@ -427,6 +436,7 @@ __global__ void __launch_bounds__(kRedThreads) k_xr(Level L, float* __restrict__
                                                     const float* __restrict__ Ap, Control* ctl,
                                                     double* partials, cudaGraphConditionalHandle cond,
                                                     int has_cond, int force = 0) {
+  pdl_enter();
   __shared__ double sh[32];
   if (!ctl->run && !force) {
     if (has_cond && blockIdx.x == 0 && threadIdx.x == 0) cudaGraphSetConditional(cond, 0);
@@ -468,6 +478,7 @@ __global__ void __launch_bounds__(kRedThreads) k_refresh(Level L, const float* _
                                                          const float* __restrict__ x, Control* ctl,
                                                          double* partials, cudaGraphConditionalHandle cond,
                                                          int has_cond) {
+  pdl_enter();
   __shared__ double sh[32];
   const bool claimed = ctl->status == MG_SOLVE_CONVERGED && !ctl->run;
   const bool due = ctl->run && ctl->refresh_every > 0 && ctl->since_refresh >= ctl->refresh_every;

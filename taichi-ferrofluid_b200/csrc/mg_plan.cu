@@ -174,20 +174,17 @@ constexpr int64_t kBottomBlockCells = 1 << 16;
 
 int launch_smooth(mg_plan* P, int l, int phase, cudaStream_t s) {
   int64_t n = level_cells(P, l) / 2 + level_cells(P, l) / (P->d.dim == 3 ? P->geom[l].n[2] : P->geom[l].n[1]);
-  k_smooth<<<grid_for(P, n), 256, 0, s>>>(P->lv[l], phase);
-  CKL("k_smooth");
+  CK(launch_k(k_smooth, grid_for(P, n), 256, 0, s, P->lv[l], phase));
   return MG_OK;
 }
 
 int launch_restrict(mg_plan* P, int l, cudaStream_t s) {
-  k_restrict<<<grid_for(P, level_cells(P, l + 1)), 256, 0, s>>>(P->lv[l], P->lv[l + 1]);
-  CKL("k_restrict");
+  CK(launch_k(k_restrict, grid_for(P, level_cells(P, l + 1)), 256, 0, s, P->lv[l], P->lv[l + 1]));
   return MG_OK;
 }
 
 int launch_prolongate(mg_plan* P, int l, cudaStream_t s) {
-  k_prolongate<<<grid_for(P, level_cells(P, l)), 256, 0, s>>>(P->lv[l], P->lv[l + 1]);
-  CKL("k_prolongate");
+  CK(launch_k(k_prolongate, grid_for(P, level_cells(P, l)), 256, 0, s, P->lv[l], P->lv[l + 1]));
   return MG_OK;
 }
 
@@ -205,8 +202,7 @@ int launch_vcycle_generic(mg_plan* P, cudaStream_t s) {
   const int nh = P->d.bottom / 2;
   if (level_cells(P, L - 1) <= kBottomBlockCells) {
     if (nh > 0) {
-      k_bottom<<<1, 1024, 0, s>>>(P->lv[L - 1], nh);
-      CKL("k_bottom");
+      CK(launch_k(k_bottom, 1, 1024, 0, s, P->lv[L - 1], nh));
     }
   } else {
     for (int i = 0; i < nh; ++i) {
@@ -348,29 +344,23 @@ int launch_zr_p(mg_plan* P, bool prologue, cudaStream_t s) {
   float* p = fptr(P, MG_FIELD_P);
   if (sizeof(ST) == 4 && P->geom[0].count % 4 == 0) {  // float32: 4-cell groups
     const int eb = grid_for(P, P->geom[0].count / 4);
+    const Control* cc = P->ctl;
     if (prologue) {
-      k_update_p4<<<eb, 256, 0, s>>>(L0, p, P->ctl);
-      CKL("k_update_p4");
-      k_zr4<<<P->red_blocks, kRedThreads, 0, s>>>(L0, P->ctl, P->partials, 0);
-      CKL("k_zr4");
+      CK(launch_k(k_update_p4, eb, 256, 0, s, L0, p, cc));
+      CK(launch_k(k_zr4, P->red_blocks, kRedThreads, 0, s, L0, P->ctl, P->partials, 0));
     } else {
-      k_zr4<<<P->red_blocks, kRedThreads, 0, s>>>(L0, P->ctl, P->partials, 1);
-      CKL("k_zr4");
-      k_update_p4<<<eb, 256, 0, s>>>(L0, p, P->ctl);
-      CKL("k_update_p4");
+      CK(launch_k(k_zr4, P->red_blocks, kRedThreads, 0, s, L0, P->ctl, P->partials, 1));
+      CK(launch_k(k_update_p4, eb, 256, 0, s, L0, p, cc));
     }
     return MG_OK;
   }
+  const Control* cc = P->ctl;
   if (prologue) {
-    k_update_p<ST><<<P->ew_blocks[0], 256, 0, s>>>(L0, p, P->ctl);
-    CKL("k_update_p");
-    k_zr<ST><<<P->red_blocks, kRedThreads, 0, s>>>(L0, P->ctl, P->partials, 0);
-    CKL("k_zr");
+    CK(launch_k(k_update_p<ST>, P->ew_blocks[0], 256, 0, s, L0, p, cc));
+    CK(launch_k(k_zr<ST>, P->red_blocks, kRedThreads, 0, s, L0, P->ctl, P->partials, 0));
   } else {
-    k_zr<ST><<<P->red_blocks, kRedThreads, 0, s>>>(L0, P->ctl, P->partials, 1);
-    CKL("k_zr");
-    k_update_p<ST><<<P->ew_blocks[0], 256, 0, s>>>(L0, p, P->ctl);
-    CKL("k_update_p");
+    CK(launch_k(k_zr<ST>, P->red_blocks, kRedThreads, 0, s, L0, P->ctl, P->partials, 1));
+    CK(launch_k(k_update_p<ST>, P->ew_blocks[0], 256, 0, s, L0, p, cc));
   }
   return MG_OK;
 }
@@ -397,22 +387,24 @@ int launch_cg_tail(mg_plan* P, cudaStream_t s, int which) {
   const int RB = P->red_blocks;
   const bool refresh = P->d.refresh_every > 0;
   if (which & 1) {
+    const float* pc = p;
     if (P->fp.valid && !P->fp.sto && x_by4(P))  // label-uniform level 0, 4-cell groups
-      k_Ap_alpha_uniform4<<<RB, kRedThreads, 0, s>>>(L0, p, Ap, P->offdiag[0], P->ctl, P->partials);
+      CK(launch_k(k_Ap_alpha_uniform4, RB, kRedThreads, 0, s, L0, pc, Ap, P->offdiag[0], P->ctl, P->partials, 0));
     else if (P->fp.valid && !P->fp.sto)
-      k_Ap_alpha_uniform<<<RB, kRedThreads, 0, s>>>(L0, p, Ap, P->offdiag[0], P->ctl, P->partials);
+      CK(launch_k(k_Ap_alpha_uniform, RB, kRedThreads, 0, s, L0, pc, Ap, P->offdiag[0], P->ctl, P->partials, 0));
     else if (x_by4(P))
-      k_Ap_alpha4<<<RB, kRedThreads, 0, s>>>(L0, p, Ap, P->ctl, P->partials);
+      CK(launch_k(k_Ap_alpha4, RB, kRedThreads, 0, s, L0, pc, Ap, P->ctl, P->partials, 0));
     else
-      k_Ap_alpha<<<RB, kRedThreads, 0, s>>>(L0, p, Ap, P->ctl, P->partials);
-    CKL("k_Ap_alpha");
+      CK(launch_k(k_Ap_alpha, RB, kRedThreads, 0, s, L0, pc, Ap, P->ctl, P->partials, 0));
   }
   if (which & 2) {
-    k_xr<<<RB, kRedThreads, 0, s>>>(L0, x, p, Ap, P->ctl, P->partials, P->cond, refresh ? 0 : P->has_cond);
-    CKL("k_xr");
+    const float* pc = p;
+    const float* Apc = Ap;
+    CK(launch_k(k_xr, RB, kRedThreads, 0, s, L0, x, pc, Apc, P->ctl, P->partials, P->cond,
+                refresh ? 0 : P->has_cond, 0));
     if (refresh) {
-      k_refresh<<<RB, kRedThreads, 0, s>>>(L0, b, x, P->ctl, P->partials, P->cond, P->has_cond);
-      CKL("k_refresh");
+      const float* bc = b;
+      CK(launch_k(k_refresh, RB, kRedThreads, 0, s, L0, bc, x, P->ctl, P->partials, P->cond, P->has_cond));
     }
   }
   return MG_OK;
@@ -425,8 +417,8 @@ int launch_pcg_part(mg_plan* P, bool prologue, cudaStream_t s) {
   float* b = fptr(P, MG_FIELD_B);
   float* x = fptr(P, MG_FIELD_X);
   if (prologue) {
-    k_pcg_begin<<<P->red_blocks, kRedThreads, 0, s>>>(L0, b, x, P->ctl, P->partials);
-    CKL("k_pcg_begin");
+    const float* bc = b;
+    CK(launch_k(k_pcg_begin, P->red_blocks, kRedThreads, 0, s, L0, bc, x, P->ctl, P->partials));
   }
   if (int rc = launch_vcycle(P, s)) return rc;
   if (int rc = launch_zr_p_any(P, prologue, s)) return rc;

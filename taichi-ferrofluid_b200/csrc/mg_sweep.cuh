@@ -90,6 +90,7 @@ __device__ __forceinline__ void ld4_r(const void* r, long long i, int r_f32, flo
 // as z = 0, Ax = 0 (rule H1).
 template <int DIM, typename ST, int NS, int TX, int TY, bool PRE, int NT, int K, bool STO = false>
 __global__ void __launch_bounds__(NT) k_sweep(SweepArgs<ST> A) {
+  pdl_enter();
   static_assert(!STO || sizeof(ST) == 4, "the stored form runs on float32 grids");
   // halos: NS cells are needed on each side; along the fastest axis the halo
   // is rounded up to 4 so every 4-wide group starts 16-byte (float) / 8-byte
