@@ -295,6 +295,13 @@ def time_stages(case, storage, reps=20):
     out = {}
     stages = {"pre_l0": (0, 0), "post_l0": (1, 0), "coarse": (2, 0), "Ap_alpha": (3, 0), "xr": (4, 0),
               "vcycle": (5, 0)}
+    on, first = s.resident()
+    if on:  # the cluster launch (levels `first` down) replaces the coarse block
+        stages.pop("coarse")
+        stages["cluster"] = (6, 0)
+        if first == 0:
+            stages.pop("pre_l0")
+            stages.pop("post_l0")
     for name, (st, lv) in stages.items():
         try:
             s.launch_stage(st, lv)
@@ -409,7 +416,9 @@ def gpu_arm(args, rank, world, local):
         "pcg_iters": {k: {"min": min(v), "max": max(v)} for k, v in per_case_iters.items()},
         "vcycle": {c.kind: {"operator_form": c.solver.operator_form(0),
                             "split_levels_bits": c.solver.split_levels()[0],
-                            "streamed_levels": c.solver.split_levels()[1]} for c in cases},
+                            "streamed_levels": c.solver.split_levels()[1],
+                            "cluster_from_level": c.solver.resident()[1] if c.solver.resident()[0] else None}
+                   for c in cases},
         "last_rel_resid": rel, "last_status": status,
         "cell_iters_per_s": round(sum(c.scene.cells * (i + 1) for c, i in iters) * world / (total_ms * 1e-3), 1),
         "e2e": {"value": round(n_solves / (total_e2e * 1e-3), 3), "unit": "solves/s",

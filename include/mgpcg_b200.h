@@ -366,6 +366,21 @@ MG_API int mg_plan_operator_form(const mg_plan_t* plan, int32_t level, int32_t* 
  * profilers, which serialise the trial launches). */
 MG_API int mg_plan_split(mg_plan_t* plan, int32_t set, uint32_t* bits, int32_t* streamed);
 
+/* The cluster-resident V-cycle (no reference counterpart: a B200 launch shape
+ * of mgpcg.py:125-148 with the same float32 values): for a label-uniform
+ * float32 3D plan whose levels [first_level, L) halve exactly, those levels run
+ * as ONE launch of one thread-block cluster (up to 16 CTAs), each CTA holding
+ * its brick of every level in shared memory and reading its neighbours'
+ * through distributed shared memory; the levels above stay streamed.  When a
+ * shape is first prepared the V-cycle is timed streamed and with the cluster
+ * from each feasible level, and the fastest kept (cached per shape);
+ * MGPCG_RESIDENT=0 / 1 replaces the timing.  set != 0 forces *on and, when
+ * *on and first_level != NULL and *first_level >= 0, the level the cluster
+ * starts at (after the plan is prepared; valid until the next prepare; fails
+ * when that level, or any, allows no bricks); *on returns the choice and
+ * *first_level (if not NULL) the cluster's first level, -1 when there is none. */
+MG_API int mg_plan_resident(mg_plan_t* plan, int32_t set, int32_t* on, int32_t* first_level);
+
 /* ---- the reference's per-kernel operations (for parity tests) ------------ */
 
 MG_API int mg_smooth(mg_plan_t* plan, int32_t level, int32_t phase, void* stream);   /* mgpcg.py:104-109 */
@@ -402,7 +417,8 @@ MG_API int mg_plan_launch_counts(mg_plan_t* plan, int32_t* prologue, int32_t* bo
  * the reference's closest tool is ti.kernel_profiler, fluid_simulator.py:16).
  * stage: 0 = level-`level` pre-smoothing (+ restriction), 1 = level-`level`
  * post-smoothing (+ prolongation), 2 = the coarse solve, 3 = the CG step
- * p/Ap/alpha, 4 = the CG step x/r/r.r, 5 = one whole V-cycle. */
+ * p/Ap/alpha, 4 = the CG step x/r/r.r, 5 = one whole V-cycle, 6 = the
+ * cluster-resident part of the V-cycle (mg_plan_resident). */
 MG_API int mg_launch_stage(mg_plan_t* plan, int32_t stage, int32_t level, void* stream);
 
 /* ---- allocation-free variant ------------------------------------------------------ */

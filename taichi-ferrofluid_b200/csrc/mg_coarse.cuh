@@ -140,11 +140,12 @@ __device__ void coarse_smooth(const CoarseArgs& A, int l, int phase, float* zm, 
   }
 }
 
+// The coarse V-cycle by the calling block, in `smem` (A.total padded cells
+// times 12 bytes, plus the couplings for STO): k_coarse runs it as its own
+// launch, the cluster-resident V-cycle (mg_resident.cuh) in its CTA 0.
 template <typename ST, bool STO = false>
-__global__ void __launch_bounds__(kCoarseThreads) k_coarse(CoarseArgs A) {
-  pdl_enter();
+__device__ void coarse_vcycle(const CoarseArgs& A, unsigned char* smem) {
   static_assert(!STO || sizeof(ST) == 4, "the stored form runs on float32 grids");
-  extern __shared__ __align__(16) unsigned char smem[];
   float* zm = (float*)smem;
   float* sr = zm + A.total;
   float* sa = sr + A.total;
@@ -305,6 +306,13 @@ __global__ void __launch_bounds__(kCoarseThreads) k_coarse(CoarseArgs A) {
     const int p = g0.at(c0, c1, c2);
     ((ST*)A.z0)[i] = from_f<ST>(sa[p] != 0.0f ? zm[p] : sr[p]);
   }
+}
+
+template <typename ST, bool STO = false>
+__global__ void __launch_bounds__(kCoarseThreads) k_coarse(CoarseArgs A) {
+  pdl_enter();
+  extern __shared__ __align__(16) unsigned char smem[];
+  coarse_vcycle<ST, STO>(A, smem);
 }
 
 }  // namespace mg

@@ -5,6 +5,7 @@
 
 #include "mg_sweep.cuh"
 #include "mg_coarse.cuh"
+#include "mg_resident.cuh"
 
 namespace mg {
 
@@ -74,6 +75,12 @@ struct FusedPlan {
   int coarse_threads = 512;
   float kappa = 1.0f, rho = 1.0f, pi = 1.0f;
   float s[kMaxLevels];
+  // cluster-resident V-cycle of levels [res_lp, L) (mg_resident.cuh): possible
+  // (res_ok) and chosen (res); bricks for [res_lp, res_lb), CTA 0 below
+  bool res_ok = false, res = false;
+  int res_lp = 0, res_lb = 0, res_blocks = 0;
+  size_t res_smem = 0;
+  ResArgs res_args;
 };
 
 // Chooses the launch shapes.  Needs pre_post in 1..3 and either every level
@@ -84,6 +91,8 @@ inline bool make_fused_plan(const Level* lv, int L, int dim, int pre_post, int b
                             const int* op_form, const int* whole, const float* offdiag, int num_sms, FusedPlan* F) {
   F->valid = false;
   F->sto = false;
+  F->res_ok = false;
+  F->res = false;
   for (int l = 0; l < kMaxLevels; ++l) F->split[l] = false;
   bool uniform = true, all_whole = true;
   for (int l = 0; l < L; ++l) {
@@ -176,6 +185,160 @@ inline bool make_fused_plan(const Level* lv, int L, int dim, int pre_post, int b
   F->coarse_threads = kCoarseThreads;
   F->valid = true;
   return true;
+}
+
+// Brick decomposition for the cluster-resident V-cycle (mg_resident.cuh) of a
+// label-uniform float32 3D plan: the coarse levels [lb, L) for CTA 0 (the
+// bottom level alone when the level above it splits into bricks, else one
+// level more, and so on) and the first level lp in [lp_min, lp_max] whose
+// levels [lp, lb) halve exactly and split into at most 16 bricks of
+// power-of-two extents (at least 2^(lb - lp) a side) that fit one CTA's shared
+// memory beside the coarse region; among those, the most bricks, then the
+// fewest face cells.  The bricks' Adiag joins them in shared memory when it
+// fits.  Fills F->res_* (res_ok); F->res stays as it was.
+inline bool make_resident_plan(FusedPlan* F, const Level* lv, int L, int pre_post, int bottom, int lp_min,
+                               int lp_max) {
+  F->res_ok = false;
+  if (!F->valid || F->sto || F->dim != 3 || F->storage != MG_STORE_F32 || L < 2) return false;
+  for (int lb = L - 1; lb >= 1; --lb) {
+    long long coarse_cells = 0;
+    for (int l = lb; l < L; ++l) coarse_cells += padded_cells(lv[l].g);
+    const long long coarse_floats = (3 * coarse_cells + 3) / 4 * 4;
+    if (coarse_cells > kCoarseMaxCells) break;
+    for (int lp = lp_min; lp < lb && lp <= lp_max; ++lp) {
+      const int D = lb - lp;
+      const Geom& g = lv[lp].g;
+      bool halves = true;
+      for (int l = lp + 1; l <= lb; ++l)
+        for (int a = 0; a < 3; ++a) halves = halves && ((long long)lv[l].g.n[a] << (l - lp)) == g.n[a];
+      if (!halves) continue;
+      int emax[3], best[3] = {0, 0, 0};
+      for (int a = 0; a < 3; ++a) {
+        emax[a] = 0;
+        while (((g.n[a] >> emax[a]) & 1) == 0 && emax[a] < 20) ++emax[a];
+      }
+      long long best_c = 0, best_faces = 0, best_fla = 0;
+      for (int e0 = D; e0 <= emax[0]; ++e0)
+        for (int e1 = D; e1 <= emax[1]; ++e1)
+          for (int e2 = D; e2 <= emax[2]; ++e2) {
+            const long long C = (long long)(g.n[0] >> e0) * (g.n[1] >> e1) * (g.n[2] >> e2);
+            if (C > kResMaxCtas || C < 1) continue;
+            long long fl = 0, fla = 0;  // without / with the bricks' Adiag
+            for (int i = 0; i < D; ++i) {
+              const long long b0 = 1LL << (e0 - i), b1 = 1LL << (e1 - i), b2 = 1LL << (e2 - i);
+              fl += ((b0 + 2) * (b1 + 2) * (b2 + 2) + 3) / 4 * 4 + (b0 * b1 * b2 + 3) / 4 * 4;
+              fla += (b0 * b1 * b2 + 3) / 4 * 4;
+            }
+            fla += fl;
+            if ((size_t)(fl + coarse_floats) * 4 + 1024 > kSmemLimit) continue;
+            const long long B0 = 1LL << e0, B1 = 1LL << e1, B2 = 1LL << e2;
+            const long long faces = 2 * (B1 * B2 + B0 * B2 + B0 * B1);
+            if (C > best_c || (C == best_c && faces < best_faces)) {
+              best_c = C;
+              best_faces = faces;
+              best_fla = fla;
+              best[0] = e0;
+              best[1] = e1;
+              best[2] = e2;
+            }
+          }
+      if (best_c == 0) continue;
+      ResArgs& R = F->res_args;
+      R.nlev = D;
+      for (int a = 0; a < 3; ++a) R.nb[a] = g.n[a] >> best[a];
+      R.ns = F->ns;
+      R.rho = F->rho;
+      R.pi = F->pi;
+      const bool sad = (size_t)(best_fla + coarse_floats) * 4 + 1024 <= kSmemLimit;
+      int off = 0;
+      for (int i = 0; i < D; ++i) {
+        ResLevel& Q = R.lv[i];
+        const Level& lev = lv[lp + i];
+        for (int a = 0; a < 3; ++a) {
+          Q.lb[a] = best[a] - i;
+          Q.n[a] = lev.g.n[a];
+        }
+        const int b0 = 1 << Q.lb[0], b1 = 1 << Q.lb[1], b2 = 1 << Q.lb[2];
+        Q.zoff = off;
+        off += ((b0 + 2) * (b1 + 2) * (b2 + 2) + 3) / 4 * 4;
+        Q.roff = off;
+        off += (b0 * b1 * b2 + 3) / 4 * 4;
+        Q.aoff = -1;
+        if (sad) {
+          Q.aoff = off;
+          off += (b0 * b1 * b2 + 3) / 4 * 4;
+        }
+        Q.s = F->s[lp + i];
+        Q.Ad = (const float*)lev.Adiag_s;
+      }
+      R.r0 = (const float*)lv[lp].r;
+      R.z0 = (float*)lv[lp].z;
+      R.rc = (float*)lv[lb].r;
+      R.zc = (const float*)lv[lb].z;
+      // the coarse levels [lb, L) laid out as the coarse block lays them out
+      CoarseArgs& C = R.coarse;
+      C = F->coarse;
+      C.dim = 3;
+      C.nlev = L - lb;
+      C.pre_post = pre_post;
+      C.bottom = bottom;
+      int coff = 0;
+      for (int i = 0; i < C.nlev; ++i) {
+        const Geom& cg = lv[lb + i].g;
+        for (int a = 0; a < 3; ++a) C.n[i][a] = cg.n[a];
+        C.off[i] = coff;
+        coff += (int)padded_cells(cg);
+        C.s[i] = F->s[lb + i];
+        C.Ad[i] = lv[lb + i].Adiag_s;
+        for (int k = 0; k < 3; ++k) C.Ax[i][k] = lv[lb + i].Ax[k];
+      }
+      C.total = coff;
+      C.r0 = lv[lb].r;
+      C.z0 = lv[lb].z;
+      C.r_f32 = 0;
+      C.rho = F->rho;
+      C.pi = F->pi;
+      R.coff = off;
+      R.smem_floats = off + (int)coarse_floats;
+      F->res_lp = lp;
+      F->res_lb = lb;
+      F->res_blocks = (int)best_c;
+      F->res_smem = (size_t)R.smem_floats * 4;
+      F->res_ok = true;
+      return true;
+    }
+  }
+  return false;
+}
+
+// One launch of the cluster-resident V-cycle: one cluster of res_blocks CTAs.
+inline cudaLaunchConfig_t resident_config(const FusedPlan& F, cudaStream_t s, cudaLaunchAttribute* at) {
+  at[0].id = cudaLaunchAttributeClusterDimension;
+  at[0].val.clusterDim.x = F.res_blocks;
+  at[0].val.clusterDim.y = 1;
+  at[0].val.clusterDim.z = 1;
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3(F.res_blocks);
+  cfg.blockDim = dim3(kResThreads);
+  cfg.dynamicSmemBytes = F.res_smem;
+  cfg.stream = s;
+  cfg.attrs = at;
+  cfg.numAttrs = 1;
+  return cfg;
+}
+
+inline cudaError_t resident_attributes(const FusedPlan& F) {
+  cudaError_t e = cudaFuncSetAttribute(k_resident, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)F.res_smem);
+  if (e == cudaSuccess) e = cudaFuncSetAttribute(k_resident, cudaFuncAttributeNonPortableClusterSizeAllowed, 1);
+  return e;
+}
+
+inline cudaError_t launch_resident(const FusedPlan& F, cudaStream_t s) {
+  cudaError_t e = resident_attributes(F);
+  if (e != cudaSuccess) return e;
+  cudaLaunchAttribute at[1];
+  const cudaLaunchConfig_t cfg = resident_config(F, s, at);
+  return cudaLaunchKernelEx(&cfg, k_resident, F.res_args);
 }
 
 template <typename ST, bool PRE>

@@ -254,6 +254,15 @@ int launch_level(mg_plan* P, int l, bool pre, cudaStream_t s) {
 // One V-cycle of a fused plan: the streamed levels down, the coarse block,
 // the streamed levels up.
 int launch_vcycle_fused(mg_plan* P, cudaStream_t s) {
+  if (P->fp.res) {  // streamed levels above the bricks, then one cluster launch
+    for (int l = 0; l < P->fp.res_lp; ++l)
+      if (int rc = launch_level(P, l, true, s)) return rc;
+    cudaError_t e = launch_resident(P->fp, s);
+    if (e != cudaSuccess) return set_err("launch_resident", e);
+    for (int l = P->fp.res_lp - 1; l >= 0; --l)
+      if (int rc = launch_level(P, l, false, s)) return rc;
+    return MG_OK;
+  }
   for (int l = 0; l < P->fp.lc; ++l)
     if (int rc = launch_level(P, l, true, s)) return rc;
   cudaError_t e = launch_coarse(P->fp, P->ctl, s);
@@ -335,6 +344,111 @@ int tune_split(mg_plan* P, cudaStream_t s) {
   }
   std::lock_guard<std::mutex> lk(g_tune_mu);
   g_tune[key] = bits;
+  return MG_OK;
+}
+
+// The cluster-resident V-cycle against the streamed one: for a label-uniform
+// float32 plan whose levels allow bricks, the V-cycle is timed streamed and
+// with the cluster starting at each feasible level (CUDA events, one warm-up,
+// three timed) the first time a shape is prepared, and the fastest kept,
+// cached per shape for the process.  All compute the same float32 values.
+// MGPCG_RESIDENT=0 / 1 replaces the timing (1: the cluster from the first
+// feasible level).
+std::map<std::array<int, 7>, int> g_tune_res;  // first brick level, -1: streamed
+
+// The cluster plan from the first feasible level in [lp_min, lp_max], checked
+// against what the device can hold; false (res_ok = false) when there is none.
+bool plan_resident(mg_plan* P, int lp_min, int lp_max, cudaStream_t s) {
+  if (!make_resident_plan(&P->fp, P->lv, P->L, P->d.pre_post, P->d.bottom, lp_min, lp_max)) return false;
+  // whether the device holds the cluster, asked once per (device, CTAs, bytes)
+  static std::map<std::array<int64_t, 3>, bool> fits;
+  const std::array<int64_t, 3> key = {P->device, P->fp.res_blocks, (int64_t)P->fp.res_smem};
+  {
+    std::lock_guard<std::mutex> lk(g_tune_mu);
+    auto it = fits.find(key);
+    if (it != fits.end()) {
+      P->fp.res_ok = it->second;
+      return it->second;
+    }
+  }
+  bool ok = resident_attributes(P->fp) == cudaSuccess;
+  if (ok) {
+    cudaLaunchAttribute at[1];
+    const cudaLaunchConfig_t cfg = resident_config(P->fp, s, at);
+    int clusters = 0;
+    ok = cudaOccupancyMaxActiveClusters(&clusters, k_resident, &cfg) == cudaSuccess && clusters >= 1;
+  }
+  if (!ok) cudaGetLastError();
+  P->fp.res_ok = ok;
+  std::lock_guard<std::mutex> lk(g_tune_mu);
+  fits[key] = ok;
+  return ok;
+}
+
+int tune_resident(mg_plan* P, cudaStream_t s) {
+  P->fp.res = false;
+  if (!P->fp.valid) return MG_OK;
+  if (!plan_resident(P, 0, P->L, s)) return MG_OK;
+  const int lp_first = P->fp.res_lp;
+  if (const char* ov = std::getenv("MGPCG_RESIDENT")) {
+    P->fp.res = std::strtol(ov, nullptr, 0) != 0;
+    return MG_OK;
+  }
+  const Geom& g = P->geom[0];
+  const std::array<int, 7> key = {g.dim, g.n[0], g.n[1], g.n[2], P->L, P->d.pre_post, P->fp.lc};
+  {
+    std::lock_guard<std::mutex> lk(g_tune_mu);
+    auto it = g_tune_res.find(key);
+    if (it != g_tune_res.end()) {
+      if (it->second >= 0 && plan_resident(P, it->second, it->second, s)) P->fp.res = true;
+      else plan_resident(P, lp_first, lp_first, s);
+      return MG_OK;
+    }
+  }
+  cudaEvent_t e0 = nullptr, e1 = nullptr;
+  CK(cudaEventCreate(&e0));
+  cudaError_t ce = cudaEventCreate(&e1);
+  if (ce != cudaSuccess) {
+    cudaEventDestroy(e0);
+    return set_err("cudaEventCreate", ce);
+  }
+  auto time_vcycle = [&](float* ms) -> int {
+    int rc = MG_OK;
+    for (int rep = 0; rep < 4 && rc == MG_OK; ++rep) {  // rep 0 warms up
+      if (rep == 1) cudaEventRecord(e0, s);
+      rc = launch_vcycle_fused(P, s);
+    }
+    if (rc != MG_OK) return rc;
+    cudaEventRecord(e1, s);
+    cudaError_t e = cudaEventSynchronize(e1);
+    if (e == cudaSuccess) e = cudaEventElapsedTime(ms, e0, e1);
+    return e == cudaSuccess ? MG_OK : set_err("tune_resident", e);
+  };
+  float best = 0.0f;
+  int best_lp = -1;
+  int rc = time_vcycle(&best);  // streamed (res = false)
+  for (int lp = lp_first; rc == MG_OK && lp < P->L; ++lp) {
+    if (!plan_resident(P, lp, lp, s)) continue;
+    P->fp.res = true;
+    float t = 0.0f;
+    rc = time_vcycle(&t);
+    P->fp.res = false;
+    if (rc == MG_OK && t < best) {
+      best = t;
+      best_lp = lp;
+    }
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  if (rc != MG_OK) return rc;
+  if (best_lp >= 0) {
+    plan_resident(P, best_lp, best_lp, s);
+    P->fp.res = true;
+  } else {
+    plan_resident(P, lp_first, lp_first, s);
+  }
+  std::lock_guard<std::mutex> lk(g_tune_mu);
+  g_tune_res[key] = best_lp;
   return MG_OK;
 }
 
@@ -429,8 +543,9 @@ int launch_pcg_part(mg_plan* P, bool prologue, cudaStream_t s) {
 int count_pcg_part(const mg_plan* P, bool prologue) {
   const int refresh = P->d.refresh_every > 0 ? 1 : 0;
   if (P->fp.valid) {
-    int v = 1;  // the coarse block
-    for (int l = 0; l < P->fp.lc; ++l) v += P->fp.split[l] ? 2 * (2 * P->d.pre_post + 1) : 2;
+    int v = 1;  // the coarse block, or the cluster-resident launch
+    const int streamed = P->fp.res ? P->fp.res_lp : P->fp.lc;
+    for (int l = 0; l < streamed; ++l) v += P->fp.split[l] ? 2 * (2 * P->d.pre_post + 1) : 2;
     return (prologue ? 1 : 0) + v + 4 + refresh;
   }
   int v = (P->L - 1) * (4 * P->d.pre_post + 2) +
@@ -1105,6 +1220,7 @@ static int finish_prepare(mg_plan_t* P, cudaStream_t s, bool declared) {
   k_set_kappa<<<1, 1, 0, s>>>(P->ctl, (double)P->fp.kappa);
   CKL("k_set_kappa");
   if (int rc = tune_split(P, s)) return rc;
+  if (int rc = tune_resident(P, s)) return rc;
   if (declared) {
     for (int l = 0; l < P->L; ++l) {
       k_verify_uniform<<<P->ew_blocks[l], 256, 0, s>>>(P->lv[l], P->offdiag[l], P->ctl);
@@ -1118,6 +1234,8 @@ static int finish_prepare(mg_plan_t* P, cudaStream_t s, bool declared) {
   mix(P->fp.valid);
   mix(P->fp.sto);
   mix(P->fp.lc);
+  mix(P->fp.res);
+  mix(P->fp.res_lp);
   for (int l = 0; l < P->L; ++l) mix(P->fp.split[l]);
   for (int l = 0; l < P->L; ++l) {
     uint32_t bits;
@@ -1152,6 +1270,23 @@ int mg_plan_split(mg_plan_t* P, int32_t set, uint32_t* bits, int32_t* streamed) 
   for (int l = 0; l < P->fp.lc; ++l)
     if (P->fp.split[l]) b |= 1u << l;
   *bits = b;
+  return MG_OK;
+}
+
+int mg_plan_resident(mg_plan_t* P, int32_t set, int32_t* on, int32_t* first_level) {
+  if (!P || !on) return bad("null pointer");
+  if (set) {
+    if (*on && first_level && *first_level >= 0) {
+      if (!P->fp.valid || !plan_resident(P, *first_level, *first_level, nullptr))
+        return bad("the plan has no cluster-resident V-cycle from that level");
+    }
+    if (*on && !(P->fp.valid && P->fp.res_ok)) return bad("the plan has no cluster-resident V-cycle");
+    P->fp.res = *on != 0;
+    destroy_graph(P);
+    P->graph_sig = 0;
+  }
+  *on = P->fp.valid && P->fp.res ? 1 : 0;
+  if (first_level) *first_level = P->fp.valid && P->fp.res_ok ? P->fp.res_lp : -1;
   return MG_OK;
 }
 
@@ -1307,6 +1442,11 @@ int mg_launch_stage(mg_plan_t* P, int32_t stage, int32_t level, void* stream) {
       return MG_OK;
     case 5:
       return launch_vcycle(P, s);
+    case 6: {
+      if (!P->fp.valid || !P->fp.res_ok) return bad("the plan has no cluster-resident V-cycle");
+      cudaError_t e = launch_resident(P->fp, s);
+      return e == cudaSuccess ? MG_OK : set_err("launch_resident", e);
+    }
   }
   return bad("stage");
 }

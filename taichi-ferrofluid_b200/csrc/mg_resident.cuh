@@ -1,0 +1,360 @@
+// The cluster-resident V-cycle: the label-uniform levels [lp, L) of a fused
+// plan in ONE launch of ONE thread-block cluster (up to 16 CTAs, one per SM).
+// Every CTA holds its brick of each brick level [lp, lb) in shared memory for
+// the whole V-cycle; CTA 0 also runs the coarse levels [lb, L) (mg_coarse.cuh)
+// in a region of its own.
+//
+// Why: below the finest levels the streamed kernel (mg_sweep.cuh) is latency-
+// bound: each level is its own launches, and each launch recomputes a halo of
+// 2 * pre_post cells around every tile for the half sweeps it fuses.  Here a
+// CTA owns a brick of the level exactly (no recomputation), and between two
+// half sweeps only the one-cell rings of the bricks move, read straight from
+// the neighbouring CTAs' shared memory (distributed shared memory) after a
+// hardware cluster barrier; nothing of the V-cycle goes through global memory
+// between the input r and the output z, except the coarse levels' r and z
+// (CTA 0 reads and writes them in the plan's level-lb arrays).  The arithmetic
+// per cell is the streamed kernel's (masked z, the reference's neighbour-sum
+// order, IEEE division), so the V-cycle's float32 values are the same bit for
+// bit.
+//
+// Shared memory per brick level: zs, the masked z of the brick with its
+// one-cell ring ((B0+2)(B1+2)(B2+2) floats; 0 on non-FLUID cells and outside
+// the level), rs, B0 B1 B2 floats holding r on FLUID cells and the unmasked z
+// on the others (which prolongation carries, mgpcg.py:120-123), and, when
+// they fit, the brick's Adiag (else read from global memory, read-only here).
+// Adiag tells FLUID cells (nonzero on exactly the FLUID cells of a
+// label-uniform level).
+//
+// Ring reads and the barrier: after a half sweep of colour c every CTA
+// arrives at the cluster barrier (release) and waits (acquire), then copies
+// the colour-c cells of its ring from its neighbours' faces.  Meanwhile a
+// neighbour may already smooth the other colour, which writes no colour-c
+// cell; colour-c cells change again only after the next barrier, which the
+// reader reaches after its copy.  The copies before a restriction and after a
+// prolongation take both colours: a cell of the colour being smoothed that is
+// read early is copied again before it is used.  A final barrier keeps every
+// CTA's shared memory alive until its neighbours' last reads.
+#pragma once
+#include <cooperative_groups.h>
+
+#include "mg_coarse.cuh"
+
+namespace mg {
+
+namespace cgx = cooperative_groups;
+
+#ifndef MG_RESIDENT_THREADS
+#define MG_RESIDENT_THREADS 1024
+#endif
+constexpr int kResThreads = MG_RESIDENT_THREADS;
+constexpr int kResMaxCtas = 16;  // non-portable cluster size of B200
+
+struct ResLevel {
+  int lb[3];         // log2 of the brick extent per axis
+  int n[3];          // extent of the level
+  int zoff, roff;    // offsets (floats) of zs and rs in shared memory
+  int aoff;          // offset of the brick's Adiag in shared memory, -1: global
+  float s;           // kappa * s_l
+  const float* Ad;   // Adiag of the level (float32)
+};
+
+struct ResArgs {
+  int nlev;          // brick levels lp .. lp + nlev - 1 (lp + nlev = lb)
+  int nb[3];         // bricks (CTAs) per axis
+  int ns;            // half sweeps per smoothing (2 pre_post)
+  float rho, pi;
+  ResLevel lv[kMaxLevels];
+  const float* r0;   // r of level lp
+  float* z0;         // z of level lp (written: the unmasked z)
+  float* rc;         // r of level lb (written by the last restriction)
+  const float* zc;   // z of level lb (written by the coarse phase)
+  CoarseArgs coarse; // levels lb .. L-1, run by CTA 0
+  int coff;          // offset (floats) of the coarse region in shared memory
+  int smem_floats;   // dynamic shared memory, in floats
+};
+
+// Brick geometry of one level for the calling CTA.
+struct RB {
+  int B0, B1, B2, l0, l1, l2;   // extents and their log2
+  int o0, o1, o2;               // origin of the brick in the level
+  int n0, n1, n2;
+  int P1, P2;                   // padded strides: zs index ((c0+1) P1 + c1+1) P2 + c2+1
+  float* zs;
+  float* rs;
+  const float* sa;              // Adiag of the brick in shared memory, or null
+  const float* Ad;              // Adiag of the level in global memory
+  float ms;                     // -(kappa s_l)
+  __device__ __forceinline__ int zp(int c0, int c1, int c2) const { return ((c0 + 1) * P1 + (c1 + 1)) * P2 + c2 + 1; }
+  __device__ __forceinline__ int ri(int c0, int c1, int c2) const { return (((c0 << l1) + c1) << l2) + c2; }
+  __device__ __forceinline__ int gi(int c0, int c1, int c2) const {
+    return ((o0 + c0) * n1 + (o1 + c1)) * n2 + (o2 + c2);
+  }
+  __device__ __forceinline__ float ad(int c0, int c1, int c2) const {
+    return sa ? sa[ri(c0, c1, c2)] : __ldg(Ad + gi(c0, c1, c2));
+  }
+};
+
+__device__ __forceinline__ RB res_brick(const ResArgs& A, int i, float* sm, int rank) {
+  const ResLevel& L = A.lv[i];
+  RB b;
+  b.l0 = L.lb[0];
+  b.l1 = L.lb[1];
+  b.l2 = L.lb[2];
+  b.B0 = 1 << b.l0;
+  b.B1 = 1 << b.l1;
+  b.B2 = 1 << b.l2;
+  const int bx = rank % A.nb[2];
+  const int t = rank / A.nb[2];
+  const int by = t % A.nb[1], bz = t / A.nb[1];
+  b.o0 = bz << b.l0;
+  b.o1 = by << b.l1;
+  b.o2 = bx << b.l2;
+  b.n0 = L.n[0];
+  b.n1 = L.n[1];
+  b.n2 = L.n[2];
+  b.P1 = b.B1 + 2;
+  b.P2 = b.B2 + 2;
+  b.zs = sm + L.zoff;
+  b.rs = sm + L.roff;
+  b.sa = L.aoff >= 0 ? sm + L.aoff : nullptr;
+  b.Ad = L.Ad;
+  b.ms = -L.s;
+  return b;
+}
+
+// Neighbour sum (mgpcg.py:96-102) on the masked padded brick, in the
+// streamed kernel's order: axis 0, axis 1, axis 2, each (lower + upper).
+__device__ __forceinline__ float res_nsum(const RB& b, int p) {
+  const float* z = b.zs;
+  const int s0 = b.P1 * b.P2, s1 = b.P2;
+  float ret = 0.0f;
+  ret = __fadd_rn(ret, __fadd_rn(__fmul_rn(b.ms, z[p - s0]), __fmul_rn(b.ms, z[p + s0])));
+  ret = __fadd_rn(ret, __fadd_rn(__fmul_rn(b.ms, z[p - s1]), __fmul_rn(b.ms, z[p + s1])));
+  ret = __fadd_rn(ret, __fadd_rn(__fmul_rn(b.ms, z[p - 1]), __fmul_rn(b.ms, z[p + 1])));
+  return ret;
+}
+
+// j-th cell of colour `col` in the brick: rows (c0, c1) of B2/2 cells.
+__device__ __forceinline__ void res_colour_cell(const RB& b, int j, int col, int& c0, int& c1, int& c2) {
+  const int lh = b.l2 - 1;
+  const int row = j >> lh;
+  const int k = j - (row << lh);
+  c1 = row & (b.B1 - 1);
+  c0 = row >> b.l1;
+  c2 = 2 * k + ((col - b.o0 - b.o1 - b.o2 - c0 - c1) & 1);
+}
+
+// One red-black half sweep (mgpcg.py:104-109) of colour `col` over the brick,
+// two cells per thread and iteration, both computed before either is stored.
+__device__ __forceinline__ void res_smooth(const RB& b, int col) {
+  const int cnt = (b.B0 * b.B1 * b.B2) >> 1;
+  for (int j0 = threadIdx.x; j0 < cnt; j0 += 2 * blockDim.x) {
+    int pz[2];
+    float val[2];
+    bool ok[2];
+#pragma unroll
+    for (int u = 0; u < 2; ++u) {
+      const int j = min(j0 + u * (int)blockDim.x, cnt - 1);
+      int c0, c1, c2;
+      res_colour_cell(b, j, col, c0, c1, c2);
+      pz[u] = b.zp(c0, c1, c2);
+      const float a = b.ad(c0, c1, c2);
+      ok[u] = j0 + u * (int)blockDim.x < cnt && a != 0.0f;
+      val[u] = ok[u] ? __fdiv_rn(__fsub_rn(b.rs[b.ri(c0, c1, c2)], res_nsum(b, pz[u])), a) : 0.0f;
+    }
+#pragma unroll
+    for (int u = 0; u < 2; ++u)
+      if (ok[u]) b.zs[pz[u]] = val[u];
+  }
+}
+
+// Cluster barrier, then the ring cells of the colours in cmask (bit c: colour
+// c) that lie inside the level, copied from the neighbours' face cells.  Ring
+// cells are enumerated face by face (axis 0, 1, 2; lower side, upper side).
+__device__ __forceinline__ void res_exchange(const RB& b, const ResArgs& A, int rank, int cmask) {
+  cgx::cluster_group cl = cgx::this_cluster();
+  cl.sync();
+  const int a0 = b.B1 * b.B2, a1 = b.B0 * b.B2, a2 = b.B0 * b.B1;
+  const int nf = 2 * (a0 + a1 + a2);
+  const int par = b.o0 + b.o1 + b.o2;
+  const int st1 = A.nb[2], st0 = A.nb[1] * A.nb[2];
+  for (int f = threadIdx.x; f < nf; f += blockDim.x) {
+    int c0, c1, c2, q0, q1, q2, nbr, side, u, g = f;
+    if (g < 2 * a0) {
+      side = g >= a0;
+      u = g - side * a0;
+      c1 = q1 = u >> b.l2;
+      c2 = q2 = u & (b.B2 - 1);
+      c0 = side ? b.B0 : -1;
+      q0 = side ? 0 : b.B0 - 1;
+      nbr = rank + (side ? st0 : -st0);
+      if (side ? b.o0 + b.B0 >= b.n0 : b.o0 == 0) continue;
+    } else if ((g -= 2 * a0) < 2 * a1) {
+      side = g >= a1;
+      u = g - side * a1;
+      c0 = q0 = u >> b.l2;
+      c2 = q2 = u & (b.B2 - 1);
+      c1 = side ? b.B1 : -1;
+      q1 = side ? 0 : b.B1 - 1;
+      nbr = rank + (side ? st1 : -st1);
+      if (side ? b.o1 + b.B1 >= b.n1 : b.o1 == 0) continue;
+    } else {
+      g -= 2 * a1;
+      side = g >= a2;
+      u = g - side * a2;
+      c0 = q0 = u >> b.l1;
+      c1 = q1 = u & (b.B1 - 1);
+      c2 = side ? b.B2 : -1;
+      q2 = side ? 0 : b.B2 - 1;
+      nbr = rank + (side ? 1 : -1);
+      if (side ? b.o2 + b.B2 >= b.n2 : b.o2 == 0) continue;
+    }
+    if (!((cmask >> ((par + c0 + c1 + c2) & 1)) & 1)) continue;
+    const float* rz = cl.map_shared_rank(b.zs, nbr);  // the neighbour's zs of this level
+    b.zs[b.zp(c0, c1, c2)] = rz[b.zp(q0, q1, q2)];
+  }
+  __syncthreads();
+}
+
+__global__ void __launch_bounds__(kResThreads, 1) k_resident(ResArgs A) {
+  extern __shared__ __align__(16) unsigned char smem[];
+  float* sm = (float*)smem;
+  cgx::cluster_group cl = cgx::this_cluster();
+  const int rank = (int)cl.block_rank();
+  const int nlev = A.nlev;
+
+  for (int i = threadIdx.x; i < A.coff; i += blockDim.x) sm[i] = 0.0f;
+  __syncthreads();
+  for (int i = 0; i < nlev; ++i) {  // the bricks' Adiag, where it has room
+    const RB b = res_brick(A, i, sm, rank);
+    if (!b.sa) continue;
+    float* sa = sm + A.lv[i].aoff;
+    const int cells = b.B0 * b.B1 * b.B2;
+#pragma unroll 4
+    for (int j = threadIdx.x; j < cells; j += blockDim.x) {
+      const int c2 = j & (b.B2 - 1), c1 = (j >> b.l2) & (b.B1 - 1), c0 = j >> (b.l1 + b.l2);
+      sa[j] = __ldg(b.Ad + b.gi(c0, c1, c2));
+    }
+  }
+  __syncthreads();
+
+  // ---- pre-smoothing and restriction, finest to coarsest ----------------------
+  for (int i = 0; i < nlev; ++i) {
+    const RB b = res_brick(A, i, sm, rank);
+    const int cells = b.B0 * b.B1 * b.B2;
+    if (i == 0) {  // r of level lp (FLUID cells; the others hold z = 0)
+#pragma unroll 4
+      for (int j = threadIdx.x; j < cells; j += blockDim.x) {
+        const int c2 = j & (b.B2 - 1), c1 = (j >> b.l2) & (b.B1 - 1), c0 = j >> (b.l1 + b.l2);
+        const float r = __ldcg(A.r0 + b.gi(c0, c1, c2));
+        b.rs[j] = b.ad(c0, c1, c2) != 0.0f ? r : 0.0f;
+      }
+      __syncthreads();
+    }
+    // first half sweep from z = 0: pointwise on colour 0
+    for (int j = threadIdx.x; j < (cells >> 1); j += blockDim.x) {
+      int c0, c1, c2;
+      res_colour_cell(b, j, 0, c0, c1, c2);
+      const float a = b.ad(c0, c1, c2);
+      if (a != 0.0f) b.zs[b.zp(c0, c1, c2)] = __fdiv_rn(b.rs[b.ri(c0, c1, c2)], a);
+    }
+    for (int m = 2; m <= A.ns; ++m) {
+      res_exchange(b, A, rank, 1 << ((m - 2) & 1));  // the colour of half sweep m - 1
+      res_smooth(b, (m - 1) & 1);
+    }
+    res_exchange(b, A, rank, 1 << ((A.ns - 1) & 1));
+    // restriction (mgpcg.py:111-118): coarse r = rho * sum over the FLUID
+    // children (lexicographic order) of r - A z; a coarse cell of the brick
+    // has all 8 children in the brick
+    const bool last = i + 1 == nlev;
+    RB c;
+    if (!last) c = res_brick(A, i + 1, sm, rank);
+    const int cl1 = b.l1 - 1, cl2 = b.l2 - 1;
+    const int ccells = cells >> 3;
+    const int cn1 = b.n1 >> 1, cn2 = b.n2 >> 1;
+    for (int j = threadIdx.x; j < ccells; j += blockDim.x) {
+      const int q2 = j & ((1 << cl2) - 1), q1 = (j >> cl2) & ((1 << cl1) - 1), q0 = j >> (cl1 + cl2);
+      float acc = 0.0f;
+#pragma unroll
+      for (int o0 = 0; o0 < 2; ++o0)
+#pragma unroll
+        for (int o1 = 0; o1 < 2; ++o1)
+#pragma unroll
+          for (int o2 = 0; o2 < 2; ++o2) {
+            const int f0 = 2 * q0 + o0, f1 = 2 * q1 + o1, f2 = 2 * q2 + o2;
+            const float a = b.ad(f0, f1, f2);
+            if (a != 0.0f) {
+              const int p = b.zp(f0, f1, f2);
+              const float Az = __fadd_rn(__fmul_rn(a, b.zs[p]), res_nsum(b, p));
+              acc = __fadd_rn(acc, __fsub_rn(b.rs[b.ri(f0, f1, f2)], Az));
+            }
+          }
+      const float rv = __fmul_rn(A.rho, acc);
+      if (last) {
+        const int g = (((b.o0 >> 1) + q0) * cn1 + ((b.o1 >> 1) + q1)) * cn2 + ((b.o2 >> 1) + q2);
+        __stcg(A.rc + g, rv);
+      } else {
+        // a non-FLUID coarse cell keeps rs = 0: its unmasked z
+        c.rs[j] = c.ad(q0, q1, q2) != 0.0f ? rv : 0.0f;
+      }
+    }
+    __syncthreads();
+  }
+
+  // ---- the coarse levels in CTA 0 -------------------------------------------------
+  cl.sync();  // level lb's r is complete
+  if (rank == 0) coarse_vcycle<float, false>(A.coarse, smem + (size_t)A.coff * 4);
+  cl.sync();  // level lb's z is complete
+
+  // ---- prolongation and post-smoothing, coarsest to finest -----------------------
+  for (int i = nlev - 1; i >= 0; --i) {
+    const RB b = res_brick(A, i, sm, rank);
+    const int cells = b.B0 * b.B1 * b.B2;
+    const bool last = i + 1 == nlev;
+    RB c;
+    if (!last) c = res_brick(A, i + 1, sm, rank);
+    const int cn1 = b.n1 >> 1, cn2 = b.n2 >> 1;
+    // prolongation (mgpcg.py:120-123): every cell += the parent's unmasked z
+#pragma unroll 4
+    for (int j = threadIdx.x; j < cells; j += blockDim.x) {
+      const int c2 = j & (b.B2 - 1), c1 = (j >> b.l2) & (b.B1 - 1), c0 = j >> (b.l1 + b.l2);
+      const int q0 = c0 >> 1, q1 = c1 >> 1, q2 = c2 >> 1;
+      float zc;
+      if (last) {
+        zc = __ldcg(A.zc + (((b.o0 >> 1) + q0) * cn1 + ((b.o1 >> 1) + q1)) * cn2 + ((b.o2 >> 1) + q2));
+      } else {
+        const int qr = (((q0 << c.l1) + q1) << c.l2) + q2;
+        zc = c.ad(q0, q1, q2) != 0.0f ? c.zs[c.zp(q0, q1, q2)] : c.rs[qr];
+      }
+      const float v = __fmul_rn(A.pi, zc);
+      if (b.ad(c0, c1, c2) != 0.0f) {
+        const int p = b.zp(c0, c1, c2);
+        b.zs[p] = __fadd_rn(b.zs[p], v);
+      } else {
+        b.rs[j] = __fadd_rn(b.rs[j], v);
+      }
+    }
+    __syncthreads();
+    // post-smoothing: colours 1, 0, 1, 0 ... (mgpcg.py:144-147), each after
+    // the ring of the colour smoothed last (both after the prolongation)
+    for (int m = 1; m <= A.ns; ++m) {
+      res_exchange(b, A, rank, m == 1 ? 3 : 1 << ((m - 1) & 1));
+      res_smooth(b, m & 1);
+    }
+    __syncthreads();
+  }
+
+  // ---- z of level lp ---------------------------------------------------------------
+  {
+    const RB b = res_brick(A, 0, sm, rank);
+    const int cells = b.B0 * b.B1 * b.B2;
+#pragma unroll 4
+    for (int j = threadIdx.x; j < cells; j += blockDim.x) {
+      const int c2 = j & (b.B2 - 1), c1 = (j >> b.l2) & (b.B1 - 1), c0 = j >> (b.l1 + b.l2);
+      A.z0[b.gi(c0, c1, c2)] = b.ad(c0, c1, c2) != 0.0f ? b.zs[b.zp(c0, c1, c2)] : b.rs[j];
+    }
+  }
+  cl.sync();  // the neighbours' last ring reads are done
+}
+
+}  // namespace mg

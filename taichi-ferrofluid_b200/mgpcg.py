@@ -179,6 +179,18 @@ class MGPCGPoissonSolver:
                                      mg_lib.ctypes.byref(n)), "mg_plan_split")
         return int(b.value), int(n.value)
 
+    def resident(self, on=None, first_level=None):
+        """(on, first level): whether the V-cycle runs its levels from the first
+        brick level down as one thread-block-cluster launch (the autotuner's
+        choice), and that level (-1: the shape has none); ``on`` forces a
+        choice until the next prepare, ``first_level`` (with ``on``) the level
+        the cluster starts at."""
+        o = mg_lib.ctypes.c_int32(0 if on is None else int(bool(on)))
+        lp = mg_lib.ctypes.c_int32(-1 if first_level is None else int(first_level))
+        check(self.lib.mg_plan_resident(self.plan, 0 if on is None else 1, mg_lib.ctypes.byref(o),
+                                        mg_lib.ctypes.byref(lp)), "mg_plan_resident")
+        return bool(o.value), int(lp.value)
+
     def operator_form(self, level=0):
         f = mg_lib.ctypes.c_int32()
         check(self.lib.mg_plan_operator_form(self.plan, level, mg_lib.ctypes.byref(f)), "mg_plan_operator_form")
