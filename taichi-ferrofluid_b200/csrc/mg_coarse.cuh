@@ -144,7 +144,7 @@ __device__ void coarse_smooth(const CoarseArgs& A, int l, int phase, float* zm, 
 // times 12 bytes, plus the couplings for STO): k_coarse runs it as its own
 // launch, the cluster-resident V-cycle (mg_resident.cuh) in its CTA 0.
 template <typename ST, bool STO = false>
-__device__ void coarse_vcycle(const CoarseArgs& A, unsigned char* smem) {
+__device__ __forceinline__ void coarse_vcycle(const CoarseArgs& A, unsigned char* smem) {
   static_assert(!STO || sizeof(ST) == 4, "the stored form runs on float32 grids");
   float* zm = (float*)smem;
   float* sr = zm + A.total;

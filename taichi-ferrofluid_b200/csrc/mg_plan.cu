@@ -352,8 +352,9 @@ int tune_split(mg_plan* P, cudaStream_t s) {
 // with the cluster starting at each feasible level (CUDA events, one warm-up,
 // three timed) the first time a shape is prepared, and the fastest kept,
 // cached per shape for the process.  All compute the same float32 values.
-// MGPCG_RESIDENT=0 / 1 replaces the timing (1: the cluster from the first
-// feasible level).
+// MGPCG_RESIDENT=<level> (the cluster from the first feasible level from
+// there) or MGPCG_RESIDENT=off replaces the timing, e.g. for profilers, which
+// serialise the trial launches.
 std::map<std::array<int, 7>, int> g_tune_res;  // first brick level, -1: streamed
 
 // The cluster plan from the first feasible level in [lp_min, lp_max], checked
@@ -390,20 +391,24 @@ int tune_resident(mg_plan* P, cudaStream_t s) {
   if (!P->fp.valid) return MG_OK;
   if (!plan_resident(P, 0, P->L, s)) return MG_OK;
   const int lp_first = P->fp.res_lp;
-  if (const char* ov = std::getenv("MGPCG_RESIDENT")) {
-    P->fp.res = std::strtol(ov, nullptr, 0) != 0;
+  if (const char* ov = std::getenv("MGPCG_RESIDENT")) {  // "off" / -1, or a start level
+    const long v = std::strcmp(ov, "off") == 0 ? -1 : std::strtol(ov, nullptr, 0);
+    if (v >= 0 && plan_resident(P, (int)v, P->L, s)) P->fp.res = true;
+    else plan_resident(P, lp_first, lp_first, s);
     return MG_OK;
   }
   const Geom& g = P->geom[0];
   const std::array<int, 7> key = {g.dim, g.n[0], g.n[1], g.n[2], P->L, P->d.pre_post, P->fp.lc};
+  int cached = -2;  // -2: not timed yet
   {
     std::lock_guard<std::mutex> lk(g_tune_mu);
     auto it = g_tune_res.find(key);
-    if (it != g_tune_res.end()) {
-      if (it->second >= 0 && plan_resident(P, it->second, it->second, s)) P->fp.res = true;
-      else plan_resident(P, lp_first, lp_first, s);
-      return MG_OK;
-    }
+    if (it != g_tune_res.end()) cached = it->second;
+  }
+  if (cached != -2) {  // (plan_resident takes the lock itself)
+    if (cached >= 0 && plan_resident(P, cached, cached, s)) P->fp.res = true;
+    else plan_resident(P, lp_first, lp_first, s);
+    return MG_OK;
   }
   cudaEvent_t e0 = nullptr, e1 = nullptr;
   CK(cudaEventCreate(&e0));
