@@ -241,6 +241,53 @@ __global__ void __launch_bounds__(kRedThreads) k_Ap_alpha(Level L, const float* 
 // extent a multiple of 4): 16-byte loads of labels, Adiag, p, the stored
 // couplings and the neighbour rows; the neighbour sum of nbr_sum_f32 per
 // cell in the same order.  Ap written on FLUID cells only.
+// Coordinates of the 4-cell groups a grid-stride loop visits, advanced by the
+// fixed stride without integer division: cell i = 4q of the level has
+// x = i % nx along the fastest axis and t = i / nx = c0 n1 + c1 (2D: c0 = t).
+struct GroupWalk {
+  int x, c0, c1;     // coordinates of the current group's first cell
+  int dx, dc0, dc1;  // the loop's stride in cells, split the same way
+  int nx, n1, dim;
+  __device__ __forceinline__ GroupWalk(const Geom& g, int q, int stride_groups) {
+    dim = g.dim;
+    nx = g.n[dim - 1];
+    n1 = g.n[1];
+    const long long i = 4LL * q, di = 4LL * stride_groups;
+    const long long t = i / nx, dt = di / nx;
+    x = (int)(i % nx);
+    dx = (int)(di % nx);
+    if (dim == 3) {
+      c0 = (int)(t / n1);
+      c1 = (int)(t % n1);
+      dc0 = (int)(dt / n1);
+      dc1 = (int)(dt % n1);
+    } else {
+      c0 = (int)t;
+      c1 = 0;
+      dc0 = (int)dt;
+      dc1 = 0;
+    }
+  }
+  __device__ __forceinline__ void advance() {
+    x += dx;
+    int carry = 0;
+    if (x >= nx) {
+      x -= nx;
+      carry = 1;
+    }
+    if (dim == 3) {
+      c1 += dc1 + carry;
+      c0 += dc0;
+      if (c1 >= n1) {
+        c1 -= n1;
+        c0 += 1;
+      }
+    } else {
+      c0 += dc0 + carry;
+    }
+  }
+};
+
 __global__ void __launch_bounds__(kRedThreads) k_Ap_alpha4(Level L, const float* __restrict__ p,
                                                            float* __restrict__ Ap, Control* ctl, double* partials,
                                                            int force = 0) {
@@ -369,18 +416,16 @@ __global__ void __launch_bounds__(kRedThreads) k_Ap_alpha_uniform4(Level L, cons
   const int nx = L.g.n[dim - 1];
   const int groups = (int)(L.g.count >> 2);
   double acc = 0.0;
-  for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < groups; q += gridDim.x * blockDim.x) {
+  const int q0 = blockIdx.x * blockDim.x + threadIdx.x, S = gridDim.x * blockDim.x;
+  GroupWalk w(L.g, q0, S);
+  for (int q = q0; q < groups; q += S, w.advance()) {
     const int i = q << 2;
     const float4 a = __ldg(reinterpret_cast<const float4*>(L.Adiag + i));
+    // a group without a FLUID cell loads nothing more (large AIR regions at
+    // sizes beyond L2)
     if (a.x == 0.0f && a.y == 0.0f && a.z == 0.0f && a.w == 0.0f) continue;
-    const int x = i % nx, t = i / nx;
-    int c[2];  // coordinates of the slower axes
-    if (dim == 3) {
-      c[0] = t / L.g.n[1];
-      c[1] = t - c[0] * L.g.n[1];
-    } else {
-      c[0] = t;
-    }
+    const int x = w.x;
+    const int c[2] = {w.c0, w.c1};  // coordinates of the slower axes
     const float4 pc = __ldg(reinterpret_cast<const float4*>(p + i));
     const float pxl = x > 0 ? __ldg(p + i - 1) : 0.0f;
     const float pxr = x + 4 < nx ? __ldg(p + i + 4) : 0.0f;
@@ -452,6 +497,60 @@ __global__ void __launch_bounds__(kRedThreads) k_xr(Level L, float* __restrict__
     float ri = __fsub_rn(r[i], __fmul_rn(alpha, Ap[i]));
     r[i] = ri;
     acc += (double)ri * (double)ri;
+  }
+  double tot;
+  if (last_block_total<kRedThreads>(acc, partials, &ctl->counter[3], sh, &tot) && threadIdx.x == 0) {
+    ctl->rTr = tot;
+    if (!isfinite(tot)) {
+      ctl->status = MG_SOLVE_NONFINITE;
+      ctl->run = 0;
+    } else if (tot < ctl->tol) {
+      ctl->status = MG_SOLVE_CONVERGED;
+      ctl->run = 0;
+    }
+    ctl->since_refresh += 1;
+    set_scales(ctl, tot);
+    if (has_cond) cudaGraphSetConditional(cond, ctl->run ? 1u : 0u);
+  }
+}
+
+// k_xr on 4-cell groups (one 16-byte vector of x, p, r, Ap and one 32-bit
+// word of labels per group; the cell count a multiple of 4): the same
+// per-cell arithmetic, r.r summed group by group.
+__global__ void __launch_bounds__(kRedThreads) k_xr4(Level L, float* __restrict__ x,
+                                                     const float* __restrict__ p,
+                                                     const float* __restrict__ Ap, Control* ctl,
+                                                     double* partials, cudaGraphConditionalHandle cond,
+                                                     int has_cond, int force = 0) {
+  pdl_enter();
+  __shared__ double sh[32];
+  if (!ctl->run && !force) {
+    if (has_cond && blockIdx.x == 0 && threadIdx.x == 0) cudaGraphSetConditional(cond, 0);
+    return;
+  }
+  const float alpha = ctl->alpha;
+  float* r = (float*)L.r;
+  const int groups = (int)(L.g.count >> 2);
+  double acc = 0.0;
+  for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < groups; q += gridDim.x * blockDim.x) {
+    const uint32_t t4 = __ldg(reinterpret_cast<const uint32_t*>(L.type) + q);
+    float4 xv = reinterpret_cast<float4*>(x)[q];
+    const float4 pv = __ldg(reinterpret_cast<const float4*>(p) + q);
+    float4 rv = reinterpret_cast<float4*>(r)[q];
+    const float4 av = __ldg(reinterpret_cast<const float4*>(Ap) + q);
+    if (t4 == 0x02020202u || t4 == 0x01010101u) continue;  // no FLUID lane
+    float* xs = reinterpret_cast<float*>(&xv);
+    float* rs = reinterpret_cast<float*>(&rv);
+    const float ps[4] = {pv.x, pv.y, pv.z, pv.w}, as[4] = {av.x, av.y, av.z, av.w};
+#pragma unroll
+    for (int e = 0; e < 4; ++e) {
+      if (!fluid_lane(t4, e)) continue;
+      xs[e] = __fadd_rn(xs[e], __fmul_rn(alpha, ps[e]));
+      rs[e] = __fsub_rn(rs[e], __fmul_rn(alpha, as[e]));
+      acc += (double)rs[e] * (double)rs[e];
+    }
+    reinterpret_cast<float4*>(x)[q] = xv;
+    reinterpret_cast<float4*>(r)[q] = rv;
   }
   double tot;
   if (last_block_total<kRedThreads>(acc, partials, &ctl->counter[3], sh, &tot) && threadIdx.x == 0) {

@@ -284,10 +284,13 @@ int launch_vcycle(mg_plan* P, cudaStream_t s) {
 // for the whole-domain stored form, which stages 24 bytes a cell, the
 // per-kernel passes win on the large levels and the streamed kernel on the
 // small ones.  So for the stored form each streamed level is timed both ways
-// (CUDA events on the plan's stream, after one warm-up) the first time a
+// (CUDA events on the plan's stream, one warm-up, kTuneReps timed) the first time a
 // shape is prepared, and the faster is kept; the choice is cached per shape
 // for the process.  Both variants compute the same float32 values.
 std::mutex g_tune_mu;
+// timed repetitions of each variant (after one warm-up); with three, the
+// choice for levels of ~20 us flipped between runs
+constexpr int kTuneReps = 10;
 std::map<std::array<int, 7>, uint32_t> g_tune;  // bit l: split level l
 
 int tune_split(mg_plan* P, cudaStream_t s) {
@@ -322,7 +325,7 @@ int tune_split(mg_plan* P, cudaStream_t s) {
     float t[2] = {0.0f, 0.0f};
     for (int mode = 0; mode < 2 && rc == MG_OK; ++mode) {
       P->fp.split[l] = mode == 1;
-      for (int rep = 0; rep < 4 && rc == MG_OK; ++rep) {  // rep 0 warms up
+      for (int rep = 0; rep < 1 + kTuneReps && rc == MG_OK; ++rep) {  // rep 0 warms up
         if (rep == 1) cudaEventRecord(e0, s);
         rc = launch_level(P, l, true, s);
         if (rc == MG_OK) rc = launch_level(P, l, false, s);
@@ -350,7 +353,7 @@ int tune_split(mg_plan* P, cudaStream_t s) {
 // The cluster-resident V-cycle against the streamed one: for a label-uniform
 // float32 plan whose levels allow bricks, the V-cycle is timed streamed and
 // with the cluster starting at each feasible level (CUDA events, one warm-up,
-// three timed) the first time a shape is prepared, and the fastest kept,
+// kTuneReps timed) the first time a shape is prepared, and the fastest kept,
 // cached per shape for the process.  All compute the same float32 values.
 // MGPCG_RESIDENT=<level> (the cluster from the first feasible level from
 // there) or MGPCG_RESIDENT=off replaces the timing, e.g. for profilers, which
@@ -419,7 +422,7 @@ int tune_resident(mg_plan* P, cudaStream_t s) {
   }
   auto time_vcycle = [&](float* ms) -> int {
     int rc = MG_OK;
-    for (int rep = 0; rep < 4 && rc == MG_OK; ++rep) {  // rep 0 warms up
+    for (int rep = 0; rep < 1 + kTuneReps && rc == MG_OK; ++rep) {  // rep 0 warms up
       if (rep == 1) cudaEventRecord(e0, s);
       rc = launch_vcycle_fused(P, s);
     }
@@ -519,8 +522,12 @@ int launch_cg_tail(mg_plan* P, cudaStream_t s, int which) {
   if (which & 2) {
     const float* pc = p;
     const float* Apc = Ap;
-    CK(launch_k(k_xr, RB, kRedThreads, 0, s, L0, x, pc, Apc, P->ctl, P->partials, P->cond,
-                refresh ? 0 : P->has_cond, 0));
+    if (P->geom[0].count % 4 == 0)  // 4-cell groups
+      CK(launch_k(k_xr4, RB, kRedThreads, 0, s, L0, x, pc, Apc, P->ctl, P->partials, P->cond,
+                  refresh ? 0 : P->has_cond, 0));
+    else
+      CK(launch_k(k_xr, RB, kRedThreads, 0, s, L0, x, pc, Apc, P->ctl, P->partials, P->cond,
+                  refresh ? 0 : P->has_cond, 0));
     if (refresh) {
       const float* bc = b;
       CK(launch_k(k_refresh, RB, kRedThreads, 0, s, L0, bc, x, P->ctl, P->partials, P->cond, P->has_cond));
@@ -1441,8 +1448,12 @@ int mg_launch_stage(mg_plan_t* P, int32_t stage, int32_t level, void* stream) {
       CKL("k_Ap_alpha");
       return MG_OK;
     case 4:
-      k_xr<<<P->red_blocks, kRedThreads, 0, s>>>(L0, fptr(P, MG_FIELD_X), fptr(P, MG_FIELD_P),
-                                                 fptr(P, MG_FIELD_AP), P->ctl, P->partials, P->cond, 0, 1);
+      if (P->geom[0].count % 4 == 0)
+        k_xr4<<<P->red_blocks, kRedThreads, 0, s>>>(L0, fptr(P, MG_FIELD_X), fptr(P, MG_FIELD_P),
+                                                    fptr(P, MG_FIELD_AP), P->ctl, P->partials, P->cond, 0, 1);
+      else
+        k_xr<<<P->red_blocks, kRedThreads, 0, s>>>(L0, fptr(P, MG_FIELD_X), fptr(P, MG_FIELD_P),
+                                                   fptr(P, MG_FIELD_AP), P->ctl, P->partials, P->cond, 0, 1);
       CKL("k_xr");
       return MG_OK;
     case 5:
