@@ -148,6 +148,19 @@ __device__ __forceinline__ void res_colour_cell(const RB& b, int j, int col, int
 // two cells per thread and iteration, both computed before either is stored.
 __device__ __forceinline__ void res_smooth(const RB& b, int col) {
   const int cnt = (b.B0 * b.B1 * b.B2) >> 1;
+  if (cnt <= (int)blockDim.x) {  // one cell per thread, no empty second item
+    const int j = threadIdx.x;
+    if (j < cnt) {
+      int c0, c1, c2;
+      res_colour_cell(b, j, col, c0, c1, c2);
+      const float a = b.ad(c0, c1, c2);
+      if (a != 0.0f) {
+        const int p = b.zp(c0, c1, c2);
+        b.zs[p] = __fdiv_rn(__fsub_rn(b.rs[b.ri(c0, c1, c2)], res_nsum(b, p)), a);
+      }
+    }
+    return;
+  }
   for (int j0 = threadIdx.x; j0 < cnt; j0 += 2 * blockDim.x) {
     int pz[2];
     float val[2];
