@@ -175,6 +175,162 @@ __global__ void k_smooth(Level L, int phase) {
   for (long long j = gtid(); j < n; j += gstride()) smooth_cell(L, j, phase);
 }
 
+// The stencil data of one 4-cell group along the fastest axis of a 3D f32
+// level (row (i0, i1), cells x .. x+3, x a multiple of 4): z and its six
+// neighbour directions, the couplings, r and Adiag, with 16-byte loads.
+struct Group4 {
+  float Z[4], Z0l[4], Z0h[4], Z1l[4], Z1h[4], zxl, zxh;
+  float A0l[4], A0h[4], A1l[4], A1h[4], A2c[4], a2l;
+  float R[4], D[4];
+  bool h0l, h0h, h1l, h1h;
+  int x, n2;
+};
+
+__device__ __forceinline__ void unpack4(const float4 v, float o[4]) {
+  o[0] = v.x;
+  o[1] = v.y;
+  o[2] = v.z;
+  o[3] = v.w;
+}
+
+__device__ __forceinline__ void load_group4(const Level& L, const float* z, int i0, int i1, int x, Group4& g) {
+  const int n0 = L.g.n[0], n1 = L.g.n[1], n2 = L.g.n[2];
+  const long long s0 = (long long)n1 * n2;
+  const int s1 = n2;
+  const long long idx = ((long long)i0 * n1 + i1) * n2 + x;
+  const float4 f0 = make_float4(0.f, 0.f, 0.f, 0.f);
+  g.x = x;
+  g.n2 = n2;
+  g.h0l = i0 > 0;
+  g.h0h = i0 + 1 < n0;
+  g.h1l = i1 > 0;
+  g.h1h = i1 + 1 < n1;
+  unpack4(*reinterpret_cast<const float4*>(z + idx), g.Z);
+  unpack4(g.h0l ? *reinterpret_cast<const float4*>(z + idx - s0) : f0, g.Z0l);
+  unpack4(g.h0h ? *reinterpret_cast<const float4*>(z + idx + s0) : f0, g.Z0h);
+  unpack4(g.h1l ? *reinterpret_cast<const float4*>(z + idx - s1) : f0, g.Z1l);
+  unpack4(g.h1h ? *reinterpret_cast<const float4*>(z + idx + s1) : f0, g.Z1h);
+  g.zxl = x > 0 ? z[idx - 1] : 0.0f;
+  g.zxh = x + 4 < n2 ? z[idx + 4] : 0.0f;
+  unpack4(g.h0l ? __ldg(reinterpret_cast<const float4*>(L.Ax[0] + idx - s0)) : f0, g.A0l);
+  unpack4(__ldg(reinterpret_cast<const float4*>(L.Ax[0] + idx)), g.A0h);
+  unpack4(g.h1l ? __ldg(reinterpret_cast<const float4*>(L.Ax[1] + idx - s1)) : f0, g.A1l);
+  unpack4(__ldg(reinterpret_cast<const float4*>(L.Ax[1] + idx)), g.A1h);
+  unpack4(__ldg(reinterpret_cast<const float4*>(L.Ax[2] + idx)), g.A2c);
+  g.a2l = x > 0 ? __ldg(L.Ax[2] + idx - 1) : 0.0f;
+  unpack4(__ldg(reinterpret_cast<const float4*>((const float*)L.r + idx)), g.R);
+  unpack4(__ldg(reinterpret_cast<const float4*>(L.Adiag + idx)), g.D);
+}
+
+// nbr_sum_f32 of the group's cell e, in its order (axis 0, 1, 2; lower + upper).
+__device__ __forceinline__ float group4_nsum(const Group4& g, int e) {
+  float ret = 0.0f;
+  ret = __fadd_rn(ret, __fadd_rn(g.h0l ? __fmul_rn(g.A0l[e], g.Z0l[e]) : 0.0f,
+                                 g.h0h ? __fmul_rn(g.A0h[e], g.Z0h[e]) : 0.0f));
+  ret = __fadd_rn(ret, __fadd_rn(g.h1l ? __fmul_rn(g.A1l[e], g.Z1l[e]) : 0.0f,
+                                 g.h1h ? __fmul_rn(g.A1h[e], g.Z1h[e]) : 0.0f));
+  const float lo = g.x + e > 0 ? __fmul_rn(e == 0 ? g.a2l : g.A2c[e - 1], e == 0 ? g.zxl : g.Z[e - 1]) : 0.0f;
+  const float hi = g.x + e + 1 < g.n2 ? __fmul_rn(g.A2c[e], e == 3 ? g.zxh : g.Z[e + 1]) : 0.0f;
+  return __fadd_rn(ret, __fadd_rn(lo, hi));
+}
+
+// smooth(l, phase) on a whole-domain level (every cell FLUID with a nonzero
+// diagonal: the stored form's levels), 3D with the fastest extent a multiple
+// of 4: one thread per 4-cell group, which holds two cells of the colour.
+// The same float32 operations in the same order as smooth_cell.  z of the
+// other colour (all a cell's neighbours) is not written during the half
+// sweep, so the group's loads see final values; each thread stores only its
+// two cells.
+__global__ void k_smooth_w4(Level L, int phase) {
+  pdl_enter();
+  const int n1 = L.g.n[1], n2 = L.g.n[2];
+  const int q2 = n2 >> 2;
+  const long long groups = L.g.count >> 2;
+  float* z = (float*)L.z;
+  for (long long q = gtid(); q < groups; q += gstride()) {
+    const long long row = q / q2;
+    const int x = (int)(q - row * q2) * 4;
+    const int i1 = (int)(row % n1), i0 = (int)(row / n1);
+    const int e0 = (phase - i0 - i1 - x) & 1;  // first cell of the colour in the group
+    Group4 g;
+    load_group4(L, z, i0, i1, x, g);
+    float out[2];
+#pragma unroll
+    for (int h = 0; h < 2; ++h) {
+      float v = 0.0f;
+#pragma unroll
+      for (int ee = 0; ee < 2; ++ee) {  // unrolled over both values of e0
+        const int e = ee + 2 * h;
+        if (ee == e0) v = __fdiv_rn(__fsub_rn(g.R[e], group4_nsum(g, e)), g.D[e]);
+      }
+      out[h] = v;
+    }
+    const long long idx = row * n2 + x;
+    z[idx + e0] = out[0];
+    z[idx + e0 + 2] = out[1];
+  }
+}
+
+// restrict(l) as k_restrict for a whole-domain fine level halving exactly
+// onto the coarse one, 3D, fine fastest extent a multiple of 4: one thread
+// per pair of coarse cells along the fastest axis, i.e. one 4-cell fine group
+// in each of the 2 x 2 fine rows; children summed in k_restrict's
+// lexicographic order.
+__global__ void k_restrict_w4(Level F, Level C) {
+  pdl_enter();
+  const float* zf = (const float*)F.z;
+  const int cn1 = C.g.n[1], cn2 = C.g.n[2];
+  const int pr = cn2 >> 1;  // coarse pairs per coarse row
+  const long long pairs = C.g.count >> 1;
+  for (long long t = gtid(); t < pairs; t += gstride()) {
+    const long long crow = t / pr;
+    const int cx = (int)(t - crow * pr) * 2;
+    const int c1 = (int)(crow % cn1), c0 = (int)(crow / cn1);
+    float acc[2] = {0.0f, 0.0f};
+#pragma unroll
+    for (int o0 = 0; o0 < 2; ++o0)
+#pragma unroll
+      for (int o1 = 0; o1 < 2; ++o1) {
+        Group4 g;
+        load_group4(F, zf, 2 * c0 + o0, 2 * c1 + o1, 2 * cx, g);
+#pragma unroll
+        for (int e = 0; e < 4; ++e) {
+          const float Az = __fadd_rn(__fmul_rn(g.D[e], g.Z[e]), group4_nsum(g, e));
+          acc[e >> 1] = __fadd_rn(acc[e >> 1], __fsub_rn(g.R[e], Az));
+        }
+      }
+    const long long ic = crow * cn2 + cx;
+    ((float*)C.r)[ic] = acc[0];
+    ((float*)C.r)[ic + 1] = acc[1];
+    ((float*)C.z)[ic] = 0.0f;
+    ((float*)C.z)[ic + 1] = 0.0f;
+  }
+}
+
+// prolongate(l) as k_prolongate for a fine level halving exactly onto the
+// coarse one, 3D, fine fastest extent a multiple of 4: one 4-cell group per
+// thread, two coarse values.
+__global__ void k_prolongate4(Level F, Level C) {
+  pdl_enter();
+  float* zf = (float*)F.z;
+  const float* zc = (const float*)C.z;
+  const int n1 = F.g.n[1], n2 = F.g.n[2], q2 = n2 >> 2;
+  const long long groups = F.g.count >> 2;
+  for (long long q = gtid(); q < groups; q += gstride()) {
+    const long long row = q / q2;
+    const int x = (int)(q - row * q2) * 4;
+    const int i1 = (int)(row % n1), i0 = (int)(row / n1);
+    const long long ic = C.g.index(i0 >> 1, i1 >> 1, x >> 1);
+    const float a = zc[ic], b = zc[ic + 1];
+    float4 v = reinterpret_cast<float4*>(zf)[q];
+    v.x = __fadd_rn(v.x, a);
+    v.y = __fadd_rn(v.y, a);
+    v.z = __fadd_rn(v.z, b);
+    v.w = __fadd_rn(v.w, b);
+    reinterpret_cast<float4*>(zf)[q] = v;
+  }
+}
+
 // restrict(l) (mgpcg.py:111-118) as a gather: coarse r = 0 + sum of the FLUID
 // children's (r - (Adiag z + nbr_sum)) in lexicographic child order.  Also
 // zeroes the coarse z (the r[l+1].fill(0), z[l+1].fill(0) of mgpcg.py:132-133).

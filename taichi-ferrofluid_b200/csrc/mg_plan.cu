@@ -173,17 +173,38 @@ int grid_for(const mg_plan* P, int64_t n, int threads = 256) {
 constexpr int64_t kBottomBlockCells = 1 << 16;
 
 int launch_smooth(mg_plan* P, int l, int phase, cudaStream_t s) {
+  if (P->whole[l] && P->d.dim == 3 && P->geom[l].n[2] % 4 == 0) {  // every cell FLUID: 4-cell groups
+    CK(launch_k(k_smooth_w4, grid_for(P, level_cells(P, l) / 4), 256, 0, s, P->lv[l], phase));
+    return MG_OK;
+  }
   int64_t n = level_cells(P, l) / 2 + level_cells(P, l) / (P->d.dim == 3 ? P->geom[l].n[2] : P->geom[l].n[1]);
   CK(launch_k(k_smooth, grid_for(P, n), 256, 0, s, P->lv[l], phase));
   return MG_OK;
 }
 
+// Level l+1 is level l halved exactly, 3D, level l's fastest extent a
+// multiple of 4 (the 4-cell-group restriction and prolongation).
+bool halves_by4(const mg_plan* P, int l) {
+  if (P->d.dim != 3 || P->geom[l].n[2] % 4 != 0) return false;
+  for (int a = 0; a < 3; ++a)
+    if (P->geom[l].n[a] != 2 * P->geom[l + 1].n[a]) return false;
+  return true;
+}
+
 int launch_restrict(mg_plan* P, int l, cudaStream_t s) {
+  if (P->whole[l] && halves_by4(P, l)) {
+    CK(launch_k(k_restrict_w4, grid_for(P, level_cells(P, l + 1) / 2), 256, 0, s, P->lv[l], P->lv[l + 1]));
+    return MG_OK;
+  }
   CK(launch_k(k_restrict, grid_for(P, level_cells(P, l + 1)), 256, 0, s, P->lv[l], P->lv[l + 1]));
   return MG_OK;
 }
 
 int launch_prolongate(mg_plan* P, int l, cudaStream_t s) {
+  if (halves_by4(P, l)) {
+    CK(launch_k(k_prolongate4, grid_for(P, level_cells(P, l) / 4), 256, 0, s, P->lv[l], P->lv[l + 1]));
+    return MG_OK;
+  }
   CK(launch_k(k_prolongate, grid_for(P, level_cells(P, l)), 256, 0, s, P->lv[l], P->lv[l + 1]));
   return MG_OK;
 }
