@@ -277,6 +277,39 @@ MG_API int mg_init_boundary(int32_t dim, const int32_t* res, int32_t* cell_type,
 MG_API int mg_level_set_redistance(int32_t dim, const int32_t* res, float* phi, float* phi_temp, int32_t* valid,
                                    double dx, int32_t repeat_times, void* stream);
 
+/* FastSweepingLevelSet.propagate (level_set.py:283-327) alone: the sweeps of
+ * mg_level_set_redistance on the caller's phi_temp (updated where valid is
+ * -1), with phi giving the sign. */
+MG_API int mg_level_set_propagate(int32_t dim, const int32_t* res, const float* phi, float* phi_temp,
+                                  const int32_t* valid, double dx, int32_t repeat_times, void* stream);
+
+/* FastSweepingLevelSet.build_from_markers (level_set.py:381-392), its first
+ * part: phi = 1e20, valid = -1, LevelSet.distance_to_markers
+ * (level_set.py:114-122: the cell of each marker - coordinates / dx
+ * truncated toward zero - takes the distance to its centre when smaller,
+ * valid = the marker's index), then markers_propagate (level_set.py:336-379:
+ * repeat_times rounds of 2 dim line sweeps; a cell takes the distance to the
+ * marker of its neighbour one step ahead when smaller).  markers: n_markers x
+ * dim float32 positions (device).  Where the reference's parallel loop races
+ * between markers of one cell, the cell keeps the smallest distance and,
+ * among equal ones, the smallest index; a neighbour without a marker is
+ * skipped (the reference reads markers[-1] there); markers with non-finite
+ * coordinates are ignored. */
+MG_API int mg_level_set_markers_distance(int32_t dim, const int32_t* res, float* phi, int32_t* valid,
+                                         const float* markers, int32_t n_markers, double dx, int32_t repeat_times,
+                                         void* stream);
+
+/* LevelSet.target_minus (level_set.py:124-146) after valid.fill(-1): phi -=
+ * 0.99 dx (the marker radius); cells beside a sign change with phi <= 0 and
+ * cells with phi > 0 are known (valid 0, phi_temp = phi), the other cells get
+ * phi_temp = -1 for mg_level_set_propagate. */
+MG_API int mg_level_set_target_minus(int32_t dim, const int32_t* res, float* phi, float* phi_temp, int32_t* valid,
+                                     double dx, void* stream);
+
+/* LevelSet.smoothing (level_set.py:148-163): out = min(mean of the in-range
+ * axis neighbours of in, in); out and in are different arrays of shape res. */
+MG_API int mg_level_set_smooth(int32_t dim, const int32_t* res, float* out, const float* in, void* stream);
+
 /* ---- the velocity steps around the projection (plan-free) ----------------
  * Velocity components vel0..2 are MAC face arrays of shape res + e_k; cell
  * arrays have shape res.

@@ -40,6 +40,10 @@ def _lib():
         lib.ors_apply_markers.argtypes = [ii, vp, vp, vp, ii]
         lib.ors_init_boundary.argtypes = [ii, vp, vp]
         lib.ors_redistance.argtypes = [ii, vp, vp, dd, ii, vp, vp]
+        lib.ors_markers_distance.argtypes = [ii, vp, vp, ii, ff, ii, vp, vp]
+        lib.ors_target_minus.argtypes = [ii, vp, vp, ff, vp, vp]
+        lib.ors_fs_propagate.argtypes = [ii, vp, vp, vp, vp, dd, ii]
+        lib.ors_ls_smooth.argtypes = [ii, vp, vp, vp]
         lib.ors_advect.argtypes = [ii, vp, vp, ii, vp, vp, ff, ff]
         lib.ors_extrapolate.argtypes = [ii, vp, ii, vp, vp, ii, vp]
         lib.ors_enforce_boundary.argtypes = [ii, vp, vp, vp]
@@ -215,6 +219,55 @@ def redistance(phi, dx, repeat_times=2):
     _lib().ors_redistance(ph.ndim, _res(ph.shape), ph.ctypes.data, float(dx), int(repeat_times), None,
                           valid.ctypes.data)
     return ph, valid
+
+
+def markers_distance(shape, markers, dx, repeat_times=2):
+    """FastSweepingLevelSet.build_from_markers' first part: distance_to_markers
+    and markers_propagate from phi = 1e20, valid = -1; returns (phi, valid)."""
+    mk = _f32(markers).reshape(-1, len(shape))
+    phi = np.zeros(shape, np.float32)
+    valid = np.zeros(shape, np.int32)
+    _lib().ors_markers_distance(len(shape), _res(shape), mk.ctypes.data, int(mk.shape[0]), float(np.float32(dx)),
+                                int(repeat_times), phi.ctypes.data, valid.ctypes.data)
+    return phi, valid
+
+
+def target_minus(phi, dx):
+    """LevelSet.target_minus after valid.fill(-1); returns (phi, phi_temp, valid)."""
+    ph = _f32(phi)
+    temp = np.zeros(ph.shape, np.float32)
+    valid = np.zeros(ph.shape, np.int32)
+    _lib().ors_target_minus(ph.ndim, _res(ph.shape), ph.ctypes.data, float(np.float32(0.99 * dx)), temp.ctypes.data,
+                            valid.ctypes.data)
+    return ph, temp, valid
+
+
+def fs_propagate(phi, phi_temp, valid, dx, repeat_times=2):
+    """FastSweepingLevelSet.propagate (lines one after another); returns phi_temp."""
+    ph = _f32(phi)
+    t = _f32(phi_temp)
+    v = np.ascontiguousarray(valid, dtype=np.int32)
+    _lib().ors_fs_propagate(ph.ndim, _res(ph.shape), ph.ctypes.data, t.ctypes.data, v.ctypes.data, float(dx),
+                            int(repeat_times))
+    return t
+
+
+def ls_smooth(src):
+    """LevelSet.smoothing: returns min(mean of the axis neighbours of src, src)."""
+    a = _f32(src)
+    out = np.zeros(a.shape, np.float32)
+    _lib().ors_ls_smooth(a.ndim, _res(a.shape), out.ctypes.data, a.ctypes.data)
+    return out
+
+
+def build_from_markers(shape, markers, dx, repeat_times=2):
+    """FastSweepingLevelSet.build_from_markers (level_set.py:381-392); returns phi."""
+    phi, _ = markers_distance(shape, markers, dx, repeat_times)
+    phi, temp, valid = target_minus(phi, dx)
+    temp = fs_propagate(phi, temp, valid, dx, repeat_times)
+    phi = ls_smooth(temp)
+    temp = ls_smooth(phi)
+    return ls_smooth(temp)
 
 
 def advect(velocity, src, field, dx, dt):

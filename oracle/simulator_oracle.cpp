@@ -22,6 +22,8 @@
 //   potential_function.py:15-55       PotentialFunctionStrategy
 //   volume_control.py:22-51           calc_volume, add_c and the PI controller
 //   surface_tension.py:23-95, 108-129 SurfaceTensionStrategy, calc_n, calc_kappa
+//   level_set.py:114-163, 266-392     markers: distance, propagation, target_minus,
+//                                     smoothing (FastSweepingLevelSet.build_from_markers)
 // Constants the reference computes in Python double before they meet f32
 // values are passed in already folded (the caller folds them in double).
 // Rule H1 of the solver oracle holds here too: a label outside the grid is
@@ -395,34 +397,16 @@ void ors_init_boundary(int dim, const int* res, int32_t* ct) {
 // (level_set.py:303, 322); here res[0] (the same on square / cubic grids).
 static float gsign(float x) { return x > 0.0f ? 1.0f : (x < 0.0f ? -1.0f : 0.0f); }
 
-void ors_redistance(int dim, const int* res, float* phi, double dx, int repeat, float* temp_out, int32_t* valid_out) {
-  const G g = make(dim, res);
+// FastSweepingLevelSet.propagate (level_set.py:266-327): repeat rounds of the
+// 2 dim sweeps (fastest axis first, forward then backward), each line walked
+// in order, update_from_neighbor (level_set.py:88-112) on every cell whose
+// valid is -1; t holds phi_temp, phi gives the sign.  Lines one after another
+// (the reference runs them in parallel, reading each other's cells).
+static void fs_propagate(const G& g, const float* phi, float* t, const int32_t* valid, double dx, int repeat) {
+  const int dim = g.dim;
   const int64_t n = g.cells();
-  std::vector<float> t(n);
-  std::vector<int32_t> valid(n, -1);
   const float fdx = (float)dx, two_dx2 = (float)(2.0 * dx * dx), dx2 = (float)(dx * dx), third = (float)(1.0 / 3.0);
   auto stride = [&](int k) -> int64_t { return k == 0 ? (int64_t)g.n[1] * g.n[2] : (k == 1 ? g.n[2] : 1); };
-  for (int64_t i = 0; i < n; ++i) {  // target_surface
-    int c[3];
-    coords(g, i, c);
-    const float p = phi[i], sp = gsign(p);
-    bool change = false;
-    float est = 1e20f;
-    for (int k = 0; k < dim; ++k)
-      for (int s = -1; s <= 1; s += 2) {
-        const int v = c[k] + s;
-        if (v < 0 || v >= g.n[k]) continue;
-        const float q = phi[i + s * stride(k)];
-        if (sp != gsign(q)) {
-          const float theta = p / (p - q);
-          const float est0 = sp * theta * fdx;
-          est = std::fabs(est0) < std::fabs(est) ? est0 : est;
-          change = true;
-        }
-      }
-    t[i] = change ? est : 1e20f;
-    if (change) valid[i] = 0;
-  }
   auto update = [&](int64_t i, const int c[3]) {
     float nb[3];
     for (int k = 0; k < dim; ++k) {
@@ -468,10 +452,189 @@ void ors_redistance(int dim, const int* res, float* phi, double dx, int repeat, 
           }
         }
       }
+}
+
+void ors_redistance(int dim, const int* res, float* phi, double dx, int repeat, float* temp_out, int32_t* valid_out) {
+  const G g = make(dim, res);
+  const int64_t n = g.cells();
+  std::vector<float> t(n);
+  std::vector<int32_t> valid(n, -1);
+  const float fdx = (float)dx;
+  auto stride = [&](int k) -> int64_t { return k == 0 ? (int64_t)g.n[1] * g.n[2] : (k == 1 ? g.n[2] : 1); };
+  for (int64_t i = 0; i < n; ++i) {  // target_surface
+    int c[3];
+    coords(g, i, c);
+    const float p = phi[i], sp = gsign(p);
+    bool change = false;
+    float est = 1e20f;
+    for (int k = 0; k < dim; ++k)
+      for (int s = -1; s <= 1; s += 2) {
+        const int v = c[k] + s;
+        if (v < 0 || v >= g.n[k]) continue;
+        const float q = phi[i + s * stride(k)];
+        if (sp != gsign(q)) {
+          const float theta = p / (p - q);
+          const float est0 = sp * theta * fdx;
+          est = std::fabs(est0) < std::fabs(est) ? est0 : est;
+          change = true;
+        }
+      }
+    t[i] = change ? est : 1e20f;
+    if (change) valid[i] = 0;
+  }
+  fs_propagate(g, phi, t.data(), valid.data(), dx, repeat);
   for (int64_t i = 0; i < n; ++i) {
     phi[i] = t[i];
     if (temp_out) temp_out[i] = t[i];
     if (valid_out) valid_out[i] = valid[i];
+  }
+}
+
+// The cell of a marker (coordinates / dx truncated toward zero, the
+// reference's cast) and its distance to the cell centre (I + 0.5) dx; false
+// when the cell is outside the grid or a coordinate is not finite.
+static bool marker_cell(const G& g, const float* m, float dx, int c[3], float* d) {
+  float s = 0.0f;
+  bool in = true;
+  c[0] = c[1] = c[2] = 0;
+  for (int a = 0; a < g.dim; ++a) {
+    const float q = m[a] / dx;
+    if (!std::isfinite(q) || std::fabs(q) > 2.0e9f) return false;
+    const int I = (int)q;
+    c[a] = I;
+    in = in && I >= 0 && I < g.n[a];
+    const float diff = m[a] - ((float)I + 0.5f) * dx;
+    s = a == 0 ? diff * diff : s + diff * diff;
+  }
+  *d = std::sqrt(s);
+  return in;
+}
+
+// FastSweepingLevelSet.build_from_markers, first part (level_set.py:381-385):
+// phi = 1e20, valid = -1, distance_to_markers (level_set.py:114-122; markers
+// in index order, a cell keeps the smallest distance and the first marker
+// reaching it - the reference's parallel loop races between markers of one
+// cell), then markers_propagate (level_set.py:336-379): repeat rounds of the
+// 2 dim sweeps, each line walked in order, a cell taking the distance to the
+// marker of its neighbour one step ahead when smaller.  A neighbour without a
+// marker (valid -1) is skipped: the reference indexes markers[-1] there.
+void ors_markers_distance(int dim, const int* res, const float* markers, int n_markers, float dx, int repeat,
+                          float* phi, int32_t* valid) {
+  const G g = make(dim, res);
+  const int64_t n = g.cells();
+  for (int64_t i = 0; i < n; ++i) {
+    phi[i] = 1e20f;
+    valid[i] = -1;
+  }
+  for (int p = 0; p < n_markers; ++p) {
+    int c[3];
+    float d;
+    if (!marker_cell(g, markers + (int64_t)p * dim, dx, c, &d)) continue;
+    const int64_t i = g.at(c[0], c[1], c[2]);
+    if (d < phi[i]) {
+      phi[i] = d;
+      valid[i] = p;
+    }
+  }
+  for (int r = 0; r < repeat; ++r)
+    for (int axis = dim - 1; axis >= 0; --axis)
+      for (int dir = 1; dir >= -1; dir -= 2) {
+        int oa[2], no = 0;
+        for (int k = 0; k < dim; ++k)
+          if (k != axis) oa[no++] = k;
+        const int64_t lines = n / g.n[axis];
+        const int nfast = no == 2 ? g.n[oa[1]] : 1;
+        for (int64_t l = 0; l < lines; ++l) {
+          int c[3] = {0, 0, 0};
+          if (no == 2) {
+            c[oa[0]] = (int)(l / nfast);
+            c[oa[1]] = (int)(l % nfast);
+          } else {
+            c[oa[0]] = (int)l;
+          }
+          for (int step = 0; step < g.n[axis]; ++step) {
+            c[axis] = dir > 0 ? step : g.n[axis] - 1 - step;
+            int nc[3] = {c[0], c[1], c[2]};
+            nc[axis] += dir;
+            if (nc[axis] < 0 || nc[axis] >= g.n[axis]) continue;
+            const int32_t v = valid[g.at(nc[0], nc[1], nc[2])];
+            if (v < 0) continue;
+            float s = 0.0f;
+            for (int a = 0; a < dim; ++a) {
+              const float diff = markers[(int64_t)v * dim + a] - ((float)c[a] + 0.5f) * dx;
+              s = a == 0 ? diff * diff : s + diff * diff;
+            }
+            const float d = std::sqrt(s);
+            const int64_t i = g.at(c[0], c[1], c[2]);
+            if (d < phi[i]) {
+              phi[i] = d;
+              valid[i] = v;
+            }
+          }
+        }
+      }
+}
+
+// LevelSet.target_minus (level_set.py:124-146) after valid.fill(-1): phi -= r
+// (r = 0.99 dx folded in double), then cells on the interface side of a sign
+// change with phi <= 0 are known (valid 0, phi_temp = phi), other phi <= 0
+// cells get phi_temp = -1 (to be swept), phi > 0 cells are known.
+void ors_target_minus(int dim, const int* res, float* phi, float r, float* phi_temp, int32_t* valid) {
+  const G g = make(dim, res);
+  const int64_t n = g.cells();
+  auto stride = [&](int k) -> int64_t { return k == 0 ? (int64_t)g.n[1] * g.n[2] : (k == 1 ? g.n[2] : 1); };
+  for (int64_t i = 0; i < n; ++i) {
+    phi[i] = phi[i] - r;
+    valid[i] = -1;
+  }
+  for (int64_t i = 0; i < n; ++i) {
+    int c[3];
+    coords(g, i, c);
+    bool change = false;
+    for (int k = 0; k < dim; ++k)
+      for (int s = -1; s <= 1; s += 2) {
+        const int v = c[k] + s;
+        if (v >= 0 && v < g.n[k] && gsign(phi[i]) != gsign(phi[i + s * stride(k)])) change = true;
+      }
+    if (change && phi[i] <= 0.0f) {
+      valid[i] = 0;
+      phi_temp[i] = phi[i];
+    } else if (phi[i] <= 0.0f) {
+      phi_temp[i] = -1.0f;
+    } else {
+      phi_temp[i] = phi[i];
+      valid[i] = 0;
+    }
+  }
+}
+
+// FastSweepingLevelSet.propagate alone (the sweeps of redistance).
+void ors_fs_propagate(int dim, const int* res, const float* phi, float* phi_temp, const int32_t* valid, double dx,
+                      int repeat) {
+  fs_propagate(make(dim, res), phi, phi_temp, valid, dx, repeat);
+}
+
+// LevelSet.smoothing (level_set.py:148-163): out = min(mean of the in-range
+// axis neighbours of in (summed axis by axis, lower then upper), in).
+void ors_ls_smooth(int dim, const int* res, float* out, const float* in) {
+  const G g = make(dim, res);
+  const int64_t n = g.cells();
+  auto stride = [&](int k) -> int64_t { return k == 0 ? (int64_t)g.n[1] * g.n[2] : (k == 1 ? g.n[2] : 1); };
+  for (int64_t i = 0; i < n; ++i) {
+    int c[3];
+    coords(g, i, c);
+    float avg = 0.0f;
+    int tot = 0;
+    for (int k = 0; k < dim; ++k)
+      for (int s = -1; s <= 1; s += 2) {
+        const int v = c[k] + s;
+        if (v >= 0 && v < g.n[k]) {
+          avg = avg + in[i + s * stride(k)];
+          ++tot;
+        }
+      }
+    avg = avg / (float)tot;
+    out[i] = avg < in[i] ? avg : in[i];
   }
 }
 

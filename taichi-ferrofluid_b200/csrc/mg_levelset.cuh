@@ -187,4 +187,173 @@ __global__ void k_fs_sweep(Geom g, int axis, int dir, float* phi_temp, const flo
   }
 }
 
+// ---- FastSweepingLevelSet.build_from_markers (level_set.py:381-392) --------
+
+// The cell of a marker (coordinates / dx truncated toward zero, the
+// reference's cast) and its distance to the cell centre (I + 0.5) dx; false
+// when the cell is outside the grid or a coordinate is not finite.
+__device__ __forceinline__ bool marker_cell(const Geom& g, const float* m, float dx, int c[3], float* d) {
+  float s = 0.0f;
+  bool in = true;
+  c[0] = c[1] = c[2] = 0;
+  for (int a = 0; a < g.dim; ++a) {
+    const float q = __fdiv_rn(m[a], dx);
+    if (!isfinite(q) || fabsf(q) > 2.0e9f) return false;
+    const int I = (int)q;  // truncation toward zero
+    c[a] = I;
+    in = in && I >= 0 && I < g.n[a];
+    const float diff = __fsub_rn(m[a], __fmul_rn(__fadd_rn((float)I, 0.5f), dx));
+    s = a == 0 ? __fmul_rn(diff, diff) : __fadd_rn(s, __fmul_rn(diff, diff));
+  }
+  *d = __fsqrt_rn(s);
+  return in;
+}
+
+// phi.fill(1e20); valid holds INT_MAX until k_marker_owner has run.
+__global__ void k_markers_init(Geom g, float* __restrict__ phi, int32_t* __restrict__ valid) {
+  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < g.count;
+       i += (long long)gridDim.x * blockDim.x) {
+    phi[i] = 1e20f;
+    valid[i] = 0x7fffffff;
+  }
+}
+
+// LevelSet.distance_to_markers (level_set.py:114-122), pass 1: every cell
+// keeps the smallest distance of its markers (non-negative floats order as
+// their bit patterns).  The reference's parallel loop races between markers
+// of one cell; the smallest distance, then the smallest marker index (pass
+// 2), is what its loop gives when the markers run in index order.
+__global__ void k_marker_min_d(Geom g, const float* __restrict__ markers, int n, float dx, float* phi) {
+  for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < n; p += gridDim.x * blockDim.x) {
+    int c[3];
+    float d;
+    if (!marker_cell(g, markers + (long long)p * g.dim, dx, c, &d)) continue;
+    atomicMin(reinterpret_cast<unsigned int*>(phi) + g.index(c[0], c[1], c[2]), __float_as_uint(d));
+  }
+}
+
+// Pass 2: the smallest index among the markers at that distance.
+__global__ void k_marker_owner(Geom g, const float* __restrict__ markers, int n, float dx,
+                               const float* __restrict__ phi, int32_t* valid) {
+  for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < n; p += gridDim.x * blockDim.x) {
+    int c[3];
+    float d;
+    if (!marker_cell(g, markers + (long long)p * g.dim, dx, c, &d)) continue;
+    const long long i = g.index(c[0], c[1], c[2]);
+    if (__float_as_uint(d) == __float_as_uint(phi[i])) atomicMin(valid + i, p);
+  }
+}
+
+__global__ void k_marker_valid_fix(Geom g, int32_t* __restrict__ valid) {
+  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < g.count;
+       i += (long long)gridDim.x * blockDim.x)
+    if (valid[i] == 0x7fffffff) valid[i] = -1;
+}
+
+// One sweep of FastSweepingLevelSet.markers_propagate (level_set.py:336-379)
+// along `axis`: a thread walks each line in direction dir; a cell whose
+// neighbour one step ahead (index + dir) is in the grid and owns a marker
+// takes that marker's distance when smaller, and the marker.  A line reads
+// only its own cells, so the result is that of the reference's serial walk.
+// A neighbour without a marker (valid -1) is skipped (the reference indexes
+// markers[-1] there).
+__global__ void k_marker_sweep(Geom g, int axis, int dir, const float* __restrict__ markers, float dx,
+                               float* __restrict__ phi, int32_t* __restrict__ valid) {
+  int oa[2], no = 0;
+  for (int k = 0; k < g.dim; ++k)
+    if (k != axis) oa[no++] = k;
+  const long long lines = g.count / g.n[axis];
+  const int nfast = no == 2 ? g.n[oa[1]] : 1;
+  const long long st = g.stride(axis) * dir;
+  for (long long l = (long long)blockIdx.x * blockDim.x + threadIdx.x; l < lines;
+       l += (long long)gridDim.x * blockDim.x) {
+    int c[3] = {0, 0, 0};
+    if (no == 2) {
+      c[oa[0]] = (int)(l / nfast);
+      c[oa[1]] = (int)(l % nfast);
+    } else {
+      c[oa[0]] = (int)l;
+    }
+    const int n = g.n[axis];
+    for (int step = 0; step < n; ++step) {
+      c[axis] = dir > 0 ? step : n - 1 - step;
+      const int na = c[axis] + dir;
+      if (na < 0 || na >= n) continue;
+      const long long i = g.index(c[0], c[1], c[2]);
+      const int32_t v = valid[i + st];
+      if (v < 0) continue;
+      float s = 0.0f;
+      for (int a = 0; a < g.dim; ++a) {
+        const float diff = __fsub_rn(markers[(long long)v * g.dim + a], __fmul_rn(__fadd_rn((float)c[a], 0.5f), dx));
+        s = a == 0 ? __fmul_rn(diff, diff) : __fadd_rn(s, __fmul_rn(diff, diff));
+      }
+      const float d = __fsqrt_rn(s);
+      if (d < phi[i]) {
+        phi[i] = d;
+        valid[i] = v;
+      }
+    }
+  }
+}
+
+// LevelSet.target_minus (level_set.py:124-146), first loop (after
+// valid.fill(-1)): phi -= r, the marker radius (0.99 dx folded in double).
+__global__ void k_target_minus_a(Geom g, float* __restrict__ phi, int32_t* __restrict__ valid, float r) {
+  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < g.count;
+       i += (long long)gridDim.x * blockDim.x) {
+    phi[i] = __fsub_rn(phi[i], r);
+    valid[i] = -1;
+  }
+}
+
+// Second loop: cells with a sign change and phi <= 0 are known (valid 0,
+// phi_temp = phi), other phi <= 0 cells get phi_temp = -1 (swept later),
+// phi > 0 cells are known with phi_temp = phi.
+__global__ void k_target_minus_b(Geom g, const float* __restrict__ phi, float* __restrict__ phi_temp,
+                                 int32_t* __restrict__ valid) {
+  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < g.count;
+       i += (long long)gridDim.x * blockDim.x) {
+    int c[3];
+    g.coords(i, c);
+    const float p = phi[i];
+    bool change = false;
+    for (int k = 0; k < g.dim; ++k)
+      for (int s = -1; s <= 1; s += 2) {
+        const int v = c[k] + s;
+        if (v >= 0 && v < g.n[k] && gsign(p) != gsign(phi[i + s * g.stride(k)])) change = true;
+      }
+    if (change && p <= 0.0f) {
+      valid[i] = 0;
+      phi_temp[i] = p;
+    } else if (p <= 0.0f) {
+      phi_temp[i] = -1.0f;
+    } else {
+      phi_temp[i] = p;
+      valid[i] = 0;
+    }
+  }
+}
+
+// LevelSet.smoothing (level_set.py:148-163): out = min(mean of the in-range
+// axis neighbours of in (summed axis by axis, lower then upper), in).
+__global__ void k_ls_smooth(Geom g, float* __restrict__ out, const float* __restrict__ in) {
+  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < g.count;
+       i += (long long)gridDim.x * blockDim.x) {
+    int c[3];
+    g.coords(i, c);
+    float avg = 0.0f;
+    int tot = 0;
+    for (int k = 0; k < g.dim; ++k)
+      for (int s = -1; s <= 1; s += 2) {
+        const int v = c[k] + s;
+        if (v >= 0 && v < g.n[k]) {
+          avg = __fadd_rn(avg, in[i + s * g.stride(k)]);
+          ++tot;
+        }
+      }
+    avg = __fdiv_rn(avg, (float)tot);
+    out[i] = avg < in[i] ? avg : in[i];
+  }
+}
+
 }  // namespace mg

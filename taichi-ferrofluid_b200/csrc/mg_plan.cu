@@ -1012,6 +1012,22 @@ int mg_init_boundary(int32_t dim, const int32_t* res, int32_t* cell_type, void* 
   return MG_OK;
 }
 
+// FastSweepingLevelSet.propagate (level_set.py:283-327): repeat rounds of the
+// 2 dim sweeps, fastest axis first, forward then backward.
+static int fs_propagate(const Geom& g, const float* phi, float* phi_temp, const int32_t* valid, double dx,
+                        int repeat_times, cudaStream_t s) {
+  const float dx1 = (float)dx, two_dx2 = (float)(2.0 * dx * dx), dx2 = (float)(dx * dx), third = (float)(1.0 / 3.0);
+  for (int t = 0; t < repeat_times; ++t)
+    for (int axis = g.dim - 1; axis >= 0; --axis)
+      for (int dir = 1; dir >= -1; dir -= 2) {
+        const long long lines = g.count / g.n[axis];
+        const int blocks = (int)((lines + 127) / 128);
+        k_fs_sweep<<<blocks, 128, 0, s>>>(g, axis, dir, phi_temp, phi, valid, dx1, two_dx2, dx2, third);
+        CKL("k_fs_sweep");
+      }
+  return MG_OK;
+}
+
 int mg_level_set_redistance(int32_t dim, const int32_t* res, float* phi, float* phi_temp, int32_t* valid,
                             double dx, int32_t repeat_times, void* stream) {
   Geom g;
@@ -1022,16 +1038,69 @@ int mg_level_set_redistance(int32_t dim, const int32_t* res, float* phi, float* 
   cudaStream_t s = S(stream);
   k_target_surface<<<blocks_of(g.count), 256, 0, s>>>(g, phi, phi_temp, valid, (float)dx);
   CKL("k_target_surface");
-  const float dx1 = (float)dx, two_dx2 = (float)(2.0 * dx * dx), dx2 = (float)(dx * dx), third = (float)(1.0 / 3.0);
+  if (int rc = fs_propagate(g, phi, phi_temp, valid, dx, repeat_times, s)) return rc;
+  CK(cudaMemcpyAsync(phi, phi_temp, g.count * sizeof(float), cudaMemcpyDeviceToDevice, s));
+  return MG_OK;
+}
+
+int mg_level_set_propagate(int32_t dim, const int32_t* res, const float* phi, float* phi_temp, const int32_t* valid,
+                           double dx, int32_t repeat_times, void* stream) {
+  Geom g;
+  if (int rc = grid_of(dim, res, &g)) return rc;
+  for (int k = 0; k < dim; ++k)
+    if (g.n[k] < 2) return bad("every axis needs at least 2 cells");
+  if (!phi || !phi_temp || !valid || !(dx > 0.0) || repeat_times < 0) return bad("inputs");
+  return fs_propagate(g, phi, phi_temp, valid, dx, repeat_times, S(stream));
+}
+
+int mg_level_set_markers_distance(int32_t dim, const int32_t* res, float* phi, int32_t* valid, const float* markers,
+                                  int32_t n_markers, double dx, int32_t repeat_times, void* stream) {
+  Geom g;
+  if (int rc = grid_of(dim, res, &g)) return rc;
+  if (!phi || !valid || (n_markers > 0 && !markers) || n_markers < 0 || !(dx > 0.0) || repeat_times < 0)
+    return bad("inputs");
+  cudaStream_t s = S(stream);
+  const float fdx = (float)dx;
+  k_markers_init<<<blocks_of(g.count), 256, 0, s>>>(g, phi, valid);
+  CKL("k_markers_init");
+  if (n_markers > 0) {
+    const int mb = (n_markers + 255) / 256 < 4096 ? (n_markers + 255) / 256 : 4096;
+    k_marker_min_d<<<mb, 256, 0, s>>>(g, markers, n_markers, fdx, phi);
+    CKL("k_marker_min_d");
+    k_marker_owner<<<mb, 256, 0, s>>>(g, markers, n_markers, fdx, phi, valid);
+    CKL("k_marker_owner");
+  }
+  k_marker_valid_fix<<<blocks_of(g.count), 256, 0, s>>>(g, valid);
+  CKL("k_marker_valid_fix");
   for (int t = 0; t < repeat_times; ++t)
     for (int axis = dim - 1; axis >= 0; --axis)
       for (int dir = 1; dir >= -1; dir -= 2) {
         const long long lines = g.count / g.n[axis];
-        const int blocks = (int)((lines + 127) / 128);
-        k_fs_sweep<<<blocks, 128, 0, s>>>(g, axis, dir, phi_temp, phi, valid, dx1, two_dx2, dx2, third);
-        CKL("k_fs_sweep");
+        k_marker_sweep<<<(int)((lines + 127) / 128), 128, 0, s>>>(g, axis, dir, markers, fdx, phi, valid);
+        CKL("k_marker_sweep");
       }
-  CK(cudaMemcpyAsync(phi, phi_temp, g.count * sizeof(float), cudaMemcpyDeviceToDevice, s));
+  return MG_OK;
+}
+
+int mg_level_set_target_minus(int32_t dim, const int32_t* res, float* phi, float* phi_temp, int32_t* valid,
+                              double dx, void* stream) {
+  Geom g;
+  if (int rc = grid_of(dim, res, &g)) return rc;
+  if (!phi || !phi_temp || !valid || !(dx > 0.0)) return bad("inputs");
+  cudaStream_t s = S(stream);
+  k_target_minus_a<<<blocks_of(g.count), 256, 0, s>>>(g, phi, valid, (float)(0.99 * dx));
+  CKL("k_target_minus_a");
+  k_target_minus_b<<<blocks_of(g.count), 256, 0, s>>>(g, phi, phi_temp, valid);
+  CKL("k_target_minus_b");
+  return MG_OK;
+}
+
+int mg_level_set_smooth(int32_t dim, const int32_t* res, float* out, const float* in, void* stream) {
+  Geom g;
+  if (int rc = grid_of(dim, res, &g)) return rc;
+  if (!out || !in || out == in) return bad("inputs (out and in must differ)");
+  k_ls_smooth<<<blocks_of(g.count), 256, 0, S(stream)>>>(g, out, in);
+  CKL("k_ls_smooth");
   return MG_OK;
 }
 

@@ -62,3 +62,39 @@ class FastSweepingLevelSet(LevelSet):
         check(self.lib.mg_level_set_redistance(self.dim, self._res, self.phi.data_ptr(), self.phi_temp.data_ptr(),
                                                self.valid.data_ptr(), self.dx, int(self.repeat_times),
                                                mg_lib.stream_ptr(self.device)), "mg_level_set_redistance")
+
+    def propagate(self):
+        """level_set.py:283-327: the fast sweeping of phi_temp where valid is -1."""
+        check(self.lib.mg_level_set_propagate(self.dim, self._res, self.phi.data_ptr(), self.phi_temp.data_ptr(),
+                                              self.valid.data_ptr(), self.dx, int(self.repeat_times),
+                                              mg_lib.stream_ptr(self.device)), "mg_level_set_propagate")
+
+    def target_minus(self):
+        """level_set.py:124-146 (after valid.fill(-1), which it includes)."""
+        check(self.lib.mg_level_set_target_minus(self.dim, self._res, self.phi.data_ptr(), self.phi_temp.data_ptr(),
+                                                 self.valid.data_ptr(), self.dx, mg_lib.stream_ptr(self.device)),
+              "mg_level_set_target_minus")
+
+    def smoothing(self, phi, phi_temp):
+        """level_set.py:148-163: phi = min(mean of the axis neighbours of phi_temp, phi_temp)."""
+        check(self.lib.mg_level_set_smooth(self.dim, self._res, phi.data_ptr(), phi_temp.data_ptr(),
+                                           mg_lib.stream_ptr(self.device)), "mg_level_set_smooth")
+
+    def build_from_markers(self, markers, total_mk=None):
+        """level_set.py:381-392: phi from marker particles - the distance to the
+        nearest marker near the markers (distance_to_markers, markers_propagate),
+        minus the marker radius 0.99 dx, swept inward (target_minus, propagate),
+        then three smoothing passes.  ``markers``: (N, dim) float32 CUDA tensor
+        of positions; ``total_mk``: how many of them (default N)."""
+        mk = markers.to(device=self.device, dtype=torch.float32).contiguous()
+        n = int(mk.shape[0] if total_mk is None else total_mk)
+        if mk.dim() != 2 or mk.shape[1] != self.dim or not 0 <= n <= mk.shape[0]:
+            raise ValueError("markers must be (N, dim) with total_mk <= N")
+        check(self.lib.mg_level_set_markers_distance(self.dim, self._res, self.phi.data_ptr(), self.valid.data_ptr(),
+                                                     mk.data_ptr(), n, self.dx, int(self.repeat_times),
+                                                     mg_lib.stream_ptr(self.device)), "mg_level_set_markers_distance")
+        self.target_minus()
+        self.propagate()
+        self.smoothing(self.phi, self.phi_temp)
+        self.smoothing(self.phi_temp, self.phi)
+        self.smoothing(self.phi, self.phi_temp)

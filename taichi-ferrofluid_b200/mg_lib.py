@@ -92,6 +92,10 @@ _SIGS = {
     "mg_apply_markers": (ctypes.c_int, [_i32, _vp, _vp, _vp, _i32, _vp]),
     "mg_init_boundary": (ctypes.c_int, [_i32, _vp, _vp, _vp]),
     "mg_level_set_redistance": (ctypes.c_int, [_i32, _vp, _vp, _vp, _vp, _f64, _i32, _vp]),
+    "mg_level_set_propagate": (ctypes.c_int, [_i32, _vp, _vp, _vp, _vp, _f64, _i32, _vp]),
+    "mg_level_set_markers_distance": (ctypes.c_int, [_i32, _vp, _vp, _vp, _vp, _i32, _f64, _i32, _vp]),
+    "mg_level_set_target_minus": (ctypes.c_int, [_i32, _vp, _vp, _vp, _vp, _f64, _vp]),
+    "mg_level_set_smooth": (ctypes.c_int, [_i32, _vp, _vp, _vp, _vp]),
     "mg_advect_quantity": (ctypes.c_int, [_i32, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _f32, _f32, _vp]),
     "mg_extrapolate_velocity": (ctypes.c_int, [_i32, _vp, _i32, _vp, _vp, _vp, _vp, _vp, _i32, _vp]),
     "mg_enforce_boundary": (ctypes.c_int, [_i32, _vp, _vp, _vp, _vp, _vp, _vp]),

@@ -107,3 +107,64 @@ def test_redistance(dim, n):
     conv = ls.phi.cpu().numpy()
     ref12, _ = S.redistance(phi, dx, 12)
     assert np.abs(conv - ref12).max() < 0.05 * dx, np.abs(conv - ref12).max() / dx
+
+
+@pytest.mark.parametrize("shape", [(40, 36, 32), (96, 80)])
+def test_markers_stages_bit_exact(shape):
+    """FastSweepingLevelSet.build_from_markers' deterministic stages against
+    the oracle, bit for bit: distance_to_markers + markers_propagate (phi and
+    the owning marker of every cell; markers sharing a cell, one just outside
+    the lower faces, one far outside), target_minus (phi, phi_temp, valid) and
+    smoothing."""
+    import torch
+    from level_set import FastSweepingLevelSet
+    from oracle import simulator as S
+    from test_oracle_strategies import _marker_cloud
+    dx = 1.0 / max(shape)
+    mk = _marker_cloud(shape, dx, 5000, 11)
+    mk = np.concatenate([mk, mk[:300]])  # exact duplicates: the smaller index owns the cell
+    ls = FastSweepingLevelSet(len(shape), shape, dx)
+    dev = ls.phi.device
+    m = torch.from_numpy(mk).to(dev)
+    from mg_lib import check, stream_ptr
+    check(ls.lib.mg_level_set_markers_distance(ls.dim, ls._res, ls.phi.data_ptr(), ls.valid.data_ptr(), m.data_ptr(),
+                                               len(mk), ls.dx, 2, stream_ptr(dev)), "markers")
+    rphi, rvalid = S.markers_distance(shape, mk, dx, 2)
+    np.testing.assert_array_equal(_bits(ls.phi), rphi.view(np.uint32))
+    np.testing.assert_array_equal(ls.valid.cpu().numpy(), rvalid)
+    ls.target_minus()
+    tphi, ttemp, tvalid = S.target_minus(rphi, dx)
+    np.testing.assert_array_equal(_bits(ls.phi), tphi.view(np.uint32))
+    np.testing.assert_array_equal(_bits(ls.phi_temp), ttemp.view(np.uint32))
+    np.testing.assert_array_equal(ls.valid.cpu().numpy(), tvalid)
+    src = torch.from_numpy(np.random.default_rng(2).uniform(-1, 1, shape).astype(np.float32)).to(dev)
+    out = torch.empty_like(src)
+    ls.smoothing(out, src)
+    np.testing.assert_array_equal(_bits(out), S.ls_smooth(src.cpu().numpy()).view(np.uint32))
+
+
+def test_build_from_markers():
+    """The whole build_from_markers on a ball filled with markers: every stage
+    but the fast sweep is bit-exact (above); the sweep's lines run in parallel
+    as in the reference, so the result is compared with the serial oracle
+    within 0.1 dx near the markers, and the signs agree."""
+    import torch
+    from level_set import FastSweepingLevelSet
+    from oracle import simulator as S
+    n = 48
+    dx = 1.0 / n
+    g = (np.arange(n) + 0.5) * dx
+    X = np.stack(np.meshgrid(g, g, g, indexing="ij"), -1).reshape(-1, 3)
+    rng = np.random.default_rng(3)
+    pts = np.concatenate([X + rng.uniform(-0.45, 0.45, X.shape) * dx for _ in range(4)])
+    pts = pts[np.linalg.norm(pts - 0.5, axis=1) < 0.3].astype(np.float32)
+    ls = FastSweepingLevelSet(3, (n, n, n), dx)
+    ls.build_from_markers(torch.from_numpy(pts).to(ls.phi.device))
+    got = ls.phi.cpu().numpy()
+    ref = S.build_from_markers((n, n, n), pts, dx)
+    near = np.abs(ref) < 3 * dx
+    assert near.sum() > 1000
+    assert np.all(np.sign(got[near]) == np.sign(ref[near]))
+    assert np.abs(got - ref)[near].max() < 0.1 * dx
+    r = np.linalg.norm(X.reshape(n, n, n, 3) - 0.5, axis=-1)
+    assert (got[r < 0.25] < 0).all()

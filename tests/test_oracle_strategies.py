@@ -383,6 +383,129 @@ def test_redistance_restores_distance(dim, n):
 
 
 # ---------------------------------------------------- advection, extrapolation
+def _markers_serial(shape, mk, dx, repeat=2):
+    """distance_to_markers + markers_propagate (level_set.py:114-122, 336-379)
+    restated with float32 scalars, markers in index order, lines in order."""
+    dim = len(shape)
+    dx = np.float32(dx)
+    phi = np.full(shape, np.float32(1e20), np.float32)
+    valid = np.full(shape, -1, np.int32)
+
+    def dist(m, c):
+        s = np.float32(0)
+        for a in range(dim):
+            diff = np.float32(np.float32(m[a]) - (np.float32(c[a]) + np.float32(0.5)) * dx)
+            s = np.float32(diff * diff) if a == 0 else np.float32(s + diff * diff)
+        return np.float32(np.sqrt(s))
+
+    for p, m in enumerate(mk):
+        c = [int(np.float32(m[a]) / dx) for a in range(dim)]  # truncation toward zero
+        if all(0 <= c[a] < shape[a] for a in range(dim)):
+            d = dist(m, c)
+            if d < phi[tuple(c)]:
+                phi[tuple(c)] = d
+                valid[tuple(c)] = p
+    for _ in range(repeat):
+        for axis in reversed(range(dim)):
+            for dr in (1, -1):
+                for idx in np.ndindex(*[shape[a] if a != axis else 1 for a in range(dim)]):
+                    for step in range(shape[axis]):
+                        c = list(idx)
+                        c[axis] = step if dr > 0 else shape[axis] - 1 - step
+                        nc = list(c)
+                        nc[axis] += dr
+                        if not 0 <= nc[axis] < shape[axis]:
+                            continue
+                        v = valid[tuple(nc)]
+                        if v < 0:
+                            continue
+                        d = dist(mk[v], c)
+                        if d < phi[tuple(c)]:
+                            phi[tuple(c)] = d
+                            valid[tuple(c)] = v
+    return phi, valid
+
+
+def _marker_cloud(shape, dx, n, seed):
+    rng = np.random.default_rng(seed)
+    ext = np.array(shape, np.float64) * dx
+    mk = rng.uniform(0.2, 0.7, (n, len(shape))) * ext
+    extra = np.array([mk[0] + 1e-4 * dx, -0.3 * np.ones(len(shape)) * dx, ext + dx], np.float64)  # same cell; truncation; outside
+    return np.concatenate([mk, extra]).astype(np.float32)
+
+
+@pytest.mark.parametrize("shape", [(7, 6, 5), (9, 8)])
+def test_markers_distance_matches_serial_restatement(shape):
+    """FastSweepingLevelSet.build_from_markers' first part: the oracle against an
+    independent float32-scalar restatement, bit for bit (a marker just outside
+    the lower faces lands in cell 0 by truncation; one far outside is ignored;
+    two markers share a cell)."""
+    dx = 0.1
+    mk = _marker_cloud(shape, dx, 9, 5)
+    phi, valid = S.markers_distance(shape, mk, dx, 2)
+    rphi, rvalid = _markers_serial(shape, mk, dx, 2)
+    np.testing.assert_array_equal(phi, rphi)
+    np.testing.assert_array_equal(valid, rvalid)
+    assert valid[(0,) * len(shape)] == len(mk) - 2  # the truncated marker
+    assert (phi < 1e20).sum() > len(mk) - 2
+
+
+def test_target_minus_and_smoothing_match_numpy():
+    rng = np.random.default_rng(7)
+    shape = (6, 7, 8)
+    dx = 0.05
+    phi0 = rng.uniform(-2, 2, shape).astype(np.float32) * np.float32(dx)
+    phi, temp, valid = S.target_minus(phi0, dx)
+    ref = (phi0 - np.float32(0.99 * dx)).astype(np.float32)
+    np.testing.assert_array_equal(phi, ref)
+    sg = np.sign(ref)
+    change = np.zeros(shape, bool)
+    for k in range(3):
+        for s in (-1, 1):
+            sh = np.roll(sg, -s, axis=k)
+            m = np.ones(shape, bool)
+            idx = [slice(None)] * 3
+            idx[k] = slice(-1, None) if s > 0 else slice(0, 1)
+            m[tuple(idx)] = False
+            change |= m & (sh != sg)
+    exp_temp = np.where(ref > 0, ref, np.where(change, ref, np.float32(-1))).astype(np.float32)
+    exp_valid = np.where((ref > 0) | change, 0, -1)
+    np.testing.assert_array_equal(temp, exp_temp)
+    np.testing.assert_array_equal(valid, exp_valid)
+    # smoothing: min(mean of the in-range axis neighbours, self), summed axis by axis
+    src = rng.uniform(-1, 1, shape).astype(np.float32)
+    tot = np.zeros(shape, np.float32)
+    cnt = np.zeros(shape, np.int32)
+    for k in range(3):
+        for s in (-1, 1):
+            nb = np.roll(src, -s, axis=k)
+            m = np.ones(shape, bool)
+            idx = [slice(None)] * 3
+            idx[k] = slice(-1, None) if s > 0 else slice(0, 1)
+            m[tuple(idx)] = False
+            tot = np.where(m, (tot + nb).astype(np.float32), tot)
+            cnt += m
+    avg = (tot / cnt.astype(np.float32)).astype(np.float32)
+    np.testing.assert_array_equal(S.ls_smooth(src), np.minimum(avg, src))
+
+
+def test_build_from_markers_fills_a_ball():
+    """A ball filled with markers (4 a cell): negative inside, about the
+    distance to the ball minus the marker radius just outside."""
+    n = 24
+    dx = 1.0 / n
+    g = (np.arange(n) + 0.5) * dx
+    X = np.stack(np.meshgrid(g, g, g, indexing="ij"), -1).reshape(-1, 3)
+    rng = np.random.default_rng(3)
+    pts = np.concatenate([X + rng.uniform(-0.45, 0.45, X.shape) * dx for _ in range(4)])
+    inside = np.linalg.norm(pts - 0.5, axis=1) < 0.25
+    phi = S.build_from_markers((n, n, n), pts[inside].astype(np.float32), dx)
+    r = np.linalg.norm(X.reshape(n, n, n, 3) - 0.5, axis=-1)
+    assert (phi[r < 0.2] < 0).all()
+    band = (r > 0.3) & (r < 0.33)
+    assert (phi[band] > 0).all() and (phi[band] < 3 * dx).all()
+
+
 def test_advect_identity_and_translation():
     """advect (fluid_simulator.py:216-221): zero velocity leaves a field
     unchanged (up to the f32 round trip (I + 0.5) dx / dx - 0.5, an ulp off I,
