@@ -75,7 +75,7 @@ NCU_DRAM_BYTES = {
     ("substep128", "pre_l0"): 16.80e6, ("substep128", "post_l0"): 26.24e6,
     ("pressure128", "pre_l0"): 16.80e6, ("pressure128", "post_l0"): 26.24e6,
     ("substep128", "Ap_alpha"): 11.67e6, ("pressure128", "Ap_alpha"): 11.67e6,
-    ("precision256", "pre_l0"): 196.06e6, ("precision256", "Ap_alpha"): 98.40e6,
+    ("precision256", "pre_l0"): 195.96e6, ("precision256", "Ap_alpha"): 114.93e6,
 }
 
 
