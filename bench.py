@@ -265,7 +265,9 @@ class GpuCase:
 
 
 def stage_bytes(solver, storage):
-    """Algorithmic bytes per level-0 cell of each pipeline stage."""
+    """Algorithmic bytes per level-0 cell of each pipeline stage: every array a
+    stage must read or write once (labels and couplings only where the stage
+    needs them; the coarse arrays per fine cell), without re-reads."""
     sv = 4 if storage == "f32" else 2
     d = solver.dim
     coarse = 2 ** d
