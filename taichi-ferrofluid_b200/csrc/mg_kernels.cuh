@@ -271,6 +271,33 @@ __global__ void k_smooth_w4(Level L, int phase) {
   }
 }
 
+// The first half sweep of pre-smoothing (colour 0 from z = 0) on a
+// whole-domain level of 4-cell groups: with every neighbour 0 the neighbour
+// sum is +0, so z = (r - 0) / Adiag = r / Adiag on colour 0 (the same float32
+// value, -0 included), and z = 0 on colour 1 - the z.fill(0) before the sweep
+// written in the same pass.
+__global__ void k_smooth_first_w4(Level L) {
+  pdl_enter();
+  const int n1 = L.g.n[1], n2 = L.g.n[2];
+  const int q2 = n2 >> 2;
+  const long long groups = L.g.count >> 2;
+  float* z = (float*)L.z;
+  for (long long q = gtid(); q < groups; q += gstride()) {
+    const long long row = q / q2;
+    const int x = (int)(q - row * q2) * 4;
+    const int i1 = (int)(row % n1), i0 = (int)(row / n1);
+    const int e0 = (0 - i0 - i1 - x) & 1;  // first colour-0 cell of the group
+    float R[4], D[4];
+    unpack4(__ldg(reinterpret_cast<const float4*>((const float*)L.r) + q), R);
+    unpack4(__ldg(reinterpret_cast<const float4*>(L.Adiag) + q), D);
+    float v[4] = {0.0f, 0.0f, 0.0f, 0.0f};
+#pragma unroll
+    for (int e = 0; e < 4; ++e)
+      if (((e - e0) & 1) == 0) v[e] = __fdiv_rn(__fsub_rn(R[e], 0.0f), D[e]);
+    reinterpret_cast<float4*>(z)[q] = make_float4(v[0], v[1], v[2], v[3]);
+  }
+}
+
 // restrict(l) as k_restrict for a whole-domain fine level halving exactly
 // onto the coarse one, 3D, fine fastest extent a multiple of 4: one thread
 // per pair of coarse cells along the fastest axis, i.e. one 4-cell fine group

@@ -257,9 +257,14 @@ int launch_level(mg_plan* P, int l, bool pre, cudaStream_t s) {
     return e == cudaSuccess ? MG_OK : set_err("launch_sweep", e);
   }
   if (pre) {
-    if (l == 0) CK(cudaMemsetAsync(P->lv[0].z, 0, level_cells(P, 0) * sizeof(float), s));
+    // pre-smoothing starts from z = 0; on a whole-domain level of 4-cell
+    // groups its first half sweep (pointwise) also writes those zeros
+    const bool first4 = P->whole[l] && P->d.dim == 3 && P->geom[l].n[2] % 4 == 0;
+    if (first4) CK(launch_k(k_smooth_first_w4, grid_for(P, level_cells(P, l) / 4), 256, 0, s, P->lv[l]));
+    else if (l == 0) CK(cudaMemsetAsync(P->lv[0].z, 0, level_cells(P, 0) * sizeof(float), s));
     for (int i = 0; i < P->d.pre_post; ++i) {
-      if (int rc = launch_smooth(P, l, 0, s)) return rc;
+      if (!(first4 && i == 0))
+        if (int rc = launch_smooth(P, l, 0, s)) return rc;
       if (int rc = launch_smooth(P, l, 1, s)) return rc;
     }
     return launch_restrict(P, l, s);
