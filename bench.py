@@ -422,6 +422,9 @@ def gpu_arm(args, rank, world, local):
     barrier(world)
     e2e_total, e2e_steps = e2e_run(args.steps)
     torch.cuda.synchronize()
+    for c in cases:  # the pipeline delivered the last step's result to the host
+        if not torch.equal(c.h_x, c.solver.x.cpu()):
+            raise RuntimeError(f"e2e read-back of the {c.kind} solve differs from the device result")
     total_ms = max_over_ranks(sum(solve_ms), world)
     total_e2e = max_over_ranks(e2e_total, world)
     n_solves = len(solve_ms) * world
