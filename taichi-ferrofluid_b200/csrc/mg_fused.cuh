@@ -169,6 +169,12 @@ struct SweepArgs {
   int r_f32;            // level 0: r is float and scaled by sigma on load
   int chunk;            // planes per block along axis 0
   int tiles_x, tiles_y; // tiles per plane
+  // POST of level 0, float32: also z.r of the PCG loop (the reduction of
+  // k_zr4 and its epilogue) over the cells it writes; -1 off, 0 before the
+  // loop, 1 in the loop
+  int zr;
+  Control* zr_ctl;
+  double* zr_partials;
 };
 
 // r of a level: level 0 holds the float32 CG residual, scaled by sigma on

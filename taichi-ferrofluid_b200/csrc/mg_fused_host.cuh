@@ -81,6 +81,11 @@ struct FusedPlan {
   int res_lp = 0, res_lb = 0, res_blocks = 0;
   size_t res_smem = 0;
   ResArgs res_args;
+  // z.r of the PCG loop inside the level-0 POST sweep while the plan launches
+  // a PCG part (-1: not now; 0 / 1: before / inside the loop)
+  int zr_mode = -1;
+  Control* zr_ctl = nullptr;
+  double* zr_partials = nullptr;
 };
 
 // Chooses the launch shapes.  Needs pre_post in 1..3 and either every level
@@ -366,6 +371,14 @@ inline SweepArgs<ST> sweep_args(const FusedPlan& F, const Level* lv, int l, cons
   a.chunk = F.chunk[l];
   a.tiles_x = F.tiles_x[l];
   a.tiles_y = F.tiles_y[l];
+  a.zr = -1;
+  a.zr_ctl = nullptr;
+  a.zr_partials = nullptr;
+  if (!PRE && l == 0 && F.zr_mode >= 0) {
+    a.zr = F.zr_mode;
+    a.zr_ctl = F.zr_ctl;
+    a.zr_partials = F.zr_partials;
+  }
   return a;
 }
 

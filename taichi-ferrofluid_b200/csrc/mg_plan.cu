@@ -486,8 +486,17 @@ int tune_resident(mg_plan* P, cudaStream_t s) {
   return MG_OK;
 }
 
+// The level-0 POST sweep can take z.r (k_zr4) over the cells it writes: the
+// label-uniform float32 form with level 0 streamed (not split, not inside the
+// cluster launch) and a grid within the partials buffer.
+bool zr_fusable(const mg_plan* P) {
+  const FusedPlan& F = P->fp;
+  return F.valid && !F.sto && P->d.storage == MG_STORE_F32 && F.lc > 0 && !F.split[0] &&
+         !(F.res && F.res_lp == 0) && F.blocks[0] <= kMaxPartials / 2;
+}
+
 template <typename ST>
-int launch_zr_p(mg_plan* P, bool prologue, cudaStream_t s) {
+int launch_zr_p(mg_plan* P, bool prologue, cudaStream_t s, bool zr_done = false) {
   const Level& L0 = P->lv[0];
   float* p = fptr(P, MG_FIELD_P);
   if (sizeof(ST) == 4 && P->geom[0].count % 4 == 0) {  // float32: 4-cell groups
@@ -495,9 +504,9 @@ int launch_zr_p(mg_plan* P, bool prologue, cudaStream_t s) {
     const Control* cc = P->ctl;
     if (prologue) {
       CK(launch_k(k_update_p4, eb, 256, 0, s, L0, p, cc));
-      CK(launch_k(k_zr4, P->red_blocks, kRedThreads, 0, s, L0, P->ctl, P->partials, 0));
+      if (!zr_done) CK(launch_k(k_zr4, P->red_blocks, kRedThreads, 0, s, L0, P->ctl, P->partials, 0));
     } else {
-      CK(launch_k(k_zr4, P->red_blocks, kRedThreads, 0, s, L0, P->ctl, P->partials, 1));
+      if (!zr_done) CK(launch_k(k_zr4, P->red_blocks, kRedThreads, 0, s, L0, P->ctl, P->partials, 1));
       CK(launch_k(k_update_p4, eb, 256, 0, s, L0, p, cc));
     }
     return MG_OK;
@@ -513,11 +522,11 @@ int launch_zr_p(mg_plan* P, bool prologue, cudaStream_t s) {
   return MG_OK;
 }
 
-int launch_zr_p_any(mg_plan* P, bool prologue, cudaStream_t s) {
+int launch_zr_p_any(mg_plan* P, bool prologue, cudaStream_t s, bool zr_done = false) {
   switch (P->d.storage) {
     case MG_STORE_F16: return launch_zr_p<__half>(P, prologue, s);
     case MG_STORE_BF16: return launch_zr_p<__nv_bfloat16>(P, prologue, s);
-    default: return launch_zr_p<float>(P, prologue, s);
+    default: return launch_zr_p<float>(P, prologue, s, zr_done);
   }
 }
 
@@ -572,8 +581,14 @@ int launch_pcg_part(mg_plan* P, bool prologue, cudaStream_t s) {
     const float* bc = b;
     CK(launch_k(k_pcg_begin, P->red_blocks, kRedThreads, 0, s, L0, bc, x, P->ctl, P->partials));
   }
-  if (int rc = launch_vcycle(P, s)) return rc;
-  if (int rc = launch_zr_p_any(P, prologue, s)) return rc;
+  const bool fuse = zr_fusable(P);
+  P->fp.zr_mode = fuse ? (prologue ? 0 : 1) : -1;
+  P->fp.zr_ctl = P->ctl;
+  P->fp.zr_partials = P->partials;
+  const int rc = launch_vcycle(P, s);
+  P->fp.zr_mode = -1;
+  if (rc) return rc;
+  if (int rc2 = launch_zr_p_any(P, prologue, s, fuse)) return rc2;
   return launch_cg_tail(P, s, 3);
 }
 
@@ -584,7 +599,7 @@ int count_pcg_part(const mg_plan* P, bool prologue) {
     int v = 1;  // the coarse block, or the cluster-resident launch
     const int streamed = P->fp.res ? P->fp.res_lp : P->fp.lc;
     for (int l = 0; l < streamed; ++l) v += P->fp.split[l] ? 2 * (2 * P->d.pre_post + 1) : 2;
-    return (prologue ? 1 : 0) + v + 4 + refresh;
+    return (prologue ? 1 : 0) + v + (zr_fusable(P) ? 3 : 4) + refresh;
   }
   int v = (P->L - 1) * (4 * P->d.pre_post + 2) +
           (P->geom[P->L - 1].count <= kBottomBlockCells ? (P->d.bottom / 2 > 0) : 2 * P->d.bottom);

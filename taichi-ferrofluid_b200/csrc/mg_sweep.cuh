@@ -280,6 +280,7 @@ __global__ void __launch_bounds__(NT) k_sweep(SweepArgs<ST> A) {
   };
 
   float acc = 0.0f;                               // restriction accumulator (PRE)
+  double zr_acc = 0.0;                            // z.r of the cells written (POST, A.zr >= 0)
   const int ct = threadIdx.x;                     // coarse in-plane cell of this thread
   const int ccx = ct % CX, ccy = ct / CX;
 
@@ -431,7 +432,10 @@ __global__ void __launch_bounds__(NT) k_sweep(SweepArgs<ST> A) {
         } else {
 #pragma unroll
           for (int e = 0; e < 4; ++e)
-            if (sa[so + c + e] != 0.0f) F.z[gi + e] = from_f<ST>(v[e]);
+            if (sa[so + c + e] != 0.0f) {
+              F.z[gi + e] = from_f<ST>(v[e]);
+              if (A.zr >= 0) zr_acc += (double)v[e] * (double)sr[so + c + e];
+            }
         }
       }
     }
@@ -468,6 +472,25 @@ __global__ void __launch_bounds__(NT) k_sweep(SweepArgs<ST> A) {
     }
     // the next store overwrites the slots of planes that are no longer read
     __syncthreads();
+  }
+  if constexpr (!PRE) {
+    if (A.zr >= 0) {  // the reduction and epilogue of k_zr4 (mgpcg.py:161-166, 197-202)
+      __shared__ double sh[32];
+      double tot;
+      Control* ctl = A.zr_ctl;
+      if (last_block_total<NT>(zr_acc, A.zr_partials, &ctl->counter[1], sh, &tot) && threadIdx.x == 0) {
+        if (A.zr == 0) {
+          ctl->old_zTr = tot;
+          if (ctl->max_iters == 0) ctl->run = 0;
+        } else {
+          ctl->new_zTr = tot;
+          ctl->beta = (float)(tot / (ctl->old_zTr + ctl->eps));
+          ctl->old_zTr = tot;
+          ctl->iter += 1;
+          if (ctl->max_iters != -1 && ctl->iter >= ctl->max_iters) ctl->run = 0;
+        }
+      }
+    }
   }
 }
 

@@ -1,13 +1,14 @@
 """The cluster-resident V-cycle (the levels from the first brick level down in
 one launch of one thread-block cluster, each CTA's bricks in shared memory)
 against the streamed V-cycle and the oracle: z of one V-cycle BIT-EXACT, and
-the solve BIT-EXACT (x and iteration count), on cubic and non-cubic grids,
-with the brick levels starting at level 0, 1 and 2 below streamed levels."""
+the solve BIT-EXACT (x and iteration count) where level 0 stays streamed, on
+cubic and non-cubic grids, with the brick levels starting at level 0, 1 and 2
+below streamed levels."""
 import numpy as np
 import pytest
 
 import mg_scenes
-from helpers import gpu_for, oracle_for, small_3d
+from helpers import gpu_for, oracle_for, rel_l2, small_3d
 
 pytestmark = pytest.mark.gpu
 
@@ -115,8 +116,15 @@ def test_resident_solve_bit_exact(name):
         g.resident(True, first_level=first)
         it1 = g.solve(500)
         assert g.last_status == "converged"
-        assert it1 == it0
-        np.testing.assert_array_equal(_np(g.x), x0)
+        if first > 0:  # level 0 streamed in both: the same kernels and sums
+            assert it1 == it0
+            np.testing.assert_array_equal(_np(g.x), x0)
+        else:
+            # level 0 inside the cluster: z.r is summed by k_zr4 instead of
+            # inside the level-0 sweep, so the FP64 sum may differ in its last
+            # bits (the V-cycle itself is bit-exact, above)
+            assert abs(it1 - it0) <= 1
+            assert rel_l2(_np(g.x), x0) < 1e-6
 
 
 def test_resident_stage_and_pcg_counts():
