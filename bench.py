@@ -477,6 +477,7 @@ def gpu_arm(args, rank, world, local):
         "vcycle": {c.kind: {"operator_form": c.solver.operator_form(0),
                             "split_levels_bits": c.solver.split_levels()[0],
                             "streamed_levels": c.solver.split_levels()[1],
+                            "one_plane_step_bits": c.solver.step_planes(),
                             "cluster_from_level": c.solver.resident()[1] if c.solver.resident()[0] else None}
                    for c in cases},
         "last_rel_resid": rel, "last_status": status,

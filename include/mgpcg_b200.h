@@ -399,6 +399,17 @@ MG_API int mg_plan_operator_form(const mg_plan_t* plan, int32_t level, int32_t* 
  * profilers, which serialise the trial launches). */
 MG_API int mg_plan_split(mg_plan_t* plan, int32_t set, uint32_t* bits, int32_t* streamed);
 
+/* Planes per pipeline step of the streamed sweep (no reference counterpart: a
+ * B200 launch shape of the same arithmetic): bit 2l set = level l's PRE sweep
+ * (pre-smoothing + restriction) steps one plane at a time, bit 2l+1 the same
+ * for its POST sweep; clear = two planes.  3D label-uniform float32 plans
+ * time both per level and direction when a shape is first prepared (cached
+ * per shape); levels whose chunks are 2 planes run as one step either way.
+ * Both shapes give bit-identical values.  set != 0 forces *bits (after the
+ * plan is prepared; valid until the next prepare); *bits returns the choice.
+ * MGPCG_STEP1=<bits> replaces the timing for every plan (for profilers). */
+MG_API int mg_plan_steps(mg_plan_t* plan, int32_t set, uint32_t* bits);
+
 /* The cluster-resident V-cycle (no reference counterpart: a B200 launch shape
  * of mgpcg.py:125-148 with the same float32 values): for a label-uniform
  * float32 3D plan whose levels [first_level, L) halve exactly, those levels run

@@ -2,6 +2,7 @@
 // streamed levels and the block-resident coarse levels, and the launches.
 #pragma once
 #include <cmath>
+#include <type_traits>
 
 #include "mg_sweep.cuh"
 #include "mg_coarse.cuh"
@@ -41,6 +42,11 @@ struct TileShape {
 #ifndef MG_TILE3_NT
 #define MG_TILE3_NT 512
 #endif
+// blocks per SM assumed when the streamed levels' grids are sized, beyond
+// those that fit its shared memory (a build-time experiment knob)
+#ifndef MG_CHUNK_SLOTS_EXTRA
+#define MG_CHUNK_SLOTS_EXTRA 0
+#endif
 constexpr TileShape kTile3 = {MG_TILE3_TX, MG_TILE3_TY, MG_TILE3_NT, MG_TILE3_K};
 constexpr TileShape kTile2 = {128, 1, 128, 4};
 // the whole-domain stored form stages twice the bytes per cell: a smaller
@@ -66,6 +72,11 @@ struct FusedPlan {
   // prolongation instead of the streamed kernel (chosen by measurement: on
   // the large levels of the stored form the per-kernel passes are faster)
   bool split[kMaxLevels] = {};
+  // per streamed level and direction (bit 0 PRE, bit 1 POST): one plane per
+  // pipeline step instead of the tile's two (3D label-uniform float32 only;
+  // chosen by measurement: one plane is faster for the 256^3 PRE sweep,
+  // slower at 128^3)
+  unsigned char step1[kMaxLevels] = {};
   int lc = 0;                      // first level of the block-resident coarse solve
   int dim = 3, ns = 4, storage = 0;
   int chunk[kMaxLevels], tiles_x[kMaxLevels], tiles_y[kMaxLevels], blocks[kMaxLevels];
@@ -98,7 +109,10 @@ inline bool make_fused_plan(const Level* lv, int L, int dim, int pre_post, int b
   F->sto = false;
   F->res_ok = false;
   F->res = false;
-  for (int l = 0; l < kMaxLevels; ++l) F->split[l] = false;
+  for (int l = 0; l < kMaxLevels; ++l) {
+    F->split[l] = false;
+    F->step1[l] = 0;
+  }
   bool uniform = true, all_whole = true;
   for (int l = 0; l < L; ++l) {
     uniform = uniform && op_form[l] == 1;
@@ -139,7 +153,8 @@ inline bool make_fused_plan(const Level* lv, int L, int dim, int pre_post, int b
   // streamed levels: the 4-wide groups need the fastest extent to be a
   // multiple of 4 (then a group is wholly inside or wholly outside the grid)
   const size_t smem = sweep_smem(dim, F->ns, F->tile, false, F->sto);
-  const int per_sm = (int)(kSmemLimit / (smem + 1024)) < 1 ? 1 : (int)(kSmemLimit / (smem + 1024));
+  const int per_sm = ((int)(kSmemLimit / (smem + 1024)) < 1 ? 1 : (int)(kSmemLimit / (smem + 1024))) +
+                     MG_CHUNK_SLOTS_EXTRA;
   for (int l = 0; l < lc; ++l) {
     const Geom& g = lv[l].g;
     const int nx = dim == 3 ? g.n[2] : g.n[1];
@@ -385,6 +400,16 @@ inline SweepArgs<ST> sweep_args(const FusedPlan& F, const Level* lv, int l, cons
 template <int DIM, typename ST, int NS, bool PRE, bool STO = false>
 inline cudaError_t launch_sweep_t(const FusedPlan& F, const Level* lv, int l, const Control* ctl, cudaStream_t s) {
   constexpr TileShape T = STO ? kTile3S : (DIM == 3 ? kTile3 : kTile2);
+  if constexpr (DIM == 3 && !STO && std::is_same<ST, float>::value && T.k != 1) {
+    if (F.chunk[l] > 2 && ((F.step1[l] >> (PRE ? 0 : 1)) & 1)) {
+      constexpr TileShape T1 = {T.tx, T.ty, T.nt, 1};
+      auto kern = k_sweep<DIM, ST, NS, T1.tx, T1.ty, PRE, T1.nt, T1.k, STO>;
+      const size_t smem = sweep_smem(DIM, NS, T1, false, STO);
+      cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+      if (e != cudaSuccess) return e;
+      return launch_k(kern, F.blocks[l], T1.nt, smem, s, sweep_args<ST, PRE>(F, lv, l, ctl));
+    }
+  }
   if (DIM == 3 && F.chunk[l] == 2) {
     // small level: each block's 2 planes + halo planes in ONE pipeline step
     constexpr TileShape T1 = {T.tx, T.ty, T.nt, 2 + 2 * NS};

@@ -376,6 +376,78 @@ int tune_split(mg_plan* P, cudaStream_t s) {
   return MG_OK;
 }
 
+// Planes per pipeline step of the label-uniform float32 streamed sweep: the
+// tile's two, or one (a shorter ring, more blocks resident, a longer serial
+// chain of steps).  Measured on B200, one plane is faster for the PRE sweep
+// of a 256^3 level (196.6 vs 225.7 us) and slower at 128^3 (49.3 vs 40.0 us),
+// so each streamed level with chunks of more than 2 planes is timed both ways
+// per direction (one warm-up, kTuneReps timed) the first time a shape is
+// prepared; the choice is cached per shape.  Both compute the same values.
+std::map<std::array<int, 7>, uint32_t> g_tune_step;  // bits 2l / 2l+1: PRE / POST of level l
+
+int tune_steps(mg_plan* P, cudaStream_t s) {
+  FusedPlan& F = P->fp;
+  if (!F.valid || F.sto || F.dim != 3 || F.storage != MG_STORE_F32) return MG_OK;
+  // MGPCG_STEP1=<bits> replaces the timing (profilers serialise the trial
+  // launches and would skew the choice)
+  if (const char* ov = std::getenv("MGPCG_STEP1")) {
+    const unsigned long v = std::strtoul(ov, nullptr, 0);
+    for (int l = 0; l < F.lc; ++l) F.step1[l] = (unsigned char)((v >> (2 * l)) & 3ul);
+    return MG_OK;
+  }
+  const Geom& g = P->geom[0];
+  const std::array<int, 7> key = {g.dim, g.n[0], g.n[1], g.n[2], P->L, P->d.pre_post, F.lc};
+  {
+    std::lock_guard<std::mutex> lk(g_tune_mu);
+    auto it = g_tune_step.find(key);
+    if (it != g_tune_step.end()) {
+      for (int l = 0; l < F.lc; ++l) F.step1[l] = (unsigned char)((it->second >> (2 * l)) & 3u);
+      return MG_OK;
+    }
+  }
+  cudaEvent_t e0 = nullptr, e1 = nullptr;
+  CK(cudaEventCreate(&e0));
+  cudaError_t ce = cudaEventCreate(&e1);
+  if (ce != cudaSuccess) {
+    cudaEventDestroy(e0);
+    return set_err("cudaEventCreate", ce);
+  }
+  uint32_t bits = 0;
+  int rc = MG_OK;
+  for (int l = 0; l < F.lc && rc == MG_OK; ++l) {
+    F.step1[l] = 0;
+    if (F.chunk[l] <= 2) continue;  // one-step launch: no pipeline
+    for (int dir = 0; dir < 2 && rc == MG_OK; ++dir) {
+      const bool pre = dir == 0;
+      float t[2] = {0.0f, 0.0f};
+      for (int mode = 0; mode < 2 && rc == MG_OK; ++mode) {
+        F.step1[l] = (unsigned char)((F.step1[l] & ~(1u << dir)) | ((unsigned)mode << dir));
+        for (int rep = 0; rep < 1 + kTuneReps && rc == MG_OK; ++rep) {  // rep 0 warms up
+          if (rep == 1) cudaEventRecord(e0, s);
+          rc = launch_level(P, l, pre, s);
+        }
+        if (rc != MG_OK) break;
+        cudaEventRecord(e1, s);
+        cudaError_t e = cudaEventSynchronize(e1);
+        if (e == cudaSuccess) e = cudaEventElapsedTime(&t[mode], e0, e1);
+        if (e != cudaSuccess) rc = set_err("tune_steps", e);
+      }
+      const bool one = rc == MG_OK && t[1] < t[0];
+      F.step1[l] = (unsigned char)((F.step1[l] & ~(1u << dir)) | ((unsigned)one << dir));
+    }
+    bits |= (uint32_t)F.step1[l] << (2 * l);
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  if (rc != MG_OK) {
+    for (int l = 0; l < kMaxLevels; ++l) F.step1[l] = 0;
+    return rc;
+  }
+  std::lock_guard<std::mutex> lk(g_tune_mu);
+  g_tune_step[key] = bits;
+  return MG_OK;
+}
+
 // The cluster-resident V-cycle against the streamed one: for a label-uniform
 // float32 plan whose levels allow bricks, the V-cycle is timed streamed and
 // with the cluster starting at each feasible level (CUDA events, one warm-up,
@@ -1342,6 +1414,7 @@ static int finish_prepare(mg_plan_t* P, cudaStream_t s, bool declared) {
   k_set_kappa<<<1, 1, 0, s>>>(P->ctl, (double)P->fp.kappa);
   CKL("k_set_kappa");
   if (int rc = tune_split(P, s)) return rc;
+  if (int rc = tune_steps(P, s)) return rc;
   if (int rc = tune_resident(P, s)) return rc;
   if (declared) {
     for (int l = 0; l < P->L; ++l) {
@@ -1359,6 +1432,7 @@ static int finish_prepare(mg_plan_t* P, cudaStream_t s, bool declared) {
   mix(P->fp.res);
   mix(P->fp.res_lp);
   for (int l = 0; l < P->L; ++l) mix(P->fp.split[l]);
+  for (int l = 0; l < P->L; ++l) mix(P->fp.step1[l]);
   for (int l = 0; l < P->L; ++l) {
     uint32_t bits;
     std::memcpy(&bits, &P->fp.s[l], 4);
@@ -1391,6 +1465,23 @@ int mg_plan_split(mg_plan_t* P, int32_t set, uint32_t* bits, int32_t* streamed) 
   uint32_t b = 0;
   for (int l = 0; l < P->fp.lc; ++l)
     if (P->fp.split[l]) b |= 1u << l;
+  *bits = b;
+  return MG_OK;
+}
+
+int mg_plan_steps(mg_plan_t* P, int32_t set, uint32_t* bits) {
+  if (!P || !bits) return bad("null pointer");
+  if (set) {
+    if (!P->fp.valid) return bad("the plan has no fused V-cycle");
+    if (*bits >> (2 * P->fp.lc)) return bad("step bits beyond the streamed levels");
+    if (*bits && (P->fp.sto || P->fp.dim != 3 || P->fp.storage != MG_STORE_F32))
+      return bad("one plane per step needs the 3D label-uniform float32 form");
+    for (int l = 0; l < P->fp.lc; ++l) P->fp.step1[l] = (unsigned char)((*bits >> (2 * l)) & 3u);
+    destroy_graph(P);
+    P->graph_sig = 0;
+  }
+  uint32_t b = 0;
+  for (int l = 0; l < P->fp.lc; ++l) b |= (uint32_t)P->fp.step1[l] << (2 * l);
   *bits = b;
   return MG_OK;
 }

@@ -179,6 +179,15 @@ class MGPCGPoissonSolver:
                                      mg_lib.ctypes.byref(n)), "mg_plan_split")
         return int(b.value), int(n.value)
 
+    def step_planes(self, bits=None):
+        """The autotuner's planes per step of the streamed sweeps: bit 2l (2l+1)
+        set = level l's PRE (POST) sweep steps one plane at a time, else two;
+        ``bits`` forces a choice until the next prepare."""
+        b = mg_lib.ctypes.c_uint32(0 if bits is None else int(bits))
+        check(self.lib.mg_plan_steps(self.plan, 0 if bits is None else 1, mg_lib.ctypes.byref(b)),
+              "mg_plan_steps")
+        return int(b.value)
+
     def resident(self, on=None, first_level=None):
         """(on, first level): whether the V-cycle runs its levels from the first
         brick level down as one thread-block-cluster launch (the autotuner's

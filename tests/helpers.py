@@ -10,6 +10,18 @@ def small_3d(n=32, seed=1, levels=3):
     return mg_scenes.ferro_drop_3d(n=n, seed=seed, levels=levels)
 
 
+def box_3d(res, levels, seed=5):
+    """A drop above a pool on a non-cubic grid (res = planes, rows, columns)."""
+    n = max(res)
+    dx = 1.0 / n
+    phi = mg_scenes.drop_pool_phi(res, dx)
+    rng = np.random.default_rng(seed)
+    vel = mg_scenes.random_velocity(rng, res, gravity_dt=-9.8 / 60.0)
+    return mg_scenes.Scene(dim=3, res=res, dx=dx, dt=1.0 / 60.0, rho=1000.0, p0=1e-3, phi=phi,
+                           cell_type=mg_scenes.labels_from_phi(phi), velocity=vel, levels=levels,
+                           gfm_clamp=100.0, name="box_" + "x".join(map(str, res)))
+
+
 def oracle_for(scene, real=np.float32, bottom=50, pre_post=2, levels=None, clamp=None):
     from oracle import OracleSolver
     L = levels or scene.levels

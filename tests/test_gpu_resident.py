@@ -8,20 +8,10 @@ import numpy as np
 import pytest
 
 import mg_scenes
+from helpers import box_3d as _box
 from helpers import gpu_for, oracle_for, rel_l2, small_3d
 
 pytestmark = pytest.mark.gpu
-
-
-def _box(res, levels, seed=5):
-    n = max(res)
-    dx = 1.0 / n
-    phi = mg_scenes.drop_pool_phi(res, dx)
-    rng = np.random.default_rng(seed)
-    vel = mg_scenes.random_velocity(rng, res, gravity_dt=-9.8 / 60.0)
-    return mg_scenes.Scene(dim=3, res=res, dx=dx, dt=1.0 / 60.0, rho=1000.0, p0=1e-3, phi=phi,
-                           cell_type=mg_scenes.labels_from_phi(phi), velocity=vel, levels=levels,
-                           gfm_clamp=100.0, name="box_" + "x".join(map(str, res)))
 
 
 # scene, first level that allows bricks (-1: none)
