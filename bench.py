@@ -478,6 +478,7 @@ def gpu_arm(args, rank, world, local):
                             "split_levels_bits": c.solver.split_levels()[0],
                             "streamed_levels": c.solver.split_levels()[1],
                             "one_plane_step_bits": c.solver.step_planes(),
+                            "grid_extra_bits": c.solver.grid_extra(),
                             "cluster_from_level": c.solver.resident()[1] if c.solver.resident()[0] else None}
                    for c in cases},
         "last_rel_resid": rel, "last_status": status,

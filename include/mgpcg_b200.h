@@ -407,8 +407,20 @@ MG_API int mg_plan_split(mg_plan_t* plan, int32_t set, uint32_t* bits, int32_t* 
  * per shape); levels whose chunks are 2 planes run as one step either way.
  * Both shapes give bit-identical values.  set != 0 forces *bits (after the
  * plan is prepared; valid until the next prepare); *bits returns the choice.
- * MGPCG_STEP1=<bits> replaces the timing for every plan (for profilers). */
+ * MGPCG_STEP1=<bits> replaces the timing for every plan (for profilers; with
+ * MGPCG_GRID unset, every grid is sized for the blocks that fit). */
 MG_API int mg_plan_steps(mg_plan_t* plan, int32_t set, uint32_t* bits);
+
+/* Grid of the streamed sweep (no reference counterpart: a B200 launch shape
+ * of the same arithmetic): bits 2l..2l+1 = the blocks per SM, beyond those
+ * that fit its shared memory, that level l's grid is sized for (0..3; more
+ * blocks, shorter chunks of planes).  Every fused plan times 0, 1 and 2 per
+ * pipelined level when a shape is first prepared (cached per shape), before
+ * the planes per step.  All grids give bit-identical V-cycles.  set != 0
+ * forces *bits (after the plan is prepared; valid until the next prepare);
+ * *bits returns the choice.  MGPCG_GRID=<bits> replaces the timing for every
+ * plan (for profilers; with MGPCG_STEP1 unset, one plane per step is off). */
+MG_API int mg_plan_grid(mg_plan_t* plan, int32_t set, uint32_t* bits);
 
 /* The cluster-resident V-cycle (no reference counterpart: a B200 launch shape
  * of mgpcg.py:125-148 with the same float32 values): for a label-uniform

@@ -42,11 +42,6 @@ struct TileShape {
 #ifndef MG_TILE3_NT
 #define MG_TILE3_NT 512
 #endif
-// blocks per SM assumed when the streamed levels' grids are sized, beyond
-// those that fit its shared memory (a build-time experiment knob)
-#ifndef MG_CHUNK_SLOTS_EXTRA
-#define MG_CHUNK_SLOTS_EXTRA 0
-#endif
 constexpr TileShape kTile3 = {MG_TILE3_TX, MG_TILE3_TY, MG_TILE3_NT, MG_TILE3_K};
 constexpr TileShape kTile2 = {128, 1, 128, 4};
 // the whole-domain stored form stages twice the bytes per cell: a smaller
@@ -74,9 +69,14 @@ struct FusedPlan {
   bool split[kMaxLevels] = {};
   // per streamed level and direction (bit 0 PRE, bit 1 POST): one plane per
   // pipeline step instead of the tile's two (3D label-uniform float32 only;
-  // chosen by measurement: one plane is faster for the 256^3 PRE sweep,
-  // slower at 128^3)
+  // chosen by measurement)
   unsigned char step1[kMaxLevels] = {};
+  // per streamed level: blocks per SM assumed when its grid is sized, beyond
+  // those that fit one SM's shared memory (shorter chunks, more blocks; chosen
+  // by measurement: 1 extra is faster for the 256^3 level-0 sweeps, slower at
+  // 128^3)
+  unsigned char grid_extra[kMaxLevels] = {};
+  int per_sm = 1, num_sms = 148;
   int lc = 0;                      // first level of the block-resident coarse solve
   int dim = 3, ns = 4, storage = 0;
   int chunk[kMaxLevels], tiles_x[kMaxLevels], tiles_y[kMaxLevels], blocks[kMaxLevels];
@@ -99,6 +99,28 @@ struct FusedPlan {
   double* zr_partials = nullptr;
 };
 
+// Grid of streamed level l: tiles of the plane times chunks of planes along
+// the slowest axis, enough blocks to fill every SM with the blocks that fit
+// its shared memory plus `extra` (then a block's chunk is shorter).  Small
+// levels are latency-bound: short chunks (more blocks, shorter serial plane
+// chains) beat the extra halo planes they load.
+inline void level_grid(FusedPlan* F, const Geom& g, int l, int extra) {
+  const int nx = F->dim == 3 ? g.n[2] : g.n[1];
+  const int ny = F->dim == 3 ? g.n[1] : 1;
+  F->tiles_x[l] = (nx + F->tile.tx - 1) / F->tile.tx;
+  F->tiles_y[l] = F->dim == 3 ? (ny + F->tile.ty - 1) / F->tile.ty : 1;
+  const long long tiles = (long long)F->tiles_x[l] * F->tiles_y[l];
+  const long long target = (long long)(F->per_sm + extra) * F->num_sms;
+  long long chunk = (long long)g.n[0] * tiles / target;
+  if (chunk < 2) chunk = 2;
+  chunk &= ~1LL;
+  if (chunk > g.n[0]) chunk = g.n[0];
+  if (chunk < 2) chunk = 2;
+  F->chunk[l] = (int)chunk;
+  F->blocks[l] = (int)(tiles * ((g.n[0] + chunk - 1) / chunk));
+  F->grid_extra[l] = (unsigned char)extra;
+}
+
 // Chooses the launch shapes.  Needs pre_post in 1..3 and either every level
 // in label-uniform form, or (the whole-domain stored form: float32 grids, 3D,
 // pre_post 1..2) every level whole-domain - every cell FLUID with a nonzero
@@ -112,6 +134,7 @@ inline bool make_fused_plan(const Level* lv, int L, int dim, int pre_post, int b
   for (int l = 0; l < kMaxLevels; ++l) {
     F->split[l] = false;
     F->step1[l] = 0;
+    F->grid_extra[l] = 0;
   }
   bool uniform = true, all_whole = true;
   for (int l = 0; l < L; ++l) {
@@ -153,27 +176,13 @@ inline bool make_fused_plan(const Level* lv, int L, int dim, int pre_post, int b
   // streamed levels: the 4-wide groups need the fastest extent to be a
   // multiple of 4 (then a group is wholly inside or wholly outside the grid)
   const size_t smem = sweep_smem(dim, F->ns, F->tile, false, F->sto);
-  const int per_sm = ((int)(kSmemLimit / (smem + 1024)) < 1 ? 1 : (int)(kSmemLimit / (smem + 1024))) +
-                     MG_CHUNK_SLOTS_EXTRA;
+  F->per_sm = (int)(kSmemLimit / (smem + 1024)) < 1 ? 1 : (int)(kSmemLimit / (smem + 1024));
+  F->num_sms = num_sms;
   for (int l = 0; l < lc; ++l) {
     const Geom& g = lv[l].g;
     const int nx = dim == 3 ? g.n[2] : g.n[1];
-    const int ny = dim == 3 ? g.n[1] : 1;
     if (nx % 4 != 0) return false;
-    F->tiles_x[l] = (nx + F->tile.tx - 1) / F->tile.tx;
-    F->tiles_y[l] = dim == 3 ? (ny + F->tile.ty - 1) / F->tile.ty : 1;
-    const long long tiles = (long long)F->tiles_x[l] * F->tiles_y[l];
-    // enough blocks to fill every SM with the blocks that fit its shared memory
-    const long long target = (long long)per_sm * num_sms;
-    // small levels are latency-bound: short chunks (more blocks, shorter
-    // serial plane chains) beat the extra halo planes they load
-    long long chunk = (long long)g.n[0] * tiles / target;
-    if (chunk < 2) chunk = 2;
-    chunk &= ~1LL;
-    if (chunk > g.n[0]) chunk = g.n[0];
-    if (chunk < 2) chunk = 2;
-    F->chunk[l] = (int)chunk;
-    F->blocks[l] = (int)(tiles * ((g.n[0] + chunk - 1) / chunk));
+    level_grid(F, g, l, 0);
   }
   // block-resident coarse levels
   CoarseArgs& C = F->coarse;

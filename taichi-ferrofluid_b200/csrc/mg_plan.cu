@@ -376,32 +376,61 @@ int tune_split(mg_plan* P, cudaStream_t s) {
   return MG_OK;
 }
 
-// Planes per pipeline step of the label-uniform float32 streamed sweep: the
-// tile's two, or one (a shorter ring, more blocks resident, a longer serial
-// chain of steps).  Measured on B200, one plane is faster for the PRE sweep
-// of a 256^3 level (196.6 vs 225.7 us) and slower at 128^3 (49.3 vs 40.0 us),
-// so each streamed level with chunks of more than 2 planes is timed both ways
-// per direction (one warm-up, kTuneReps timed) the first time a shape is
-// prepared; the choice is cached per shape.  Both compute the same values.
-std::map<std::array<int, 7>, uint32_t> g_tune_step;  // bits 2l / 2l+1: PRE / POST of level l
+// Grid and planes per pipeline step of the streamed levels.  The grid of a
+// level is sized for the blocks that fit one SM's shared memory plus 0, 1 or
+// 2 more (shorter chunks, more blocks); measured on B200, 1 more makes the
+// 256^3 level-0 sweeps faster (PRE 225.7 -> 170.2 us, POST 240.5 -> 210.9 us)
+// and the 128^3 ones slower (PRE 40.2 -> 44.3 us).  Then, for the 3D
+// label-uniform float32 form, one plane per step or the tile's two, per
+// direction (a shorter ring; with the grid held fixed two planes won on every
+// level measured).  Each pipelined level is timed every way (one warm-up,
+// kTuneReps timed) the first time a shape is prepared; the choice is cached
+// per shape.  All choices compute the same values.
+std::map<std::array<int, 7>, std::pair<uint32_t, uint32_t>> g_tune_stream;  // (step bits, grid bits)
 
-int tune_steps(mg_plan* P, cudaStream_t s) {
+void apply_stream_bits(mg_plan* P, uint32_t step, uint32_t grid) {
   FusedPlan& F = P->fp;
-  if (!F.valid || F.sto || F.dim != 3 || F.storage != MG_STORE_F32) return MG_OK;
-  // MGPCG_STEP1=<bits> replaces the timing (profilers serialise the trial
-  // launches and would skew the choice)
-  if (const char* ov = std::getenv("MGPCG_STEP1")) {
-    const unsigned long v = std::strtoul(ov, nullptr, 0);
-    for (int l = 0; l < F.lc; ++l) F.step1[l] = (unsigned char)((v >> (2 * l)) & 3ul);
+  const bool steps_ok = !F.sto && F.dim == 3 && F.storage == MG_STORE_F32;
+  for (int l = 0; l < F.lc; ++l) {
+    level_grid(&F, P->lv[l].g, l, (int)((grid >> (2 * l)) & 3u));
+    F.step1[l] = steps_ok ? (unsigned char)((step >> (2 * l)) & 3u) : 0;
+  }
+}
+
+int time_level(mg_plan* P, int l, int dirs, cudaEvent_t e0, cudaEvent_t e1, cudaStream_t s, float* ms) {
+  int rc = MG_OK;
+  for (int rep = 0; rep < 1 + kTuneReps && rc == MG_OK; ++rep) {  // rep 0 warms up
+    if (rep == 1) cudaEventRecord(e0, s);
+    if (dirs & 1) rc = launch_level(P, l, true, s);
+    if (rc == MG_OK && (dirs & 2)) rc = launch_level(P, l, false, s);
+  }
+  if (rc != MG_OK) return rc;
+  cudaEventRecord(e1, s);
+  cudaError_t e = cudaEventSynchronize(e1);
+  if (e == cudaSuccess) e = cudaEventElapsedTime(ms, e0, e1);
+  return e == cudaSuccess ? MG_OK : set_err("tune_stream", e);
+}
+
+int tune_stream(mg_plan* P, cudaStream_t s) {
+  FusedPlan& F = P->fp;
+  if (!F.valid) return MG_OK;
+  const bool steps_ok = !F.sto && F.dim == 3 && F.storage == MG_STORE_F32;
+  // MGPCG_STEP1=<bits> / MGPCG_GRID=<bits> replace the timing (profilers
+  // serialise the trial launches and would skew the choice)
+  const char* ov_step = std::getenv("MGPCG_STEP1");
+  const char* ov_grid = std::getenv("MGPCG_GRID");
+  if (ov_step || ov_grid) {
+    apply_stream_bits(P, ov_step ? (uint32_t)std::strtoul(ov_step, nullptr, 0) : 0u,
+                      ov_grid ? (uint32_t)std::strtoul(ov_grid, nullptr, 0) : 0u);
     return MG_OK;
   }
   const Geom& g = P->geom[0];
   const std::array<int, 7> key = {g.dim, g.n[0], g.n[1], g.n[2], P->L, P->d.pre_post, F.lc};
   {
     std::lock_guard<std::mutex> lk(g_tune_mu);
-    auto it = g_tune_step.find(key);
-    if (it != g_tune_step.end()) {
-      for (int l = 0; l < F.lc; ++l) F.step1[l] = (unsigned char)((it->second >> (2 * l)) & 3u);
+    auto it = g_tune_stream.find(key);
+    if (it != g_tune_stream.end()) {
+      apply_stream_bits(P, it->second.first, it->second.second);
       return MG_OK;
     }
   }
@@ -412,39 +441,46 @@ int tune_steps(mg_plan* P, cudaStream_t s) {
     cudaEventDestroy(e0);
     return set_err("cudaEventCreate", ce);
   }
-  uint32_t bits = 0;
+  uint32_t step = 0, grid = 0;
   int rc = MG_OK;
   for (int l = 0; l < F.lc && rc == MG_OK; ++l) {
     F.step1[l] = 0;
-    if (F.chunk[l] <= 2) continue;  // one-step launch: no pipeline
+    if (F.split[l] || F.chunk[l] <= 2) continue;  // per-kernel passes / one-step launch
+    float best = 0.0f;
+    int best_extra = 0, last_chunk = -1;
+    for (int extra = 0; extra <= 2 && rc == MG_OK; ++extra) {
+      level_grid(&F, P->lv[l].g, l, extra);
+      if (F.chunk[l] == last_chunk) continue;  // the same grid
+      last_chunk = F.chunk[l];
+      float t = 0.0f;
+      rc = time_level(P, l, 3, e0, e1, s, &t);
+      if (rc == MG_OK && (extra == 0 || t < best)) {
+        best = t;
+        best_extra = extra;
+      }
+    }
+    level_grid(&F, P->lv[l].g, l, rc == MG_OK ? best_extra : 0);
+    grid |= (uint32_t)F.grid_extra[l] << (2 * l);
+    if (!steps_ok || F.chunk[l] <= 2) continue;
     for (int dir = 0; dir < 2 && rc == MG_OK; ++dir) {
-      const bool pre = dir == 0;
       float t[2] = {0.0f, 0.0f};
       for (int mode = 0; mode < 2 && rc == MG_OK; ++mode) {
         F.step1[l] = (unsigned char)((F.step1[l] & ~(1u << dir)) | ((unsigned)mode << dir));
-        for (int rep = 0; rep < 1 + kTuneReps && rc == MG_OK; ++rep) {  // rep 0 warms up
-          if (rep == 1) cudaEventRecord(e0, s);
-          rc = launch_level(P, l, pre, s);
-        }
-        if (rc != MG_OK) break;
-        cudaEventRecord(e1, s);
-        cudaError_t e = cudaEventSynchronize(e1);
-        if (e == cudaSuccess) e = cudaEventElapsedTime(&t[mode], e0, e1);
-        if (e != cudaSuccess) rc = set_err("tune_steps", e);
+        rc = time_level(P, l, 1 << dir, e0, e1, s, &t[mode]);
       }
       const bool one = rc == MG_OK && t[1] < t[0];
       F.step1[l] = (unsigned char)((F.step1[l] & ~(1u << dir)) | ((unsigned)one << dir));
     }
-    bits |= (uint32_t)F.step1[l] << (2 * l);
+    step |= (uint32_t)F.step1[l] << (2 * l);
   }
   cudaEventDestroy(e0);
   cudaEventDestroy(e1);
   if (rc != MG_OK) {
-    for (int l = 0; l < kMaxLevels; ++l) F.step1[l] = 0;
+    apply_stream_bits(P, 0u, 0u);
     return rc;
   }
   std::lock_guard<std::mutex> lk(g_tune_mu);
-  g_tune_step[key] = bits;
+  g_tune_stream[key] = {step, grid};
   return MG_OK;
 }
 
@@ -1414,7 +1450,7 @@ static int finish_prepare(mg_plan_t* P, cudaStream_t s, bool declared) {
   k_set_kappa<<<1, 1, 0, s>>>(P->ctl, (double)P->fp.kappa);
   CKL("k_set_kappa");
   if (int rc = tune_split(P, s)) return rc;
-  if (int rc = tune_steps(P, s)) return rc;
+  if (int rc = tune_stream(P, s)) return rc;
   if (int rc = tune_resident(P, s)) return rc;
   if (declared) {
     for (int l = 0; l < P->L; ++l) {
@@ -1433,6 +1469,7 @@ static int finish_prepare(mg_plan_t* P, cudaStream_t s, bool declared) {
   mix(P->fp.res_lp);
   for (int l = 0; l < P->L; ++l) mix(P->fp.split[l]);
   for (int l = 0; l < P->L; ++l) mix(P->fp.step1[l]);
+  for (int l = 0; l < P->fp.lc; ++l) mix((uint64_t)P->fp.chunk[l] << 32 | (uint32_t)P->fp.blocks[l]);
   for (int l = 0; l < P->L; ++l) {
     uint32_t bits;
     std::memcpy(&bits, &P->fp.s[l], 4);
@@ -1482,6 +1519,21 @@ int mg_plan_steps(mg_plan_t* P, int32_t set, uint32_t* bits) {
   }
   uint32_t b = 0;
   for (int l = 0; l < P->fp.lc; ++l) b |= (uint32_t)P->fp.step1[l] << (2 * l);
+  *bits = b;
+  return MG_OK;
+}
+
+int mg_plan_grid(mg_plan_t* P, int32_t set, uint32_t* bits) {
+  if (!P || !bits) return bad("null pointer");
+  if (set) {
+    if (!P->fp.valid) return bad("the plan has no fused V-cycle");
+    if (*bits >> (2 * P->fp.lc)) return bad("grid bits beyond the streamed levels");
+    for (int l = 0; l < P->fp.lc; ++l) level_grid(&P->fp, P->lv[l].g, l, (int)((*bits >> (2 * l)) & 3u));
+    destroy_graph(P);
+    P->graph_sig = 0;
+  }
+  uint32_t b = 0;
+  for (int l = 0; l < P->fp.lc; ++l) b |= (uint32_t)P->fp.grid_extra[l] << (2 * l);
   *bits = b;
   return MG_OK;
 }

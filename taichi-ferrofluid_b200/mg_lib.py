@@ -110,6 +110,7 @@ _SIGS = {
     "mg_plan_operator_form": (ctypes.c_int, [_vp, _i32, ctypes.POINTER(_i32)]),
     "mg_plan_split": (ctypes.c_int, [_vp, _i32, ctypes.POINTER(ctypes.c_uint32), ctypes.POINTER(_i32)]),
     "mg_plan_steps": (ctypes.c_int, [_vp, _i32, ctypes.POINTER(ctypes.c_uint32)]),
+    "mg_plan_grid": (ctypes.c_int, [_vp, _i32, ctypes.POINTER(ctypes.c_uint32)]),
     "mg_plan_resident": (ctypes.c_int, [_vp, _i32, ctypes.POINTER(_i32), ctypes.POINTER(_i32)]),
     "mg_smooth": (ctypes.c_int, [_vp, _i32, _i32, _vp]),
     "mg_restrict": (ctypes.c_int, [_vp, _i32, _vp]),

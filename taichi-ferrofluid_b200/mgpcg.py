@@ -188,6 +188,15 @@ class MGPCGPoissonSolver:
               "mg_plan_steps")
         return int(b.value)
 
+    def grid_extra(self, bits=None):
+        """The autotuner's grid per streamed level: bits 2l..2l+1 = blocks per SM,
+        beyond those that fit its shared memory, that level's grid is sized for;
+        ``bits`` forces a choice until the next prepare."""
+        b = mg_lib.ctypes.c_uint32(0 if bits is None else int(bits))
+        check(self.lib.mg_plan_grid(self.plan, 0 if bits is None else 1, mg_lib.ctypes.byref(b)),
+              "mg_plan_grid")
+        return int(b.value)
+
     def resident(self, on=None, first_level=None):
         """(on, first level): whether the V-cycle runs its levels from the first
         brick level down as one thread-block-cluster launch (the autotuner's
