@@ -87,3 +87,28 @@ def test_unbound_plan_is_refused():
         assert lib.mg_plan_bind(p, ctypes.c_void_p(1234)) == mg_lib.MG_E_BADARG  # misaligned
     finally:
         lib.mg_plan_destroy(p)
+
+
+def test_launch_shape_choices_need_a_prepared_plan():
+    """mg_plan_split / mg_plan_grid / mg_plan_steps read 0 (no streamed levels)
+    and refuse to force a choice before prepare, and refuse null pointers."""
+    lib = mg_lib.load()
+    rc, p = _create(_desc())
+    assert rc == 0
+    try:
+        bits = ctypes.c_uint32(0)
+        streamed = ctypes.c_int32(-1)
+        assert lib.mg_plan_split(p, 0, ctypes.byref(bits), ctypes.byref(streamed)) == 0
+        assert (bits.value, streamed.value) == (0, 0)
+        for fn in (lib.mg_plan_grid, lib.mg_plan_steps):
+            bits.value = 0
+            assert fn(p, 0, ctypes.byref(bits)) == 0 and bits.value == 0
+            bits.value = 1
+            assert fn(p, 1, ctypes.byref(bits)) == mg_lib.MG_E_BADARG
+            assert "no fused V-cycle" in mg_lib.last_error()
+            assert fn(p, 0, None) == mg_lib.MG_E_BADARG
+            assert fn(None, 0, ctypes.byref(bits)) == mg_lib.MG_E_BADARG
+        bits.value = 1
+        assert lib.mg_plan_split(p, 1, ctypes.byref(bits), None) == mg_lib.MG_E_BADARG
+    finally:
+        lib.mg_plan_destroy(p)
