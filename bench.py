@@ -49,13 +49,13 @@ def _substep128():
 # ghost-fluid pressure solve, "psi" the magnetic potential solve (chi = 1 in the fluid)
 WORKLOADS = {
     "substep128": dict(desc="3D ferrofluid substep 128^3, 5 levels: (a) ghost-fluid pressure solve + "
-                            "(b) magnetic potential solve", cases=_substep128),
+                            "(b) magnetic potential solve", cases=_substep128, solves=2),
     "pressure128": dict(desc="3D ghost-fluid pressure solve 128^3, 5 levels",
-                        cases=lambda: [("pressure", mg_scenes.ferro_drop_3d(n=128, seed=1, levels=5))]),
+                        cases=lambda: [("pressure", mg_scenes.ferro_drop_3d(n=128, seed=1, levels=5))], solves=1),
     "precision256": dict(desc="3D drop/pool 256^3 with smooth source, 6 levels",
-                         cases=lambda: [("pressure", mg_scenes.precision_3d(n=256, seed=2, levels=6))]),
+                         cases=lambda: [("pressure", mg_scenes.precision_3d(n=256, seed=2, levels=6))], solves=1),
     "dam2d": dict(desc="2D dam break 128^2, 4 levels",
-                  cases=lambda: [("pressure", mg_scenes.dam_break_2d())]),
+                  cases=lambda: [("pressure", mg_scenes.dam_break_2d())], solves=1),
 }
 
 PSI_H = (0.0, 1.0, 0.0)
@@ -79,6 +79,14 @@ NCU_DRAM_BYTES = {
     ("substep128", "Ap_alpha"): 11.67e6, ("pressure128", "Ap_alpha"): 11.67e6,
     ("precision256", "pre_l0"): 195.96e6, ("precision256", "Ap_alpha"): 114.93e6,
 }
+
+
+def workload_config(args, world):
+    """The workload both arms run (the same dict in the GPU and reference lines)."""
+    wl = WORKLOADS[args.workload]
+    return {"workload": args.workload, "desc": wl["desc"], "storage": args.storage,
+            "solves_per_step": wl["solves"],
+            "max_iters": MAX_ITERS, "rel_resid": 1e-6, "parallelism": f"replicas x{world}"}
 
 
 def parse():
@@ -451,13 +459,7 @@ def gpu_arm(args, rank, world, local):
             gbs = sb[k] * cells / (ms * 1e-3) / 1e9
             kernels[k].update({"bytes_per_cell": sb[k], "GB_s": round(gbs, 1)})
     dom = max((k for k in kernels if k in sb), key=lambda k: kernels[k]["ms"])
-    peaks = {}
-    try:
-        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
-            peaks = json.load(f)
-    except Exception:
-        pass
-    peak = float(peaks.get("hbm_gbs", 6650.0))
+    peak, peak_source = _hbm_peak()
     lat = sorted(solve_ms)
     res = {
         "metric": "Poisson solves/s at 1e-6 relative residual (p50/p99 ms per solve)",
@@ -468,9 +470,8 @@ def gpu_arm(args, rank, world, local):
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
         "dtype": "f32" if args.storage == "f32" else f"{args.storage}-storage/f32-arith/f64-dots",
         "data": "synthetic (seeded mg_scenes)",
-        "config": {"workload": args.workload, "desc": wl["desc"], "storage": args.storage,
-                   "solves_per_step": len(cases), "max_iters": MAX_ITERS, "rel_resid": 1e-6,
-                   "l2": "flushed before every timed solve", "parallelism": f"replicas x{world}",
+        "config": workload_config(args, world),
+        "timing": {"l2": "flushed before every timed solve",
                    "launch": "direct host loop (profiling)" if DIRECT_LAUNCH else "CUDA graph, device-side while"},
         "p50_ms": round(lat[len(lat) // 2], 4), "p99_ms": round(lat[min(len(lat) - 1, int(0.99 * len(lat)))], 4),
         "pcg_iters": {k: {"min": min(v), "max": max(v)} for k, v in per_case_iters.items()},
@@ -491,8 +492,7 @@ def gpu_arm(args, rank, world, local):
         "gpu_launches": launches * world,
         "roofline": {"bound": "hbm", "kernel": dom,
                      "achieved": kernels[dom]["GB_s"], "peak": peak, "unit": "GB/s",
-                     "frac": round(kernels[dom]["GB_s"] / peak, 4), "peak_source": "MEASURED_PEAKS.json hbm_gbs"
-                     if "hbm_gbs" in peaks else "fallback 6650 GB/s",
+                     "frac": round(kernels[dom]["GB_s"] / peak, 4), "peak_source": peak_source,
                      "traffic": NCU_DRAM_BYTES.get((args.workload, dom)) if args.storage == "f32" else None,
                      "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum per launch, profiles/"},
         "kernels": kernels,
@@ -503,13 +503,20 @@ def gpu_arm(args, rank, world, local):
 
 # ---------------------------------------------------------------- batched / served forms
 def variants(dev, reps=3):
-    """The 96-instance uneven batch and the served session stream, each against
-    the plain FP32 one-at-a-time form on the same GPU (device-resident inputs;
-    the batch is timed with CUDA events, serving by wall clock per request)."""
+    """The 96-instance uneven batch, the served session stream at swept
+    arrival rates, and the 256^3 precision scene in f32 / f16 / bf16 storage,
+    each against the plain FP32 one-at-a-time form on the same GPU
+    (device-resident inputs; the batch and the precision solves are timed
+    with CUDA events, serving by wall clock per request)."""
+    out = {"batched": batched_variant(dev, reps), "served": served_variant(dev)}
+    out["precision256"], xs = precision_variant(dev)
+    return out, xs
+
+
+def batched_variant(dev, reps=3):
     import torch
     import mg_batch
     import mg_serve
-    out = {}
     params = mg_scenes.batch_scene_params(seed=3)
     scenes = [mg_scenes.instance_scene(d, s, ss, levels=mg_serve.levels_for(d, s)) for d, s, ss in params]
     bt = {"instances": len(scenes), "cells": int(sum(s.cells for s in scenes))}
@@ -530,27 +537,135 @@ def variants(dev, reps=3):
         torch.cuda.empty_cache()
     base = bt["plain_f32_one_at_a_time"]["solves_per_s"]
     bt["speedup_vs_plain"] = {k: round(bt[k]["solves_per_s"] / base, 2) for k in ("batched_f32", "batched_f16")}
-    out["batched"] = bt
-    specs = mg_scenes.serving_sessions(seed=4, n_sessions=32, substeps=20, rate_hz=400)
-    sv = {"sessions": len(specs), "substeps": 20, "arrival_rate_hz": 400, "hbm_budget_gb": 120}
-    # request payloads exist before serving; both forms start with their
-    # solvers resident (no allocation or graph build while timed)
-    scenes = mg_serve.SolveServer(device=dev).scenes_for(specs)
-    for storage in ("f32", "f16"):
-        srv = mg_serve.SolveServer(storage=storage, streams=32, device=dev)
-        srv.warm(specs)
-        recs, wall = srv.run(specs, scenes=scenes)
-        sv[f"served_{storage}"] = mg_serve.summarize(recs, wall)
-        del srv
+    return bt
+
+
+SERVE_RATES_HZ = (100, 400, 1600, 6400)
+
+
+def served_variant(dev, n_sessions=32, substeps=20):
+    """Open-loop Poisson arrivals of scene sessions drawn from the batch's size
+    and domain distribution, at each rate of SERVE_RATES_HZ: served (warm
+    starts, continuous batching on 32 streams) in f32 and f16 against the same
+    stream solved one request at a time in plain f32 from a cold start; then
+    the highest rate again with an HBM budget of a quarter of the sessions'
+    total workspace, so that admission queues."""
+    import torch
+    import mg_serve
+    sweep = {}
+    for rate in SERVE_RATES_HZ:
+        specs = mg_scenes.serving_sessions(seed=4, n_sessions=n_sessions, substeps=substeps, rate_hz=rate)
+        scenes = mg_serve.SolveServer(device=dev).scenes_for(specs)
+        row = {}
+        for storage in ("f32", "f16"):
+            srv = mg_serve.SolveServer(storage=storage, streams=32, device=dev)
+            srv.warm(specs)
+            recs, wall = srv.run(specs, scenes=scenes)
+            row[f"served_{storage}"] = dict(mg_serve.summarize(recs, wall), start="warm (previous substep)")
+            del srv
+            torch.cuda.empty_cache()
+        srv = mg_serve.SolveServer(storage="f32", streams=1, device=dev)
+        srv.run_one_at_a_time(specs, scenes=scenes)  # creates and warms one solver per shape
+        recs, wall = srv.run_one_at_a_time(specs, scenes=scenes)
+        row["plain_f32_one_at_a_time"] = dict(mg_serve.summarize(recs, wall), start="cold (x = 0, mgpcg.py:70)")
+        base = row["plain_f32_one_at_a_time"]["solves_per_s"]
+        row["speedup_vs_plain"] = {k: round(row[k]["solves_per_s"] / base, 2) for k in ("served_f32", "served_f16")}
+        sweep[str(rate)] = row
+        del srv, scenes
         torch.cuda.empty_cache()
-    srv = mg_serve.SolveServer(storage="f32", streams=1, device=dev)
-    srv.run_one_at_a_time(specs, scenes=scenes)  # creates and warms one solver per shape
-    recs, wall = srv.run_one_at_a_time(specs, scenes=scenes)
-    sv["plain_f32_one_at_a_time"] = mg_serve.summarize(recs, wall)
-    base = sv["plain_f32_one_at_a_time"]["solves_per_s"]
-    sv["speedup_vs_plain"] = {k: round(sv[k]["solves_per_s"] / base, 2) for k in ("served_f32", "served_f16")}
-    out["served"] = sv
-    return out
+    # the highest rate with a budget that binds
+    rate = SERVE_RATES_HZ[-1]
+    specs = mg_scenes.serving_sessions(seed=4, n_sessions=n_sessions, substeps=substeps, rate_hz=rate)
+    sizes = [mg_serve.plan_bytes(s["dim"], (s["side"],) * s["dim"], mg_serve.levels_for(s["dim"], s["side"]), "f16")
+             for s in specs]
+    need = sum(sizes)
+    budget = max(0.25 * need, 1.05 * max(sizes))  # binds, yet every session fits alone
+    scenes = mg_serve.SolveServer(device=dev).scenes_for(specs)
+    srv = mg_serve.SolveServer(storage="f16", streams=32, device=dev, hbm_budget=budget)
+    srv.warm(specs)
+    recs, wall = srv.run(specs, scenes=scenes)
+    bound = dict(mg_serve.summarize(recs, wall), rate_hz=rate, budget_bytes=int(budget), demand_bytes=int(need),
+                 peak_in_use_bytes=int(srv.peak_in_use), peak_resident_bytes=int(srv.peak_resident),
+                 admission_waits=srv.admission_waits, evictions=srv.evictions)
+    del srv, scenes
+    torch.cuda.empty_cache()
+    return {"sessions": n_sessions, "substeps": substeps, "hbm_budget_gb": 120, "rates_hz": list(SERVE_RATES_HZ),
+            "by_rate": sweep, "budget_bound_f16": bound}
+
+
+def true_rel_resid(solver):
+    """||b - A x|| / ||b|| over FLUID cells in float64 on the host, from the
+    solver's own float32 A, b and x (a check of the reported residual, not a
+    solve)."""
+    x = solver.x.double().cpu().numpy()
+    b = solver.b.double().cpu().numpy()
+    ad = solver.Adiag[0].double().cpu().numpy()
+    ax = np.moveaxis(solver.Ax[0].double().cpu().numpy(), -1, 0)
+    fl = solver.grid_type[0].cpu().numpy() == 0
+    Axv = ad * x
+    for k in range(solver.dim):
+        lo = [slice(None)] * solver.dim
+        hi = [slice(None)] * solver.dim
+        lo[k] = slice(0, -1)
+        hi[k] = slice(1, None)
+        lo, hi = tuple(lo), tuple(hi)
+        Axv[hi] += ax[k][lo] * x[lo]
+        Axv[lo] += ax[k][lo] * x[hi]
+    r = np.where(fl, b - Axv, 0.0)
+    return float(np.linalg.norm(r) / np.linalg.norm(np.where(fl, b, 0.0)))
+
+
+def precision_variant(dev, reps=3):
+    """The 256^3 precision scene (6 levels, smooth extra source) in float32
+    and in FP16 / BF16 V-cycle storage: solves/s (inputs larger than L2),
+    iterations, the true relative residual and the level-0 sweeps' roofline.
+    Returns the row and each storage's solution (for the error against the
+    FP64 oracle, computed in the CPU leg)."""
+    import torch
+    sc = mg_scenes.precision_3d(n=256, seed=2, levels=6)
+    row = {"scene": sc.name, "cells": sc.cells, "levels": sc.levels}
+    xs = {}
+    peak = _hbm_peak()[0]
+    stream = torch.cuda.current_stream(dev)
+    for storage in ("f32", "f16", "bf16"):
+        c = GpuCase(sc, storage, dev)
+        c.run()
+        torch.cuda.synchronize()
+        ms = []
+        for _ in range(reps):
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            c.run()
+            e1.record(stream)
+            torch.cuda.synchronize()
+            ms.append(e0.elapsed_time(e1))
+        st = c.solver.stats()
+        stage_ms = time_stages(c, storage)
+        sb = stage_bytes(c.solver, storage)
+        kern = {}
+        for k in ("pre_l0", "post_l0", "Ap_alpha", "xr"):
+            if k in stage_ms and k in sb:
+                gbs = sb[k] * sc.cells / (stage_ms[k] * 1e-3) / 1e9
+                kern[k] = {"ms": round(stage_ms[k], 5), "bytes_per_cell": sb[k], "GB_s": round(gbs, 1),
+                           "frac_of_measured_hbm": round(gbs / peak, 4)}
+        row[storage] = {"solves_per_s": round(1e3 / min(ms), 3), "ms_per_solve": round(min(ms), 3),
+                        "iters": st.iters, "status": c.solver.last_status,
+                        "true_rel_resid": true_rel_resid(c.solver), "kernels": kern}
+        xs[storage] = c.solver.x.cpu().numpy()
+        del c
+        torch.cuda.empty_cache()
+    row["speedup_vs_f32"] = {k: round(row[k]["solves_per_s"] / row["f32"]["solves_per_s"], 3) for k in ("f16", "bf16")}
+    return row, (sc, xs)
+
+
+def _hbm_peak():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            peaks = json.load(f)
+        return float(peaks["hbm_gbs"]), "MEASURED_PEAKS.json hbm_gbs"
+    except Exception:
+        return 6650.0, "fallback 6650 GB/s"
 
 
 # ---------------------------------------------------------------- CPU (oracle)
@@ -585,26 +700,52 @@ def cpu_solve_rate(cases, seconds, threads=None):
     return n / dt, n, dt, omod.max_threads(), iters
 
 
+def fp64_errors(scene, xs):
+    """Relative L2 error of each solution against the FP64 oracle solve
+    converged to a 1e-12 relative residual (the CPU leg's check of the
+    precision variant)."""
+    from oracle import OracleSolver
+    t0 = time.perf_counter()
+    o = OracleSolver(scene.dim, scene.res, scene.levels, 2, 50, real=np.float64)
+    o.reinitialize_pressure(scene.cell_type, scene.velocity, scene.phi, scene.p0, scene.scale_A, scene.scale_b, True,
+                            scene.gfm_clamp)
+    b = o.get("b")
+    fl = o.get("grid_type") == 0
+    b[fl] = b[fl] + scene.extra_rhs[fl].astype(np.float64)
+    o.set("b", b)
+    it = o.solve(1000, rel_tol=1e-24)
+    x64 = o.get("x")
+    d = np.linalg.norm(x64)
+    out = {k: float(np.linalg.norm(x.astype(np.float64) - x64) / d) for k, x in xs.items()}
+    out["fp64_iters"] = it
+    out["fp64_solve_s"] = round(time.perf_counter() - t0, 2)
+    return out
+
+
 def reference_arm(args, rank, world):
     if rank != 0:
         return None
     wl = WORKLOADS[args.workload]
     cases = wl["cases"]()
-    per_step = []
+    per_step = []   # seconds per step (all of the workload's solves)
+    per_solve = []
+    n_solves = 0
     for i in range(args.warmup + args.steps):
         rate, n, dt, cores, iters = cpu_solve_rate(cases, 0.0)
         if i >= args.warmup:
-            per_step.append(dt / n)
+            per_step.append(dt)
+            per_solve += [dt / n] * n
+            n_solves += n
     tot = sum(per_step)
-    v = len(per_step) / tot
-    lat = sorted(x * 1e3 for x in per_step)
+    v = n_solves / tot
+    lat = sorted(x * 1e3 for x in per_solve)
     return {
         "impl": "reference",
         "metric": "Poisson solves/s at 1e-6 relative residual (p50/p99 ms per solve)",
         "value": round(v, 4), "unit": "solves/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": round(tot / args.steps * 1e3, 3), "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded mg_scenes)",
-        "config": {"workload": args.workload, "desc": wl["desc"], "storage": "f32"},
+        "config": workload_config(args, world),
         "p50_ms": round(lat[len(lat) // 2], 3), "p99_ms": round(lat[-1], 3),
         "cpu_baseline": {"value": round(v, 4), "unit": "solves/s", "cores": cores, "kind": "port",
                          "sample": f"{args.steps} timed solves of the workload by the C++/OpenMP oracle "
@@ -634,7 +775,9 @@ def main():
                                              f"(float32, {cores} threads); CPU iterations {min(iters)}-{max(iters)}"}
         if world == 1 and not args.no_variants:
             import torch
-            res["variants"] = variants(torch.device("cuda", local))
+            res["variants"], (sc256, xs256) = variants(torch.device("cuda", local))
+            if with_cpu:
+                res["variants"]["precision256"]["error_vs_fp64"] = fp64_errors(sc256, xs256)
         print(json.dumps(res))
     if world > 1:
         import torch.distributed as dist

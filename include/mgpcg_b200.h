@@ -45,6 +45,7 @@ extern "C" {
 #define MG_SOLVE_MAX_ITERS 1   /* stopped at max_iters (the reference is silent) */
 #define MG_SOLVE_NONFINITE 2   /* a reduction produced NaN/Inf (H3: zero Adiag) */
 #define MG_SOLVE_BAD_OPERATOR 3 /* mg_plan_prepare_declared's declaration was wrong */
+#define MG_SOLVE_TIMEOUT 4      /* a bounded wait on a TMA copy ran out (the sweep left its chunk) */
 
 /* V-cycle grid storage type */
 #define MG_STORE_F32 0
@@ -422,6 +423,20 @@ MG_API int mg_plan_steps(mg_plan_t* plan, int32_t set, uint32_t* bits);
  * plan (for profilers; with MGPCG_STEP1 unset, one plane per step is off). */
 MG_API int mg_plan_grid(mg_plan_t* plan, int32_t set, uint32_t* bits);
 
+/* Kernel of each streamed level's sweeps (no reference counterpart: a B200
+ * implementation choice for the same arithmetic, mgpcg.py:104-123): bits
+ * 2l..2l+1 = 0 for the shared-memory ring kernel, 1..3 for the
+ * column-register kernel (TMA-staged planes, z in registers) with a tile of
+ * 32x16, 32x32 or 64x16 columns.  The column kernel runs 3D label-uniform
+ * plans with pre_post 2 whose fastest extent is a multiple of 16 bytes.
+ * Every prepared shape times both kernels, every tile and grid per level when
+ * first prepared (cached per shape).  All choices give bit-identical
+ * V-cycles.  set != 0 forces *bits (after the plan is prepared; valid until
+ * the next prepare; MG_E_BADARG where a level cannot run the column kernel);
+ * *bits returns the choice.  MGPCG_COL=<bits> replaces the timing for every
+ * plan (for profilers). */
+MG_API int mg_plan_sweep_kernel(mg_plan_t* plan, int32_t set, uint32_t* bits);
+
 /* The cluster-resident V-cycle (no reference counterpart: a B200 launch shape
  * of mgpcg.py:125-148 with the same float32 values): for a label-uniform
  * float32 3D plan whose levels [first_level, L) halve exactly, those levels run
@@ -488,8 +503,10 @@ MG_API int mg_launch_stage(mg_plan_t* plan, int32_t stage, int32_t level, void* 
  * cudaMalloc/cudaFree would synchronise the device, or code without a solver
  * plan.  It allocates nothing: its scratch (64 KB of FP64 partial sums and a
  * counter) is a static array inside the library, held by every GPU that loads
- * it.  The first call on a device looks that array up (cudaGetSymbolAddress)
- * and should come before any stream capture.  n must be at most 33,554,432
+ * it.  Each call looks that array up (cudaGetSymbolAddress) except while its
+ * stream is being captured, when the address kept from an earlier call on the
+ * device is used: the first call on a device must come before any stream
+ * capture (else MG_E_CUDA).  n must be at most 33,554,432
  * (else MG_E_TOO_BIG).  Calls share the array: calls that overlap on the GPU
  * race; order them on one stream. */
 MG_API int mg_reduce_static(const int8_t* grid_type, const float* a, const float* b, int64_t n, double* out,

@@ -1,0 +1,397 @@
+// Column-register streamed sweeps of the fused V-cycle (label-uniform 3D
+// operator): the same smoothing, restriction and prolongation as k_sweep
+// (mg_sweep.cuh), with the same float32 operations in the same order, laid
+// out for the B200 instead of around a shared-memory ring of every array.
+//
+// A block owns a (TY x TX) tile of columns plus a halo (NS rows, HX >= NS
+// columns rounded up for 16-byte TMA coordinates) and a chunk [z0, z1) of
+// planes along axis 0, streamed plane by plane (temporal blocking: half sweep
+// m acts on the plane `shift(m)` behind the newest, so it sees its
+// neighbours after half sweep m-1, as in mgpcg.py:125-148).
+//
+// * Thread -> a y-pair of columns (x, rows 2i and 2i+1).  The pair's two cells
+//   have opposite colours in every plane, so each half sweep updates exactly
+//   one of them: all lanes work.  A plane's active cell is the one whose
+//   x + y has the parity of the plane step, the same for every half sweep of
+//   a step, so it is fixed per unrolled step (A at even steps, B at odd).
+// * Each thread keeps its two columns' z, r and Adiag for the planes in
+//   flight in REGISTERS (NS + 2 planes), so the neighbours along axis 0 and
+//   the pair's own other cell never touch shared memory; only the three
+//   in-plane neighbours (x - 1, x + 1, the row outside the pair) are read from
+//   a shared z plane that each thread publishes its updates into.
+// * The half sweeps of one step touch disjoint planes and read in-plane
+//   neighbours published in the previous step, so a step needs ONE block
+//   barrier, not one per half sweep.
+// * r, Adiag (and POST's input z) arrive by TMA (cp.async.bulk.tensor, 3D
+//   tile loads of the region plane, no multicast) into a ring of NS + 2
+//   shared slots, NS + 1 planes ahead of the one being smoothed, completed on
+//   one mbarrier per slot.  Out-of-grid boxes are zero-filled, which makes
+//   those cells non-FLUID (Adiag 0) with z 0: rule H1 with no bounds checks.
+//   Every wait is bounded; a wait that runs out sets Control::wait_timeout
+//   and the block leaves the chunk (the solve then reports MG_SOLVE_TIMEOUT).
+// * The restriction's 2 x 2 x 2 children sum in the reference oracle's order:
+//   the x-partner's two residuals come by warp shuffle (the partner is the
+//   adjacent lane), the two planes from consecutive steps.
+#pragma once
+#include <cuda.h>
+
+#include "mg_fused.cuh"
+
+namespace mg {
+
+// ---- shared-memory barrier and TMA primitives (PTX) ----------------------------------
+__device__ __forceinline__ uint32_t smem_addr(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
+
+__device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_addr(bar)), "r"(count) : "memory");
+}
+__device__ __forceinline__ void mbar_fence_init() {
+  asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+}
+__device__ __forceinline__ void mbar_expect_tx(uint64_t* bar, uint32_t bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_addr(bar)), "r"(bytes)
+               : "memory");
+}
+__device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity) {
+  uint32_t ok;
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+      "selp.u32 %0, 1, 0, p;\n\t}"
+      : "=r"(ok)
+      : "r"(smem_addr(bar)), "r"(parity)
+      : "memory");
+  return ok != 0;
+}
+// A wait that gives up after about a second (kWaitCycles SM clocks).
+constexpr long long kWaitCycles = 2000000000LL;
+__device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, uint32_t parity) {
+  if (mbar_try_wait(bar, parity)) return true;
+  const long long t0 = clock64();
+  while (!mbar_try_wait(bar, parity))
+    if (clock64() - t0 > kWaitCycles) return false;
+  return true;
+}
+__device__ __forceinline__ void tma_load_3d(void* dst, const CUtensorMap* map, uint64_t* bar, int x, int y,
+                                            int z) {
+  asm volatile(
+      "cp.async.bulk.tensor.3d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4}], "
+      "[%5];" ::"r"(smem_addr(dst)),
+      "l"(reinterpret_cast<uint64_t>(map)), "r"(x), "r"(y), "r"(z), "r"(smem_addr(bar))
+      : "memory");
+}
+
+// ---- shape of one instantiation -------------------------------------------------------
+template <typename ST, int NS, int TX, int TY>
+struct ColGeom {
+  // x halo: NS rounded up so that the region's first column is a multiple of
+  // 16 bytes for every array (4 float32 / 8 16-bit cells)
+  static constexpr int HX = (sizeof(ST) == 4 && NS <= 4) ? 4 : 8;
+  static constexpr int RX = TX + 2 * HX;     // region columns
+  static constexpr int RY = TY + 2 * NS;     // region rows (even)
+  static constexpr int PLC = RX * RY;        // cells of a region plane
+  static constexpr int PAIRS = RX * (RY / 2);
+  static constexpr int NT = (PAIRS + 31) / 32 * 32;
+  static constexpr int W = NS + 2;           // planes in registers = TMA ring slots = shared z planes
+  static constexpr int SLOT_R = (PLC * 4 + 127) / 128 * 128;               // r (float32 or ST)
+  static constexpr int SLOT_S = (PLC * (int)sizeof(ST) + 127) / 128 * 128;  // Adiag, input z (ST)
+  static constexpr int ZPL = (PLC + 31) / 32 * 32;                         // floats of a shared z plane
+  static constexpr int slot_bytes(bool pre) { return SLOT_R + SLOT_S * (pre ? 1 : 2); }
+  static constexpr size_t smem(bool pre) {
+    return 128 /* alignment */ + 128 /* mbarriers */ + (size_t)W * slot_bytes(pre) + (size_t)W * ZPL * 4;
+  }
+  static_assert(TX % 8 == 0 && TY % 2 == 0 && NS % 2 == 0, "even pairs, 16-byte TMA rows");
+  static_assert(RX <= 256 && RY <= 256, "TMA box extents");
+  static_assert(W <= 16, "mbarriers in 128 bytes");
+};
+
+// ---------------------------------------------------------------------------
+// k_colsweep: PRE (z = 0, 2 pre_post half sweeps in colour order 0,1,..., then
+// the restriction r[l+1] = rho * sum of the children's r - A z and z[l+1] = 0)
+// or POST (z += pi * z[l+1][I/2], then half sweeps in colour order 1,0,...),
+// with the level-0 POST also summing z.r for the PCG loop (A.zr >= 0).
+// ---------------------------------------------------------------------------
+template <typename ST, int NS, int TX, int TY, bool PRE, int MINB>
+__global__ void __launch_bounds__(ColGeom<ST, NS, TX, TY>::NT, MINB)
+    k_colsweep(SweepArgs<ST> A, Control* flag, const __grid_constant__ CUtensorMap tm_r,
+               const __grid_constant__ CUtensorMap tm_ad, const __grid_constant__ CUtensorMap tm_zin) {
+  using G = ColGeom<ST, NS, TX, TY>;
+  constexpr int HX = G::HX, RX = G::RX, RY = G::RY, W = G::W, NT = G::NT, ZPL = G::ZPL;
+  constexpr int SLOT = G::slot_bytes(PRE);
+  constexpr int D = PRE ? NS - 1 : NS;  // steps from a plane's load to its final z
+  pdl_enter();
+
+  extern __shared__ unsigned char smem_raw[];
+  unsigned char* smem = (unsigned char*)(((uintptr_t)smem_raw + 127) & ~(uintptr_t)127);
+  uint64_t* bar = (uint64_t*)smem;
+  unsigned char* slots = smem + 128;
+  float* zs = (float*)(slots + W * SLOT);
+  __shared__ int abort_flag;
+
+  const FLevel<ST>& F = A.f;
+  const int n0 = F.n[0], n1 = F.n[1], n2 = F.n[2];
+  const int ntile = A.tiles_x * A.tiles_y;
+  const int tile = blockIdx.x % ntile;
+  const int chunk_id = blockIdx.x / ntile;
+  const int tx0 = (tile % A.tiles_x) * TX;
+  const int ty0 = (tile / A.tiles_x) * TY;
+  const int z0 = chunk_id * A.chunk;
+  const int z1 = min(z0 + A.chunk, n0);
+  const int p_first = z0 - NS;
+  const int p_last = z1 + NS - 1;
+  const int ox = tx0 - HX, oy = ty0 - NS;  // region origin (both even)
+  const float sigma = A.r_f32 ? (float)A.ctl->scale_r : 1.0f;
+  const float ms = -F.s;
+  const long long pstride = (long long)n1 * n2;
+  const int ncx = A.nc[2], ncy = A.nc[1];
+  const bool r32 = sizeof(ST) == 4 || A.r_f32;
+  const uint32_t tx_bytes =
+      (uint32_t)(G::PLC * ((r32 ? 4 : (int)sizeof(ST)) + (int)sizeof(ST) * (PRE ? 1 : 2)));
+
+  // ---- this thread's pair of columns ----------------------------------------------------
+  const int t = threadIdx.x;
+  const bool live = t < G::PAIRS;
+  const int tt = live ? t : 0;
+  const int rx = tt % RX, pr2 = tt / RX;
+  const int gx = ox + rx, gy0 = oy + 2 * pr2;
+  const int odd = rx & 1;                               // gx parity (ox even)
+  const int rowA = 2 * pr2 + odd, rowB = 2 * pr2 + 1 - odd;  // A: x + y even
+  const int yo = 2 * pr2 - 1, yu = 2 * pr2 + 2;          // the rows beyond the pair
+  const int outA = min(max(odd ? yu : yo, 0), RY - 1);   // (clamped: such reads feed
+  const int outB = min(max(odd ? yo : yu, 0), RY - 1);   //  only cells never smoothed)
+  const int cA = rowA * RX + rx, cB = rowB * RX + rx;
+  const int oA = outA * RX + rx, oB = outB * RX + rx;
+  const int xm = rx > 0 ? -1 : 0, xp = rx < RX - 1 ? 1 : 0;
+  const int dx = max(max(HX - rx, rx - (HX + TX - 1)), 0);
+  const int ringA = live ? max(dx, max(max(NS - rowA, rowA - (NS + TY - 1)), 0)) : 1 << 20;
+  const int ringB = live ? max(dx, max(max(NS - rowB, rowB - (NS + TY - 1)), 0)) : 1 << 20;
+  // n1 even and gy0 even: the pair's rows are both inside the grid or both outside
+  const bool in_grid = live && gx >= 0 && gx < n2 && gy0 >= 0 && gy0 < n1;
+  const bool ownA = in_grid && ringA == 0, ownB = in_grid && ringB == 0;
+  const long long giA = (long long)(oy + rowA) * n2 + gx, giB = (long long)(oy + rowB) * n2 + gx;
+
+  float zA[W], zB[W], rA[W], rB[W], aA[W], aB[W];
+#pragma unroll
+  for (int j = 0; j < W; ++j) {
+    zA[j] = 0.0f; zB[j] = 0.0f; rA[j] = 0.0f; rB[j] = 0.0f; aA[j] = 0.0f; aB[j] = 0.0f;
+  }
+  float acc = 0.0f;      // restriction accumulator (PRE, even-x threads)
+  double zr_acc = 0.0;   // z.r of the cells written (POST, A.zr >= 0)
+
+  auto issue = [&](int p, int slot) {  // TMA loads of plane p into a ring slot (thread 0)
+    unsigned char* sl = slots + slot * SLOT;
+    mbar_expect_tx(&bar[slot], tx_bytes);
+    tma_load_3d(sl, &tm_r, &bar[slot], ox, oy, p);
+    tma_load_3d(sl + G::SLOT_R, &tm_ad, &bar[slot], ox, oy, p);
+    if (!PRE) tma_load_3d(sl + G::SLOT_R + G::SLOT_S, &tm_zin, &bar[slot], ox, oy, p);
+  };
+
+  if (t == 0) {
+#pragma unroll
+    for (int j = 0; j < W; ++j) mbar_init(&bar[j], 1);
+    mbar_fence_init();
+    abort_flag = 0;
+  }
+  __syncthreads();
+  if (t == 0)
+    for (int k = 0; k < W - 1; ++k)
+      if (p_first + k <= p_last) issue(p_first + k, k);
+
+  bool aborted = false;
+  int stop_p = p_last;  // the first plane not known to be delivered (abort)
+  for (int P0 = p_first; P0 <= p_last && !aborted; P0 += W) {
+    const uint32_t parity = (uint32_t)(((P0 - p_first) / W) & 1);
+#pragma unroll
+    for (int u = 0; u < W; ++u) {
+      const int P = P0 + u;
+      if (P > p_last) break;
+      const int q = P - p_first;
+      // plane P + W - 1 into the slot of plane P - 1 (read before the last barrier)
+      if (t == 0 && P + W - 1 <= p_last) issue(P + W - 1, (u + W - 1) % W);
+      if (!mbar_wait_bounded(&bar[u], parity)) abort_flag = 1;
+
+      // ---- plane P: r, Adiag (and the prolongated z) into the registers --------------
+      {
+        const unsigned char* sl = slots + u * SLOT;
+        if (r32) {
+          const float* sr = (const float*)sl;
+          rA[u] = sizeof(ST) == 4 ? sr[cA] : __fmul_rn(sigma, sr[cA]);
+          rB[u] = sizeof(ST) == 4 ? sr[cB] : __fmul_rn(sigma, sr[cB]);
+        } else {
+          const ST* sr = (const ST*)sl;
+          rA[u] = to_f<ST>(sr[cA]);
+          rB[u] = to_f<ST>(sr[cB]);
+        }
+        const ST* sa = (const ST*)(sl + G::SLOT_R);
+        aA[u] = to_f<ST>(sa[cA]);
+        aB[u] = to_f<ST>(sa[cB]);
+        if constexpr (PRE) {
+          // the first half sweep is pointwise (z = 0 before it): z = r / Adiag on
+          // the colour-0 cell, the one active in this step
+          if ((u & 1) == 0) {
+            zA[u] = aA[u] != 0.0f ? __fdiv_rn(rA[u], aA[u]) : 0.0f;
+            zB[u] = 0.0f;
+          } else {
+            zB[u] = aB[u] != 0.0f ? __fdiv_rn(rB[u], aB[u]) : 0.0f;
+            zA[u] = 0.0f;
+          }
+        } else {
+          const ST* si = (const ST*)(sl + G::SLOT_R + G::SLOT_S);
+          float c = 0.0f;
+          if (in_grid && P >= 0 && P < n0)
+            c = to_f<ST>(A.zc[((long long)(P >> 1) * ncy + (gy0 >> 1)) * ncx + (gx >> 1)]);
+          const float fa = __fadd_rn(to_f<ST>(si[cA]), __fmul_rn(A.pi, c));
+          const float fb = __fadd_rn(to_f<ST>(si[cB]), __fmul_rn(A.pi, c));
+          zA[u] = aA[u] != 0.0f ? fa : 0.0f;
+          zB[u] = aB[u] != 0.0f ? fb : 0.0f;
+          // an owned non-FLUID cell is never smoothed: its output is this value
+          if (P >= z0 && P < z1) {
+            if (ownA && aA[u] == 0.0f) F.z[(long long)P * pstride + giA] = from_f<ST>(fa);
+            if (ownB && aB[u] == 0.0f) F.z[(long long)P * pstride + giB] = from_f<ST>(fb);
+          }
+        }
+        if (live) {
+          zs[u * ZPL + cA] = zA[u];
+          zs[u * ZPL + cB] = zB[u];
+        }
+      }
+
+      // ---- half sweeps: m on the plane shift(m) behind P ------------------------------
+#pragma unroll
+      for (int m = PRE ? 2 : 1; m <= NS; ++m) {
+        const int s = PRE ? m - 1 : m;      // planes behind P
+        const int j = (u - s + 2 * W) % W, jm = (j + W - 1) % W, jp = (j + 1) % W;
+        if (q < s + 1) continue;            // the plane below was not loaded
+        float* zp = zs + j * ZPL;
+        // cells at ring distance <= NS - s from the tile are needed after this sweep
+        if ((u & 1) == 0) {
+          const float a = aA[j];
+          if (ringA <= NS - s && a != 0.0f) {
+            float ret = 0.0f;
+            ret = __fadd_rn(ret, __fadd_rn(__fmul_rn(ms, zA[jm]), __fmul_rn(ms, zA[jp])));
+            ret = __fadd_rn(ret, __fadd_rn(__fmul_rn(ms, zp[oA]), __fmul_rn(ms, zB[j])));
+            ret = __fadd_rn(ret, __fadd_rn(__fmul_rn(ms, zp[cA + xm]), __fmul_rn(ms, zp[cA + xp])));
+            const float v = __fdiv_rn(__fsub_rn(rA[j], ret), a);
+            zA[j] = v;
+            zp[cA] = v;
+          }
+        } else {
+          const float a = aB[j];
+          if (ringB <= NS - s && a != 0.0f) {
+            float ret = 0.0f;
+            ret = __fadd_rn(ret, __fadd_rn(__fmul_rn(ms, zB[jm]), __fmul_rn(ms, zB[jp])));
+            ret = __fadd_rn(ret, __fadd_rn(__fmul_rn(ms, zp[oB]), __fmul_rn(ms, zA[j])));
+            ret = __fadd_rn(ret, __fadd_rn(__fmul_rn(ms, zp[cB + xm]), __fmul_rn(ms, zp[cB + xp])));
+            const float v = __fdiv_rn(__fsub_rn(rB[j], ret), a);
+            zB[j] = v;
+            zp[cB] = v;
+          }
+        }
+      }
+
+      // ---- the finished plane P - D ------------------------------------------------------
+      {
+        const int pw = P - D;
+        if (pw >= z0 && pw < z1) {
+          const int jw = (u - D + 2 * W) % W;
+          const long long base = (long long)pw * pstride;
+          if constexpr (PRE) {  // non-FLUID cells hold z = 0
+            if (ownA) F.z[base + giA] = from_f<ST>(zA[jw]);
+            if (ownB) F.z[base + giB] = from_f<ST>(zB[jw]);
+          } else {
+            if (ownA && aA[jw] != 0.0f) {
+              F.z[base + giA] = from_f<ST>(zA[jw]);
+              if (A.zr >= 0) zr_acc += (double)zA[jw] * (double)rA[jw];
+            }
+            if (ownB && aB[jw] != 0.0f) {
+              F.z[base + giB] = from_f<ST>(zB[jw]);
+              if (A.zr >= 0) zr_acc += (double)zB[jw] * (double)rB[jw];
+            }
+          }
+        }
+      }
+
+      // ---- PRE: residual of plane P - NS and restriction ------------------------------
+      if constexpr (PRE) {
+        const int pr = P - NS;
+        if (pr >= z0 && pr < z1) {
+          const int jr = (u - NS + 2 * W) % W, jrm = (jr + W - 1) % W, jrp = (jr + 1) % W;
+          const float* zp = zs + jr * ZPL;
+          float vA = 0.0f, vB = 0.0f;
+          const bool fA = ownA && aA[jr] != 0.0f, fB = ownB && aB[jr] != 0.0f;
+          if (fA) {
+            float ret = 0.0f;
+            ret = __fadd_rn(ret, __fadd_rn(__fmul_rn(ms, zA[jrm]), __fmul_rn(ms, zA[jrp])));
+            ret = __fadd_rn(ret, __fadd_rn(__fmul_rn(ms, zp[oA]), __fmul_rn(ms, zB[jr])));
+            ret = __fadd_rn(ret, __fadd_rn(__fmul_rn(ms, zp[cA + xm]), __fmul_rn(ms, zp[cA + xp])));
+            vA = __fsub_rn(rA[jr], __fadd_rn(__fmul_rn(aA[jr], zA[jr]), ret));
+          }
+          if (fB) {
+            float ret = 0.0f;
+            ret = __fadd_rn(ret, __fadd_rn(__fmul_rn(ms, zB[jrm]), __fmul_rn(ms, zB[jrp])));
+            ret = __fadd_rn(ret, __fadd_rn(__fmul_rn(ms, zp[oB]), __fmul_rn(ms, zA[jr])));
+            ret = __fadd_rn(ret, __fadd_rn(__fmul_rn(ms, zp[cB + xm]), __fmul_rn(ms, zp[cB + xp])));
+            vB = __fsub_rn(rB[jr], __fadd_rn(__fmul_rn(aB[jr], zB[jr]), ret));
+          }
+          // rows y0 (even) and y1 of this column; the x + 1 column is the next lane
+          const float v0 = odd ? vB : vA, v1 = odd ? vA : vB;
+          const int f = odd ? ((int)fB | ((int)fA << 1)) : ((int)fA | ((int)fB << 1));
+          const float p0 = __shfl_xor_sync(0xffffffffu, v0, 1);
+          const float p1 = __shfl_xor_sync(0xffffffffu, v1, 1);
+          const int pf = __shfl_xor_sync(0xffffffffu, f, 1);
+          if (!odd) {
+            // children in the order (y0, x0), (y0, x1), (y1, x0), (y1, x1), plane by plane
+            if ((pr & 1) == 0) acc = 0.0f;
+            if (f & 1) acc = __fadd_rn(acc, v0);
+            if (pf & 1) acc = __fadd_rn(acc, p0);
+            if (f & 2) acc = __fadd_rn(acc, v1);
+            if (pf & 2) acc = __fadd_rn(acc, p1);
+            if ((pr & 1) == 1 && ownA) {
+              const long long gc = ((long long)(pr >> 1) * ncy + (gy0 >> 1)) * ncx + (gx >> 1);
+              A.rc[gc] = from_f<ST>(__fmul_rn(A.rho, acc));
+              A.zc[gc] = from_f<ST>(0.0f);
+            }
+          }
+        }
+      }
+      __syncthreads();
+      if (abort_flag) {
+        aborted = true;
+        stop_p = P;
+        break;
+      }
+    }
+  }
+
+  if (aborted && t == 0) {
+    // a TMA load did not complete within the bound: flag it, then wait
+    // (bounded) for this block's loads still in flight before leaving
+    atomicOr(&flag->wait_timeout, 1);
+    const int last_issued = min(stop_p + W - 1, p_last);
+    for (int p = stop_p; p <= last_issued; ++p) {
+      const int k = p - p_first;
+      mbar_wait_bounded(&bar[k % W], (uint32_t)((k / W) & 1));
+    }
+  }
+  if constexpr (!PRE) {
+    if (A.zr >= 0) {  // the reduction and epilogue of k_zr4 (mgpcg.py:161-166, 197-202)
+      __shared__ double sh[32];
+      double tot;
+      Control* ctl = A.zr_ctl;
+      if (last_block_total<NT>(zr_acc, A.zr_partials, &ctl->counter[1], sh, &tot) && threadIdx.x == 0) {
+        if (A.zr == 0) {
+          ctl->old_zTr = tot;
+          if (ctl->max_iters == 0) ctl->run = 0;
+        } else {
+          ctl->new_zTr = tot;
+          ctl->beta = (float)(tot / (ctl->old_zTr + ctl->eps));
+          ctl->old_zTr = tot;
+          ctl->iter += 1;
+          if (ctl->max_iters != -1 && ctl->iter >= ctl->max_iters) ctl->run = 0;
+        }
+      }
+    }
+  }
+}
+
+}  // namespace mg

@@ -64,7 +64,7 @@ struct Control {
   double kappa;               // coefficient scale of 16-bit grids
   double n_fluid;             // FLUID cells of level 0
   int bad_operator;           // set when a declared label-uniform form is wrong
-  int pad1;
+  int wait_timeout;           // set when a bounded wait in a kernel ran out
   unsigned int counter[8];    // arrival counters of the last-block reductions
   double scratch[8];          // single-value results of mg_reduce
   double det[4 * 12];         // operator detection per level (k_detect_uniform)

@@ -2,9 +2,11 @@
 // streamed levels and the block-resident coarse levels, and the launches.
 #pragma once
 #include <cmath>
+#include <cstring>
 #include <type_traits>
 
 #include "mg_sweep.cuh"
+#include "mg_colsweep.cuh"
 #include "mg_coarse.cuh"
 #include "mg_resident.cuh"
 
@@ -60,6 +62,15 @@ inline size_t sweep_smem(int dim, int ns, TileShape t, bool one_step = false, bo
   return (size_t)W * RX * RY * (12 + (sto ? 4 * dim : 0));
 }
 
+// Tile shapes of the column-register sweep (k_colsweep) a streamed level may
+// run instead of k_sweep: (TX, TY) columns and the blocks per SM its launch
+// bounds aim at.  Index 0 is k_sweep.
+struct ColShape {
+  int tx, ty, minb;
+};
+constexpr ColShape kColShapes[] = {{0, 0, 0}, {32, 16, 2}, {32, 32, 1}, {64, 16, 1}};
+constexpr int kColShapeCount = 4;
+
 struct FusedPlan {
   bool valid = false;
   bool sto = false;                // whole-domain stored form (else label-uniform)
@@ -76,6 +87,10 @@ struct FusedPlan {
   // by measurement: 1 extra is faster for the 256^3 level-0 sweeps, slower at
   // 128^3)
   unsigned char grid_extra[kMaxLevels] = {};
+  // per streamed level: 0 = k_sweep, k = k_colsweep with kColShapes[k]
+  // (chosen by measurement; possible where col_ok holds)
+  unsigned char col[kMaxLevels] = {};
+  int col_per_sm[kColShapeCount] = {};  // resident blocks of each shape (occupancy)
   int per_sm = 1, num_sms = 148;
   int lc = 0;                      // first level of the block-resident coarse solve
   int dim = 3, ns = 4, storage = 0;
@@ -107,10 +122,13 @@ struct FusedPlan {
 inline void level_grid(FusedPlan* F, const Geom& g, int l, int extra) {
   const int nx = F->dim == 3 ? g.n[2] : g.n[1];
   const int ny = F->dim == 3 ? g.n[1] : 1;
-  F->tiles_x[l] = (nx + F->tile.tx - 1) / F->tile.tx;
-  F->tiles_y[l] = F->dim == 3 ? (ny + F->tile.ty - 1) / F->tile.ty : 1;
+  const int c = F->col[l];
+  const int tx = c ? kColShapes[c].tx : F->tile.tx, ty = c ? kColShapes[c].ty : F->tile.ty;
+  const int per_sm = c ? (F->col_per_sm[c] > 0 ? F->col_per_sm[c] : 1) : F->per_sm;
+  F->tiles_x[l] = (nx + tx - 1) / tx;
+  F->tiles_y[l] = F->dim == 3 ? (ny + ty - 1) / ty : 1;
   const long long tiles = (long long)F->tiles_x[l] * F->tiles_y[l];
-  const long long target = (long long)(F->per_sm + extra) * F->num_sms;
+  const long long target = (long long)(per_sm + extra) * F->num_sms;
   long long chunk = (long long)g.n[0] * tiles / target;
   if (chunk < 2) chunk = 2;
   chunk &= ~1LL;
@@ -135,6 +153,7 @@ inline bool make_fused_plan(const Level* lv, int L, int dim, int pre_post, int b
     F->split[l] = false;
     F->step1[l] = 0;
     F->grid_extra[l] = 0;
+    F->col[l] = 0;
   }
   bool uniform = true, all_whole = true;
   for (int l = 0; l < L; ++l) {
@@ -454,8 +473,130 @@ inline cudaError_t launch_sweep_st(const FusedPlan& F, const Level* lv, int l, c
   return cudaErrorInvalidValue;
 }
 
+// ---- the column-register sweep (mg_colsweep.cuh) -------------------------------------
+
+// cuTensorMapEncodeTiled from the driver, looked up once through the runtime
+// (the library links no driver stub).
+typedef CUresult (*EncodeTiledFn)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*, const cuuint64_t*,
+                                  const cuuint64_t*, const cuuint32_t*, const cuuint32_t*, CUtensorMapInterleave,
+                                  CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+inline EncodeTiledFn encode_tiled() {
+  static EncodeTiledFn fn = [] {
+    void* p = nullptr;
+    cudaDriverEntryPointQueryResult q = cudaDriverEntryPointSymbolNotFound;
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) != cudaSuccess ||
+        q != cudaDriverEntryPointSuccess) {
+      cudaGetLastError();
+      return (EncodeTiledFn) nullptr;
+    }
+    return (EncodeTiledFn)p;
+  }();
+  return fn;
+}
+
+// A 3D tiled tensor map over one array of a level (axis 0 slowest), box =
+// (bx columns, by rows, 1 plane), zero fill outside the grid.
+inline bool tensor_map_3d(CUtensorMap* m, const void* base, int es, const Geom& g, int bx, int by) {
+  EncodeTiledFn fn = encode_tiled();
+  if (!fn || ((uintptr_t)base & 15) || ((long long)g.n[2] * es) % 16) return false;
+  const cuuint64_t dims[3] = {(cuuint64_t)g.n[2], (cuuint64_t)g.n[1], (cuuint64_t)g.n[0]};
+  const cuuint64_t strides[2] = {(cuuint64_t)g.n[2] * es, (cuuint64_t)g.n[1] * g.n[2] * es};
+  const cuuint32_t box[3] = {(cuuint32_t)bx, (cuuint32_t)by, 1};
+  const cuuint32_t est[3] = {1, 1, 1};
+  return fn(m, es == 4 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT32 : CU_TENSOR_MAP_DATA_TYPE_UINT16, 3, const_cast<void*>(base),
+            dims, strides, box, est, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+            CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+}
+
+// The column kernel runs streamed level l of a 3D label-uniform plan with
+// pre_post 2 whose rows are whole 16-byte units of every array and whose
+// extents halve evenly (pairs of rows, pairs of planes).
+inline bool col_ok(const FusedPlan& F, const Level* lv, int l) {
+  if (!F.valid || F.sto || F.dim != 3 || F.ns != 4 || l >= F.lc || F.split[l]) return false;
+  const Geom& g = lv[l].g;
+  const int es = F.storage == MG_STORE_F32 ? 4 : 2;
+  return g.n[2] % (16 / es) == 0 && g.n[1] % 2 == 0 && g.n[0] % 2 == 0 && encode_tiled() != nullptr;
+}
+
+template <typename ST, int NS, int TX, int TY, bool PRE, int MINB>
+inline cudaError_t launch_col_t(const FusedPlan& F, const Level* lv, int l, const Control* ctl, cudaStream_t s) {
+  using G = ColGeom<ST, NS, TX, TY>;
+  const Level& f = lv[l];
+  CUtensorMap tr, ta, tz;
+  std::memset(&tz, 0, sizeof(tz));
+  if (!tensor_map_3d(&tr, f.r, l == 0 ? 4 : (int)sizeof(ST), f.g, G::RX, G::RY) ||
+      !tensor_map_3d(&ta, f.Adiag_s, (int)sizeof(ST), f.g, G::RX, G::RY) ||
+      (!PRE && !tensor_map_3d(&tz, f.zt, (int)sizeof(ST), f.g, G::RX, G::RY)))
+    return cudaErrorInvalidValue;
+  if (PRE) tz = ta;  // unused by PRE
+  auto kern = k_colsweep<ST, NS, TX, TY, PRE, MINB>;
+  const size_t smem = G::smem(PRE);
+  cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (e != cudaSuccess) return e;
+  return launch_k(kern, F.blocks[l], G::NT, smem, s, sweep_args<ST, PRE>(F, lv, l, ctl), const_cast<Control*>(ctl),
+                  tr, ta, tz);
+}
+
+template <typename ST, bool PRE>
+inline cudaError_t launch_col_st(const FusedPlan& F, const Level* lv, int l, const Control* ctl, cudaStream_t s) {
+  switch (F.col[l]) {
+    case 1: return launch_col_t<ST, 4, 32, 16, PRE, 2>(F, lv, l, ctl, s);
+    case 2: return launch_col_t<ST, 4, 32, 32, PRE, 1>(F, lv, l, ctl, s);
+    case 3: return launch_col_t<ST, 4, 64, 16, PRE, 1>(F, lv, l, ctl, s);
+  }
+  return cudaErrorInvalidValue;
+}
+
+template <bool PRE>
+inline cudaError_t launch_col(const FusedPlan& F, const Level* lv, int l, const Control* ctl, cudaStream_t s) {
+  switch (F.storage) {
+    case MG_STORE_F32: return launch_col_st<float, PRE>(F, lv, l, ctl, s);
+    case MG_STORE_F16: return launch_col_st<__half, PRE>(F, lv, l, ctl, s);
+    case MG_STORE_BF16: return launch_col_st<__nv_bfloat16, PRE>(F, lv, l, ctl, s);
+  }
+  return cudaErrorInvalidValue;
+}
+
+// Resident blocks per SM of column shape c (the smaller of PRE and POST).
+template <typename ST, int TX, int TY, int MINB>
+inline int col_occupancy_t(int num_sms) {
+  using G = ColGeom<ST, 4, TX, TY>;
+  int a = 0, b = 0;
+  auto kp = k_colsweep<ST, 4, TX, TY, true, MINB>;
+  auto kq = k_colsweep<ST, 4, TX, TY, false, MINB>;
+  if (cudaFuncSetAttribute(kp, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)G::smem(true)) != cudaSuccess ||
+      cudaFuncSetAttribute(kq, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)G::smem(false)) != cudaSuccess ||
+      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&a, kp, G::NT, G::smem(true)) != cudaSuccess ||
+      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, kq, G::NT, G::smem(false)) != cudaSuccess) {
+    cudaGetLastError();
+    return 0;
+  }
+  (void)num_sms;
+  return a < b ? a : b;
+}
+
+template <typename ST>
+inline int col_occupancy_st(int c, int num_sms) {
+  switch (c) {
+    case 1: return col_occupancy_t<ST, 32, 16, 2>(num_sms);
+    case 2: return col_occupancy_t<ST, 32, 32, 1>(num_sms);
+    case 3: return col_occupancy_t<ST, 64, 16, 1>(num_sms);
+  }
+  return 0;
+}
+
+inline int col_occupancy(const FusedPlan& F, int c) {
+  switch (F.storage) {
+    case MG_STORE_F32: return col_occupancy_st<float>(c, F.num_sms);
+    case MG_STORE_F16: return col_occupancy_st<__half>(c, F.num_sms);
+    case MG_STORE_BF16: return col_occupancy_st<__nv_bfloat16>(c, F.num_sms);
+  }
+  return 0;
+}
+
 template <bool PRE>
 inline cudaError_t launch_sweep(const FusedPlan& F, const Level* lv, int l, const Control* ctl, cudaStream_t s) {
+  if (F.col[l]) return launch_col<PRE>(F, lv, l, ctl, s);
   if (F.sto) {
     switch (F.ns) {
       case 2: return launch_sweep_t<3, float, 2, PRE, true>(F, lv, l, ctl, s);

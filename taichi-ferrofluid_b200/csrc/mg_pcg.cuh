@@ -52,7 +52,7 @@ __device__ void set_scales(Control* ctl, double rTr);
 // Epilogue: rTr0, tol = max(abs_tol, rTr0 * rel_tol) (mgpcg.py:157-164).
 __global__ void __launch_bounds__(kRedThreads) k_pcg_begin(Level L, const float* __restrict__ b,
                                                            float* __restrict__ x, Control* ctl,
-                                                           double* partials) {
+                                                           double* partials, double* __restrict__ xh) {
   pdl_enter();
   __shared__ double sh[32];
   float* r = (float*)L.r;
@@ -75,6 +75,8 @@ __global__ void __launch_bounds__(kRedThreads) k_pcg_begin(Level L, const float*
     }
     r[i] = ri;
     if (L.type[i] == FLUID) acc += (double)ri * (double)ri;
+    // mixed form: the FP64 copy of x that the loop accumulates into
+    if (xh) xh[i] = warm && L.type[i] == FLUID ? (double)x[i] : 0.0;
   }
   double tot, totb;
   // b.b first (its own counter), then r.r; both blocks orders are fixed
@@ -95,6 +97,7 @@ __global__ void __launch_bounds__(kRedThreads) k_pcg_begin(Level L, const float*
       ctl->status = MG_SOLVE_BAD_OPERATOR;
       ctl->run = 0;
     }
+    ctl->wait_timeout = 0;
     set_scales(ctl, tot);
   }
 }
@@ -480,7 +483,7 @@ __global__ void __launch_bounds__(kRedThreads) k_xr(Level L, float* __restrict__
                                                     const float* __restrict__ p,
                                                     const float* __restrict__ Ap, Control* ctl,
                                                     double* partials, cudaGraphConditionalHandle cond,
-                                                    int has_cond, int force = 0) {
+                                                    int has_cond, int force = 0, double* __restrict__ xh = nullptr) {
   pdl_enter();
   __shared__ double sh[32];
   if (!ctl->run && !force) {
@@ -493,7 +496,13 @@ __global__ void __launch_bounds__(kRedThreads) k_xr(Level L, float* __restrict__
   for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < L.g.count;
        i += (long long)gridDim.x * blockDim.x) {
     if (L.type[i] != FLUID) continue;
-    x[i] = __fadd_rn(x[i], __fmul_rn(alpha, p[i]));
+    if (xh) {  // mixed form: x accumulates in FP64, x (float32) is its rounding
+      const double v = xh[i] + (double)alpha * (double)p[i];
+      xh[i] = v;
+      x[i] = (float)v;
+    } else {
+      x[i] = __fadd_rn(x[i], __fmul_rn(alpha, p[i]));
+    }
     float ri = __fsub_rn(r[i], __fmul_rn(alpha, Ap[i]));
     r[i] = ri;
     acc += (double)ri * (double)ri;
@@ -506,6 +515,10 @@ __global__ void __launch_bounds__(kRedThreads) k_xr(Level L, float* __restrict__
       ctl->run = 0;
     } else if (tot < ctl->tol) {
       ctl->status = MG_SOLVE_CONVERGED;
+      ctl->run = 0;
+    }
+    if (ctl->wait_timeout) {  // a sweep gave up waiting for its TMA loads
+      ctl->status = MG_SOLVE_TIMEOUT;
       ctl->run = 0;
     }
     ctl->since_refresh += 1;
@@ -521,7 +534,7 @@ __global__ void __launch_bounds__(kRedThreads) k_xr4(Level L, float* __restrict_
                                                      const float* __restrict__ p,
                                                      const float* __restrict__ Ap, Control* ctl,
                                                      double* partials, cudaGraphConditionalHandle cond,
-                                                     int has_cond, int force = 0) {
+                                                     int has_cond, int force = 0, double* __restrict__ xh = nullptr) {
   pdl_enter();
   __shared__ double sh[32];
   if (!ctl->run && !force) {
@@ -542,10 +555,23 @@ __global__ void __launch_bounds__(kRedThreads) k_xr4(Level L, float* __restrict_
     float* xs = reinterpret_cast<float*>(&xv);
     float* rs = reinterpret_cast<float*>(&rv);
     const float ps[4] = {pv.x, pv.y, pv.z, pv.w}, as[4] = {av.x, av.y, av.z, av.w};
+    if (xh) {  // mixed form: x accumulates in FP64, x (float32) is its rounding
+      double2* xh2 = reinterpret_cast<double2*>(xh) + 2 * q;
+      double2 h0 = xh2[0], h1 = xh2[1];
+      double hv[4] = {h0.x, h0.y, h1.x, h1.y};
+#pragma unroll
+      for (int e = 0; e < 4; ++e) {
+        if (!fluid_lane(t4, e)) continue;
+        hv[e] += (double)alpha * (double)ps[e];
+        xs[e] = (float)hv[e];
+      }
+      xh2[0] = make_double2(hv[0], hv[1]);
+      xh2[1] = make_double2(hv[2], hv[3]);
+    }
 #pragma unroll
     for (int e = 0; e < 4; ++e) {
       if (!fluid_lane(t4, e)) continue;
-      xs[e] = __fadd_rn(xs[e], __fmul_rn(alpha, ps[e]));
+      if (!xh) xs[e] = __fadd_rn(xs[e], __fmul_rn(alpha, ps[e]));
       rs[e] = __fsub_rn(rs[e], __fmul_rn(alpha, as[e]));
       acc += (double)rs[e] * (double)rs[e];
     }
@@ -562,6 +588,10 @@ __global__ void __launch_bounds__(kRedThreads) k_xr4(Level L, float* __restrict_
       ctl->status = MG_SOLVE_CONVERGED;
       ctl->run = 0;
     }
+    if (ctl->wait_timeout) {  // a sweep gave up waiting for its TMA loads
+      ctl->status = MG_SOLVE_TIMEOUT;
+      ctl->run = 0;
+    }
     ctl->since_refresh += 1;
     set_scales(ctl, tot);
     if (has_cond) cudaGraphSetConditional(cond, ctl->run ? 1u : 0u);
@@ -576,7 +606,7 @@ __global__ void __launch_bounds__(kRedThreads) k_xr4(Level L, float* __restrict_
 __global__ void __launch_bounds__(kRedThreads) k_refresh(Level L, const float* __restrict__ b,
                                                          const float* __restrict__ x, Control* ctl,
                                                          double* partials, cudaGraphConditionalHandle cond,
-                                                         int has_cond) {
+                                                         int has_cond, const double* __restrict__ xh) {
   pdl_enter();
   __shared__ double sh[32];
   const bool claimed = ctl->status == MG_SOLVE_CONVERGED && !ctl->run;
@@ -592,11 +622,13 @@ __global__ void __launch_bounds__(kRedThreads) k_refresh(Level L, const float* _
     if (L.type[i] != FLUID) continue;
     int c[3];
     L.g.coords(i, c);
-    double ax = (double)L.Adiag[i] * (double)x[i];
+    // x in FP64 (the mixed form's accumulated copy) or the float32 x
+    auto xv = [&](long long j) { return xh ? xh[j] : (double)x[j]; };
+    double ax = (double)L.Adiag[i] * xv(i);
     for (int k = 0; k < L.g.dim; ++k) {
       const long long s = L.g.stride(k);
-      if (c[k] > 0) ax += (double)L.Ax[k][i - s] * (double)x[i - s];
-      if (c[k] + 1 < L.g.n[k]) ax += (double)L.Ax[k][i] * (double)x[i + s];
+      if (c[k] > 0) ax += (double)L.Ax[k][i - s] * xv(i - s);
+      if (c[k] + 1 < L.g.n[k]) ax += (double)L.Ax[k][i] * xv(i + s);
     }
     const double rr = (double)b[i] - ax;
     r[i] = (float)rr;
@@ -616,6 +648,10 @@ __global__ void __launch_bounds__(kRedThreads) k_refresh(Level L, const float* _
       // the recursive residual was too optimistic: keep iterating
       ctl->status = MG_SOLVE_MAX_ITERS;
       ctl->run = ctl->max_iters == -1 || ctl->iter + 1 < ctl->max_iters;
+    }
+    if (ctl->wait_timeout) {
+      ctl->status = MG_SOLVE_TIMEOUT;
+      ctl->run = 0;
     }
     set_scales(ctl, tot);
     if (has_cond) cudaGraphSetConditional(cond, ctl->run ? 1u : 0u);

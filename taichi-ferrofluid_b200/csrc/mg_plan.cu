@@ -54,7 +54,8 @@ int bad(const char* what) {
 constexpr int kFields = 9;
 constexpr int kFieldAdiagS = 9;  // internal: storage copy of Adiag
 constexpr int kFieldZT = 10;     // internal: second z buffer of the fused V-cycle
-constexpr int kFieldCount = 11;
+constexpr int kFieldXH = 11;     // internal: FP64 x of the mixed form (refresh plans)
+constexpr int kFieldCount = 12;
 
 struct Loc {
   int64_t off = -1, bytes = 0;
@@ -131,6 +132,7 @@ void layout(mg_plan* P) {
   put(MG_FIELD_X, 0, 0, n0 * 4);
   put(MG_FIELD_P, 0, 0, n0 * 4);
   put(MG_FIELD_AP, 0, 0, n0 * 4);
+  if (P->d.refresh_every > 0) put(kFieldXH, 0, 0, n0 * 8);
   P->off_partials = off;
   off = align256(off + sizeof(double) * kMaxPartials);
   P->off_ctl = off;
@@ -159,6 +161,10 @@ void bind_views(mg_plan* P) {
 inline cudaStream_t S(void* s) { return (cudaStream_t)s; }
 
 float* fptr(mg_plan* P, int f) { return (float*)(P->base + P->loc[f][0][0].off); }
+// The mixed form's FP64 x (refresh plans), else null.
+double* xhptr(mg_plan* P) {
+  return P->d.refresh_every > 0 ? (double*)(P->base + P->loc[kFieldXH][0][0].off) : nullptr;
+}
 
 int grid_for(const mg_plan* P, int64_t n, int threads = 256) {
   int64_t b = (n + threads - 1) / threads;
@@ -386,14 +392,35 @@ int tune_split(mg_plan* P, cudaStream_t s) {
 // level measured).  Each pipelined level is timed every way (one warm-up,
 // kTuneReps timed) the first time a shape is prepared; the choice is cached
 // per shape.  All choices compute the same values.
-std::map<std::array<int, 7>, std::pair<uint32_t, uint32_t>> g_tune_stream;  // (step bits, grid bits)
+//
+// Each streamed level also runs, where col_ok allows, the column-register
+// kernel (k_colsweep) in each tile shape of kColShapes with its grid sized
+// for its resident blocks plus 0 or 1 more; the fastest of every variant is
+// kept (MGPCG_COL=<bits>, 2 bits a level, pins the kernel).
+struct StreamChoice {
+  uint32_t step, grid, col;
+};
+std::map<std::array<int, 7>, StreamChoice> g_tune_stream;
 
-void apply_stream_bits(mg_plan* P, uint32_t step, uint32_t grid) {
+// Forces column shape c (0: k_sweep) on streamed level l; false where the
+// level cannot run it.
+bool set_col(mg_plan* P, int l, int c) {
+  FusedPlan& F = P->fp;
+  if (c < 0 || c >= kColShapeCount) return false;
+  if (c && !col_ok(F, P->lv, l)) return false;
+  if (c && F.col_per_sm[c] == 0) F.col_per_sm[c] = col_occupancy(F, c);
+  if (c && F.col_per_sm[c] <= 0) return false;
+  F.col[l] = (unsigned char)c;
+  return true;
+}
+
+void apply_stream_bits(mg_plan* P, uint32_t step, uint32_t grid, uint32_t col) {
   FusedPlan& F = P->fp;
   const bool steps_ok = !F.sto && F.dim == 3 && F.storage == MG_STORE_F32;
   for (int l = 0; l < F.lc; ++l) {
+    if (!set_col(P, l, (int)((col >> (2 * l)) & 3u))) F.col[l] = 0;
     level_grid(&F, P->lv[l].g, l, (int)((grid >> (2 * l)) & 3u));
-    F.step1[l] = steps_ok ? (unsigned char)((step >> (2 * l)) & 3u) : 0;
+    F.step1[l] = steps_ok && !F.col[l] ? (unsigned char)((step >> (2 * l)) & 3u) : 0;
   }
 }
 
@@ -419,9 +446,11 @@ int tune_stream(mg_plan* P, cudaStream_t s) {
   // serialise the trial launches and would skew the choice)
   const char* ov_step = std::getenv("MGPCG_STEP1");
   const char* ov_grid = std::getenv("MGPCG_GRID");
-  if (ov_step || ov_grid) {
+  const char* ov_col = std::getenv("MGPCG_COL");
+  if (ov_step || ov_grid || ov_col) {
     apply_stream_bits(P, ov_step ? (uint32_t)std::strtoul(ov_step, nullptr, 0) : 0u,
-                      ov_grid ? (uint32_t)std::strtoul(ov_grid, nullptr, 0) : 0u);
+                      ov_grid ? (uint32_t)std::strtoul(ov_grid, nullptr, 0) : 0u,
+                      ov_col ? (uint32_t)std::strtoul(ov_col, nullptr, 0) : 0u);
     return MG_OK;
   }
   const Geom& g = P->geom[0];
@@ -430,7 +459,7 @@ int tune_stream(mg_plan* P, cudaStream_t s) {
     std::lock_guard<std::mutex> lk(g_tune_mu);
     auto it = g_tune_stream.find(key);
     if (it != g_tune_stream.end()) {
-      apply_stream_bits(P, it->second.first, it->second.second);
+      apply_stream_bits(P, it->second.step, it->second.grid, it->second.col);
       return MG_OK;
     }
   }
@@ -441,14 +470,17 @@ int tune_stream(mg_plan* P, cudaStream_t s) {
     cudaEventDestroy(e0);
     return set_err("cudaEventCreate", ce);
   }
-  uint32_t step = 0, grid = 0;
+  uint32_t step = 0, grid = 0, col = 0;
   int rc = MG_OK;
   for (int l = 0; l < F.lc && rc == MG_OK; ++l) {
     F.step1[l] = 0;
-    if (F.split[l] || F.chunk[l] <= 2) continue;  // per-kernel passes / one-step launch
+    F.col[l] = 0;
+    if (F.split[l]) continue;  // per-kernel passes
+    level_grid(&F, P->lv[l].g, l, 0);
+    const bool one_step = F.chunk[l] <= 2;  // k_sweep's one-step launch
     float best = 0.0f;
-    int best_extra = 0, last_chunk = -1;
-    for (int extra = 0; extra <= 2 && rc == MG_OK; ++extra) {
+    int best_extra = 0, best_col = 0, last_chunk = -1;
+    for (int extra = 0; extra <= (one_step ? 0 : 2) && rc == MG_OK; ++extra) {
       level_grid(&F, P->lv[l].g, l, extra);
       if (F.chunk[l] == last_chunk) continue;  // the same grid
       last_chunk = F.chunk[l];
@@ -459,9 +491,27 @@ int tune_stream(mg_plan* P, cudaStream_t s) {
         best_extra = extra;
       }
     }
+    for (int c = 1; c < kColShapeCount && rc == MG_OK; ++c) {
+      if (!set_col(P, l, c)) continue;
+      last_chunk = -1;
+      for (int extra = 0; extra <= 1 && rc == MG_OK; ++extra) {
+        level_grid(&F, P->lv[l].g, l, extra);
+        if (F.chunk[l] == last_chunk) continue;
+        last_chunk = F.chunk[l];
+        float t = 0.0f;
+        rc = time_level(P, l, 3, e0, e1, s, &t);
+        if (rc == MG_OK && t < best) {
+          best = t;
+          best_extra = extra;
+          best_col = c;
+        }
+      }
+    }
+    F.col[l] = (unsigned char)(rc == MG_OK ? best_col : 0);
     level_grid(&F, P->lv[l].g, l, rc == MG_OK ? best_extra : 0);
     grid |= (uint32_t)F.grid_extra[l] << (2 * l);
-    if (!steps_ok || F.chunk[l] <= 2) continue;
+    col |= (uint32_t)F.col[l] << (2 * l);
+    if (!steps_ok || F.chunk[l] <= 2 || F.col[l]) continue;
     for (int dir = 0; dir < 2 && rc == MG_OK; ++dir) {
       float t[2] = {0.0f, 0.0f};
       for (int mode = 0; mode < 2 && rc == MG_OK; ++mode) {
@@ -476,11 +526,11 @@ int tune_stream(mg_plan* P, cudaStream_t s) {
   cudaEventDestroy(e0);
   cudaEventDestroy(e1);
   if (rc != MG_OK) {
-    apply_stream_bits(P, 0u, 0u);
+    apply_stream_bits(P, 0u, 0u, 0u);
     return rc;
   }
   std::lock_guard<std::mutex> lk(g_tune_mu);
-  g_tune_stream[key] = {step, grid};
+  g_tune_stream[key] = {step, grid, col};
   return MG_OK;
 }
 
@@ -665,15 +715,17 @@ int launch_cg_tail(mg_plan* P, cudaStream_t s, int which) {
   if (which & 2) {
     const float* pc = p;
     const float* Apc = Ap;
+    double* xh = xhptr(P);
     if (P->geom[0].count % 4 == 0)  // 4-cell groups
       CK(launch_k(k_xr4, RB, kRedThreads, 0, s, L0, x, pc, Apc, P->ctl, P->partials, P->cond,
-                  refresh ? 0 : P->has_cond, 0));
+                  refresh ? 0 : P->has_cond, 0, xh));
     else
       CK(launch_k(k_xr, RB, kRedThreads, 0, s, L0, x, pc, Apc, P->ctl, P->partials, P->cond,
-                  refresh ? 0 : P->has_cond, 0));
+                  refresh ? 0 : P->has_cond, 0, xh));
     if (refresh) {
       const float* bc = b;
-      CK(launch_k(k_refresh, RB, kRedThreads, 0, s, L0, bc, x, P->ctl, P->partials, P->cond, P->has_cond));
+      const double* xhc = xh;
+      CK(launch_k(k_refresh, RB, kRedThreads, 0, s, L0, bc, x, P->ctl, P->partials, P->cond, P->has_cond, xhc));
     }
   }
   return MG_OK;
@@ -687,7 +739,7 @@ int launch_pcg_part(mg_plan* P, bool prologue, cudaStream_t s) {
   float* x = fptr(P, MG_FIELD_X);
   if (prologue) {
     const float* bc = b;
-    CK(launch_k(k_pcg_begin, P->red_blocks, kRedThreads, 0, s, L0, bc, x, P->ctl, P->partials));
+    CK(launch_k(k_pcg_begin, P->red_blocks, kRedThreads, 0, s, L0, bc, x, P->ctl, P->partials, xhptr(P)));
   }
   const bool fuse = zr_fusable(P);
   P->fp.zr_mode = fuse ? (prologue ? 0 : 1) : -1;
@@ -1469,6 +1521,7 @@ static int finish_prepare(mg_plan_t* P, cudaStream_t s, bool declared) {
   mix(P->fp.res_lp);
   for (int l = 0; l < P->L; ++l) mix(P->fp.split[l]);
   for (int l = 0; l < P->L; ++l) mix(P->fp.step1[l]);
+  for (int l = 0; l < P->L; ++l) mix(P->fp.col[l]);
   for (int l = 0; l < P->fp.lc; ++l) mix((uint64_t)P->fp.chunk[l] << 32 | (uint32_t)P->fp.blocks[l]);
   for (int l = 0; l < P->L; ++l) {
     uint32_t bits;
@@ -1519,6 +1572,32 @@ int mg_plan_steps(mg_plan_t* P, int32_t set, uint32_t* bits) {
   }
   uint32_t b = 0;
   for (int l = 0; l < P->fp.lc; ++l) b |= (uint32_t)P->fp.step1[l] << (2 * l);
+  *bits = b;
+  return MG_OK;
+}
+
+int mg_plan_sweep_kernel(mg_plan_t* P, int32_t set, uint32_t* bits) {
+  if (!P || !bits) return bad("null pointer");
+  if (set) {
+    if (!P->fp.valid) return bad("the plan has no fused V-cycle");
+    if (*bits >> (2 * P->fp.lc)) return bad("kernel bits beyond the streamed levels");
+    unsigned char old[kMaxLevels];
+    for (int l = 0; l < P->fp.lc; ++l) old[l] = P->fp.col[l];
+    for (int l = 0; l < P->fp.lc; ++l) {
+      if (!set_col(P, l, (int)((*bits >> (2 * l)) & 3u))) {
+        for (int k = 0; k < P->fp.lc; ++k) P->fp.col[k] = old[k];
+        return bad("the column-register sweep cannot run that level");
+      }
+    }
+    for (int l = 0; l < P->fp.lc; ++l) {
+      if (P->fp.col[l]) P->fp.step1[l] = 0;
+      level_grid(&P->fp, P->lv[l].g, l, P->fp.grid_extra[l]);
+    }
+    destroy_graph(P);
+    P->graph_sig = 0;
+  }
+  uint32_t b = 0;
+  for (int l = 0; l < P->fp.lc; ++l) b |= (uint32_t)P->fp.col[l] << (2 * l);
   *bits = b;
   return MG_OK;
 }
@@ -1703,10 +1782,12 @@ int mg_launch_stage(mg_plan_t* P, int32_t stage, int32_t level, void* stream) {
     case 4:
       if (P->geom[0].count % 4 == 0)
         k_xr4<<<P->red_blocks, kRedThreads, 0, s>>>(L0, fptr(P, MG_FIELD_X), fptr(P, MG_FIELD_P),
-                                                    fptr(P, MG_FIELD_AP), P->ctl, P->partials, P->cond, 0, 1);
+                                                    fptr(P, MG_FIELD_AP), P->ctl, P->partials, P->cond, 0, 1,
+                                                    xhptr(P));
       else
         k_xr<<<P->red_blocks, kRedThreads, 0, s>>>(L0, fptr(P, MG_FIELD_X), fptr(P, MG_FIELD_P),
-                                                   fptr(P, MG_FIELD_AP), P->ctl, P->partials, P->cond, 0, 1);
+                                                   fptr(P, MG_FIELD_AP), P->ctl, P->partials, P->cond, 0, 1,
+                                                   xhptr(P));
       CKL("k_xr");
       return MG_OK;
     case 5:

@@ -13,9 +13,13 @@
 // The array is a file-scope `static __device__` object: every GPU that loads
 // the library holds its 64 KB until the process exits.  Host code cannot use
 // its name as a device address (the host-side symbol is only a stand-in), so
-// the first call on each device looks the address up with
-// cudaGetSymbolAddress, with that device current, and caches it.  That first
-// call should therefore come before any stream capture.
+// each call looks the address up with cudaGetSymbolAddress, with the device
+// current, and keeps it per device; a call made while its stream is being
+// captured uses the kept address instead (the look-up is not a stream
+// operation and may load the module).  The first call on a device should
+// therefore come before any stream capture.  Looking it up again on every
+// other call keeps the address valid after a cudaDeviceReset, which destroys
+// the context that held the array.
 //
 // All calls share the one array and it keeps the last call's contents: the
 // counter is cleared at the start of every call, and calls that overlap on the
@@ -77,18 +81,25 @@ extern "C" MG_API int mg_reduce_static(const int8_t* grid_type, const float* a, 
   int dev = -1;
   cudaError_t e = cudaGetDevice(&dev);
   if (e != cudaSuccess || dev < 0 || dev >= kMaxDevices) return fail(MG_E_CUDA, "mg_reduce_static: cudaGetDevice failed");
+  cudaStream_t s = (cudaStream_t)stream;
+  cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+  if (cudaStreamIsCapturing(s, &cap) != cudaSuccess) {
+    cudaGetLastError();  // a stream that cannot be queried: use the kept address
+    cap = cudaStreamCaptureStatusActive;
+  }
   StaticScratch* S;
   {
     std::lock_guard<std::mutex> lk(g_mu);
-    if (!g_addr[dev]) {
+    if (cap == cudaStreamCaptureStatusNone) {
       void* p = nullptr;
       e = cudaGetSymbolAddress(&p, g_scratch);
       if (e != cudaSuccess || !p) return fail(MG_E_CUDA, "mg_reduce_static: cudaGetSymbolAddress failed");
       g_addr[dev] = (StaticScratch*)p;
+    } else if (!g_addr[dev]) {
+      return fail(MG_E_CUDA, "mg_reduce_static: the first call on a device must come before stream capture");
     }
     S = g_addr[dev];
   }
-  cudaStream_t s = (cudaStream_t)stream;
   e = cudaMemsetAsync(&S->counter, 0, sizeof(unsigned int), s);
   if (e != cudaSuccess) return fail(MG_E_CUDA, "mg_reduce_static: clearing the counter failed");
   long long blocks = (n + (long long)kThreads * kCellsPerThread - 1) / ((long long)kThreads * kCellsPerThread);

@@ -21,7 +21,7 @@ MG_E_UNBOUND = -3
 MG_E_TOO_BIG = -4
 
 SOLVE_CONVERGED, SOLVE_MAX_ITERS, SOLVE_NONFINITE, SOLVE_BAD_OPERATOR = 0, 1, 2, 3
-STATUS_NAMES = {0: "converged", 1: "max_iters", 2: "nonfinite", 3: "bad_operator"}
+STATUS_NAMES = {0: "converged", 1: "max_iters", 2: "nonfinite", 3: "bad_operator", 4: "timeout"}
 
 STORE = {"f32": 0, "fp32": 0, "float32": 0, "f16": 1, "fp16": 1, "float16": 1, "bf16": 2, "bfloat16": 2}
 STORE_BYTES = {0: 4, 1: 2, 2: 2}
@@ -111,6 +111,7 @@ _SIGS = {
     "mg_plan_split": (ctypes.c_int, [_vp, _i32, ctypes.POINTER(ctypes.c_uint32), ctypes.POINTER(_i32)]),
     "mg_plan_steps": (ctypes.c_int, [_vp, _i32, ctypes.POINTER(ctypes.c_uint32)]),
     "mg_plan_grid": (ctypes.c_int, [_vp, _i32, ctypes.POINTER(ctypes.c_uint32)]),
+    "mg_plan_sweep_kernel": (ctypes.c_int, [_vp, _i32, ctypes.POINTER(ctypes.c_uint32)]),
     "mg_plan_resident": (ctypes.c_int, [_vp, _i32, ctypes.POINTER(_i32), ctypes.POINTER(_i32)]),
     "mg_smooth": (ctypes.c_int, [_vp, _i32, _i32, _vp]),
     "mg_restrict": (ctypes.c_int, [_vp, _i32, _vp]),

@@ -135,6 +135,10 @@ class SolveServer:
         self.pool = {}        # (dim, side, levels) -> free solvers (resident workspaces)
         self.in_use = 0.0     # bytes held by admitted sessions
         self.peak_in_use = 0.0
+        self.admission_waits = 0  # sessions that arrived while the budget was full
+        self.idle = 0.0       # bytes of pooled workspaces no session holds
+        self.evictions = 0
+        self.peak_resident = 0.0  # admitted + idle workspace bytes
         self.bytes_of = {}
 
     def warm(self, specs):
@@ -146,7 +150,7 @@ class SolveServer:
         for sp in specs:
             key = (sp["dim"], sp["side"], levels_for(sp["dim"], sp["side"]))
             need[key] = need.get(key, 0) + 1
-        total = 0.0
+        total = self.in_use + self.idle
         for key, n in sorted(need.items(), key=lambda kv: -kv[0][1]):
             dim, side, L = key
             if key not in self.bytes_of:
@@ -159,10 +163,12 @@ class SolveServer:
                 if total + self.bytes_of[key] > self.budget:
                     break
                 total += self.bytes_of[key]
+                self.idle += self.bytes_of[key]
                 solver = MGPCGPoissonSolver(dim, (side,) * dim, L, 2, 50, storage=self.storage, device=self.device)
                 solver.pressure_solve_async(scene.ct, scene.vel, scene.phi, scene.p0, scene.scale_A, scene.scale_b,
                                             True, scene.gfm_clamp, max_iters=self.max_iters, rel_tol=self.rel_tol)
                 self.pool.setdefault(key, []).append(solver)
+        self.peak_resident = max(self.peak_resident, self.in_use + self.idle)
         torch.cuda.synchronize(self.device)
 
     def scenes_for(self, specs):
@@ -176,18 +182,42 @@ class SolveServer:
         if key not in self.bytes_of:
             self.bytes_of[key] = plan_bytes(dim, (side,) * dim, L, self.storage)
         need = self.bytes_of[key]
+        if need > self.budget:
+            raise ValueError(f"a {dim}D {side}-cell session needs {need} bytes, more than the whole "
+                             f"HBM budget of {int(self.budget)}")
         if self.in_use + need > self.budget:
             return None, key
-        self.in_use += need
-        self.peak_in_use = max(self.peak_in_use, self.in_use)
         free = self.pool.get(key)
         if free:
+            self.in_use += need
+            self.idle -= need
+            self.peak_in_use = max(self.peak_in_use, self.in_use)
             return free.pop(), key
+        # a new workspace: idle workspaces of other shapes are freed first when
+        # resident bytes (admitted + idle) would pass the budget
+        self._evict(self.budget - need)
+        self.in_use += need
+        self.peak_in_use = max(self.peak_in_use, self.in_use)
+        self.peak_resident = max(self.peak_resident, self.in_use + self.idle)
         return MGPCGPoissonSolver(dim, (side,) * dim, L, 2, 50, storage=self.storage, device=self.device), key
+
+    def _evict(self, limit):
+        """Frees idle pooled workspaces, largest first, until admitted + idle
+        bytes are at most ``limit``."""
+        while self.in_use + self.idle > limit:
+            keys = [k for k, v in self.pool.items() if v]
+            if not keys:
+                return
+            k = max(keys, key=lambda k: self.bytes_of[k])
+            solver = self.pool[k].pop()
+            solver.close()
+            self.idle -= self.bytes_of[k]
+            self.evictions += 1
 
     def _release(self, sess):
         self.pool.setdefault(sess.key, []).append(sess.solver)
         self.in_use -= self.bytes_of[sess.key]
+        self.idle += self.bytes_of[sess.key]
         sess.solver = None
 
     def run(self, specs, warm_start=True, on_complete=None, scenes=None):
@@ -211,6 +241,9 @@ class SolveServer:
                 s = waiting[0]
                 solver, key = self._acquire(s.spec["dim"], s.spec["side"])
                 if solver is None:
+                    if not getattr(s, "waited", False):
+                        s.waited = True
+                        self.admission_waits += 1
                     break
                 waiting.pop(0)
                 s.solver, s.key = solver, key

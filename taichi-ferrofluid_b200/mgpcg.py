@@ -197,6 +197,16 @@ class MGPCGPoissonSolver:
               "mg_plan_grid")
         return int(b.value)
 
+    def sweep_kernel(self, bits=None):
+        """The autotuner's kernel per streamed level: bits 2l..2l+1 = 0 for the
+        shared-memory ring sweep, 1..3 for the column-register sweep with a
+        32x16, 32x32 or 64x16 tile; ``bits`` forces a choice until the next
+        prepare."""
+        b = mg_lib.ctypes.c_uint32(0 if bits is None else int(bits))
+        check(self.lib.mg_plan_sweep_kernel(self.plan, 0 if bits is None else 1, mg_lib.ctypes.byref(b)),
+              "mg_plan_sweep_kernel")
+        return int(b.value)
+
     def resident(self, on=None, first_level=None):
         """(on, first level): whether the V-cycle runs its levels from the first
         brick level down as one thread-block-cluster launch (the autotuner's

@@ -112,3 +112,19 @@ def test_launch_shape_choices_need_a_prepared_plan():
         assert lib.mg_plan_split(p, 1, ctypes.byref(bits), None) == mg_lib.MG_E_BADARG
     finally:
         lib.mg_plan_destroy(p)
+
+
+def test_static_reduce_refuses_bad_arguments_before_any_cuda_call():
+    """mg_reduce_static checks its pointers, its cell count and its scratch
+    limit on the host, before it touches a device."""
+    lib = mg_lib.load()
+    p = ctypes.c_void_p(256)  # never dereferenced: every call below is refused first
+    assert lib.mg_reduce_static(None, p, p, 16, p, None) == mg_lib.MG_E_BADARG
+    assert "null pointer" in mg_lib.last_error()
+    assert lib.mg_reduce_static(p, None, p, 16, p, None) == mg_lib.MG_E_BADARG
+    assert lib.mg_reduce_static(p, p, None, 16, p, None) == mg_lib.MG_E_BADARG
+    assert lib.mg_reduce_static(p, p, p, 16, None, None) == mg_lib.MG_E_BADARG
+    assert lib.mg_reduce_static(p, p, p, -1, p, None) == mg_lib.MG_E_BADARG
+    assert "negative cell count" in mg_lib.last_error()
+    assert lib.mg_reduce_static(p, p, p, 33_554_433, p, None) == mg_lib.MG_E_TOO_BIG
+    assert "static scratch limit" in mg_lib.last_error()

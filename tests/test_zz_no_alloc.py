@@ -60,3 +60,32 @@ def test_static_reduce_rejects_sizes_beyond_its_scratch():
                               ctypes.c_void_p(out.data_ptr()), None)
     assert rc == mg_lib.MG_E_TOO_BIG
     assert "static scratch limit" in mg_lib.last_error()
+
+
+@pytest.mark.parametrize("n", [0, 1, 4097, 256 ** 3, 33_554_432])
+def test_static_reduce_sizes(n):
+    """No cells (the sum is 0), a ragged count, 4,096 blocks (256^3 cells) and
+    the largest count the static scratch holds (8,192 blocks), each twice in a
+    row, against an FP64 sum of the same products."""
+    import torch
+    lib = mg_lib.load()
+    g = torch.Generator(device="cuda").manual_seed(n + 7)
+    m = max(n, 1)
+    a = torch.randn(m, device="cuda", generator=g)
+    b = torch.randn(m, device="cuda", generator=g)
+    lab = torch.randint(0, 3, (m,), device="cuda", generator=g, dtype=torch.int8)
+    stream = torch.cuda.current_stream().cuda_stream
+    out = torch.full((2,), float("nan"), dtype=torch.float64, device="cuda")
+    for k in range(2):
+        assert lib.mg_reduce_static(ctypes.c_void_p(lab.data_ptr()), ctypes.c_void_p(a.data_ptr()),
+                                    ctypes.c_void_p(b.data_ptr()), ctypes.c_int64(n),
+                                    ctypes.c_void_p(out[k:k + 1].data_ptr()), ctypes.c_void_p(stream)) == 0, \
+            mg_lib.last_error()
+    torch.cuda.synchronize()
+    fl = (lab[:n] == 0).double()
+    ref = float((a[:n].double() * b[:n].double() * fl).sum()) if n else 0.0
+    got = out.cpu().numpy()
+    for v in got:
+        assert abs(v - ref) <= 1e-12 * max(abs(ref), 1.0), (v, ref)
+    if n == 0:
+        assert got[0] == 0.0 and got[1] == 0.0
