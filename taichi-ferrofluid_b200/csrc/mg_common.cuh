@@ -68,6 +68,7 @@ struct Control {
   unsigned int counter[8];    // arrival counters of the last-block reductions
   double scratch[8];          // single-value results of mg_reduce
   double det[4 * 12];         // operator detection per level (k_detect_uniform)
+  double zAp;                 // z.Ap of the mixed form's flexible beta
 };
 
 template <typename T> __device__ __forceinline__ float to_f(T v);

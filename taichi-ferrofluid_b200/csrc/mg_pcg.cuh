@@ -137,25 +137,50 @@ __global__ void k_update_p(Level L, float* __restrict__ p, const Control* ctl) {
 //  mode 0 (before the loop): old_zTr = z.r; the loop runs iff max_iters != 0.
 //  mode 1 (end of an iteration): beta = new / (old + eps); old = new; iter++;
 //          stop at max_iters (mgpcg.py:176, :200-209).
+//
+// Ap != null (the mixed form): flexible beta, the A-orthogonalisation of the
+// new z against the last direction, beta = -z.Ap / p.Ap (Notay's flexible
+// CG with one direction kept; equal to the reference's z.r ratio for a fixed
+// SPD preconditioner in exact arithmetic).  A V-cycle on 16-bit grids is a
+// slightly different operator at every application, for which the
+// reference's beta loses conjugacy and stalls.
 template <typename ST>
-__global__ void __launch_bounds__(kRedThreads) k_zr(Level L, Control* ctl, double* partials, int mode) {
+__global__ void __launch_bounds__(kRedThreads) k_zr(Level L, Control* ctl, double* partials, int mode,
+                                                    const float* __restrict__ Ap = nullptr) {
   pdl_enter();
   __shared__ double sh[32];
   const ST* z = (const ST*)L.z;
   const float* r = (const float*)L.r;
   const float sz = (float)ctl->scale_z;
-  double acc = 0.0;
+  const bool flex = Ap != nullptr && mode == 1;
+  double acc = 0.0, zap = 0.0;
   for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < L.g.count;
        i += (long long)gridDim.x * blockDim.x)
-    if (L.type[i] == FLUID) acc += (double)z_true<ST>(z, i, sz) * (double)r[i];
+    if (L.type[i] == FLUID) {
+      const double zi = (double)z_true<ST>(z, i, sz);
+      acc += zi * (double)r[i];
+      if (flex) zap += zi * (double)Ap[i];
+    }
   double tot;
+  if (flex) {  // z.Ap first (its own counter); the z.r epilogue below reads it
+    double tz;
+    if (last_block_total<kRedThreads>(zap, partials + kMaxPartials / 2, &ctl->counter[5], sh, &tz) &&
+        threadIdx.x == 0)
+      ctl->zAp = tz;
+  }
   if (last_block_total<kRedThreads>(acc, partials, &ctl->counter[1], sh, &tot) && threadIdx.x == 0) {
     if (mode == 0) {
       ctl->old_zTr = tot;
       if (ctl->max_iters == 0) ctl->run = 0;
     } else {
       ctl->new_zTr = tot;
-      ctl->beta = (float)(tot / (ctl->old_zTr + ctl->eps));
+      if (flex) {
+        __threadfence();
+        const double zap_t = ((volatile Control*)ctl)->zAp;
+        ctl->beta = (float)(-zap_t / (ctl->pAp + ctl->eps));
+      } else {
+        ctl->beta = (float)(tot / (ctl->old_zTr + ctl->eps));
+      }
       ctl->old_zTr = tot;
       ctl->iter += 1;
       if (ctl->max_iters != -1 && ctl->iter >= ctl->max_iters) ctl->run = 0;

@@ -670,11 +670,13 @@ int launch_zr_p(mg_plan* P, bool prologue, cudaStream_t s, bool zr_done = false)
     return MG_OK;
   }
   const Control* cc = P->ctl;
+  // the mixed form (true-residual refresh) takes the flexible beta
+  const float* Ap = P->d.refresh_every > 0 && P->d.storage != MG_STORE_F32 ? fptr(P, MG_FIELD_AP) : nullptr;
   if (prologue) {
     CK(launch_k(k_update_p<ST>, P->ew_blocks[0], 256, 0, s, L0, p, cc));
-    CK(launch_k(k_zr<ST>, P->red_blocks, kRedThreads, 0, s, L0, P->ctl, P->partials, 0));
+    CK(launch_k(k_zr<ST>, P->red_blocks, kRedThreads, 0, s, L0, P->ctl, P->partials, 0, Ap));
   } else {
-    CK(launch_k(k_zr<ST>, P->red_blocks, kRedThreads, 0, s, L0, P->ctl, P->partials, 1));
+    CK(launch_k(k_zr<ST>, P->red_blocks, kRedThreads, 0, s, L0, P->ctl, P->partials, 1, Ap));
     CK(launch_k(k_update_p<ST>, P->ew_blocks[0], 256, 0, s, L0, p, cc));
   }
   return MG_OK;
