@@ -493,6 +493,42 @@ MG_API int mg_plan_launch_counts(mg_plan_t* plan, int32_t* prologue, int32_t* bo
  * cluster-resident part of the V-cycle (mg_plan_resident). */
 MG_API int mg_launch_stage(mg_plan_t* plan, int32_t stage, int32_t level, void* stream);
 
+/* ---- batched solves ------------------------------------------------------------------ */
+
+/* The system half of mg_pressure_solve_async: initialize (keeping x when
+ * warm_start), labels, build_b, build_A per level, coarse labels and the
+ * declared operator form, enqueued on `stream` with no host synchronisation
+ * (mgpcg.py:63-94 with pressure_project.py:15-70).  mg_pcg_solve_async or a
+ * batch solve then runs the PCG loop. */
+MG_API int mg_pressure_setup_async(mg_plan_t* plan, const int32_t* cell_type, const float* v0, const float* v1,
+                                   const float* v2, const float* phi, float p0, float scale_A, float scale_b,
+                                   int32_t ghost_fluid, float gfm_clamp, int32_t warm_start, void* stream);
+
+/* A batch: many plans' PCG loops advanced together, ONE kernel launch per
+ * V-cycle stage (the sweeps of one level depth, the coarse blocks) and per CG
+ * step for every instance, each launch driven by a table of (instance, block)
+ * entries; every instance keeps its own reductions, alpha, beta, iteration
+ * count and convergence test on the device, and the whole loop is one CUDA
+ * graph that runs while any instance is unconverged.  No reference
+ * counterpart: the reference solves one system per call (mgpcg.py:150-209).
+ * Every plan must be bound and prepared in the label-uniform fused form
+ * (mg_pressure_setup_async), with pre_post 2 and one storage type; each
+ * instance's arithmetic is that of its own solve (the same blocks; the level
+ * sweeps use the tiled ring kernel).  The batch's tables live in a workspace
+ * the caller allocates (mg_batch_workspace_bytes) and binds. */
+typedef struct mg_batch mg_batch_t;
+MG_API int mg_batch_create(mg_plan_t* const* plans, int32_t n, mg_batch_t** out);
+MG_API void mg_batch_destroy(mg_batch_t* batch);
+MG_API int64_t mg_batch_workspace_bytes(const mg_batch_t* batch);
+/* Uploads the tables into `workspace` (256-byte aligned) and builds the graph. */
+MG_API int mg_batch_bind(mg_batch_t* batch, void* workspace, void* stream);
+/* Solves every instance (its b, A as last set up; warm_start keeps each x);
+ * MG_E_BADARG if an instance's plan was prepared to another shape since
+ * mg_batch_create.  Results and mg_pcg_stats stay per plan. */
+MG_API int mg_batch_solve_async(mg_batch_t* batch, const mg_solve_params_t* params, void* stream);
+/* Kernels one batch launches before its loop and per loop pass. */
+MG_API int mg_batch_launch_counts(const mg_batch_t* batch, int32_t* prologue, int32_t* body);
+
 /* ---- allocation-free variant ------------------------------------------------------ */
 
 /* Sum of a[i] * b[i] over the n cells with grid_type[i] == MG_FLUID, in FP64,

@@ -58,7 +58,8 @@ struct Control {
   double rel_tol, abs_tol, eps;
   float alpha, beta;          // the reference's f32 scalar fields (mgpcg.py:43-44)
   int iter, status, max_iters, run;
-  int warm_start, refresh_every, since_refresh, pad0;
+  int warm_start, refresh_every, since_refresh;
+  int done;                   // a batched solve: this instance has finished (its blocks return)
   double scale_z;             // z (true) = scale_z * z (stored), 16-bit storage only
   double scale_r;             // r (stored, level 0 input of the V-cycle) = scale_r * r
   double kappa;               // coefficient scale of 16-bit grids
@@ -167,31 +168,39 @@ __device__ __forceinline__ double block_sum(double v, double* sh) {
 
 // Last-block reduction: every block stores its partial; the block that
 // arrives last sums all partials in index order (deterministic for a fixed
-// grid) and returns true with the total in *total (thread 0 only).
+// grid) and returns true with the total in *total (thread 0 only).  The _at
+// form takes the block's index and the block count of its reduction, so that
+// one launch can hold the reductions of several solves (a batch), each over
+// its own blocks, partials and counter.
 template <int NT>
-__device__ __forceinline__ bool last_block_total(double partial, double* partials,
-                                                 unsigned int* counter, double* sh,
-                                                 double* total) {
+__device__ __forceinline__ bool last_block_total_at(double partial, double* partials, unsigned int* counter,
+                                                    double* sh, double* total, int bid, int nb) {
   __shared__ bool am_last;
   double s = block_sum<NT>(partial, sh);
   if (threadIdx.x == 0) {
-    partials[blockIdx.x] = s;
+    partials[bid] = s;
     __threadfence();
     unsigned int prev = atomicAdd(counter, 1u);
-    am_last = (prev == gridDim.x - 1);
+    am_last = (prev == (unsigned int)nb - 1);
   }
   __syncthreads();
   if (!am_last) return false;
   __threadfence();
   double acc = 0.0;
-  for (unsigned int i = threadIdx.x; i < gridDim.x; i += NT)
-    acc += ((volatile double*)partials)[i];
+  for (int i = threadIdx.x; i < nb; i += NT) acc += ((volatile double*)partials)[i];
   double t = block_sum<NT>(acc, sh);
   if (threadIdx.x == 0) {
     *total = t;
     *counter = 0u;  // ready for the next launch
   }
   return true;
+}
+
+template <int NT>
+__device__ __forceinline__ bool last_block_total(double partial, double* partials,
+                                                 unsigned int* counter, double* sh,
+                                                 double* total) {
+  return last_block_total_at<NT>(partial, partials, counter, sh, total, (int)blockIdx.x, (int)gridDim.x);
 }
 
 }  // namespace mg

@@ -50,16 +50,16 @@ __device__ void set_scales(Control* ctl, double rTr);
 
 // r = b (reference), or r = b - A x (warm start); then r.r over FLUID cells.
 // Epilogue: rTr0, tol = max(abs_tol, rTr0 * rel_tol) (mgpcg.py:157-164).
-__global__ void __launch_bounds__(kRedThreads) k_pcg_begin(Level L, const float* __restrict__ b,
+__device__ __forceinline__ void pcg_begin_body(int bid_, int nb_, Level L, const float* __restrict__ b,
                                                            float* __restrict__ x, Control* ctl,
                                                            double* partials, double* __restrict__ xh) {
-  pdl_enter();
+
   __shared__ double sh[32];
   float* r = (float*)L.r;
   const int warm = ctl->warm_start;
   double acc = 0.0, accb = 0.0;
-  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < L.g.count;
-       i += (long long)gridDim.x * blockDim.x) {
+  for (long long i = (long long)bid_ * blockDim.x + threadIdx.x; i < L.g.count;
+       i += (long long)nb_ * blockDim.x) {
     float ri = b[i];
     if (L.type[i] == FLUID) accb += (double)ri * (double)ri;
     if (warm && L.type[i] == FLUID) {
@@ -80,9 +80,9 @@ __global__ void __launch_bounds__(kRedThreads) k_pcg_begin(Level L, const float*
   }
   double tot, totb;
   // b.b first (its own counter), then r.r; both blocks orders are fixed
-  bool lastb = last_block_total<kRedThreads>(accb, partials + kMaxPartials / 2, &ctl->counter[6], sh, &totb);
+  bool lastb = last_block_total_at<kRedThreads>(accb, partials + kMaxPartials / 2, &ctl->counter[6], sh, &totb, bid_, nb_);
   if (lastb && threadIdx.x == 0) ctl->bTb = totb;
-  if (last_block_total<kRedThreads>(acc, partials, &ctl->counter[0], sh, &tot) && threadIdx.x == 0) {
+  if (last_block_total_at<kRedThreads>(acc, partials, &ctl->counter[0], sh, &tot, bid_, nb_) && threadIdx.x == 0) {
     __threadfence();
     const double bb = ((volatile Control*)ctl)->bTb;
     ctl->rTr0 = tot;
@@ -100,6 +100,13 @@ __global__ void __launch_bounds__(kRedThreads) k_pcg_begin(Level L, const float*
     ctl->wait_timeout = 0;
     set_scales(ctl, tot);
   }
+}
+
+__global__ void __launch_bounds__(kRedThreads) k_pcg_begin(Level L, const float* __restrict__ b,
+                                                           float* __restrict__ x, Control* ctl,
+                                                           double* partials, double* __restrict__ xh) {
+  pdl_enter();
+  pcg_begin_body(blockIdx.x, gridDim.x, L, b, x, ctl, partials, xh);
 }
 
 // z of level 0 as float32: 16-bit grids hold z~ = z / scale_z (a power of two).
@@ -123,14 +130,20 @@ __device__ void set_scales(Control* ctl, double rTr) {
 
 // update_p (mgpcg.py:234-238): p = z + beta p on FLUID cells.
 template <typename ST>
-__global__ void k_update_p(Level L, float* __restrict__ p, const Control* ctl) {
-  pdl_enter();
+__device__ __forceinline__ void update_p_body(int bid_, int nb_, Level L, float* __restrict__ p, const Control* ctl) {
+
   const float beta = ctl->beta;
   const float sz = (float)ctl->scale_z;
   const ST* z = (const ST*)L.z;
-  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < L.g.count;
-       i += (long long)gridDim.x * blockDim.x)
+  for (long long i = (long long)bid_ * blockDim.x + threadIdx.x; i < L.g.count;
+       i += (long long)nb_ * blockDim.x)
     if (L.type[i] == FLUID) p[i] = __fadd_rn(z_true<ST>(z, i, sz), __fmul_rn(beta, p[i]));
+}
+
+template <typename ST>
+__global__ void k_update_p(Level L, float* __restrict__ p, const Control* ctl) {
+  pdl_enter();
+  update_p_body<ST>(blockIdx.x, gridDim.x, L, p, ctl);
 }
 
 // reduce(z, r) (mgpcg.py:171, :201) with the scalar epilogue.
@@ -145,17 +158,17 @@ __global__ void k_update_p(Level L, float* __restrict__ p, const Control* ctl) {
 // slightly different operator at every application, for which the
 // reference's beta loses conjugacy and stalls.
 template <typename ST>
-__global__ void __launch_bounds__(kRedThreads) k_zr(Level L, Control* ctl, double* partials, int mode,
-                                                    const float* __restrict__ Ap = nullptr) {
-  pdl_enter();
+__device__ __forceinline__ void zr_body(int bid_, int nb_, Level L, Control* ctl, double* partials, int mode,
+                                                    const float* __restrict__ Ap) {
+
   __shared__ double sh[32];
   const ST* z = (const ST*)L.z;
   const float* r = (const float*)L.r;
   const float sz = (float)ctl->scale_z;
   const bool flex = Ap != nullptr && mode == 1;
   double acc = 0.0, zap = 0.0;
-  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < L.g.count;
-       i += (long long)gridDim.x * blockDim.x)
+  for (long long i = (long long)bid_ * blockDim.x + threadIdx.x; i < L.g.count;
+       i += (long long)nb_ * blockDim.x)
     if (L.type[i] == FLUID) {
       const double zi = (double)z_true<ST>(z, i, sz);
       acc += zi * (double)r[i];
@@ -164,11 +177,11 @@ __global__ void __launch_bounds__(kRedThreads) k_zr(Level L, Control* ctl, doubl
   double tot;
   if (flex) {  // z.Ap first (its own counter); the z.r epilogue below reads it
     double tz;
-    if (last_block_total<kRedThreads>(zap, partials + kMaxPartials / 2, &ctl->counter[5], sh, &tz) &&
+    if (last_block_total_at<kRedThreads>(zap, partials + kMaxPartials / 2, &ctl->counter[5], sh, &tz, bid_, nb_) &&
         threadIdx.x == 0)
       ctl->zAp = tz;
   }
-  if (last_block_total<kRedThreads>(acc, partials, &ctl->counter[1], sh, &tot) && threadIdx.x == 0) {
+  if (last_block_total_at<kRedThreads>(acc, partials, &ctl->counter[1], sh, &tot, bid_, nb_) && threadIdx.x == 0) {
     if (mode == 0) {
       ctl->old_zTr = tot;
       if (ctl->max_iters == 0) ctl->run = 0;
@@ -188,15 +201,22 @@ __global__ void __launch_bounds__(kRedThreads) k_zr(Level L, Control* ctl, doubl
   }
 }
 
+template <typename ST>
+__global__ void __launch_bounds__(kRedThreads) k_zr(Level L, Control* ctl, double* partials, int mode,
+                                                    const float* __restrict__ Ap = nullptr) {
+  pdl_enter();
+  zr_body<ST>(blockIdx.x, gridDim.x, L, ctl, partials, mode, Ap);
+}
+
 // float32 grids whose cell count is a multiple of 4: the same two kernels
 // over 4-cell groups (16-byte loads of z, r, p; 4 labels in one load).
 __device__ __forceinline__ bool fluid_lane(uint32_t t4, int e) { return ((t4 >> (8 * e)) & 0xffu) == (uint32_t)FLUID; }
 
-__global__ void k_update_p4(Level L, float* __restrict__ p, const Control* ctl) {
-  pdl_enter();
+__device__ __forceinline__ void update_p4_body(int bid_, int nb_, Level L, float* __restrict__ p, const Control* ctl) {
+
   const float beta = ctl->beta;
   const int groups = (int)(L.g.count >> 2);
-  for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < groups; q += gridDim.x * blockDim.x) {
+  for (int q = bid_ * blockDim.x + threadIdx.x; q < groups; q += nb_ * blockDim.x) {
     const uint32_t t4 = __ldg(reinterpret_cast<const uint32_t*>(L.type) + q);
     if (t4 == 0x02020202u || t4 == 0x01010101u) continue;  // no FLUID lane (all SOLID / all AIR)
     const float4 z = __ldg(reinterpret_cast<const float4*>((const float*)L.z) + q);
@@ -210,12 +230,17 @@ __global__ void k_update_p4(Level L, float* __restrict__ p, const Control* ctl) 
   }
 }
 
-__global__ void __launch_bounds__(kRedThreads) k_zr4(Level L, Control* ctl, double* partials, int mode) {
+__global__ void k_update_p4(Level L, float* __restrict__ p, const Control* ctl) {
   pdl_enter();
+  update_p4_body(blockIdx.x, gridDim.x, L, p, ctl);
+}
+
+__device__ __forceinline__ void zr4_body(int bid_, int nb_, Level L, Control* ctl, double* partials, int mode) {
+
   __shared__ double sh[32];
   const int groups = (int)(L.g.count >> 2);
   double acc = 0.0;
-  for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < groups; q += gridDim.x * blockDim.x) {
+  for (int q = bid_ * blockDim.x + threadIdx.x; q < groups; q += nb_ * blockDim.x) {
     const uint32_t t4 = __ldg(reinterpret_cast<const uint32_t*>(L.type) + q);
     if (t4 == 0x02020202u || t4 == 0x01010101u) continue;
     const float4 z = __ldg(reinterpret_cast<const float4*>((const float*)L.z) + q);
@@ -226,7 +251,7 @@ __global__ void __launch_bounds__(kRedThreads) k_zr4(Level L, Control* ctl, doub
     if (fluid_lane(t4, 3)) acc += (double)z.w * (double)r.w;
   }
   double tot;
-  if (last_block_total<kRedThreads>(acc, partials, &ctl->counter[1], sh, &tot) && threadIdx.x == 0) {
+  if (last_block_total_at<kRedThreads>(acc, partials, &ctl->counter[1], sh, &tot, bid_, nb_) && threadIdx.x == 0) {
     if (mode == 0) {
       ctl->old_zTr = tot;
       if (ctl->max_iters == 0) ctl->run = 0;
@@ -238,6 +263,11 @@ __global__ void __launch_bounds__(kRedThreads) k_zr4(Level L, Control* ctl, doub
       if (ctl->max_iters != -1 && ctl->iter >= ctl->max_iters) ctl->run = 0;
     }
   }
+}
+
+__global__ void __launch_bounds__(kRedThreads) k_zr4(Level L, Control* ctl, double* partials, int mode) {
+  pdl_enter();
+  zr4_body(blockIdx.x, gridDim.x, L, ctl, partials, mode);
 }
 
 // compute_Ap (mgpcg.py:218-224) + reduce(p, Ap) + alpha = zTr / (pAp + eps).
@@ -392,16 +422,16 @@ __global__ void __launch_bounds__(kRedThreads) k_Ap_alpha4(Level L, const float*
 // equals the reference's Ax * p up to the sign of a zero product; FLUID is
 // Adiag != 0 (checked by mg_plan_prepare).  No Ax arrays, no labels: 12 bytes
 // per cell instead of 25, the same values and the same summation order.
-__global__ void __launch_bounds__(kRedThreads) k_Ap_alpha_uniform(Level L, const float* __restrict__ p,
+__device__ __forceinline__ void Ap_alpha_uniform_body(int bid_, int nb_, Level L, const float* __restrict__ p,
                                                                   float* __restrict__ Ap, float s, Control* ctl,
-                                                                  double* partials, int force = 0) {
-  pdl_enter();
+                                                                  double* partials, int force) {
+
   if (!ctl->run && !force) return;
   __shared__ double sh[32];
   const float ms = -s;
   double acc = 0.0;
-  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < L.g.count;
-       i += (long long)gridDim.x * blockDim.x) {
+  for (long long i = (long long)bid_ * blockDim.x + threadIdx.x; i < L.g.count;
+       i += (long long)nb_ * blockDim.x) {
     const float a = L.Adiag[i];
     if (a == 0.0f) continue;
     int c[3];
@@ -421,10 +451,17 @@ __global__ void __launch_bounds__(kRedThreads) k_Ap_alpha_uniform(Level L, const
     acc += (double)pi * (double)v;
   }
   double tot;
-  if (last_block_total<kRedThreads>(acc, partials, &ctl->counter[2], sh, &tot) && threadIdx.x == 0) {
+  if (last_block_total_at<kRedThreads>(acc, partials, &ctl->counter[2], sh, &tot, bid_, nb_) && threadIdx.x == 0) {
     ctl->pAp = tot;
     ctl->alpha = (float)(ctl->old_zTr / (tot + ctl->eps));
   }
+}
+
+__global__ void __launch_bounds__(kRedThreads) k_Ap_alpha_uniform(Level L, const float* __restrict__ p,
+                                                                  float* __restrict__ Ap, float s, Control* ctl,
+                                                                  double* partials, int force = 0) {
+  pdl_enter();
+  Ap_alpha_uniform_body(blockIdx.x, gridDim.x, L, p, Ap, s, ctl, partials, force);
 }
 
 // k_Ap_alpha_uniform over groups of 4 consecutive cells along the fastest
@@ -433,10 +470,10 @@ __global__ void __launch_bounds__(kRedThreads) k_Ap_alpha_uniform(Level L, const
 // the x neighbours, 32-bit indices, several groups in flight per thread.  The
 // same float32 operations per cell in the same axis order; non-FLUID cells
 // keep their Ap (written only where Adiag != 0).
-__global__ void __launch_bounds__(kRedThreads) k_Ap_alpha_uniform4(Level L, const float* __restrict__ p,
+__device__ __forceinline__ void Ap_alpha_uniform4_body(int bid_, int nb_, Level L, const float* __restrict__ p,
                                                                    float* __restrict__ Ap, float s, Control* ctl,
-                                                                   double* partials, int force = 0) {
-  pdl_enter();
+                                                                   double* partials, int force) {
+
   if (!ctl->run && !force) return;
   __shared__ double sh[32];
   const float ms = -s;
@@ -444,7 +481,7 @@ __global__ void __launch_bounds__(kRedThreads) k_Ap_alpha_uniform4(Level L, cons
   const int nx = L.g.n[dim - 1];
   const int groups = (int)(L.g.count >> 2);
   double acc = 0.0;
-  const int q0 = blockIdx.x * blockDim.x + threadIdx.x, S = gridDim.x * blockDim.x;
+  const int q0 = bid_ * blockDim.x + threadIdx.x, S = nb_ * blockDim.x;
   GroupWalk w(L.g, q0, S);
   for (int q = q0; q < groups; q += S, w.advance()) {
     const int i = q << 2;
@@ -496,30 +533,37 @@ __global__ void __launch_bounds__(kRedThreads) k_Ap_alpha_uniform4(Level L, cons
     }
   }
   double tot;
-  if (last_block_total<kRedThreads>(acc, partials, &ctl->counter[2], sh, &tot) && threadIdx.x == 0) {
+  if (last_block_total_at<kRedThreads>(acc, partials, &ctl->counter[2], sh, &tot, bid_, nb_) && threadIdx.x == 0) {
     ctl->pAp = tot;
     ctl->alpha = (float)(ctl->old_zTr / (tot + ctl->eps));
   }
 }
 
+__global__ void __launch_bounds__(kRedThreads) k_Ap_alpha_uniform4(Level L, const float* __restrict__ p,
+                                                                   float* __restrict__ Ap, float s, Control* ctl,
+                                                                   double* partials, int force = 0) {
+  pdl_enter();
+  Ap_alpha_uniform4_body(blockIdx.x, gridDim.x, L, p, Ap, s, ctl, partials, force);
+}
+
 // update_xr (mgpcg.py:226-232) + reduce(r, r) + the convergence test
 // (mgpcg.py:188-195).  Sets the while-node condition to ctl->run.
-__global__ void __launch_bounds__(kRedThreads) k_xr(Level L, float* __restrict__ x,
+__device__ __forceinline__ void xr_body(int bid_, int nb_, Level L, float* __restrict__ x,
                                                     const float* __restrict__ p,
                                                     const float* __restrict__ Ap, Control* ctl,
                                                     double* partials, cudaGraphConditionalHandle cond,
-                                                    int has_cond, int force = 0, double* __restrict__ xh = nullptr) {
-  pdl_enter();
+                                                    int has_cond, int force, double* __restrict__ xh) {
+
   __shared__ double sh[32];
   if (!ctl->run && !force) {
-    if (has_cond && blockIdx.x == 0 && threadIdx.x == 0) cudaGraphSetConditional(cond, 0);
+    if (has_cond && bid_ == 0 && threadIdx.x == 0) cudaGraphSetConditional(cond, 0);
     return;
   }
   const float alpha = ctl->alpha;
   float* r = (float*)L.r;
   double acc = 0.0;
-  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < L.g.count;
-       i += (long long)gridDim.x * blockDim.x) {
+  for (long long i = (long long)bid_ * blockDim.x + threadIdx.x; i < L.g.count;
+       i += (long long)nb_ * blockDim.x) {
     if (L.type[i] != FLUID) continue;
     if (xh) {  // mixed form: x accumulates in FP64, x (float32) is its rounding
       const double v = xh[i] + (double)alpha * (double)p[i];
@@ -533,7 +577,7 @@ __global__ void __launch_bounds__(kRedThreads) k_xr(Level L, float* __restrict__
     acc += (double)ri * (double)ri;
   }
   double tot;
-  if (last_block_total<kRedThreads>(acc, partials, &ctl->counter[3], sh, &tot) && threadIdx.x == 0) {
+  if (last_block_total_at<kRedThreads>(acc, partials, &ctl->counter[3], sh, &tot, bid_, nb_) && threadIdx.x == 0) {
     ctl->rTr = tot;
     if (!isfinite(tot)) {
       ctl->status = MG_SOLVE_NONFINITE;
@@ -552,25 +596,34 @@ __global__ void __launch_bounds__(kRedThreads) k_xr(Level L, float* __restrict__
   }
 }
 
+__global__ void __launch_bounds__(kRedThreads) k_xr(Level L, float* __restrict__ x,
+                                                    const float* __restrict__ p,
+                                                    const float* __restrict__ Ap, Control* ctl,
+                                                    double* partials, cudaGraphConditionalHandle cond,
+                                                    int has_cond, int force = 0, double* __restrict__ xh = nullptr) {
+  pdl_enter();
+  xr_body(blockIdx.x, gridDim.x, L, x, p, Ap, ctl, partials, cond, has_cond, force, xh);
+}
+
 // k_xr on 4-cell groups (one 16-byte vector of x, p, r, Ap and one 32-bit
 // word of labels per group; the cell count a multiple of 4): the same
 // per-cell arithmetic, r.r summed group by group.
-__global__ void __launch_bounds__(kRedThreads) k_xr4(Level L, float* __restrict__ x,
+__device__ __forceinline__ void xr4_body(int bid_, int nb_, Level L, float* __restrict__ x,
                                                      const float* __restrict__ p,
                                                      const float* __restrict__ Ap, Control* ctl,
                                                      double* partials, cudaGraphConditionalHandle cond,
-                                                     int has_cond, int force = 0, double* __restrict__ xh = nullptr) {
-  pdl_enter();
+                                                     int has_cond, int force, double* __restrict__ xh) {
+
   __shared__ double sh[32];
   if (!ctl->run && !force) {
-    if (has_cond && blockIdx.x == 0 && threadIdx.x == 0) cudaGraphSetConditional(cond, 0);
+    if (has_cond && bid_ == 0 && threadIdx.x == 0) cudaGraphSetConditional(cond, 0);
     return;
   }
   const float alpha = ctl->alpha;
   float* r = (float*)L.r;
   const int groups = (int)(L.g.count >> 2);
   double acc = 0.0;
-  for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < groups; q += gridDim.x * blockDim.x) {
+  for (int q = bid_ * blockDim.x + threadIdx.x; q < groups; q += nb_ * blockDim.x) {
     const uint32_t t4 = __ldg(reinterpret_cast<const uint32_t*>(L.type) + q);
     float4 xv = reinterpret_cast<float4*>(x)[q];
     const float4 pv = __ldg(reinterpret_cast<const float4*>(p) + q);
@@ -604,7 +657,7 @@ __global__ void __launch_bounds__(kRedThreads) k_xr4(Level L, float* __restrict_
     reinterpret_cast<float4*>(r)[q] = rv;
   }
   double tot;
-  if (last_block_total<kRedThreads>(acc, partials, &ctl->counter[3], sh, &tot) && threadIdx.x == 0) {
+  if (last_block_total_at<kRedThreads>(acc, partials, &ctl->counter[3], sh, &tot, bid_, nb_) && threadIdx.x == 0) {
     ctl->rTr = tot;
     if (!isfinite(tot)) {
       ctl->status = MG_SOLVE_NONFINITE;
@@ -623,27 +676,36 @@ __global__ void __launch_bounds__(kRedThreads) k_xr4(Level L, float* __restrict_
   }
 }
 
+__global__ void __launch_bounds__(kRedThreads) k_xr4(Level L, float* __restrict__ x,
+                                                     const float* __restrict__ p,
+                                                     const float* __restrict__ Ap, Control* ctl,
+                                                     double* partials, cudaGraphConditionalHandle cond,
+                                                     int has_cond, int force = 0, double* __restrict__ xh = nullptr) {
+  pdl_enter();
+  xr4_body(blockIdx.x, gridDim.x, L, x, p, Ap, ctl, partials, cond, has_cond, force, xh);
+}
+
 // True-residual refresh (the mixed form's iterative refinement): every
 // refresh_every iterations, and whenever the recursive residual claims
 // convergence, r = b - A x is recomputed in FP64 arithmetic from the stored
 // float32 x, and the convergence test is taken again on it.  The recursive
 // residual of the reference never does this (mgpcg.py:226-232).
-__global__ void __launch_bounds__(kRedThreads) k_refresh(Level L, const float* __restrict__ b,
+__device__ __forceinline__ void refresh_body(int bid_, int nb_, Level L, const float* __restrict__ b,
                                                          const float* __restrict__ x, Control* ctl,
                                                          double* partials, cudaGraphConditionalHandle cond,
                                                          int has_cond, const double* __restrict__ xh) {
-  pdl_enter();
+
   __shared__ double sh[32];
   const bool claimed = ctl->status == MG_SOLVE_CONVERGED && !ctl->run;
   const bool due = ctl->run && ctl->refresh_every > 0 && ctl->since_refresh >= ctl->refresh_every;
   if (!(claimed || due)) {
-    if (has_cond && blockIdx.x == 0 && threadIdx.x == 0) cudaGraphSetConditional(cond, ctl->run ? 1u : 0u);
+    if (has_cond && bid_ == 0 && threadIdx.x == 0) cudaGraphSetConditional(cond, ctl->run ? 1u : 0u);
     return;
   }
   float* r = (float*)L.r;
   double acc = 0.0;
-  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < L.g.count;
-       i += (long long)gridDim.x * blockDim.x) {
+  for (long long i = (long long)bid_ * blockDim.x + threadIdx.x; i < L.g.count;
+       i += (long long)nb_ * blockDim.x) {
     if (L.type[i] != FLUID) continue;
     int c[3];
     L.g.coords(i, c);
@@ -660,7 +722,7 @@ __global__ void __launch_bounds__(kRedThreads) k_refresh(Level L, const float* _
     acc += rr * rr;
   }
   double tot;
-  if (last_block_total<kRedThreads>(acc, partials, &ctl->counter[7], sh, &tot) && threadIdx.x == 0) {
+  if (last_block_total_at<kRedThreads>(acc, partials, &ctl->counter[7], sh, &tot, bid_, nb_) && threadIdx.x == 0) {
     ctl->rTr = tot;
     ctl->since_refresh = 0;
     if (!isfinite(tot)) {
@@ -681,6 +743,14 @@ __global__ void __launch_bounds__(kRedThreads) k_refresh(Level L, const float* _
     set_scales(ctl, tot);
     if (has_cond) cudaGraphSetConditional(cond, ctl->run ? 1u : 0u);
   }
+}
+
+__global__ void __launch_bounds__(kRedThreads) k_refresh(Level L, const float* __restrict__ b,
+                                                         const float* __restrict__ x, Control* ctl,
+                                                         double* partials, cudaGraphConditionalHandle cond,
+                                                         int has_cond, const double* __restrict__ xh) {
+  pdl_enter();
+  refresh_body(blockIdx.x, gridDim.x, L, b, x, ctl, partials, cond, has_cond, xh);
 }
 
 // Plain masked dot of two level-0 f32 fields into ctl->scratch[slot]

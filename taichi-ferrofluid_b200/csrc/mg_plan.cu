@@ -5,6 +5,7 @@
 // mg_plan_workspace_bytes() bytes; every solver field (mgpcg.py:21-44) lives at
 // a fixed 256-byte aligned offset in it.  This file allocates host memory only
 // (the plan, a pinned parameter block) plus the CUDA graph objects.
+#include <algorithm>
 #include <array>
 #include <cmath>
 #include <cstdio>
@@ -20,6 +21,7 @@
 #include "mg_kernels.cuh"
 #include "mg_pcg.cuh"
 #include "mg_fused_host.cuh"
+#include "mg_batch.cuh"
 #include "mg_strategies.cuh"
 #include "mg_levelset.cuh"
 #include "mg_advect.cuh"
@@ -1807,10 +1809,20 @@ int mg_pressure_solve_async(mg_plan_t* P, const int32_t* ct, const float* v0, co
                             const float* phi, float p0, float sA, float sB, int32_t ghost, float clamp,
                             const mg_solve_params_t* prm, void* stream) {
   NEED_BOUND(P);
-  if (!prm || !ct) return bad("params / cell_type");
+  if (!prm) return bad("params");
+  if (int rc = mg_pressure_setup_async(P, ct, v0, v1, v2, phi, p0, sA, sB, ghost, clamp, prm->warm_start, stream))
+    return rc;
+  return mg_pcg_solve_async(P, prm, stream);
+}
+
+int mg_pressure_setup_async(mg_plan_t* P, const int32_t* ct, const float* v0, const float* v1, const float* v2,
+                            const float* phi, float p0, float sA, float sB, int32_t ghost, float clamp,
+                            int32_t warm_start, void* stream) {
+  NEED_BOUND(P);
+  if (!ct) return bad("cell_type");
   cudaStream_t s = S(stream);
   // initialize() (mgpcg.py:63-77); a warm start keeps x
-  if (prm->warm_start) {
+  if (warm_start) {
     const Loc& lx = P->loc[MG_FIELD_X][0][0];
     CK(cudaMemsetAsync(P->base, 0, lx.off, s));
     const int64_t after = lx.off + lx.bytes;
@@ -1827,13 +1839,379 @@ int mg_pressure_solve_async(mg_plan_t* P, const int32_t* ct, const float* v0, co
   }
   float od[kMaxLevels];
   for (int l = 0; l < P->L; ++l) od[l] = sA;  // Ax = -scale_A between FLUID cells
-  if (int rc = mg_plan_prepare_declared(P, od, stream)) return rc;
-  return mg_pcg_solve_async(P, prm, stream);
+  return mg_plan_prepare_declared(P, od, stream);
 }
 
 int mg_pcg_solve(mg_plan_t* P, const mg_solve_params_t* prm, mg_solve_stats_t* st, void* stream) {
   if (int rc = mg_pcg_solve_async(P, prm, stream)) return rc;
   return mg_pcg_stats(P, st, stream);
+}
+
+}  // extern "C"
+
+// ---------------------------------------------------------------------------
+// Batched solves (mg_batch.cuh): tables of blocks, one launch per V-cycle
+// stage and CG step for all instances, one CUDA graph for the whole loop.
+// ---------------------------------------------------------------------------
+struct mg_batch {
+  std::vector<mg_plan*> plans;
+  std::vector<uint64_t> sigs;   // each plan's launch signature when the tables were built
+  int n = 0, storage = 0;
+  bool refresh = false;
+  // one sweep launch: instances of one kernel form at one level depth
+  struct Group {
+    int dim, one, pre, depth, blocks, ninst;
+    int64_t tab_off, args_off;
+  };
+  std::vector<Group> groups;
+  std::vector<unsigned char> blob;  // every table, laid out as in the workspace
+  int64_t off_red = 0, off_ew = 0, off_cg = 0, off_coarse = 0, off_any = 0, ws_bytes = 0;
+  int red_total = 0, ew_total = 0, maxlc = 0;
+  size_t coarse_smem = 0;
+  char* base = nullptr;
+  cudaStream_t cap = nullptr;
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t exec = nullptr;
+  cudaGraphConditionalHandle cond = 0;
+};
+
+namespace {
+
+int64_t put_blob(std::vector<unsigned char>& blob, const void* src, size_t bytes) {
+  const int64_t off = align256((int64_t)blob.size());
+  blob.resize(off + bytes);
+  if (bytes) std::memcpy(blob.data() + off, src, bytes);
+  return off;
+}
+
+// Planes a block of a batched sweep streams at least (measured on B200, the
+// 96-instance batch: 58.1 / 55.9 / 55.3 / 57.9 ms for 8 / 16 / 32 / 64 in f32,
+// 68.1 / 65.8 / 65.1 / 67.8 ms in f16).  A solve alone sizes
+// its grid to fill the GPU by itself, which gives a small level chunks of 2
+// planes that recompute 2 NS halo planes each (5x the work at NS = 4); in a
+// batch the other instances fill the GPU, so chunks stay long.
+#ifndef MG_BATCH_MIN_CHUNK
+#define MG_BATCH_MIN_CHUNK 32
+#endif
+
+// The fused plan of an instance as the batch runs it: the tiled ring kernel on
+// every streamed level (no column kernel, two planes a step), chunks of at
+// least MG_BATCH_MIN_CHUNK planes, the coarse block for the levels from lc
+// (no cluster launch).  Every grid gives the same values.
+FusedPlan batch_plan(const mg_plan* P) {
+  FusedPlan F = P->fp;
+  F.res = false;
+  F.zr_mode = -1;
+  int min_chunk = MG_BATCH_MIN_CHUNK;  // MGPCG_BATCH_CHUNK=<planes> overrides (even, >= 2)
+  if (const char* ov = std::getenv("MGPCG_BATCH_CHUNK")) min_chunk = std::max(2, (int)std::strtol(ov, nullptr, 0) & ~1);
+  for (int l = 0; l < F.lc; ++l) {
+    F.col[l] = 0;
+    F.step1[l] = 0;
+    level_grid(&F, P->lv[l].g, l, F.grid_extra[l]);
+    const int n0 = P->lv[l].g.n[0];
+    if (F.chunk[l] < min_chunk) {
+      F.chunk[l] = std::min(n0, min_chunk);
+      F.blocks[l] = F.tiles_x[l] * F.tiles_y[l] * ((n0 + F.chunk[l] - 1) / F.chunk[l]);
+    }
+  }
+  return F;
+}
+
+template <typename ST, bool PRE>
+void batch_sweep_args(mg_batch* B, const std::vector<FusedPlan>& fps, int depth, int dim, int one) {
+  std::vector<SweepArgs<ST>> args;
+  std::vector<BatchBlock> tab;
+  for (int i = 0; i < B->n; ++i) {
+    const mg_plan* P = B->plans[i];
+    const FusedPlan& F = fps[i];
+    if (depth >= F.lc || P->d.dim != dim) continue;
+    const int is_one = dim == 3 && F.chunk[depth] == 2;
+    if (is_one != one) continue;
+    const int k = (int)args.size();
+    args.push_back(sweep_args<ST, PRE>(F, P->lv, depth, P->ctl));
+    for (int b = 0; b < F.blocks[depth]; ++b) tab.push_back({k, b, F.blocks[depth]});
+  }
+  if (args.empty()) return;
+  mg_batch::Group g;
+  g.dim = dim;
+  g.one = one;
+  g.pre = PRE;
+  g.depth = depth;
+  g.blocks = (int)tab.size();
+  g.ninst = (int)args.size();
+  g.args_off = put_blob(B->blob, args.data(), args.size() * sizeof(SweepArgs<ST>));
+  g.tab_off = put_blob(B->blob, tab.data(), tab.size() * sizeof(BatchBlock));
+  B->groups.push_back(g);
+}
+
+template <typename ST>
+void batch_tables(mg_batch* B) {
+  std::vector<FusedPlan> fps;
+  for (auto* P : B->plans) fps.push_back(batch_plan(P));
+  B->maxlc = 0;
+  for (auto& F : fps) B->maxlc = std::max(B->maxlc, F.lc);
+  // sweeps in V-cycle order: PRE by depth, (coarse), POST by depth upward
+  for (int d = 0; d < B->maxlc; ++d)
+    for (int dim = 3; dim >= 2; --dim)
+      for (int one = 0; one <= 1; ++one) batch_sweep_args<ST, true>(B, fps, d, dim, one);
+  for (int d = B->maxlc - 1; d >= 0; --d)
+    for (int dim = 3; dim >= 2; --dim)
+      for (int one = 0; one <= 1; ++one) batch_sweep_args<ST, false>(B, fps, d, dim, one);
+  std::vector<CoarseArgs> coarse;
+  B->coarse_smem = 0;
+  for (int i = 0; i < B->n; ++i) {
+    CoarseArgs a = fps[i].coarse;
+    a.ctl = B->plans[i]->ctl;
+    coarse.push_back(a);
+    B->coarse_smem = std::max(B->coarse_smem, fps[i].coarse_smem);
+  }
+  B->off_coarse = put_blob(B->blob, coarse.data(), coarse.size() * sizeof(CoarseArgs));
+  std::vector<BatchCg> cg;
+  std::vector<BatchBlock> red, ew;
+  for (int i = 0; i < B->n; ++i) {
+    mg_plan* P = B->plans[i];
+    BatchCg c;
+    c.L0 = P->lv[0];
+    c.b = fptr(P, MG_FIELD_B);
+    c.x = fptr(P, MG_FIELD_X);
+    c.p = fptr(P, MG_FIELD_P);
+    c.Ap = fptr(P, MG_FIELD_AP);
+    c.xh = xhptr(P);
+    c.ctl = P->ctl;
+    c.partials = P->partials;
+    c.s0 = P->offdiag[0];
+    c.by4 = x_by4(P) ? 1 : 0;
+    c.c4 = P->geom[0].count % 4 == 0 ? 1 : 0;
+    c.refresh = P->d.refresh_every > 0 ? 1 : 0;
+    c.refresh_every = P->d.refresh_every;
+    c.flex = c.refresh && P->d.storage != MG_STORE_F32 ? 1 : 0;
+    cg.push_back(c);
+    for (int b = 0; b < P->red_blocks; ++b) red.push_back({i, b, P->red_blocks});
+    for (int b = 0; b < P->ew_blocks[0]; ++b) ew.push_back({i, b, P->ew_blocks[0]});
+  }
+  B->off_cg = put_blob(B->blob, cg.data(), cg.size() * sizeof(BatchCg));
+  B->off_red = put_blob(B->blob, red.data(), red.size() * sizeof(BatchBlock));
+  B->off_ew = put_blob(B->blob, ew.data(), ew.size() * sizeof(BatchBlock));
+  B->red_total = (int)red.size();
+  B->ew_total = (int)ew.size();
+  const int zero = 0;
+  B->off_any = put_blob(B->blob, &zero, sizeof(int));
+  B->ws_bytes = align256((int64_t)B->blob.size());
+}
+
+template <typename T>
+const T* bptr(const mg_batch* B, int64_t off) { return (const T*)(B->base + off); }
+
+template <typename ST, bool PRE>
+cudaError_t launch_bt_group(const mg_batch* B, const mg_batch::Group& g, cudaStream_t s) {
+  const BatchBlock* tab = bptr<BatchBlock>(B, g.tab_off);
+  const SweepArgs<ST>* args = bptr<SweepArgs<ST>>(B, g.args_off);
+  constexpr int NS = 4;
+  if (g.dim == 3) {
+    constexpr TileShape T = kTile3;
+    if (g.one) {
+      constexpr int K = 2 + 2 * NS;
+      auto kern = k_bt_sweep<3, ST, NS, T.tx, T.ty, PRE, T.nt, K>;
+      const size_t smem = sweep_smem(3, NS, {T.tx, T.ty, T.nt, K}, true, false);
+      cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+      if (e != cudaSuccess) return e;
+      return launch_k(kern, g.blocks, T.nt, smem, s, tab, args);
+    }
+    auto kern = k_bt_sweep<3, ST, NS, T.tx, T.ty, PRE, T.nt, T.k>;
+    const size_t smem = sweep_smem(3, NS, T, false, false);
+    cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return e;
+    return launch_k(kern, g.blocks, T.nt, smem, s, tab, args);
+  }
+  constexpr TileShape T = kTile2;
+  auto kern = k_bt_sweep<2, ST, NS, T.tx, T.ty, PRE, T.nt, T.k>;
+  const size_t smem = sweep_smem(2, NS, T, false, false);
+  cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (e != cudaSuccess) return e;
+  return launch_k(kern, g.blocks, T.nt, smem, s, tab, args);
+}
+
+// One V-cycle of every instance (the stages in the order of the tables).
+template <typename ST>
+int launch_bt_vcycle(mg_batch* B, cudaStream_t s) {
+  bool coarse_done = false;
+  for (const auto& g : B->groups) {
+    if (!g.pre && !coarse_done) {
+      auto kern = k_bt_coarse<ST>;
+      CK(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)B->coarse_smem));
+      CK(launch_k(kern, B->n, kCoarseThreads, B->coarse_smem, s, bptr<CoarseArgs>(B, B->off_coarse)));
+      coarse_done = true;
+    }
+    cudaError_t e = g.pre ? launch_bt_group<ST, true>(B, g, s) : launch_bt_group<ST, false>(B, g, s);
+    if (e != cudaSuccess) return set_err("k_bt_sweep", e);
+  }
+  if (!coarse_done) {  // no streamed level in the batch
+    auto kern = k_bt_coarse<ST>;
+    CK(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)B->coarse_smem));
+    CK(launch_k(kern, B->n, kCoarseThreads, B->coarse_smem, s, bptr<CoarseArgs>(B, B->off_coarse)));
+  }
+  return MG_OK;
+}
+
+// The batch's PCG pass: the prologue (mgpcg.py:157-173) or one loop iteration
+// (mgpcg.py:175-209), for every instance.
+template <typename ST>
+int launch_bt_part(mg_batch* B, bool prologue, cudaStream_t s, int has_cond) {
+  const BatchBlock* red = bptr<BatchBlock>(B, B->off_red);
+  const BatchBlock* ew = bptr<BatchBlock>(B, B->off_ew);
+  const BatchCg* cg = bptr<BatchCg>(B, B->off_cg);
+  if (prologue) CK(launch_k(k_bt_begin, B->red_total, kRedThreads, 0, s, red, cg));
+  if (int rc = launch_bt_vcycle<ST>(B, s)) return rc;
+  if (prologue) {
+    CK(launch_k(k_bt_update_p<ST>, B->ew_total, 256, 0, s, ew, cg));
+    CK(launch_k(k_bt_zr<ST>, B->red_total, kRedThreads, 0, s, red, cg, 0));
+  } else {
+    CK(launch_k(k_bt_zr<ST>, B->red_total, kRedThreads, 0, s, red, cg, 1));
+    CK(launch_k(k_bt_update_p<ST>, B->ew_total, 256, 0, s, ew, cg));
+  }
+  CK(launch_k(k_bt_Ap, B->red_total, kRedThreads, 0, s, red, cg));
+  CK(launch_k(k_bt_xr, B->red_total, kRedThreads, 0, s, red, cg));
+  if (B->refresh) CK(launch_k(k_bt_refresh, B->red_total, kRedThreads, 0, s, red, cg));
+  int* any = (int*)(B->base + B->off_any);
+  CK(launch_k(k_bt_cond, 1, 256, 0, s, cg, B->n, B->cond, has_cond, any));
+  return MG_OK;
+}
+
+template <typename ST>
+int build_batch_graph(mg_batch* B) {
+  if (B->exec) cudaGraphExecDestroy(B->exec);
+  if (B->graph) cudaGraphDestroy(B->graph);
+  B->exec = nullptr;
+  B->graph = nullptr;
+  if (!B->cap) CK(cudaStreamCreateWithFlags(&B->cap, cudaStreamNonBlocking));
+  CK(cudaGraphCreate(&B->graph, 0));
+  CK(cudaGraphConditionalHandleCreate(&B->cond, B->graph, 0, cudaGraphCondAssignDefault));
+  CK(cudaStreamBeginCaptureToGraph(B->cap, B->graph, nullptr, nullptr, 0, cudaStreamCaptureModeRelaxed));
+  int rc = launch_bt_part<ST>(B, true, B->cap, 1);
+  if (rc) {
+    cudaGraph_t g;
+    cudaStreamEndCapture(B->cap, &g);
+    return rc;
+  }
+  cudaStreamCaptureStatus st;
+  const cudaGraphNode_t* deps = nullptr;
+  size_t ndeps = 0;
+  cudaGraph_t capg;
+  CK(cudaStreamGetCaptureInfo(B->cap, &st, nullptr, &capg, &deps, &ndeps));
+  cudaGraphNodeParams cp = {};
+  cp.type = cudaGraphNodeTypeConditional;
+  cp.conditional.handle = B->cond;
+  cp.conditional.type = cudaGraphCondTypeWhile;
+  cp.conditional.size = 1;
+  cudaGraphNode_t cnode;
+  CK(cudaGraphAddNode(&cnode, capg, deps, ndeps, &cp));
+  cudaGraph_t body = cp.conditional.phGraph_out[0];
+  CK(cudaStreamUpdateCaptureDependencies(B->cap, &cnode, 1, cudaStreamSetCaptureDependencies));
+  cudaGraph_t out;
+  CK(cudaStreamEndCapture(B->cap, &out));
+  CK(cudaStreamBeginCaptureToGraph(B->cap, body, nullptr, nullptr, 0, cudaStreamCaptureModeRelaxed));
+  rc = launch_bt_part<ST>(B, false, B->cap, 1);
+  {
+    cudaGraph_t g2;
+    cudaError_t e = cudaStreamEndCapture(B->cap, &g2);
+    if (rc) return rc;
+    if (e != cudaSuccess) return set_err("cudaStreamEndCapture(batch body)", e);
+  }
+  CK(cudaGraphInstantiate(&B->exec, B->graph, 0));
+  return MG_OK;
+}
+
+int build_batch_graph_any(mg_batch* B) {
+  switch (B->storage) {
+    case MG_STORE_F16: return build_batch_graph<__half>(B);
+    case MG_STORE_BF16: return build_batch_graph<__nv_bfloat16>(B);
+    default: return build_batch_graph<float>(B);
+  }
+}
+
+}  // namespace
+
+extern "C" {
+
+int mg_batch_create(mg_plan_t* const* plans, int32_t n, mg_batch_t** out) {
+  if (!plans || !out || n < 1) return bad("mg_batch_create: plans / count / out");
+  *out = nullptr;
+  mg_batch* B = new (std::nothrow) mg_batch();
+  if (!B) return bad("mg_batch_create: out of host memory");
+  B->n = n;
+  for (int i = 0; i < n; ++i) {
+    mg_plan* P = plans[i];
+    if (!P || !P->base) {
+      delete B;
+      return bad("mg_batch_create: every plan must be bound");
+    }
+    if (!P->prepared || !P->fp.valid || P->fp.sto) {
+      delete B;
+      return bad("mg_batch_create: every plan must be prepared in the label-uniform fused form");
+    }
+    if (P->d.pre_post != 2) {
+      delete B;
+      return bad("mg_batch_create: batched sweeps run pre_and_post_smoothing = 2");
+    }
+    if (i > 0 && (P->d.storage != plans[0]->d.storage || P->device != plans[0]->device)) {
+      delete B;
+      return bad("mg_batch_create: every plan must have the same storage type and device");
+    }
+    B->plans.push_back(P);
+    B->sigs.push_back(P->graph_sig);
+  }
+  B->storage = plans[0]->d.storage;
+  B->refresh = plans[0]->d.refresh_every > 0;
+  for (auto* P : B->plans) B->refresh = B->refresh || P->d.refresh_every > 0;
+  switch (B->storage) {
+    case MG_STORE_F16: batch_tables<__half>(B); break;
+    case MG_STORE_BF16: batch_tables<__nv_bfloat16>(B); break;
+    default: batch_tables<float>(B);
+  }
+  *out = B;
+  return MG_OK;
+}
+
+void mg_batch_destroy(mg_batch_t* B) {
+  if (!B) return;
+  if (B->exec) cudaGraphExecDestroy(B->exec);
+  if (B->graph) cudaGraphDestroy(B->graph);
+  if (B->cap) cudaStreamDestroy(B->cap);
+  delete B;
+}
+
+int64_t mg_batch_workspace_bytes(const mg_batch_t* B) { return B ? B->ws_bytes : 0; }
+
+int mg_batch_bind(mg_batch_t* B, void* workspace, void* stream) {
+  if (!B || !workspace) return bad("mg_batch_bind: null pointer");
+  if ((uintptr_t)workspace & 255) return bad("mg_batch_bind: workspace not 256-byte aligned");
+  B->base = (char*)workspace;
+  CK(cudaMemcpyAsync(B->base, B->blob.data(), B->blob.size(), cudaMemcpyHostToDevice, S(stream)));
+  CK(cudaStreamSynchronize(S(stream)));
+  return build_batch_graph_any(B);
+}
+
+int mg_batch_solve_async(mg_batch_t* B, const mg_solve_params_t* prm, void* stream) {
+  if (!B || !prm) return bad("mg_batch_solve_async: null pointer");
+  if (!B->base || !B->exec) return bad("mg_batch_solve_async: batch not bound");
+  if (prm->max_iters < -1) return bad("max_iters");
+  for (int i = 0; i < B->n; ++i)
+    if (B->plans[i]->graph_sig != B->sigs[i] || !B->plans[i]->prepared)
+      return bad("mg_batch_solve_async: an instance's plan changed shape since mg_batch_create");
+  const BatchCg* cg = bptr<BatchCg>(B, B->off_cg);
+  k_bt_params<<<(B->n + 127) / 128, 128, 0, S(stream)>>>(cg, B->n, *prm);
+  CKL("k_bt_params");
+  CK(cudaGraphLaunch(B->exec, S(stream)));
+  return MG_OK;
+}
+
+int mg_batch_launch_counts(const mg_batch_t* B, int32_t* prologue, int32_t* body) {
+  if (!B || !prologue || !body) return bad("null pointer");
+  const int v = (int)B->groups.size() + 1;  // sweep groups + the coarse launch
+  const int cg = 4 + (B->refresh ? 1 : 0) + 1;  // zr, update_p, Ap, xr, [refresh], cond
+  *prologue = 1 + v + cg;
+  *body = v + cg;
+  return MG_OK;
 }
 
 }  // extern "C"

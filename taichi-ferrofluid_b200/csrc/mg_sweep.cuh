@@ -107,8 +107,7 @@ __device__ __forceinline__ void ld4_r(const void* r, long long i, int r_f32, flo
 // with the same operation order, and a neighbour outside the grid is loaded
 // as z = 0, Ax = 0 (rule H1).
 template <int DIM, typename ST, int NS, int TX, int TY, bool PRE, int NT, int K, bool STO = false>
-__global__ void __launch_bounds__(NT) k_sweep(SweepArgs<ST> A) {
-  pdl_enter();
+__device__ __forceinline__ void sweep_body(const SweepArgs<ST>& A, int bid_, int nb_) {
   static_assert(!STO || sizeof(ST) == 4, "the stored form runs on float32 grids");
   // halos: NS cells are needed on each side; along the fastest axis the halo
   // is rounded up to 4 so every 4-wide group starts 16-byte (float) / 8-byte
@@ -145,8 +144,8 @@ __global__ void __launch_bounds__(NT) k_sweep(SweepArgs<ST> A) {
   const int nx = DIM == 3 ? n2 : n1;             // in-plane fastest extent (multiple of 4)
   const int ny = DIM == 3 ? n1 : 1;
   const int ntile = A.tiles_x * A.tiles_y;
-  const int tile = blockIdx.x % ntile;
-  const int chunk_id = blockIdx.x / ntile;
+  const int tile = bid_ % ntile;
+  const int chunk_id = bid_ / ntile;
   const int tx0 = (tile % A.tiles_x) * TX;        // interior origin in the plane
   const int ty0 = DIM == 3 ? (tile / A.tiles_x) * TY : 0;
   const int z0 = chunk_id * A.chunk;
@@ -478,7 +477,8 @@ __global__ void __launch_bounds__(NT) k_sweep(SweepArgs<ST> A) {
       __shared__ double sh[32];
       double tot;
       Control* ctl = A.zr_ctl;
-      if (last_block_total<NT>(zr_acc, A.zr_partials, &ctl->counter[1], sh, &tot) && threadIdx.x == 0) {
+      if (last_block_total_at<NT>(zr_acc, A.zr_partials, &ctl->counter[1], sh, &tot, bid_, nb_) &&
+          threadIdx.x == 0) {
         if (A.zr == 0) {
           ctl->old_zTr = tot;
           if (ctl->max_iters == 0) ctl->run = 0;
@@ -492,6 +492,12 @@ __global__ void __launch_bounds__(NT) k_sweep(SweepArgs<ST> A) {
       }
     }
   }
+}
+
+template <int DIM, typename ST, int NS, int TX, int TY, bool PRE, int NT, int K, bool STO = false>
+__global__ void __launch_bounds__(NT) k_sweep(SweepArgs<ST> A) {
+  pdl_enter();
+  sweep_body<DIM, ST, NS, TX, TY, PRE, NT, K, STO>(A, (int)blockIdx.x, (int)gridDim.x);
 }
 
 }  // namespace mg

@@ -1,5 +1,11 @@
 """Batched solves of many independent pressure problems of uneven sizes.
 
+Two forms.  ``solve_batched``: one kernel launch per V-cycle stage and CG
+step for ALL instances, driven by per-instance tables of blocks, the whole
+PCG loop in one CUDA graph that runs while any instance is unconverged
+(mg_batch_* in the library).  ``solve``: each instance's own graph on a pool
+of streams (below).
+
 Every instance keeps its own solver plan and workspace resident on the device
 (its multigrid hierarchy, its previous pressure) and is solved by ONE library
 call, ``mg_pressure_solve_async``: reinitialize(cell_type, strategy) + the
@@ -37,6 +43,11 @@ class Instance:
     def workspace_bytes(self):
         return self.solver.workspace.numel()
 
+    def setup(self, stream, warm_start=False):
+        sc = self.scene
+        self.solver.pressure_setup_async(self.ct, self.vel, self.phi, sc.p0, sc.scale_A, sc.scale_b, True,
+                                         sc.gfm_clamp, warm_start=warm_start, stream=stream)
+
     def launch(self, stream, max_iters, rel_tol, warm_start=False):
         sc = self.scene
         self.solver.pressure_solve_async(self.ct, self.vel, self.phi, sc.p0, sc.scale_A, sc.scale_b, True,
@@ -64,6 +75,7 @@ class BatchSolver:
         self.streams = [torch.cuda.Stream(self.device) for _ in range(streams)]
         # largest instances first: the long solves start early
         self.order = sorted(range(len(self.instances)), key=lambda i: -self.instances[i].scene.cells)
+        self._batch = None
 
     @property
     def workspace_bytes(self):
@@ -87,6 +99,58 @@ class BatchSolver:
         torch.cuda.synchronize(self.device)
         stats = [inst.solver.stats() for inst in self.instances]
         return e0.elapsed_time(e1), stats
+
+    def solve_batched(self, max_iters=500, rel_tol=1e-12, warm_start=False):
+        """Every instance's system built (one library call each, no host
+        synchronisation), then ONE batched solve: one kernel launch per
+        V-cycle stage and CG step for all instances, driven by tables of
+        (instance, block), the whole loop in one CUDA graph (mg_batch_*).
+        Returns (device ms from the first set-up to the end, stats)."""
+        main = torch.cuda.current_stream(self.device)
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(main)
+        for i in self.order:
+            self.instances[i].setup(main, warm_start)
+        if self._batch is None:
+            self._make_batch(main)
+        prm = mg_lib.SolveParams()
+        prm.max_iters = int(max_iters)
+        prm.rel_tol = float(rel_tol)
+        prm.abs_tol = 1e-14
+        prm.eps = 1e-12
+        prm.warm_start = 1 if warm_start else 0
+        mg_lib.check(self._lib.mg_batch_solve_async(self._batch, mg_lib.ctypes.byref(prm), main.cuda_stream),
+                     "mg_batch_solve_async")
+        e1.record(main)
+        torch.cuda.synchronize(self.device)
+        stats = [inst.solver.stats() for inst in self.instances]
+        return e0.elapsed_time(e1), stats
+
+    def _make_batch(self, stream):
+        """Tables and graph of the batched solve, from the instances' prepared
+        plans (their launch shapes are fixed once a shape is prepared)."""
+        self._lib = mg_lib.load()
+        arr = (mg_lib.ctypes.c_void_p * len(self.instances))(*[i.solver.plan.value for i in self.instances])
+        b = mg_lib.ctypes.c_void_p()
+        torch.cuda.synchronize(self.device)  # the plans are prepared
+        mg_lib.check(self._lib.mg_batch_create(arr, len(self.instances), mg_lib.ctypes.byref(b)), "mg_batch_create")
+        self._batch = b
+        n = int(self._lib.mg_batch_workspace_bytes(b))
+        self._batch_ws = torch.empty(max(n, 256), dtype=torch.uint8, device=self.device)
+        mg_lib.check(self._lib.mg_batch_bind(b, self._batch_ws.data_ptr(), stream.cuda_stream), "mg_batch_bind")
+
+    def batch_launch_counts(self):
+        a, c = mg_lib.ctypes.c_int32(), mg_lib.ctypes.c_int32()
+        mg_lib.check(self._lib.mg_batch_launch_counts(self._batch, mg_lib.ctypes.byref(a), mg_lib.ctypes.byref(c)),
+                     "mg_batch_launch_counts")
+        return int(a.value), int(c.value)
+
+    def __del__(self):
+        b = getattr(self, "_batch", None)
+        if b is not None and b.value:
+            self._lib.mg_batch_destroy(b)
+            self._batch = None
 
     def solve_one_at_a_time(self, max_iters=500, rel_tol=1e-12):
         """The plain form: each instance reinitialized and solved (blocking) in turn."""

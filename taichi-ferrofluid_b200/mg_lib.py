@@ -107,6 +107,14 @@ _SIGS = {
     "mg_plan_prepare_declared": (ctypes.c_int, [_vp, ctypes.POINTER(_f32), _vp]),
     "mg_pressure_solve_async": (ctypes.c_int, [_vp, _vp, _vp, _vp, _vp, _vp, _f32, _f32, _f32, _i32, _f32,
                                                ctypes.c_void_p, _vp]),
+    "mg_pressure_setup_async": (ctypes.c_int, [_vp, _vp, _vp, _vp, _vp, _vp, _f32, _f32, _f32, _i32, _f32, _i32,
+                                               _vp]),
+    "mg_batch_create": (ctypes.c_int, [ctypes.POINTER(_vp), _i32, ctypes.POINTER(_vp)]),
+    "mg_batch_destroy": (None, [_vp]),
+    "mg_batch_workspace_bytes": (ctypes.c_int64, [_vp]),
+    "mg_batch_bind": (ctypes.c_int, [_vp, _vp, _vp]),
+    "mg_batch_solve_async": (ctypes.c_int, [_vp, ctypes.POINTER(SolveParams), _vp]),
+    "mg_batch_launch_counts": (ctypes.c_int, [_vp, ctypes.POINTER(_i32), ctypes.POINTER(_i32)]),
     "mg_plan_operator_form": (ctypes.c_int, [_vp, _i32, ctypes.POINTER(_i32)]),
     "mg_plan_split": (ctypes.c_int, [_vp, _i32, ctypes.POINTER(ctypes.c_uint32), ctypes.POINTER(_i32)]),
     "mg_plan_steps": (ctypes.c_int, [_vp, _i32, ctypes.POINTER(ctypes.c_uint32)]),

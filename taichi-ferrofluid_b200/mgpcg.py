@@ -327,6 +327,18 @@ class MGPCGPoissonSolver:
             mg_lib.ptr(phi), float(p0), float(scale_A), float(scale_b), int(bool(ghost_fluid_method)),
             float(gfm_clamp), mg_lib.ctypes.byref(prm), s), "mg_pressure_solve_async")
 
+    def pressure_setup_async(self, cell_type, velocity, phi, p0, scale_A, scale_b, ghost_fluid_method=True,
+                             gfm_clamp=1e3, warm_start=False, stream=None):
+        """The system half of pressure_solve_async (labels, b, A, coarse
+        labels, declared operator form) with no solve: a batch solve
+        (mg_batch.BatchSolver.solve_batched) runs the PCG loops of many."""
+        v2 = velocity[2] if self.dim == 3 else None
+        s = stream.cuda_stream if stream is not None else self._s()
+        check(self.lib.mg_pressure_setup_async(
+            self.plan, cell_type.data_ptr(), velocity[0].data_ptr(), velocity[1].data_ptr(), mg_lib.ptr(v2),
+            mg_lib.ptr(phi), float(p0), float(scale_A), float(scale_b), int(bool(ghost_fluid_method)),
+            float(gfm_clamp), int(bool(warm_start)), s), "mg_pressure_setup_async")
+
     def launch_counts(self):
         """(kernels before the PCG loop, kernels per further iteration)."""
         a, b = mg_lib.ctypes.c_int32(), mg_lib.ctypes.c_int32()

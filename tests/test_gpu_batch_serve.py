@@ -38,7 +38,9 @@ def test_batch_equals_alone(storage):
 def test_batch_plain_matches_oracle():
     """Every instance of the 96-scene uneven batch (64 2D sides 64..512, 32 3D
     sides 32..160, level counts as the batch bench uses them), solved in one
-    batch, against the float32 oracle: iterations +-1, pressure within 1e-5."""
+    batch both ways (each instance's graph on a pool of streams, and the
+    batched kernels with one launch per stage for all instances), against the
+    float32 oracle: iterations +-1, pressure within 1e-5."""
     from helpers import oracle_for, rel_l2
     from mg_batch import BatchSolver
     from mg_serve import levels_for
@@ -47,16 +49,50 @@ def test_batch_plain_matches_oracle():
     assert len(scenes) == 96
     batch = BatchSolver(scenes, storage="f32", streams=32)
     _, stats = batch.solve()
+    xs = [inst.solver.x.cpu().numpy() for inst in batch.instances]
+    _, stats_b = batch.solve_batched()
+    xb = [inst.solver.x.cpu().numpy() for inst in batch.instances]
     worst = 0.0
-    for inst, st in zip(batch.instances, stats):
-        assert st.status == 0, (inst.scene.name, st.status)
+    for inst, st, stb, x, x2 in zip(batch.instances, stats, stats_b, xs, xb):
+        assert st.status == 0 and stb.status == 0, (inst.scene.name, st.status, stb.status)
         o = oracle_for(inst.scene)
         it_o = o.solve(500)
-        assert abs(st.iters - it_o) <= 1, (inst.scene.name, st.iters, it_o)
-        e = rel_l2(inst.solver.x.cpu().numpy(), o.get("x"))
-        assert e < 1e-5, (inst.scene.name, e)
-        worst = max(worst, e)
+        for it, xx in ((st.iters, x), (stb.iters, x2)):
+            assert abs(it - it_o) <= 1, (inst.scene.name, it, it_o)
+            e = rel_l2(xx, o.get("x"))
+            assert e < 1e-5, (inst.scene.name, e)
+            worst = max(worst, e)
     print(f"96-instance batch vs oracle: worst rel L2 {worst:.2e}")
+
+
+@pytest.mark.parametrize("storage", ["f32", "f16", "bf16"])
+def test_batched_kernels_match_alone(storage):
+    """The batched kernels (tables of blocks, one launch per stage for every
+    instance, one graph) give each instance the solve it gets alone: the same
+    V-cycle arithmetic and reduction blocks, the z.r sum in its own kernel
+    rather than inside the level-0 sweep (so the FP64 sums may part by an
+    ulp): iterations +-1 and x within 1e-5.  Repeated and warm-started batch
+    solves converge too."""
+    from helpers import rel_l2
+    from mg_batch import BatchSolver
+    scenes = _small_batch_scenes()
+    batch = BatchSolver(scenes, storage=storage, streams=4)
+    _, stats = batch.solve_batched()
+    assert all(st.status == 0 for st in stats), [st.status for st in stats]
+    xs = [inst.solver.x.clone() for inst in batch.instances]
+    its = [st.iters for st in stats]
+    pro, body = batch.batch_launch_counts()
+    assert body < 4 * len(scenes)  # one launch per stage, not per instance
+    _, again = batch.solve_batched()
+    assert [st.iters for st in again] == its
+    for inst, x in zip(batch.instances, xs):
+        assert torch.equal(inst.solver.x, x)
+    _, warm = batch.solve_batched(warm_start=True)
+    assert all(st.status == 0 and st.iters <= 2 for st in warm), [(st.status, st.iters) for st in warm]
+    for inst, x, it in zip(batch.instances, xs, its):
+        it_alone = inst.solve_blocking(500, 1e-12)
+        assert abs(it_alone - it) <= 1, (inst.scene.name, it_alone, it)
+        assert rel_l2(inst.solver.x.cpu().numpy(), x.cpu().numpy()) < 1e-5, inst.scene.name
 
 
 def _specs(n=6, substeps=4):
