@@ -84,26 +84,67 @@ __device__ __forceinline__ void tma_load_3d(void* dst, const CUtensorMap* map, u
 // ---- shape of one instantiation -------------------------------------------------------
 template <typename ST, int NS, int TX, int TY>
 struct ColGeom {
-  // x halo: NS rounded up so that the region's first column is a multiple of
-  // 16 bytes for every array (4 float32 / 8 16-bit cells)
-  static constexpr int HX = (sizeof(ST) == 4 && NS <= 4) ? 4 : 8;
-  static constexpr int RX = TX + 2 * HX;     // region columns
+  // x halo of the TMA box: NS rounded up so that the box's first column is a
+  // multiple of 16 bytes for every array (4 float32 / 8 16-bit cells); the
+  // threads cover only NS columns of it (the rest is loaded, never used)
+  static constexpr int HB = (sizeof(ST) == 4 && NS <= 4) ? 4 : 8;
+  static constexpr int HX = NS;              // x halo of the threads' region
+  static constexpr int RXB = TX + 2 * HB;    // box columns (TMA slots)
+  static constexpr int RX = TX + 2 * HX;     // region columns (threads, shared z planes)
   static constexpr int RY = TY + 2 * NS;     // region rows (even)
+  static constexpr int PLB = RXB * RY;       // cells of a box plane
   static constexpr int PLC = RX * RY;        // cells of a region plane
   static constexpr int PAIRS = RX * (RY / 2);
   static constexpr int NT = (PAIRS + 31) / 32 * 32;
   static constexpr int W = NS + 2;           // planes in registers = TMA ring slots = shared z planes
-  static constexpr int SLOT_R = (PLC * 4 + 127) / 128 * 128;               // r (float32 or ST)
-  static constexpr int SLOT_S = (PLC * (int)sizeof(ST) + 127) / 128 * 128;  // Adiag, input z (ST)
+  static constexpr int SLOT_R = (PLB * 4 + 127) / 128 * 128;               // r (float32 or ST)
+  static constexpr int SLOT_S = (PLB * (int)sizeof(ST) + 127) / 128 * 128;  // Adiag, input z (ST)
   static constexpr int ZPL = (PLC + 31) / 32 * 32;                         // floats of a shared z plane
   static constexpr int slot_bytes(bool pre) { return SLOT_R + SLOT_S * (pre ? 1 : 2); }
   static constexpr size_t smem(bool pre) {
     return 128 /* alignment */ + 128 /* mbarriers */ + (size_t)W * slot_bytes(pre) + (size_t)W * ZPL * 4;
   }
   static_assert(TX % 8 == 0 && TY % 2 == 0 && NS % 2 == 0, "even pairs, 16-byte TMA rows");
-  static_assert(RX <= 256 && RY <= 256, "TMA box extents");
+  static_assert(RXB <= 256 && RY <= 256, "TMA box extents");
   static_assert(W <= 16, "mbarriers in 128 bytes");
 };
+
+// One red-black update of a label-uniform cell from its six neighbours: the
+// two along axis 0, the two along the rows, the two along the fastest axis.
+// Exact: the reference's order (mgpcg.py:96-109) in float32, z = (r - sum_k
+// (-s) z_nb) / Adiag with six products, the axis pairs summed in turn and an
+// IEEE division.  FAST (16-bit grids): z = (r + s * sum z_nb) / Adiag with the
+// sum as a tree, one FMA and the approximate reciprocal.
+template <bool FAST>
+__device__ __forceinline__ float smooth_cell(float ms, float s, float r, float a, float z0m, float z0p, float z1m,
+                                             float z1p, float z2m, float z2p) {
+  if constexpr (FAST) {
+    const float sum = __fadd_rn(__fadd_rn(__fadd_rn(z0m, z0p), __fadd_rn(z1m, z1p)), __fadd_rn(z2m, z2p));
+    return __fdividef(fmaf(s, sum, r), a);
+  } else {
+    float ret = 0.0f;
+    ret = __fadd_rn(ret, __fadd_rn(__fmul_rn(ms, z0m), __fmul_rn(ms, z0p)));
+    ret = __fadd_rn(ret, __fadd_rn(__fmul_rn(ms, z1m), __fmul_rn(ms, z1p)));
+    ret = __fadd_rn(ret, __fadd_rn(__fmul_rn(ms, z2m), __fmul_rn(ms, z2p)));
+    return __fdiv_rn(__fsub_rn(r, ret), a);
+  }
+}
+
+// r - A z of one label-uniform cell (mgpcg.py:111-118), the same two forms.
+template <bool FAST>
+__device__ __forceinline__ float residual_cell(float ms, float s, float r, float a, float z, float z0m, float z0p,
+                                               float z1m, float z1p, float z2m, float z2p) {
+  if constexpr (FAST) {
+    const float sum = __fadd_rn(__fadd_rn(__fadd_rn(z0m, z0p), __fadd_rn(z1m, z1p)), __fadd_rn(z2m, z2p));
+    return fmaf(-a, z, fmaf(s, sum, r));
+  } else {
+    float ret = 0.0f;
+    ret = __fadd_rn(ret, __fadd_rn(__fmul_rn(ms, z0m), __fmul_rn(ms, z0p)));
+    ret = __fadd_rn(ret, __fadd_rn(__fmul_rn(ms, z1m), __fmul_rn(ms, z1p)));
+    ret = __fadd_rn(ret, __fadd_rn(__fmul_rn(ms, z2m), __fmul_rn(ms, z2p)));
+    return __fsub_rn(r, __fadd_rn(__fmul_rn(a, z), ret));
+  }
+}
 
 // ---------------------------------------------------------------------------
 // k_colsweep: PRE (z = 0, 2 pre_post half sweeps in colour order 0,1,..., then
@@ -117,6 +158,11 @@ __global__ void __launch_bounds__(ColGeom<ST, NS, TX, TY>::NT, MINB)
                const __grid_constant__ CUtensorMap tm_ad, const __grid_constant__ CUtensorMap tm_zin) {
   using G = ColGeom<ST, NS, TX, TY>;
   constexpr int HX = G::HX, RX = G::RX, RY = G::RY, W = G::W, NT = G::NT, ZPL = G::ZPL;
+  constexpr int RXB = G::RXB, XOFF = G::HB - G::HX;  // box columns; box column of region column 0
+  // the mixed form (16-bit grids) needs no bit-exact float32: a neighbour-sum
+  // tree, one FMA and the approximate reciprocal instead of six products,
+  // five dependent sums and an IEEE division
+  constexpr bool FAST = sizeof(ST) != 4;
   constexpr int SLOT = G::slot_bytes(PRE);
   constexpr int D = PRE ? NS - 1 : NS;  // steps from a plane's load to its final z
   pdl_enter();
@@ -140,13 +186,15 @@ __global__ void __launch_bounds__(ColGeom<ST, NS, TX, TY>::NT, MINB)
   const int p_first = z0 - NS;
   const int p_last = z1 + NS - 1;
   const int ox = tx0 - HX, oy = ty0 - NS;  // region origin (both even)
+  const int bx = tx0 - G::HB;               // TMA box origin along x (16-byte aligned)
   const float sigma = A.r_f32 ? (float)A.ctl->scale_r : 1.0f;
   const float ms = -F.s;
   const long long pstride = (long long)n1 * n2;
   const int ncx = A.nc[2], ncy = A.nc[1];
   const bool r32 = sizeof(ST) == 4 || A.r_f32;
   const uint32_t tx_bytes =
-      (uint32_t)(G::PLC * ((r32 ? 4 : (int)sizeof(ST)) + (int)sizeof(ST) * (PRE ? 1 : 2)));
+      (uint32_t)(G::PLB * ((r32 ? 4 : (int)sizeof(ST)) + (int)sizeof(ST) * (PRE ? 1 : 2)));
+  const float s_pos = F.s;
 
   // ---- this thread's pair of columns ----------------------------------------------------
   const int t = threadIdx.x;
@@ -159,8 +207,9 @@ __global__ void __launch_bounds__(ColGeom<ST, NS, TX, TY>::NT, MINB)
   const int yo = 2 * pr2 - 1, yu = 2 * pr2 + 2;          // the rows beyond the pair
   const int outA = min(max(odd ? yu : yo, 0), RY - 1);   // (clamped: such reads feed
   const int outB = min(max(odd ? yo : yu, 0), RY - 1);   //  only cells never smoothed)
-  const int cA = rowA * RX + rx, cB = rowB * RX + rx;
+  const int cA = rowA * RX + rx, cB = rowB * RX + rx;      // in a shared z plane
   const int oA = outA * RX + rx, oB = outB * RX + rx;
+  const int kA = rowA * RXB + rx + XOFF, kB = rowB * RXB + rx + XOFF;  // in a TMA slot
   const int xm = rx > 0 ? -1 : 0, xp = rx < RX - 1 ? 1 : 0;
   const int dx = max(max(HX - rx, rx - (HX + TX - 1)), 0);
   const int ringA = live ? max(dx, max(max(NS - rowA, rowA - (NS + TY - 1)), 0)) : 1 << 20;
@@ -181,9 +230,9 @@ __global__ void __launch_bounds__(ColGeom<ST, NS, TX, TY>::NT, MINB)
   auto issue = [&](int p, int slot) {  // TMA loads of plane p into a ring slot (thread 0)
     unsigned char* sl = slots + slot * SLOT;
     mbar_expect_tx(&bar[slot], tx_bytes);
-    tma_load_3d(sl, &tm_r, &bar[slot], ox, oy, p);
-    tma_load_3d(sl + G::SLOT_R, &tm_ad, &bar[slot], ox, oy, p);
-    if (!PRE) tma_load_3d(sl + G::SLOT_R + G::SLOT_S, &tm_zin, &bar[slot], ox, oy, p);
+    tma_load_3d(sl, &tm_r, &bar[slot], bx, oy, p);
+    tma_load_3d(sl + G::SLOT_R, &tm_ad, &bar[slot], bx, oy, p);
+    if (!PRE) tma_load_3d(sl + G::SLOT_R + G::SLOT_S, &tm_zin, &bar[slot], bx, oy, p);
   };
 
   if (t == 0) {
@@ -215,24 +264,24 @@ __global__ void __launch_bounds__(ColGeom<ST, NS, TX, TY>::NT, MINB)
         const unsigned char* sl = slots + u * SLOT;
         if (r32) {
           const float* sr = (const float*)sl;
-          rA[u] = sizeof(ST) == 4 ? sr[cA] : __fmul_rn(sigma, sr[cA]);
-          rB[u] = sizeof(ST) == 4 ? sr[cB] : __fmul_rn(sigma, sr[cB]);
+          rA[u] = sizeof(ST) == 4 ? sr[kA] : __fmul_rn(sigma, sr[kA]);
+          rB[u] = sizeof(ST) == 4 ? sr[kB] : __fmul_rn(sigma, sr[kB]);
         } else {
           const ST* sr = (const ST*)sl;
-          rA[u] = to_f<ST>(sr[cA]);
-          rB[u] = to_f<ST>(sr[cB]);
+          rA[u] = to_f<ST>(sr[kA]);
+          rB[u] = to_f<ST>(sr[kB]);
         }
         const ST* sa = (const ST*)(sl + G::SLOT_R);
-        aA[u] = to_f<ST>(sa[cA]);
-        aB[u] = to_f<ST>(sa[cB]);
+        aA[u] = to_f<ST>(sa[kA]);
+        aB[u] = to_f<ST>(sa[kB]);
         if constexpr (PRE) {
           // the first half sweep is pointwise (z = 0 before it): z = r / Adiag on
           // the colour-0 cell, the one active in this step
           if ((u & 1) == 0) {
-            zA[u] = aA[u] != 0.0f ? __fdiv_rn(rA[u], aA[u]) : 0.0f;
+            zA[u] = aA[u] != 0.0f ? (FAST ? __fdividef(rA[u], aA[u]) : __fdiv_rn(rA[u], aA[u])) : 0.0f;
             zB[u] = 0.0f;
           } else {
-            zB[u] = aB[u] != 0.0f ? __fdiv_rn(rB[u], aB[u]) : 0.0f;
+            zB[u] = aB[u] != 0.0f ? (FAST ? __fdividef(rB[u], aB[u]) : __fdiv_rn(rB[u], aB[u])) : 0.0f;
             zA[u] = 0.0f;
           }
         } else {
@@ -240,8 +289,8 @@ __global__ void __launch_bounds__(ColGeom<ST, NS, TX, TY>::NT, MINB)
           float c = 0.0f;
           if (in_grid && P >= 0 && P < n0)
             c = to_f<ST>(A.zc[((long long)(P >> 1) * ncy + (gy0 >> 1)) * ncx + (gx >> 1)]);
-          const float fa = __fadd_rn(to_f<ST>(si[cA]), __fmul_rn(A.pi, c));
-          const float fb = __fadd_rn(to_f<ST>(si[cB]), __fmul_rn(A.pi, c));
+          const float fa = __fadd_rn(to_f<ST>(si[kA]), __fmul_rn(A.pi, c));
+          const float fb = __fadd_rn(to_f<ST>(si[kB]), __fmul_rn(A.pi, c));
           zA[u] = aA[u] != 0.0f ? fa : 0.0f;
           zB[u] = aB[u] != 0.0f ? fb : 0.0f;
           // an owned non-FLUID cell is never smoothed: its output is this value
@@ -267,22 +316,16 @@ __global__ void __launch_bounds__(ColGeom<ST, NS, TX, TY>::NT, MINB)
         if ((u & 1) == 0) {
           const float a = aA[j];
           if (ringA <= NS - s && a != 0.0f) {
-            float ret = 0.0f;
-            ret = __fadd_rn(ret, __fadd_rn(__fmul_rn(ms, zA[jm]), __fmul_rn(ms, zA[jp])));
-            ret = __fadd_rn(ret, __fadd_rn(__fmul_rn(ms, zp[oA]), __fmul_rn(ms, zB[j])));
-            ret = __fadd_rn(ret, __fadd_rn(__fmul_rn(ms, zp[cA + xm]), __fmul_rn(ms, zp[cA + xp])));
-            const float v = __fdiv_rn(__fsub_rn(rA[j], ret), a);
+            const float v = smooth_cell<FAST>(ms, s_pos, rA[j], a, zA[jm], zA[jp], zp[oA], zB[j], zp[cA + xm],
+                                              zp[cA + xp]);
             zA[j] = v;
             zp[cA] = v;
           }
         } else {
           const float a = aB[j];
           if (ringB <= NS - s && a != 0.0f) {
-            float ret = 0.0f;
-            ret = __fadd_rn(ret, __fadd_rn(__fmul_rn(ms, zB[jm]), __fmul_rn(ms, zB[jp])));
-            ret = __fadd_rn(ret, __fadd_rn(__fmul_rn(ms, zp[oB]), __fmul_rn(ms, zA[j])));
-            ret = __fadd_rn(ret, __fadd_rn(__fmul_rn(ms, zp[cB + xm]), __fmul_rn(ms, zp[cB + xp])));
-            const float v = __fdiv_rn(__fsub_rn(rB[j], ret), a);
+            const float v = smooth_cell<FAST>(ms, s_pos, rB[j], a, zB[jm], zB[jp], zp[oB], zA[j], zp[cB + xm],
+                                              zp[cB + xp]);
             zB[j] = v;
             zp[cB] = v;
           }
@@ -319,20 +362,12 @@ __global__ void __launch_bounds__(ColGeom<ST, NS, TX, TY>::NT, MINB)
           const float* zp = zs + jr * ZPL;
           float vA = 0.0f, vB = 0.0f;
           const bool fA = ownA && aA[jr] != 0.0f, fB = ownB && aB[jr] != 0.0f;
-          if (fA) {
-            float ret = 0.0f;
-            ret = __fadd_rn(ret, __fadd_rn(__fmul_rn(ms, zA[jrm]), __fmul_rn(ms, zA[jrp])));
-            ret = __fadd_rn(ret, __fadd_rn(__fmul_rn(ms, zp[oA]), __fmul_rn(ms, zB[jr])));
-            ret = __fadd_rn(ret, __fadd_rn(__fmul_rn(ms, zp[cA + xm]), __fmul_rn(ms, zp[cA + xp])));
-            vA = __fsub_rn(rA[jr], __fadd_rn(__fmul_rn(aA[jr], zA[jr]), ret));
-          }
-          if (fB) {
-            float ret = 0.0f;
-            ret = __fadd_rn(ret, __fadd_rn(__fmul_rn(ms, zB[jrm]), __fmul_rn(ms, zB[jrp])));
-            ret = __fadd_rn(ret, __fadd_rn(__fmul_rn(ms, zp[oB]), __fmul_rn(ms, zA[jr])));
-            ret = __fadd_rn(ret, __fadd_rn(__fmul_rn(ms, zp[cB + xm]), __fmul_rn(ms, zp[cB + xp])));
-            vB = __fsub_rn(rB[jr], __fadd_rn(__fmul_rn(aB[jr], zB[jr]), ret));
-          }
+          if (fA)
+            vA = residual_cell<FAST>(ms, s_pos, rA[jr], aA[jr], zA[jr], zA[jrm], zA[jrp], zp[oA], zB[jr],
+                                     zp[cA + xm], zp[cA + xp]);
+          if (fB)
+            vB = residual_cell<FAST>(ms, s_pos, rB[jr], aB[jr], zB[jr], zB[jrm], zB[jrp], zp[oB], zA[jr],
+                                     zp[cB + xm], zp[cB + xp]);
           // rows y0 (even) and y1 of this column; the x + 1 column is the next lane
           const float v0 = odd ? vB : vA, v1 = odd ? vA : vB;
           const int f = odd ? ((int)fB | ((int)fA << 1)) : ((int)fA | ((int)fB << 1));

@@ -524,9 +524,9 @@ inline cudaError_t launch_col_t(const FusedPlan& F, const Level* lv, int l, cons
   const Level& f = lv[l];
   CUtensorMap tr, ta, tz;
   std::memset(&tz, 0, sizeof(tz));
-  if (!tensor_map_3d(&tr, f.r, l == 0 ? 4 : (int)sizeof(ST), f.g, G::RX, G::RY) ||
-      !tensor_map_3d(&ta, f.Adiag_s, (int)sizeof(ST), f.g, G::RX, G::RY) ||
-      (!PRE && !tensor_map_3d(&tz, f.zt, (int)sizeof(ST), f.g, G::RX, G::RY)))
+  if (!tensor_map_3d(&tr, f.r, l == 0 ? 4 : (int)sizeof(ST), f.g, G::RXB, G::RY) ||
+      !tensor_map_3d(&ta, f.Adiag_s, (int)sizeof(ST), f.g, G::RXB, G::RY) ||
+      (!PRE && !tensor_map_3d(&tz, f.zt, (int)sizeof(ST), f.g, G::RXB, G::RY)))
     return cudaErrorInvalidValue;
   if (PRE) tz = ta;  // unused by PRE
   auto kern = k_colsweep<ST, NS, TX, TY, PRE, MINB>;

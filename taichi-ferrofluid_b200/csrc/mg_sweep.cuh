@@ -138,6 +138,10 @@ __device__ __forceinline__ void sweep_body(const SweepArgs<ST>& A, int bid_, int
   float* sx1 = sx0 + W * PL;                      // STO, 3D: Ax[1] (rows)
   float* sxx = DIM == 3 ? sx1 + W * PL : sx1;     // STO: Ax[dim-1] (fastest axis)
   constexpr int NX = STO ? DIM : 1;               // coefficient arrays loaded per cell
+  // 16-bit grids (the mixed form) need no bit-exact float32: the plain
+  // neighbour sum as a tree, one FMA and the approximate reciprocal (the
+  // column kernel's smooth_cell / residual_cell take the same operations)
+  constexpr bool FAST = sizeof(ST) != 4 && !STO;
 
   const FLevel<ST>& F = A.f;
   const int n0 = F.n[0], n1 = F.n[1], n2 = F.n[2];
@@ -210,7 +214,7 @@ __device__ __forceinline__ void sweep_body(const SweepArgs<ST>& A, int bid_, int
     for (int e = 0; e < 4; ++e) {
       if (PRE) {
         const bool c0 = ((p + gy + gx + e) & 1) == 0;
-        zv[e] = (c0 && a[e] != 0.0f) ? __fdiv_rn(r[e], a[e]) : 0.0f;
+        zv[e] = (c0 && a[e] != 0.0f) ? (FAST ? __fdividef(r[e], a[e]) : __fdiv_rn(r[e], a[e])) : 0.0f;
       } else {
         zv[e] = a[e] != 0.0f ? z[e] : 0.0f;
       }
@@ -278,6 +282,20 @@ __device__ __forceinline__ void sweep_body(const SweepArgs<ST>& A, int bid_, int
     return ret;
   };
 
+  const float spos = F.s;
+  auto zsum = [&](int sb, int sc, int sa_, int c) {
+    if constexpr (DIM == 3)
+      return __fadd_rn(__fadd_rn(__fadd_rn(sz[sb + c], sz[sa_ + c]), __fadd_rn(sz[sc + c - RX], sz[sc + c + RX])),
+                       __fadd_rn(sz[sc + c - 1], sz[sc + c + 1]));
+    else
+      return __fadd_rn(__fadd_rn(sz[sb + c], sz[sa_ + c]), __fadd_rn(sz[sc + c - 1], sz[sc + c + 1]));
+  };
+  // smooth (mgpcg.py:104-109) of the FLUID cell c with diagonal a and residual r
+  auto upd = [&](float r, int sb, int sc, int sa_, int c, float a) -> float {
+    if constexpr (FAST) return __fdividef(fmaf(spos, zsum(sb, sc, sa_, c), r), a);
+    else return __fdiv_rn(__fsub_rn(r, nsum(sb, sc, sa_, c)), a);
+  };
+
   float acc = 0.0f;                               // restriction accumulator (PRE)
   double zr_acc = 0.0;                            // z.r of the cells written (POST, A.zr >= 0)
   const int ct = threadIdx.x;                     // coarse in-plane cell of this thread
@@ -329,7 +347,7 @@ __device__ __forceinline__ void sweep_body(const SweepArgs<ST>& A, int bid_, int
                     2 * k + ((colour - org - row) & 1) < cols;
             const float a = ok[u] ? sa[cc[u]] : 0.0f;
             ok[u] = ok[u] && a != 0.0f;              // FLUID
-            val[u] = ok[u] ? __fdiv_rn(__fsub_rn(sr[cc[u]], nsum(sb, sc, sa_, cc[u] - sc)), a) : 0.0f;
+            val[u] = ok[u] ? upd(sr[cc[u]], sb, sc, sa_, cc[u] - sc, a) : 0.0f;
           }
 #pragma unroll
           for (int u = 0; u < 2; ++u)
@@ -357,7 +375,7 @@ __device__ __forceinline__ void sweep_body(const SweepArgs<ST>& A, int bid_, int
         ok[kp] = (int)threadIdx.x < rows * hc && cxr < cols && !(pm - 1 < p_first || pm < 0 || pm >= n0);
         const float a = ok[kp] ? sa[sc + c] : 0.0f;
         ok[kp] = ok[kp] && a != 0.0f;              // FLUID
-        val[kp] = ok[kp] ? __fdiv_rn(__fsub_rn(sr[sc + c], nsum(sb, sc, sa_, c)), a) : 0.0f;
+        val[kp] = ok[kp] ? upd(sr[sc + c], sb, sc, sa_, c, a) : 0.0f;
       }
 #pragma unroll
       for (int kp = 0; kp < K; ++kp)
@@ -380,7 +398,7 @@ __device__ __forceinline__ void sweep_body(const SweepArgs<ST>& A, int bid_, int
             if (cxr < cols) {
               const int c = (lo + row) * RX + (x0 + cxr);
               const float a = sa[sc + c];
-              if (a != 0.0f) sz[sc + c] = __fdiv_rn(__fsub_rn(sr[sc + c], nsum(sb, sc, sa_, c)), a);
+              if (a != 0.0f) sz[sc + c] = upd(sr[sc + c], sb, sc, sa_, c, a);
             }
           }
           continue;
@@ -402,7 +420,7 @@ __device__ __forceinline__ void sweep_body(const SweepArgs<ST>& A, int bid_, int
             ok[u] = j0 + u * NT < rows * hc && 2 * k + ((colour - org - row) & 1) < cols;
             const float a = ok[u] ? sa[sc + cc[u]] : 0.0f;
             ok[u] = ok[u] && a != 0.0f;              // FLUID
-            val[u] = ok[u] ? __fdiv_rn(__fsub_rn(sr[sc + cc[u]], nsum(sb, sc, sa_, cc[u])), a) : 0.0f;
+            val[u] = ok[u] ? upd(sr[sc + cc[u]], sb, sc, sa_, cc[u], a) : 0.0f;
           }
 #pragma unroll
           for (int u = 0; u < 2; ++u)
@@ -454,8 +472,14 @@ __device__ __forceinline__ void sweep_body(const SweepArgs<ST>& A, int bid_, int
             const int c = (DIM == 3 ? HY + 2 * ccy + o1 : 0) * RX + (HX + 2 * ccx + o2);
             const float a = sa[sc + c];
             if (a != 0.0f) {
-              const float Az = __fadd_rn(__fmul_rn(a, sz[sc + c]), nsum(sb, sc, sa_, c));
-              acc = __fadd_rn(acc, __fsub_rn(sr[sc + c], Az));
+              float res;  // r - A z (mgpcg.py:111-118)
+              if constexpr (FAST) {
+                res = fmaf(-a, sz[sc + c], fmaf(spos, zsum(sb, sc, sa_, c), sr[sc + c]));
+              } else {
+                const float Az = __fadd_rn(__fmul_rn(a, sz[sc + c]), nsum(sb, sc, sa_, c));
+                res = __fsub_rn(sr[sc + c], Az);
+              }
+              acc = __fadd_rn(acc, res);
             }
           }
         }
