@@ -197,10 +197,32 @@ __global__ void __launch_bounds__(ColGeom<ST, NS, TX, TY>::NT, MINB)
   const float s_pos = F.s;
 
   // ---- this thread's pair of columns ----------------------------------------------------
+  // Interior first: threads [0, TX * TY / 2) hold the tile's own pairs, one
+  // pair row of TX columns per TX threads (whole warps for TX = 32, 64); the
+  // halo pairs follow (the top and bottom bands of NS / 2 pair rows, then the
+  // left and right bands of HX columns).  A half sweep's active region shrinks
+  // towards the tile, so halo warps fall idle as a whole instead of idling
+  // lanes inside every warp; the residual runs on the interior warps only.
+  constexpr int NI = TX * (TY / 2), NB = (NS / 2) * RX;
   const int t = threadIdx.x;
   const bool live = t < G::PAIRS;
   const int tt = live ? t : 0;
-  const int rx = tt % RX, pr2 = tt / RX;
+  int rx, pr2;
+  if (tt < NI) {
+    pr2 = NS / 2 + tt / TX;
+    rx = HX + tt % TX;
+  } else if (tt < NI + NB) {
+    pr2 = (tt - NI) / RX;
+    rx = (tt - NI) % RX;
+  } else if (tt < NI + 2 * NB) {
+    pr2 = NS / 2 + TY / 2 + (tt - NI - NB) / RX;
+    rx = (tt - NI - NB) % RX;
+  } else {
+    const int h = tt - NI - 2 * NB;
+    pr2 = NS / 2 + h / (2 * HX);
+    const int k = h % (2 * HX);
+    rx = k < HX ? k : TX + k;
+  }
   const int gx = ox + rx, gy0 = oy + 2 * pr2;
   const int odd = rx & 1;                               // gx parity (ox even)
   const int rowA = 2 * pr2 + odd, rowB = 2 * pr2 + 1 - odd;  // A: x + y even
@@ -224,6 +246,14 @@ __global__ void __launch_bounds__(ColGeom<ST, NS, TX, TY>::NT, MINB)
   for (int j = 0; j < W; ++j) {
     zA[j] = 0.0f; zB[j] = 0.0f; rA[j] = 0.0f; rB[j] = 0.0f; aA[j] = 0.0f; aB[j] = 0.0f;
   }
+  // POST: the coarse z of the pair's column for plane p (prolongation), read
+  // one step ahead so its latency overlaps a step's work
+  auto zc_of = [&](int p) -> float {
+    return (!PRE && in_grid && p >= 0 && p < n0)
+               ? to_f<ST>(A.zc[((long long)(p >> 1) * ncy + (gy0 >> 1)) * ncx + (gx >> 1)])
+               : 0.0f;
+  };
+  float zc_next = zc_of(p_first);
   float acc = 0.0f;      // restriction accumulator (PRE, even-x threads)
   double zr_acc = 0.0;   // z.r of the cells written (POST, A.zr >= 0)
 
@@ -286,9 +316,8 @@ __global__ void __launch_bounds__(ColGeom<ST, NS, TX, TY>::NT, MINB)
           }
         } else {
           const ST* si = (const ST*)(sl + G::SLOT_R + G::SLOT_S);
-          float c = 0.0f;
-          if (in_grid && P >= 0 && P < n0)
-            c = to_f<ST>(A.zc[((long long)(P >> 1) * ncy + (gy0 >> 1)) * ncx + (gx >> 1)]);
+          const float c = zc_next;          // loaded during the previous step
+          zc_next = zc_of(P + 1);
           const float fa = __fadd_rn(to_f<ST>(si[kA]), __fmul_rn(A.pi, c));
           const float fb = __fadd_rn(to_f<ST>(si[kB]), __fmul_rn(A.pi, c));
           zA[u] = aA[u] != 0.0f ? fa : 0.0f;
