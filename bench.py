@@ -481,6 +481,8 @@ def gpu_arm(args, rank, world, local):
                             "streamed_levels": c.solver.split_levels()[1],
                             "one_plane_step_bits": c.solver.step_planes(),
                             "grid_extra_bits": c.solver.grid_extra(),
+                            "sweep_kernel_bits": c.solver.sweep_kernel(),
+                            "levels": c.solver.n_mg_levels, "pre_post": 2, "bottom": 50,
                             "cluster_from_level": c.solver.resident()[1] if c.solver.resident()[0] else None}
                    for c in cases},
         "last_rel_resid": rel, "last_status": status,
@@ -548,10 +550,48 @@ def batched_variant(dev, reps=3):
                                              "batch_ms": round(ms1, 3)}
         del b
         torch.cuda.empty_cache()
+    # the sweeps per level, bottom sweeps and level count chosen by measurement
+    # (mg_tune) per size class, instead of the fixed rule (2, 50, levels_for)
+    import mg_tune
+    per_scene, classes = mg_tune.tune_classes(scenes, "f32", dev, bottoms=(10, 50), reps=1)
+    b = mg_batch.BatchSolver(scenes, storage="f32", streams=32, device=dev, params=per_scene)
+    b.solve()
+    ms = min(b.solve()[0] for _ in range(reps))
+    _, st = b.solve()
+    bt["batched_tuned_f32"] = {"solves_per_s": round(len(scenes) / (ms * 1e-3), 1), "batch_ms": round(ms, 3),
+                               "form": "streams, tuned (levels, pre_post, bottom) per size class",
+                               "converged": sum(s.status == 0 for s in st), "iters_max": max(s.iters for s in st),
+                               "classes": {f"{k[0]}D-{['small', 'medium', 'large'][k[1]]}":
+                                           {"levels_offset": r["offset"], "pre_post": r["pre_post"],
+                                            "bottom": r["bottom"], "ms": r["ms"], "iters": r["iters"],
+                                            "tuned_on": r["scene"]} for k, r in classes.items()}}
+    del b
+    torch.cuda.empty_cache()
+    if all(pp == 2 for _, pp, _ in per_scene):  # the batched kernels run pre_post 2
+        for storage in ("f32", "f16"):
+            b = mg_batch.BatchSolver(scenes, storage=storage, streams=32, device=dev, params=per_scene)
+            b.solve_batched()
+            ms = min(b.solve_batched()[0] for _ in range(reps))
+            _, st = b.solve_batched()
+            bt[f"batched_kernels_tuned_{storage}"] = {
+                "solves_per_s": round(len(scenes) / (ms * 1e-3), 1), "batch_ms": round(ms, 3),
+                "form": "batched kernels, tuned (levels, pre_post, bottom) per size class",
+                "converged": sum(s.status == 0 for s in st), "iters_max": max(s.iters for s in st)}
+            del b
+            torch.cuda.empty_cache()
     base = bt["plain_f32_one_at_a_time"]["solves_per_s"]
-    bt["speedup_vs_plain"] = {k: round(bt[k]["solves_per_s"] / base, 2)
-                              for k in ("batched_f32", "batched_f16", "batched_kernels_f32", "batched_kernels_f16")}
+    bt["speedup_vs_plain"] = {k: round(bt[k]["solves_per_s"] / base, 2) for k in bt
+                              if k.startswith("batched_") and isinstance(bt[k], dict) and "solves_per_s" in bt[k]}
+    bt["tuned_params"] = per_scene_summary(scenes, per_scene)
     return bt
+
+
+def per_scene_summary(scenes, params):
+    """Distinct (dim, side) -> (levels, pre_post, bottom) of a tuned batch."""
+    out = {}
+    for sc, (L, pp, bot) in zip(scenes, params):
+        out[f"{sc.dim}D-{sc.res[0]}"] = [L, pp, bot]
+    return out
 
 
 SERVE_RATES_HZ = (100, 400, 1600, 6400)

@@ -253,7 +253,9 @@ inline bool make_resident_plan(FusedPlan* F, const Level* lv, int L, int pre_pos
     for (int l = lb; l < L; ++l) coarse_cells += padded_cells(lv[l].g);
     const long long coarse_floats = (3 * coarse_cells + 3) / 4 * 4;
     if (coarse_cells > kCoarseMaxCells) break;
-    for (int lp = lp_min; lp < lb && lp <= lp_max; ++lp) {
+    // the levels above the bricks run streamed, and only [0, lc) have
+    // streamed launch shapes: the bricks start at lc at the latest
+    for (int lp = lp_min; lp < lb && lp <= lp_max && lp <= F->lc; ++lp) {
       const int D = lb - lp;
       const Geom& g = lv[lp].g;
       bool halves = true;

@@ -67,11 +67,16 @@ class Instance:
 
 
 class BatchSolver:
-    def __init__(self, scenes, storage="f32", streams=16, device=None, levels=None, pre_post=2, bottom=50):
+    def __init__(self, scenes, storage="f32", streams=16, device=None, levels=None, pre_post=2, bottom=50,
+                 params=None):
+        """``params``: per scene (levels, pre_and_post_smoothing, bottom_smoothing),
+        e.g. mg_tune.tune_classes' choice; else ``levels`` (one value or one
+        per scene), ``pre_post`` and ``bottom`` for all."""
         self.device = torch.device(device) if device is not None else torch.device("cuda", torch.cuda.current_device())
-        self.instances = [Instance(sc, storage, self.device,
-                                   levels[i] if isinstance(levels, (list, tuple)) else levels, pre_post, bottom)
-                          for i, sc in enumerate(scenes)]
+        if params is None:
+            params = [(levels[i] if isinstance(levels, (list, tuple)) else levels, pre_post, bottom)
+                      for i in range(len(scenes))]
+        self.instances = [Instance(sc, storage, self.device, *params[i]) for i, sc in enumerate(scenes)]
         self.streams = [torch.cuda.Stream(self.device) for _ in range(streams)]
         # largest instances first: the long solves start early
         self.order = sorted(range(len(self.instances)), key=lambda i: -self.instances[i].scene.cells)

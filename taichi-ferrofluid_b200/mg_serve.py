@@ -36,7 +36,9 @@ FLUID, AIR, SOLID = mg_lib.FLUID, mg_lib.AIR, mg_lib.SOLID
 
 
 def plan_bytes(dim, res, levels, storage):
-    """Workspace bytes a solver of this shape needs (host-side computation)."""
+    """Workspace bytes a solver of this shape needs (host-side computation),
+    with the defaults MGPCGPoissonSolver takes (the mixed form's true-residual
+    refresh and its FP64 x)."""
     lib = mg_lib.load()
     d = mg_lib.PlanDesc()
     d.dim = dim
@@ -46,6 +48,7 @@ def plan_bytes(dim, res, levels, storage):
     d.pre_post = 2
     d.bottom = 50
     d.storage = mg_lib.STORE[storage]
+    d.refresh_every = 10 if d.storage != 0 else 0
     p = mg_lib.ctypes.c_void_p()
     mg_lib.check(lib.mg_plan_create(mg_lib.ctypes.byref(d), mg_lib.ctypes.byref(p)), "mg_plan_create")
     n = int(lib.mg_plan_workspace_bytes(p))
@@ -125,7 +128,11 @@ class Session:
 
 
 class SolveServer:
-    def __init__(self, storage="f16", streams=16, hbm_budget=120e9, device=None, max_iters=500, rel_tol=1e-12):
+    def __init__(self, storage="f16", streams=16, hbm_budget=120e9, device=None, max_iters=500, rel_tol=1e-12,
+                 params=None):
+        """``params(dim, side)`` -> (levels, pre_and_post_smoothing, bottom_smoothing)
+        of a session's solver (e.g. from mg_tune); default: levels_for, 2, 50."""
+        self.params = params or (lambda dim, side: (levels_for(dim, side), 2, 50))
         self.device = torch.device(device) if device is not None else torch.device("cuda", torch.cuda.current_device())
         self.storage = storage
         self.streams = [torch.cuda.Stream(self.device) for _ in range(streams)]
@@ -148,11 +155,11 @@ class SolveServer:
         allocation or graph build synchronises the device while serving."""
         need = {}
         for sp in specs:
-            key = (sp["dim"], sp["side"], levels_for(sp["dim"], sp["side"]))
+            key = (sp["dim"], sp["side"]) + tuple(self.params(sp["dim"], sp["side"]))
             need[key] = need.get(key, 0) + 1
         total = self.in_use + self.idle
         for key, n in sorted(need.items(), key=lambda kv: -kv[0][1]):
-            dim, side, L = key
+            dim, side, L, pp, bot = key
             if key not in self.bytes_of:
                 self.bytes_of[key] = plan_bytes(dim, (side,) * dim, L, self.storage)
             spec = next(sp for sp in specs if (sp["dim"], sp["side"]) == (dim, side))
@@ -164,7 +171,7 @@ class SolveServer:
                     break
                 total += self.bytes_of[key]
                 self.idle += self.bytes_of[key]
-                solver = MGPCGPoissonSolver(dim, (side,) * dim, L, 2, 50, storage=self.storage, device=self.device)
+                solver = MGPCGPoissonSolver(dim, (side,) * dim, L, pp, bot, storage=self.storage, device=self.device)
                 solver.pressure_solve_async(scene.ct, scene.vel, scene.phi, scene.p0, scene.scale_A, scene.scale_b,
                                             True, scene.gfm_clamp, max_iters=self.max_iters, rel_tol=self.rel_tol)
                 self.pool.setdefault(key, []).append(solver)
@@ -177,8 +184,8 @@ class SolveServer:
         return [DeviceScene(s, self.device) for s in sorted(specs, key=lambda s: s["t_arrive"])]
 
     def _acquire(self, dim, side):
-        L = levels_for(dim, side)
-        key = (dim, side, L)
+        L, pp, bot = self.params(dim, side)
+        key = (dim, side, L, pp, bot)
         if key not in self.bytes_of:
             self.bytes_of[key] = plan_bytes(dim, (side,) * dim, L, self.storage)
         need = self.bytes_of[key]
@@ -199,7 +206,7 @@ class SolveServer:
         self.in_use += need
         self.peak_in_use = max(self.peak_in_use, self.in_use)
         self.peak_resident = max(self.peak_resident, self.in_use + self.idle)
-        return MGPCGPoissonSolver(dim, (side,) * dim, L, 2, 50, storage=self.storage, device=self.device), key
+        return MGPCGPoissonSolver(dim, (side,) * dim, L, pp, bot, storage=self.storage, device=self.device), key
 
     def _evict(self, limit):
         """Frees idle pooled workspaces, largest first, until admitted + idle

@@ -136,3 +136,19 @@ def test_no_bricks_in_2d():
     from mg_lib import MGError
     with pytest.raises(MGError):
         g.resident(True)
+
+
+@pytest.mark.parametrize("n,levels", [(32, 4), (64, 5)])
+def test_hierarchy_down_to_4_cells(n, levels):
+    """A 3D hierarchy whose coarsest grid is 4^3 (the coarse block then holds
+    several levels): every V-cycle the autotuner may choose (streamed or the
+    cluster from a start level no deeper than the coarse block's first level)
+    launches, and the solve matches the oracle."""
+    sc = small_3d(n, levels=levels)
+    g, _ = gpu_for(sc)
+    it = g.solve(500)
+    assert g.last_status == "converged"
+    o = oracle_for(sc)
+    it_o = o.solve(500)
+    assert abs(it - it_o) <= 1
+    assert rel_l2(g.x.cpu().numpy(), o.get("x")) < 1e-5
