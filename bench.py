@@ -511,7 +511,9 @@ def variants(dev, reps=3):
     each against the plain FP32 one-at-a-time form on the same GPU
     (device-resident inputs; the batch and the precision solves are timed
     with CUDA events, serving by wall clock per request)."""
-    out = {"batched": batched_variant(dev, reps), "served": served_variant(dev)}
+    batched, classes = batched_variant(dev, reps)
+    import mg_tune
+    out = {"batched": batched, "served": served_variant(dev, tuned=mg_tune.class_params(classes))}
     out["precision256"], xs = precision_variant(dev)
     return out, xs
 
@@ -570,7 +572,12 @@ def batched_variant(dev, reps=3):
     if all(pp == 2 for _, pp, _ in per_scene):  # the batched kernels run pre_post 2
         for storage in ("f32", "f16"):
             b = mg_batch.BatchSolver(scenes, storage=storage, streams=32, device=dev, params=per_scene)
-            b.solve_batched()
+            try:
+                b.solve_batched()
+            except Exception as e:  # an instance outside the batched kernels' form
+                bt[f"batched_kernels_tuned_{storage}"] = {"skipped": str(e)[:200]}
+                del b
+                continue
             ms = min(b.solve_batched()[0] for _ in range(reps))
             _, st = b.solve_batched()
             bt[f"batched_kernels_tuned_{storage}"] = {
@@ -583,7 +590,7 @@ def batched_variant(dev, reps=3):
     bt["speedup_vs_plain"] = {k: round(bt[k]["solves_per_s"] / base, 2) for k in bt
                               if k.startswith("batched_") and isinstance(bt[k], dict) and "solves_per_s" in bt[k]}
     bt["tuned_params"] = per_scene_summary(scenes, per_scene)
-    return bt
+    return bt, classes
 
 
 def per_scene_summary(scenes, params):
@@ -597,7 +604,7 @@ def per_scene_summary(scenes, params):
 SERVE_RATES_HZ = (100, 400, 1600, 6400)
 
 
-def served_variant(dev, n_sessions=32, substeps=20):
+def served_variant(dev, n_sessions=32, substeps=20, tuned=None):
     """Open-loop Poisson arrivals of scene sessions drawn from the batch's size
     and domain distribution, at each rate of SERVE_RATES_HZ: served (warm
     starts, continuous batching on 32 streams) in f32 and f16 against the same
@@ -623,7 +630,17 @@ def served_variant(dev, n_sessions=32, substeps=20):
         recs, wall = srv.run_one_at_a_time(specs, scenes=scenes)
         row["plain_f32_one_at_a_time"] = dict(mg_serve.summarize(recs, wall), start="cold (x = 0, mgpcg.py:70)")
         base = row["plain_f32_one_at_a_time"]["solves_per_s"]
-        row["speedup_vs_plain"] = {k: round(row[k]["solves_per_s"] / base, 2) for k in ("served_f32", "served_f16")}
+        if tuned is not None and rate == SERVE_RATES_HZ[-1]:
+            # the batch's tuned (levels, pre_post, bottom) per size class
+            for storage in ("f32", "f16"):
+                tsrv = mg_serve.SolveServer(storage=storage, streams=32, device=dev, params=tuned)
+                tsrv.warm(specs)
+                recs, wall = tsrv.run(specs, scenes=scenes)
+                row[f"served_tuned_{storage}"] = dict(mg_serve.summarize(recs, wall), start="warm (previous substep)")
+                del tsrv
+                torch.cuda.empty_cache()
+        row["speedup_vs_plain"] = {k: round(row[k]["solves_per_s"] / base, 2) for k in row
+                                   if k.startswith("served_")}
         sweep[str(rate)] = row
         del srv, scenes
         torch.cuda.empty_cache()

@@ -2147,7 +2147,11 @@ int mg_batch_create(mg_plan_t* const* plans, int32_t n, mg_batch_t** out) {
     }
     if (!P->prepared || !P->fp.valid || P->fp.sto) {
       delete B;
-      return bad("mg_batch_create: every plan must be prepared in the label-uniform fused form");
+      snprintf(g_err, sizeof(g_err),
+               "bad argument: mg_batch_create: plan %d (%dD %dx%dx%d, %d levels) is not prepared in the "
+               "label-uniform fused form (prepared %d, fused %d)", i, P->d.dim, P->geom[0].n[0], P->geom[0].n[1],
+               P->geom[0].n[2], P->L, (int)P->prepared, (int)P->fp.valid);
+      return MG_E_BADARG;
     }
     if (P->d.pre_post != 2) {
       delete B;

@@ -138,3 +138,19 @@ def tune_classes(scenes, storage="f32", device=None, **kw):
             L = min(choices, key=lambda c: abs(c - L))
         per_scene.append((L, r["pre_post"], r["bottom"]))
     return per_scene, results
+
+
+def class_params(results):
+    """(dim, side) -> (levels, pre_post, bottom) from tune_classes' per-class
+    results, for sessions of the same size distribution (the rule's levels,
+    2 and 50 for a class that was not tuned)."""
+    def params(dim, side):
+        r = results.get(size_class(dim, side))
+        if r is None:
+            return rule_levels(dim, side), 2, 50
+        L = rule_levels(dim, side) + r["offset"]
+        choices = level_choices((side,) * dim)
+        if L not in choices:
+            L = min(choices, key=lambda c: abs(c - L))
+        return L, r["pre_post"], r["bottom"]
+    return params
