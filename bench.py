@@ -72,13 +72,15 @@ REL_TOL = 1e-12  # squared: 1e-6 relative residual
 DIRECT_LAUNCH = False  # set by --direct
 
 # DRAM bytes (read + write) per launch of the dominant kernels, from one ncu
-# capture each (profiles/dram_traffic_pressure128.md,
-# profiles/k_sweep_pre_l0_precision256.md); the bench line's roofline.traffic.
+# capture each of the column-register sweep the autotuner picks for level 0
+# (profiles/k_colsweep_l0_precision256.md, profiles/dram_traffic_substep128.md);
+# the bench line's roofline.traffic.  At 128^3 the sweeps' writes stay in L2.
 NCU_DRAM_BYTES = {
-    ("substep128", "pre_l0"): 16.80e6, ("substep128", "post_l0"): 26.24e6,
-    ("pressure128", "pre_l0"): 16.80e6, ("pressure128", "post_l0"): 26.24e6,
-    ("substep128", "Ap_alpha"): 11.67e6, ("pressure128", "Ap_alpha"): 11.67e6,
-    ("precision256", "pre_l0"): 195.96e6, ("precision256", "Ap_alpha"): 114.93e6,
+    ("substep128", "pre_l0"): 16.83e6, ("substep128", "post_l0"): 26.29e6,
+    ("pressure128", "pre_l0"): 16.83e6, ("pressure128", "post_l0"): 26.29e6,
+    ("substep128", "Ap_alpha"): 11.70e6, ("pressure128", "Ap_alpha"): 11.70e6,
+    ("substep128", "xr"): 24.33e6, ("pressure128", "xr"): 24.33e6,
+    ("precision256", "pre_l0"): 189.5e6, ("precision256", "post_l0"): 271.8e6,
 }
 
 
@@ -93,7 +95,7 @@ def workload_config(args, world):
 def parse():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--steps", type=int, default=60)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--workload", default="substep128", choices=list(WORKLOADS))
@@ -138,7 +140,7 @@ def barrier(world):
 
 # ---------------------------------------------------------------- clocks
 class Clocks:
-    """nvidia-smi sampled every 200 ms while the timed region runs."""
+    """nvidia-smi sampled every 100 ms while the timed region runs."""
 
     def __init__(self, index):
         self.index = index
@@ -153,7 +155,7 @@ class Clocks:
              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
         try:
             self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.index}", f"--query-gpu={q}",
-                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                          "--format=csv,noheader,nounits", "-lms", "100"],
                                          stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
         except Exception:
             self.proc = None
@@ -852,6 +854,14 @@ def main():
             res["variants"], (sc256, xs256) = variants(torch.device("cuda", local))
             if with_cpu:
                 res["variants"]["precision256"]["error_vs_fp64"] = fp64_errors(sc256, xs256)
+            # the same roofline on the 256^3 scene, whose working set does not
+            # fit L2 (the honest HBM case for the level-0 sweeps)
+            k256 = res["variants"]["precision256"]["f32"]["kernels"]
+            dom = max((k for k in ("pre_l0", "post_l0") if k in k256), key=lambda k: k256[k]["ms"])
+            res["roofline_hbm_256"] = {"bound": "hbm", "kernel": dom, "workload": "precision256 (256^3, f32)",
+                                       "achieved": k256[dom]["GB_s"], "peak": res["roofline"]["peak"],
+                                       "unit": "GB/s", "frac": k256[dom]["frac_of_measured_hbm"],
+                                       "traffic": NCU_DRAM_BYTES.get(("precision256", dom))}
         print(json.dumps(res))
     if world > 1:
         import torch.distributed as dist
