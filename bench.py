@@ -516,8 +516,42 @@ def variants(dev, reps=3):
     batched, classes = batched_variant(dev, reps)
     import mg_tune
     out = {"batched": batched, "served": served_variant(dev, tuned=mg_tune.class_params(classes))}
+    out["psi_coarse_forms"] = psi_coarse_variant(dev)
     out["precision256"], xs = precision_variant(dev)
     return out, xs
+
+
+def psi_coarse_variant(dev, reps=3):
+    """The substep's magnetic potential solve at 128^3 with its coarse levels
+    as half the Galerkin operator (the default) and rediscretised as the
+    reference's potential Strategy builds them (chi re-sampled per level, dx
+    2^l): iterations and device ms of full_reinitialize + solve."""
+    import torch
+    from magnetic_potential import MagneticPotentialStrategy
+    from mgpcg import MGPCGPoissonSolver
+    sc = mg_scenes.ferro_drop_3d(n=128, seed=1, levels=5)
+    chi = torch.from_numpy(psi_chi(sc)).to(dev)
+    stream = torch.cuda.current_stream(dev)
+    out = {}
+    for coarse in ("galerkin", "rediscretise"):
+        g = MGPCGPoissonSolver(3, sc.res, 5, 2, 50, device=dev)
+        st = MagneticPotentialStrategy(3, chi, PSI_H, sc.dx, PSI_PIN, coarse=coarse)
+        g.full_reinitialize(st)
+        g.solve(MAX_ITERS)
+        ms = []
+        for _ in range(reps):
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            g.full_reinitialize(st)
+            g.solve_async(MAX_ITERS, REL_TOL)
+            e1.record(stream)
+            stt = g.stats()
+            ms.append(e0.elapsed_time(e1))
+        out["half_galerkin" if coarse == "galerkin" else "rediscretised"] = {
+            "iters": stt.iters, "status": g.last_status, "ms_per_solve": round(min(ms), 3)}
+        g.close()
+    return out
 
 
 def batched_variant(dev, reps=3):

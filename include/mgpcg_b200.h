@@ -180,6 +180,16 @@ MG_API int mg_build_psi_A(mg_plan_t* plan, const float* chi, float dx, int32_t p
  * above. */
 MG_API int mg_galerkin_coarsen(mg_plan_t* plan, int32_t level, float scale, void* stream);
 
+/* The same operator rediscretised on coarse level `level` (>= 1), as the
+ * reference's potential Strategy builds its coarse levels
+ * (potential_function.py:39-55: the coefficient field re-sampled per level,
+ * spacing dx * 2^level): chi_level (the level's shape, written) = the mean of
+ * the 2^dim children of chi_fine (the finer level's chi), then face
+ * coefficients mu(I, J) / (dx 2^level)^2 and the pin's coarse cell pinned.
+ * Call per level in increasing order, each with the previous level's chi. */
+MG_API int mg_build_psi_A_level(mg_plan_t* plan, int32_t level, const float* chi_fine, float* chi_level, float dx,
+                                int32_t pin0, int32_t pin1, int32_t pin2, void* stream);
+
 /* ---- the reference's other Strategies (all f32, all on `stream`) ----------
  * Fields are dense row-major device arrays, last axis fastest: cell fields
  * have the plan's level-0 shape res, MAC face fields of axis k have shape

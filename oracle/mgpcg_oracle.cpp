@@ -514,11 +514,15 @@ struct Solver {
       b[i] = -(acc / dx);
     }
   }
-  void build_psi_A0(const Real* chi, Real dx, const int pin[3]) {
-    const Grid& gg = g[0];
+  void build_psi_A0(const Real* chi, Real dx, const int pin[3]) { build_psi_A(0, chi, dx, pin); }
+  // level l of the operator from that level's chi and spacing (level 0: the
+  // fine chi and dx; rediscretised coarse levels: the children's mean of chi,
+  // dx * 2^l, the pin's coarse cell)
+  void build_psi_A(int l, const Real* chi, Real dx, const int pin[3]) {
+    const Grid& gg = g[l];
     const Real dx2 = dx * dx;
-    Real* ad = Adiag[0].data();
-    Real* ax = Ax[0].data();
+    Real* ad = Adiag[l].data();
+    Real* ax = Ax[l].data();
     for (int64_t i = 0; i < gg.count; ++i) {
       int c[3];
       gg.coords(i, c);
@@ -569,13 +573,45 @@ struct Solver {
       for (int k = 0; k < dim; ++k) Ax[l][k * gc.count + ic] = (cc[k] + 1 < gc.n[k]) ? scale * axc[k] : Real(0);
     }
   }
-  // full_reinitialize(strategy) (mgpcg.py:89-94) with the potential Strategy
+  // chi of level l: the mean of the 2^dim children of level l-1, summed in
+  // lexicographic order from 0 and multiplied by 2^-dim (exact)
+  void mean_children(int l, const Real* fine, Real* coarse) const {
+    const Grid& gf = g[l - 1];
+    const Grid& gc = g[l];
+    const Real w = Real(1) / Real(dim == 3 ? 8 : 4);
+    for (int64_t ic = 0; ic < gc.count; ++ic) {
+      int cc[3];
+      gc.coords(ic, cc);
+      Real acc = Real(0);
+      for (int o0 = 0; o0 < 2; ++o0)
+        for (int o1 = 0; o1 < 2; ++o1)
+          for (int o2 = 0; o2 < (dim == 3 ? 2 : 1); ++o2)
+            acc = acc + fine[(int64_t)(2 * cc[0] + o0) * gf.stride[0] + (int64_t)(2 * cc[1] + o1) * gf.stride[1] +
+                             (dim == 3 ? 2 * cc[2] + o2 : 0)];
+      coarse[ic] = acc * w;
+    }
+  }
+  // full_reinitialize(strategy) (mgpcg.py:89-94) with the potential Strategy;
+  // coarse_scale > 0: A_l = coarse_scale * P^T A_(l-1) P; coarse_scale == 0:
+  // each coarse level rediscretised as the reference's potential Strategy
+  // does (potential_function.py:39-55: chi re-sampled per level, dx * 2^l)
   void full_reinitialize_psi(const Real* chi, const Real H[3], Real dx, const int pin[3], Real coarse_scale) {
     initialize();
     build_psi_b(chi, H, dx, pin);
     for (auto& t : type) std::fill(t.begin(), t.end(), (int8_t)FLUID);
     build_psi_A0(chi, dx, pin);
-    for (int l = 1; l < L; ++l) galerkin(l, coarse_scale);
+    if (coarse_scale > Real(0)) {
+      for (int l = 1; l < L; ++l) galerkin(l, coarse_scale);
+      return;
+    }
+    std::vector<Real> prev(chi, chi + g[0].count), cur;
+    for (int l = 1; l < L; ++l) {
+      cur.assign(g[l].count, Real(0));
+      mean_children(l, prev.data(), cur.data());
+      const int pl[3] = {pin[0] >> l, pin[1] >> l, pin[2] >> l};
+      build_psi_A(l, cur.data(), dx * Real(1 << l), pl);
+      prev.swap(cur);
+    }
   }
 
   // mgpcg.py:79-87 with the pressure Strategy

@@ -159,7 +159,8 @@ class OracleSolver:
     def full_reinitialize_psi(self, chi, H=(0.0, 1.0, 0.0), dx=1.0, pin=(1, 1, 1), coarse_scale=0.5):
         """full_reinitialize (mgpcg.py:89-94) with the magnetic potential Strategy
         of the 3D substep benchmark (harmonic-mean mu faces, pinned cell,
-        coarse levels coarse_scale * P^T A P)."""
+        coarse levels coarse_scale * P^T A P for coarse_scale > 0; for 0 each
+        coarse level rediscretised: chi the mean of the children, dx * 2^l)."""
         c = np.ascontiguousarray(chi, dtype=self.real)
         assert c.shape == self.res
         H = list(H) + [0.0] * (3 - len(H))

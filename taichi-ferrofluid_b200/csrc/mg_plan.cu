@@ -1023,6 +1023,22 @@ int mg_build_psi_A(mg_plan_t* P, const float* chi, float dx, int32_t p0, int32_t
   return MG_OK;
 }
 
+int mg_build_psi_A_level(mg_plan_t* P, int32_t level, const float* chi_fine, float* chi_level, float dx,
+                         int32_t p0, int32_t p1, int32_t p2, void* stream) {
+  NEED_BOUND(P);
+  if (level < 1 || level >= P->L) return bad("level");
+  if (!chi_fine || !chi_level || !(dx > 0.0f)) return bad("chi / dx");
+  k_mean_children<<<P->ew_blocks[level], 256, 0, S(stream)>>>(P->geom[level - 1], chi_fine, P->geom[level],
+                                                               chi_level);
+  CKL("k_mean_children");
+  const float dxl = dx * (float)(1 << level);  // exact: a power of two
+  k_build_psi_A<<<P->ew_blocks[level], 256, 0, S(stream)>>>(P->lv[level], chi_level, dxl, p0 >> level, p1 >> level,
+                                                             P->d.dim == 3 ? (p2 >> level) : 0);
+  CKL("k_build_psi_A");
+  P->prepared = false;
+  return MG_OK;
+}
+
 int mg_galerkin_coarsen(mg_plan_t* P, int32_t level, float scale, void* stream) {
   NEED_BOUND(P);
   if (level < 1 || level >= P->L) return bad("level");

@@ -76,6 +76,24 @@ __global__ void k_build_psi_A(Level L, const float* __restrict__ chi, float dx, 
   }
 }
 
+// chi of a coarse level: the mean of the 2^dim children of the finer level,
+// summed in lexicographic order from 0 and multiplied by 2^-dim (exact) - the
+// coarse coefficient field of a rediscretised level.
+__global__ void k_mean_children(Geom gf, const float* __restrict__ fine, Geom gc, float* __restrict__ coarse) {
+  const float w = gc.dim == 3 ? 0.125f : 0.25f;
+  for (long long ic = (long long)blockIdx.x * blockDim.x + threadIdx.x; ic < gc.count;
+       ic += (long long)gridDim.x * blockDim.x) {
+    int cc[3];
+    gc.coords(ic, cc);
+    float acc = 0.0f;
+    for (int o0 = 0; o0 < 2; ++o0)
+      for (int o1 = 0; o1 < 2; ++o1)
+        for (int o2 = 0; o2 < (gc.dim == 3 ? 2 : 1); ++o2)
+          acc = __fadd_rn(acc, fine[gf.index(2 * cc[0] + o0, 2 * cc[1] + o1, gc.dim == 3 ? 2 * cc[2] + o2 : 0)]);
+    coarse[ic] = __fmul_rn(acc, w);
+  }
+}
+
 // Galerkin coarse operator A_c = P^T A P for the reference's transfer pair
 // (prolongation: piecewise constant, mgpcg.py:120-123; restriction: the
 // unweighted sum of the 2^d children, mgpcg.py:111-118):

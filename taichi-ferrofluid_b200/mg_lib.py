@@ -77,6 +77,7 @@ _SIGS = {
     "mg_build_psi_b": (ctypes.c_int, [_vp, _vp, _f32, _f32, _f32, _f32, _i32, _i32, _i32, _vp]),
     "mg_build_psi_A": (ctypes.c_int, [_vp, _vp, _f32, _i32, _i32, _i32, _vp]),
     "mg_galerkin_coarsen": (ctypes.c_int, [_vp, _i32, _f32, _vp]),
+    "mg_build_psi_A_level": (ctypes.c_int, [_vp, _i32, _vp, _vp, _f32, _i32, _i32, _i32, _vp]),
     "mg_build_magnetic_b": (ctypes.c_int, [_vp, _vp, _vp, _vp, _vp, _vp, _vp, _f32, _f32, _f32, _f32, _vp]),
     "mg_build_potential_b": (ctypes.c_int, [_vp, _vp, _vp, _vp, _vp, _vp]),
     "mg_build_potential_A": (ctypes.c_int, [_vp, _i32, _vp, _f64, _vp]),

@@ -149,3 +149,30 @@ def test_precision256(storage, precision256):
         assert g.last_rel_resid <= 1e-6, g.last_rel_resid
         # the float32 rounding of the solution alone leaves 0.84e-6 at 256^3
         assert res < 2e-6, res
+
+
+def test_substep128_psi_coarse_forms(drop128):
+    """The psi solve of the 3D substep with its coarse levels as half the
+    Galerkin operator (the default) and rediscretised as the reference's
+    potential Strategy does: both converge and match the float32 oracle run
+    the same way; the iteration counts are printed side by side."""
+    import torch
+    from magnetic_potential import MagneticPotentialStrategy
+    from mgpcg import MGPCGPoissonSolver
+    from oracle import OracleSolver
+    sc = drop128
+    chi = (sc.phi < 0).astype(np.float32)
+    out = {}
+    for coarse, scale in (("galerkin", 0.5), ("rediscretise", 0.0)):
+        g = MGPCGPoissonSolver(3, sc.res, 5, 2, 50, device="cuda")
+        g.full_reinitialize(MagneticPotentialStrategy(3, torch.from_numpy(chi).cuda(), PSI_H, sc.dx, PSI_PIN,
+                                                      coarse=coarse))
+        it = g.solve(500)
+        assert g.last_status == "converged"
+        o = OracleSolver(3, sc.res, 5, 2, 50, real=np.float32)
+        o.full_reinitialize_psi(chi, PSI_H, sc.dx, PSI_PIN, coarse_scale=scale)
+        it_o = o.solve(500)
+        assert abs(it - it_o) <= 1, (coarse, it, it_o)
+        assert rel_l2(g.x.cpu().numpy(), o.get("x")) < 1e-5
+        out[coarse] = it
+    print(f"psi 128^3 iterations: half Galerkin {out['galerkin']}, rediscretised {out['rediscretise']}")

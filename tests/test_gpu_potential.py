@@ -13,7 +13,7 @@ from helpers import rel_l2
 pytestmark = pytest.mark.gpu
 
 
-def _pair(n, levels):
+def _pair(n, levels, coarse="galerkin"):
     import torch
     from mgpcg import MGPCGPoissonSolver
     from magnetic_potential import MagneticPotentialStrategy
@@ -21,10 +21,10 @@ def _pair(n, levels):
     sc = mg_scenes.ferro_drop_3d(n=n, levels=levels)
     chi = (sc.phi < 0).astype(np.float32)
     g = MGPCGPoissonSolver(3, sc.res, levels, 2, 50, device="cuda")
-    st = MagneticPotentialStrategy(3, torch.from_numpy(chi).cuda(), (0.0, 1.0, 0.0), sc.dx, (1, 1, 1))
+    st = MagneticPotentialStrategy(3, torch.from_numpy(chi).cuda(), (0.0, 1.0, 0.0), sc.dx, (1, 1, 1), coarse=coarse)
     g.full_reinitialize(st)
     o = OracleSolver(3, sc.res, levels, 2, 50, real=np.float32)
-    o.full_reinitialize_psi(chi, (0.0, 1.0, 0.0), sc.dx, (1, 1, 1))
+    o.full_reinitialize_psi(chi, (0.0, 1.0, 0.0), sc.dx, (1, 1, 1), coarse_scale=0.5 if coarse == "galerkin" else 0.0)
     return sc, chi, g, o
 
 
@@ -57,3 +57,23 @@ def test_potential_solve_parity(n, levels):
     err = rel_l2(x, o64.get("x"))
     print(f"potential {n}^3: error vs FP64 = {err:.2e}")
     assert err < 2e-3
+
+
+@pytest.mark.parametrize("n,levels", [(32, 3), (48, 4)])
+def test_rediscretised_potential_system_bit_exact(n, levels):
+    """Coarse levels rebuilt as the reference's potential Strategy builds
+    them (potential_function.py:39-55: coefficients re-sampled per level,
+    dx * 2^l): every level bit-exact with the float32 oracle."""
+    sc, chi, g, o = _pair(n, levels, coarse="rediscretise")
+    for l in range(levels):
+        np.testing.assert_array_equal(g.Adiag[l].cpu().numpy(), o.get("Adiag", l))
+        np.testing.assert_array_equal(np.moveaxis(g.Ax[l].cpu().numpy(), -1, 0), o.get("Ax", l))
+
+
+def test_rediscretised_potential_solve_parity():
+    sc, chi, g, o = _pair(64, 4, coarse="rediscretise")
+    it = g.solve(500)
+    assert g.last_status == "converged"
+    it_o = o.solve(500)
+    assert abs(it - it_o) <= 1, (it, it_o)
+    assert rel_l2(g.x.cpu().numpy(), o.get("x")) < 1e-5

@@ -202,3 +202,76 @@ def test_golden_fixture_reproduced(fname):
 def test_oracle_rejects_uneven_levels():
     with pytest.raises(ValueError):
         OracleSolver(2, (100, 64), 4)
+
+
+def _psi_numpy(chi, dx, pin):
+    """Independent numpy assembly of the magnetic potential operator of one
+    level: harmonic-mean mu faces over dx^2, Neumann boundary, the pinned row
+    the identity over dx^2 and the couplings into the pinned cell removed.
+    Returns (Adiag, Ax[k] as the + side coupling)."""
+    mu = 1.0 + chi.astype(np.float64)
+    dim = chi.ndim
+    ad = np.zeros(chi.shape)
+    ax = np.zeros((dim,) + chi.shape)
+    for k in range(dim):
+        lo = [slice(None)] * dim
+        hi = [slice(None)] * dim
+        lo[k] = slice(0, -1)
+        hi[k] = slice(1, None)
+        lo, hi = tuple(lo), tuple(hi)
+        f = 2.0 * mu[lo] * mu[hi] / (mu[lo] + mu[hi]) / (dx * dx)
+        ad[lo] += f
+        ad[hi] += f
+        ax[k][lo] = -f
+        # couplings into the pinned cell are removed (its row is the identity)
+        pk = list(pin)
+        pk[k] -= 1
+        if pk[k] >= 0:
+            ax[k][tuple(pk)] = 0.0
+    ad[tuple(pin)] = 1.0 / (dx * dx)
+    for k in range(dim):
+        ax[k][tuple(pin)] = 0.0
+    return ad, ax
+
+
+@pytest.mark.parametrize("coarse", ["galerkin", "rediscretise"])
+def test_psi_operator_matches_numpy(coarse):
+    """The magnetic potential operator of the 3D substep benchmark in the
+    FP64 oracle against an independent numpy assembly: level 0, then level 1
+    either as half the Galerkin operator (P piecewise constant, R its
+    transpose) or rediscretised (chi the mean of the children, dx * 2, the
+    pin's coarse cell), as potential_function.py:39-55 rebuilds its levels."""
+    n, L, dx, pin = 16, 3, 1.0 / 16, (1, 1, 1)
+    rng = np.random.default_rng(9)
+    chi = (rng.random((n, n, n)) < 0.4).astype(np.float64)
+    o = OracleSolver(3, (n, n, n), L, 2, 50, real=np.float64)
+    o.full_reinitialize_psi(chi, (0.0, 1.0, 0.0), dx, pin, coarse_scale=0.5 if coarse == "galerkin" else 0.0)
+    ad0, ax0 = _psi_numpy(chi, dx, pin)
+    np.testing.assert_allclose(o.get("Adiag", 0), ad0, rtol=1e-12)
+    np.testing.assert_allclose(o.get("Ax", 0), ax0, rtol=1e-12, atol=0)
+    if coarse == "rediscretise":
+        chi1 = chi.reshape(n // 2, 2, n // 2, 2, n // 2, 2).mean(axis=(1, 3, 5))
+        ad1, ax1 = _psi_numpy(chi1, 2 * dx, tuple(p >> 1 for p in pin))
+    else:
+        # 1/2 P^T A P: the coarse diagonal sums the children's diagonals and
+        # twice the couplings between children; the coarse + coupling sums the
+        # children's couplings across the coarse face
+        m = n // 2
+        ad1 = np.zeros((m, m, m))
+        ax1 = np.zeros((3, m, m, m))
+        for off in np.ndindex(2, 2, 2):
+            ch = tuple(slice(off[a], None, 2) for a in range(3))
+            ad1 += ad0[ch]
+            for k in range(3):
+                if off[k] == 0:
+                    ad1 += 2.0 * ax0[k][ch]
+                else:
+                    ax1[k] += ax0[k][ch]
+        for k in range(3):
+            sl = [slice(None)] * 3
+            sl[k] = m - 1
+            ax1[k][tuple(sl)] = 0.0
+        ad1 *= 0.5
+        ax1 *= 0.5
+    np.testing.assert_allclose(o.get("Adiag", 1), ad1, rtol=1e-12)
+    np.testing.assert_allclose(o.get("Ax", 1), ax1, rtol=1e-12, atol=1e-9)
