@@ -90,21 +90,25 @@ struct ColGeom {
   static constexpr int HB = (sizeof(ST) == 4 && NS <= 4) ? 4 : 8;
   static constexpr int HX = NS;              // x halo of the threads' region
   static constexpr int RXB = TX + 2 * HB;    // box columns (TMA slots)
-  static constexpr int RX = TX + 2 * HX;     // region columns (threads, shared z planes)
+  static constexpr int RX = TX + 2 * HX;     // region columns (threads)
   static constexpr int RY = TY + 2 * NS;     // region rows (even)
   static constexpr int PLB = RXB * RY;       // cells of a box plane
-  static constexpr int PLC = RX * RY;        // cells of a region plane
   static constexpr int PAIRS = RX * (RY / 2);
-  static constexpr int NT = (PAIRS + 31) / 32 * 32;
+  static constexpr int NT = PAIRS;
   static constexpr int W = NS + 2;           // planes in registers = TMA ring slots = shared z planes
+  // a shared z plane holds the region plus a one-cell border, so every cell's
+  // four in-plane neighbours are at fixed offsets (the border feeds only halo
+  // cells that are never smoothed)
+  static constexpr int ZX = RX + 2, ZY = RY + 2;
+  static constexpr int ZPL = (ZX * ZY + 31) / 32 * 32;                     // floats of a shared z plane
   static constexpr int SLOT_R = (PLB * 4 + 127) / 128 * 128;               // r (float32 or ST)
   static constexpr int SLOT_S = (PLB * (int)sizeof(ST) + 127) / 128 * 128;  // Adiag, input z (ST)
-  static constexpr int ZPL = (PLC + 31) / 32 * 32;                         // floats of a shared z plane
   static constexpr int slot_bytes(bool pre) { return SLOT_R + SLOT_S * (pre ? 1 : 2); }
   static constexpr size_t smem(bool pre) {
     return 128 /* alignment */ + 128 /* mbarriers */ + (size_t)W * slot_bytes(pre) + (size_t)W * ZPL * 4;
   }
   static_assert(TX % 8 == 0 && TY % 2 == 0 && NS % 2 == 0, "even pairs, 16-byte TMA rows");
+  static_assert(PAIRS % 32 == 0 && (TX * (TY / 2)) % 32 == 0, "whole warps of pairs, interior warps first");
   static_assert(RXB <= 256 && RY <= 256, "TMA box extents");
   static_assert(W <= 16, "mbarriers in 128 bytes");
 };
@@ -151,13 +155,19 @@ __device__ __forceinline__ float residual_cell(float ms, float s, float r, float
 // the restriction r[l+1] = rho * sum of the children's r - A z and z[l+1] = 0)
 // or POST (z += pi * z[l+1][I/2], then half sweeps in colour order 1,0,...),
 // with the level-0 POST also summing z.r for the PCG loop (A.zr >= 0).
+//
+// The step body is written for few instructions per cell: shared-memory
+// pointers fixed per thread (the planes at immediate offsets), 32-bit cell
+// indices, plane parities known at compile time (chunks start on even
+// planes), and one thread that waits for the next plane's loads before the
+// step's block barrier.
 // ---------------------------------------------------------------------------
 template <typename ST, int NS, int TX, int TY, bool PRE, int MINB>
 __global__ void __launch_bounds__(ColGeom<ST, NS, TX, TY>::NT, MINB)
     k_colsweep(SweepArgs<ST> A, Control* flag, const __grid_constant__ CUtensorMap tm_r,
                const __grid_constant__ CUtensorMap tm_ad, const __grid_constant__ CUtensorMap tm_zin) {
   using G = ColGeom<ST, NS, TX, TY>;
-  constexpr int HX = G::HX, RX = G::RX, RY = G::RY, W = G::W, NT = G::NT, ZPL = G::ZPL;
+  constexpr int HX = G::HX, RX = G::RX, W = G::W, NT = G::NT, ZPL = G::ZPL, ZX = G::ZX;
   constexpr int RXB = G::RXB, XOFF = G::HB - G::HX;  // box columns; box column of region column 0
   // the mixed form (16-bit grids) needs no bit-exact float32: a neighbour-sum
   // tree, one FMA and the approximate reciprocal instead of six products,
@@ -165,36 +175,52 @@ __global__ void __launch_bounds__(ColGeom<ST, NS, TX, TY>::NT, MINB)
   constexpr bool FAST = sizeof(ST) != 4;
   constexpr int SLOT = G::slot_bytes(PRE);
   constexpr int D = PRE ? NS - 1 : NS;  // steps from a plane's load to its final z
+  constexpr int NI = TX * (TY / 2), NB = (NS / 2) * RX;
   pdl_enter();
 
-  extern __shared__ unsigned char smem_raw[];
-  unsigned char* smem = (unsigned char*)(((uintptr_t)smem_raw + 127) & ~(uintptr_t)127);
-  uint64_t* bar = (uint64_t*)smem;
+  extern __shared__ __align__(128) unsigned char smem_raw[];
+  // 128-byte aligned by pointer arithmetic on the shared array (the compiler
+  // keeps shared-space loads and stores)
+  unsigned char* smem = smem_raw + ((128u - (smem_addr(smem_raw) & 127u)) & 127u);
+  uint64_t* bar = reinterpret_cast<uint64_t*>(smem);
   unsigned char* slots = smem + 128;
-  float* zs = (float*)(slots + W * SLOT);
+  float* zs = reinterpret_cast<float*>(slots + W * SLOT);
   __shared__ int abort_flag;
 
   const FLevel<ST>& F = A.f;
   const int n0 = F.n[0], n1 = F.n[1], n2 = F.n[2];
+  // one wave of blocks: tile t is cut into q or q + 1 chunks of nearly equal
+  // even length (the first r tiles get q + 1; the host launches
+  // ntile <= gridDim.x <= ntile * n0 / 2 blocks)
   const int ntile = A.tiles_x * A.tiles_y;
-  const int tile = blockIdx.x % ntile;
-  const int chunk_id = blockIdx.x / ntile;
+  const int nq = (int)gridDim.x / ntile, nr = (int)gridDim.x % ntile;
+  int tile, cid, nch;
+  if ((int)blockIdx.x < nr * (nq + 1)) {
+    tile = blockIdx.x / (nq + 1);
+    cid = blockIdx.x % (nq + 1);
+    nch = nq + 1;
+  } else {
+    const int b2 = blockIdx.x - nr * (nq + 1);
+    tile = nr + b2 / nq;
+    cid = b2 % nq;
+    nch = nq;
+  }
   const int tx0 = (tile % A.tiles_x) * TX;
   const int ty0 = (tile / A.tiles_x) * TY;
-  const int z0 = chunk_id * A.chunk;
-  const int z1 = min(z0 + A.chunk, n0);
-  const int p_first = z0 - NS;
+  const int z0 = (cid * n0 / nch) & ~1;  // even
+  const int z1 = cid + 1 == nch ? n0 : ((cid + 1) * n0 / nch) & ~1;
+  const int p_first = z0 - NS;        // even
   const int p_last = z1 + NS - 1;
   const int ox = tx0 - HX, oy = ty0 - NS;  // region origin (both even)
   const int bx = tx0 - G::HB;               // TMA box origin along x (16-byte aligned)
   const float sigma = A.r_f32 ? (float)A.ctl->scale_r : 1.0f;
   const float ms = -F.s;
-  const long long pstride = (long long)n1 * n2;
-  const int ncx = A.nc[2], ncy = A.nc[1];
+  const float s_pos = F.s;
+  const int pstride = n1 * n2;  // 32-bit cell indices (the host checks the level's size)
+  const int ncx = A.nc[2], cps = A.nc[1] * A.nc[2];
   const bool r32 = sizeof(ST) == 4 || A.r_f32;
   const uint32_t tx_bytes =
       (uint32_t)(G::PLB * ((r32 ? 4 : (int)sizeof(ST)) + (int)sizeof(ST) * (PRE ? 1 : 2)));
-  const float s_pos = F.s;
 
   // ---- this thread's pair of columns ----------------------------------------------------
   // Interior first: threads [0, TX * TY / 2) hold the tile's own pairs, one
@@ -203,57 +229,57 @@ __global__ void __launch_bounds__(ColGeom<ST, NS, TX, TY>::NT, MINB)
   // left and right bands of HX columns).  A half sweep's active region shrinks
   // towards the tile, so halo warps fall idle as a whole instead of idling
   // lanes inside every warp; the residual runs on the interior warps only.
-  constexpr int NI = TX * (TY / 2), NB = (NS / 2) * RX;
   const int t = threadIdx.x;
-  const bool live = t < G::PAIRS;
-  const int tt = live ? t : 0;
   int rx, pr2;
-  if (tt < NI) {
-    pr2 = NS / 2 + tt / TX;
-    rx = HX + tt % TX;
-  } else if (tt < NI + NB) {
-    pr2 = (tt - NI) / RX;
-    rx = (tt - NI) % RX;
-  } else if (tt < NI + 2 * NB) {
-    pr2 = NS / 2 + TY / 2 + (tt - NI - NB) / RX;
-    rx = (tt - NI - NB) % RX;
+  if (t < NI) {
+    pr2 = NS / 2 + t / TX;
+    rx = HX + t % TX;
+  } else if (t < NI + NB) {
+    pr2 = (t - NI) / RX;
+    rx = (t - NI) % RX;
+  } else if (t < NI + 2 * NB) {
+    pr2 = NS / 2 + TY / 2 + (t - NI - NB) / RX;
+    rx = (t - NI - NB) % RX;
   } else {
-    const int h = tt - NI - 2 * NB;
+    const int h = t - NI - 2 * NB;
     pr2 = NS / 2 + h / (2 * HX);
     const int k = h % (2 * HX);
     rx = k < HX ? k : TX + k;
   }
+  const bool interior_warp = t < NI;  // warp-uniform
   const int gx = ox + rx, gy0 = oy + 2 * pr2;
-  const int odd = rx & 1;                               // gx parity (ox even)
+  const int odd = rx & 1;                                    // gx parity (ox even)
   const int rowA = 2 * pr2 + odd, rowB = 2 * pr2 + 1 - odd;  // A: x + y even
-  const int yo = 2 * pr2 - 1, yu = 2 * pr2 + 2;          // the rows beyond the pair
-  const int outA = min(max(odd ? yu : yo, 0), RY - 1);   // (clamped: such reads feed
-  const int outB = min(max(odd ? yo : yu, 0), RY - 1);   //  only cells never smoothed)
-  const int cA = rowA * RX + rx, cB = rowB * RX + rx;      // in a shared z plane
-  const int oA = outA * RX + rx, oB = outB * RX + rx;
+  const int outA = odd ? rowA + 1 : rowA - 1;                // the row beyond the pair next to A
+  const int outB = odd ? rowB - 1 : rowB + 1;
+  float* const pA = zs + (rowA + 1) * ZX + rx + 1;  // own cells in shared z plane 0
+  float* const pB = zs + (rowB + 1) * ZX + rx + 1;
+  const float* const qA = zs + (outA + 1) * ZX + rx + 1;  // the out-of-pair row neighbours
+  const float* const qB = zs + (outB + 1) * ZX + rx + 1;
   const int kA = rowA * RXB + rx + XOFF, kB = rowB * RXB + rx + XOFF;  // in a TMA slot
-  const int xm = rx > 0 ? -1 : 0, xp = rx < RX - 1 ? 1 : 0;
-  const int dx = max(max(HX - rx, rx - (HX + TX - 1)), 0);
-  const int ringA = live ? max(dx, max(max(NS - rowA, rowA - (NS + TY - 1)), 0)) : 1 << 20;
-  const int ringB = live ? max(dx, max(max(NS - rowB, rowB - (NS + TY - 1)), 0)) : 1 << 20;
+  const int dxr = max(max(HX - rx, rx - (HX + TX - 1)), 0);
+  const int ringA = max(dxr, max(max(NS - rowA, rowA - (NS + TY - 1)), 0));
+  const int ringB = max(dxr, max(max(NS - rowB, rowB - (NS + TY - 1)), 0));
   // n1 even and gy0 even: the pair's rows are both inside the grid or both outside
-  const bool in_grid = live && gx >= 0 && gx < n2 && gy0 >= 0 && gy0 < n1;
+  const bool in_grid = gx >= 0 && gx < n2 && gy0 >= 0 && gy0 < n1;
   const bool ownA = in_grid && ringA == 0, ownB = in_grid && ringB == 0;
-  const long long giA = (long long)(oy + rowA) * n2 + gx, giB = (long long)(oy + rowB) * n2 + gx;
+  const int giA = (oy + rowA) * n2 + gx, giB = (oy + rowB) * n2 + gx;
+  // the coarse column of the pair (clamped into the grid: only in-grid cells use it)
+  const int cc = (min(max(gy0, 0), n1 - 1) >> 1) * ncx + (min(max(gx, 0), n2 - 1) >> 1);
 
   float zA[W], zB[W], rA[W], rB[W], aA[W], aB[W];
 #pragma unroll
   for (int j = 0; j < W; ++j) {
     zA[j] = 0.0f; zB[j] = 0.0f; rA[j] = 0.0f; rB[j] = 0.0f; aA[j] = 0.0f; aB[j] = 0.0f;
   }
-  // POST: the coarse z of the pair's column for plane p (prolongation), read
-  // one step ahead so its latency overlaps a step's work
+  // POST: the coarse z of the pair's column for the plane pair (p, p + 1), p
+  // even, read two steps before its use; planes outside the grid read a
+  // clamped plane (their cells are not FLUID and never written)
   auto zc_of = [&](int p) -> float {
-    return (!PRE && in_grid && p >= 0 && p < n0)
-               ? to_f<ST>(A.zc[((long long)(p >> 1) * ncy + (gy0 >> 1)) * ncx + (gx >> 1)])
-               : 0.0f;
+    const int h = min(max(p >> 1, 0), (n0 >> 1) - 1);
+    return to_f<ST>(A.zc[h * cps + cc]);
   };
-  float zc_next = zc_of(p_first);
+  float zc_next = PRE ? 0.0f : zc_of(p_first), zc_cur = 0.0f;
   float acc = 0.0f;      // restriction accumulator (PRE, even-x threads)
   double zr_acc = 0.0;   // z.r of the cells written (POST, A.zr >= 0)
 
@@ -271,15 +297,20 @@ __global__ void __launch_bounds__(ColGeom<ST, NS, TX, TY>::NT, MINB)
     mbar_fence_init();
     abort_flag = 0;
   }
+  // the border of every shared z plane (read only for halo cells never smoothed)
+  for (int i = t; i < W * ZPL; i += NT) zs[i] = 0.0f;
   __syncthreads();
-  if (t == 0)
+  int stop_p = p_first;  // the plane whose loads did not complete (abort)
+  if (t == 0) {
     for (int k = 0; k < W - 1; ++k)
       if (p_first + k <= p_last) issue(p_first + k, k);
+    if (!mbar_wait_bounded(&bar[0], 0u)) abort_flag = 1;
+  }
+  __syncthreads();
 
-  bool aborted = false;
-  int stop_p = p_last;  // the first plane not known to be delivered (abort)
+  bool aborted = abort_flag != 0;
   for (int P0 = p_first; P0 <= p_last && !aborted; P0 += W) {
-    const uint32_t parity = (uint32_t)(((P0 - p_first) / W) & 1);
+    const int k0 = (P0 - p_first) / W;  // ring pass of this group of W planes
 #pragma unroll
     for (int u = 0; u < W; ++u) {
       const int P = P0 + u;
@@ -287,26 +318,25 @@ __global__ void __launch_bounds__(ColGeom<ST, NS, TX, TY>::NT, MINB)
       const int q = P - p_first;
       // plane P + W - 1 into the slot of plane P - 1 (read before the last barrier)
       if (t == 0 && P + W - 1 <= p_last) issue(P + W - 1, (u + W - 1) % W);
-      if (!mbar_wait_bounded(&bar[u], parity)) abort_flag = 1;
 
-      // ---- plane P: r, Adiag (and the prolongated z) into the registers --------------
+      // ---- plane P (delivered: waited for before the last barrier) into the registers --
       {
         const unsigned char* sl = slots + u * SLOT;
         if (r32) {
-          const float* sr = (const float*)sl;
+          const float* sr = reinterpret_cast<const float*>(sl);
           rA[u] = sizeof(ST) == 4 ? sr[kA] : __fmul_rn(sigma, sr[kA]);
           rB[u] = sizeof(ST) == 4 ? sr[kB] : __fmul_rn(sigma, sr[kB]);
         } else {
-          const ST* sr = (const ST*)sl;
+          const ST* sr = reinterpret_cast<const ST*>(sl);
           rA[u] = to_f<ST>(sr[kA]);
           rB[u] = to_f<ST>(sr[kB]);
         }
-        const ST* sa = (const ST*)(sl + G::SLOT_R);
+        const ST* sa = reinterpret_cast<const ST*>(sl + G::SLOT_R);
         aA[u] = to_f<ST>(sa[kA]);
         aB[u] = to_f<ST>(sa[kB]);
         if constexpr (PRE) {
           // the first half sweep is pointwise (z = 0 before it): z = r / Adiag on
-          // the colour-0 cell, the one active in this step
+          // the colour-0 cell, the one active in this step (A: even P)
           if ((u & 1) == 0) {
             zA[u] = aA[u] != 0.0f ? (FAST ? __fdividef(rA[u], aA[u]) : __fdiv_rn(rA[u], aA[u])) : 0.0f;
             zB[u] = 0.0f;
@@ -315,23 +345,25 @@ __global__ void __launch_bounds__(ColGeom<ST, NS, TX, TY>::NT, MINB)
             zA[u] = 0.0f;
           }
         } else {
-          const ST* si = (const ST*)(sl + G::SLOT_R + G::SLOT_S);
-          const float c = zc_next;          // loaded during the previous step
-          zc_next = zc_of(P + 1);
-          const float fa = __fadd_rn(to_f<ST>(si[kA]), __fmul_rn(A.pi, c));
-          const float fb = __fadd_rn(to_f<ST>(si[kB]), __fmul_rn(A.pi, c));
+          if ((u & 1) == 0) {  // the coarse value of planes (P, P + 1); prefetch (P + 2, P + 3)
+            zc_cur = zc_next;
+            zc_next = zc_of(P + 2);
+          }
+          const ST* si = reinterpret_cast<const ST*>(sl + G::SLOT_R + G::SLOT_S);
+          const float c = __fmul_rn(A.pi, zc_cur);
+          const float fa = __fadd_rn(to_f<ST>(si[kA]), c);
+          const float fb = __fadd_rn(to_f<ST>(si[kB]), c);
           zA[u] = aA[u] != 0.0f ? fa : 0.0f;
           zB[u] = aB[u] != 0.0f ? fb : 0.0f;
           // an owned non-FLUID cell is never smoothed: its output is this value
           if (P >= z0 && P < z1) {
-            if (ownA && aA[u] == 0.0f) F.z[(long long)P * pstride + giA] = from_f<ST>(fa);
-            if (ownB && aB[u] == 0.0f) F.z[(long long)P * pstride + giB] = from_f<ST>(fb);
+            const int base = P * pstride;
+            if (ownA && aA[u] == 0.0f) F.z[base + giA] = from_f<ST>(fa);
+            if (ownB && aB[u] == 0.0f) F.z[base + giB] = from_f<ST>(fb);
           }
         }
-        if (live) {
-          zs[u * ZPL + cA] = zA[u];
-          zs[u * ZPL + cB] = zB[u];
-        }
+        pA[u * ZPL] = zA[u];
+        pB[u * ZPL] = zB[u];
       }
 
       // ---- half sweeps: m on the plane shift(m) behind P ------------------------------
@@ -340,23 +372,21 @@ __global__ void __launch_bounds__(ColGeom<ST, NS, TX, TY>::NT, MINB)
         const int s = PRE ? m - 1 : m;      // planes behind P
         const int j = (u - s + 2 * W) % W, jm = (j + W - 1) % W, jp = (j + 1) % W;
         if (q < s + 1) continue;            // the plane below was not loaded
-        float* zp = zs + j * ZPL;
         // cells at ring distance <= NS - s from the tile are needed after this sweep
+        // (a branch: most warps of a scene's air or solid skip the division)
         if ((u & 1) == 0) {
-          const float a = aA[j];
-          if (ringA <= NS - s && a != 0.0f) {
-            const float v = smooth_cell<FAST>(ms, s_pos, rA[j], a, zA[jm], zA[jp], zp[oA], zB[j], zp[cA + xm],
-                                              zp[cA + xp]);
+          if (ringA <= NS - s && aA[j] != 0.0f) {
+            const float v = smooth_cell<FAST>(ms, s_pos, rA[j], aA[j], zA[jm], zA[jp], qA[j * ZPL], zB[j],
+                                              pA[j * ZPL - 1], pA[j * ZPL + 1]);
             zA[j] = v;
-            zp[cA] = v;
+            pA[j * ZPL] = v;
           }
         } else {
-          const float a = aB[j];
-          if (ringB <= NS - s && a != 0.0f) {
-            const float v = smooth_cell<FAST>(ms, s_pos, rB[j], a, zB[jm], zB[jp], zp[oB], zA[j], zp[cB + xm],
-                                              zp[cB + xp]);
+          if (ringB <= NS - s && aB[j] != 0.0f) {
+            const float v = smooth_cell<FAST>(ms, s_pos, rB[j], aB[j], zB[jm], zB[jp], qB[j * ZPL], zA[j],
+                                              pB[j * ZPL - 1], pB[j * ZPL + 1]);
             zB[j] = v;
-            zp[cB] = v;
+            pB[j * ZPL] = v;
           }
         }
       }
@@ -366,62 +396,65 @@ __global__ void __launch_bounds__(ColGeom<ST, NS, TX, TY>::NT, MINB)
         const int pw = P - D;
         if (pw >= z0 && pw < z1) {
           const int jw = (u - D + 2 * W) % W;
-          const long long base = (long long)pw * pstride;
+          const int base = pw * pstride;
           if constexpr (PRE) {  // non-FLUID cells hold z = 0
             if (ownA) F.z[base + giA] = from_f<ST>(zA[jw]);
             if (ownB) F.z[base + giB] = from_f<ST>(zB[jw]);
           } else {
-            if (ownA && aA[jw] != 0.0f) {
-              F.z[base + giA] = from_f<ST>(zA[jw]);
-              if (A.zr >= 0) zr_acc += (double)zA[jw] * (double)rA[jw];
-            }
-            if (ownB && aB[jw] != 0.0f) {
-              F.z[base + giB] = from_f<ST>(zB[jw]);
-              if (A.zr >= 0) zr_acc += (double)zB[jw] * (double)rB[jw];
+            const bool wa = ownA && aA[jw] != 0.0f, wb = ownB && aB[jw] != 0.0f;
+            if (wa) F.z[base + giA] = from_f<ST>(zA[jw]);
+            if (wb) F.z[base + giB] = from_f<ST>(zB[jw]);
+            if (A.zr >= 0) {
+              zr_acc += wa ? (double)zA[jw] * (double)rA[jw] : 0.0;
+              zr_acc += wb ? (double)zB[jw] * (double)rB[jw] : 0.0;
             }
           }
         }
       }
 
-      // ---- PRE: residual of plane P - NS and restriction ------------------------------
+      // ---- PRE: residual of plane P - NS and restriction (interior warps) ---------------
       if constexpr (PRE) {
-        const int pr = P - NS;
-        if (pr >= z0 && pr < z1) {
+        const int pr = P - NS;  // parity of u (P0 and NS even)
+        if (interior_warp && pr >= z0 && pr < z1) {
           const int jr = (u - NS + 2 * W) % W, jrm = (jr + W - 1) % W, jrp = (jr + 1) % W;
-          const float* zp = zs + jr * ZPL;
+          const bool fA = in_grid && aA[jr] != 0.0f, fB = in_grid && aB[jr] != 0.0f;
           float vA = 0.0f, vB = 0.0f;
-          const bool fA = ownA && aA[jr] != 0.0f, fB = ownB && aB[jr] != 0.0f;
           if (fA)
-            vA = residual_cell<FAST>(ms, s_pos, rA[jr], aA[jr], zA[jr], zA[jrm], zA[jrp], zp[oA], zB[jr],
-                                     zp[cA + xm], zp[cA + xp]);
+            vA = residual_cell<FAST>(ms, s_pos, rA[jr], aA[jr], zA[jr], zA[jrm], zA[jrp], qA[jr * ZPL], zB[jr],
+                                     pA[jr * ZPL - 1], pA[jr * ZPL + 1]);
           if (fB)
-            vB = residual_cell<FAST>(ms, s_pos, rB[jr], aB[jr], zB[jr], zB[jrm], zB[jrp], zp[oB], zA[jr],
-                                     zp[cB + xm], zp[cB + xp]);
+            vB = residual_cell<FAST>(ms, s_pos, rB[jr], aB[jr], zB[jr], zB[jrm], zB[jrp], qB[jr * ZPL], zA[jr],
+                                     pB[jr * ZPL - 1], pB[jr * ZPL + 1]);
           // rows y0 (even) and y1 of this column; the x + 1 column is the next lane
           const float v0 = odd ? vB : vA, v1 = odd ? vA : vB;
-          const int f = odd ? ((int)fB | ((int)fA << 1)) : ((int)fA | ((int)fB << 1));
+          const bool f0 = odd ? fB : fA, f1 = odd ? fA : fB;
           const float p0 = __shfl_xor_sync(0xffffffffu, v0, 1);
           const float p1 = __shfl_xor_sync(0xffffffffu, v1, 1);
-          const int pf = __shfl_xor_sync(0xffffffffu, f, 1);
-          if (!odd) {
-            // children in the order (y0, x0), (y0, x1), (y1, x0), (y1, x1), plane by plane
-            if ((pr & 1) == 0) acc = 0.0f;
-            if (f & 1) acc = __fadd_rn(acc, v0);
-            if (pf & 1) acc = __fadd_rn(acc, p0);
-            if (f & 2) acc = __fadd_rn(acc, v1);
-            if (pf & 2) acc = __fadd_rn(acc, p1);
-            if ((pr & 1) == 1 && ownA) {
-              const long long gc = ((long long)(pr >> 1) * ncy + (gy0 >> 1)) * ncx + (gx >> 1);
-              A.rc[gc] = from_f<ST>(__fmul_rn(A.rho, acc));
-              A.zc[gc] = from_f<ST>(0.0f);
-            }
+          const unsigned pf = __shfl_xor_sync(0xffffffffu, (unsigned)f0 | ((unsigned)f1 << 1), 1);
+          // children in the order (y0, x0), (y0, x1), (y1, x0), (y1, x1), plane by
+          // plane, FLUID children only; even-x lanes keep the sum
+          if ((u & 1) == 0) acc = 0.0f;
+          acc = f0 ? __fadd_rn(acc, v0) : acc;
+          acc = (pf & 1u) ? __fadd_rn(acc, p0) : acc;
+          acc = f1 ? __fadd_rn(acc, v1) : acc;
+          acc = (pf & 2u) ? __fadd_rn(acc, p1) : acc;
+          if ((u & 1) == 1 && !odd && in_grid) {
+            const int gc = (pr >> 1) * cps + cc;
+            A.rc[gc] = from_f<ST>(__fmul_rn(A.rho, acc));
+            A.zc[gc] = from_f<ST>(0.0f);
           }
         }
+      }
+
+      // ---- the next plane's loads, then the step's barrier ------------------------------
+      if (t == 0 && P + 1 <= p_last) {
+        const uint32_t par = (uint32_t)((k0 + (u + 1 == W ? 1 : 0)) & 1);
+        if (!mbar_wait_bounded(&bar[(u + 1) % W], par)) abort_flag = 1;
       }
       __syncthreads();
       if (abort_flag) {
         aborted = true;
-        stop_p = P;
+        stop_p = P + 1;
         break;
       }
     }
@@ -431,7 +464,7 @@ __global__ void __launch_bounds__(ColGeom<ST, NS, TX, TY>::NT, MINB)
     // a TMA load did not complete within the bound: flag it, then wait
     // (bounded) for this block's loads still in flight before leaving
     atomicOr(&flag->wait_timeout, 1);
-    const int last_issued = min(stop_p + W - 1, p_last);
+    const int last_issued = min(stop_p + W - 2, p_last);  // issued at step stop_p - 1 (or before the loop)
     for (int p = stop_p; p <= last_issued; ++p) {
       const int k = p - p_first;
       mbar_wait_bounded(&bar[k % W], (uint32_t)((k / W) & 1));

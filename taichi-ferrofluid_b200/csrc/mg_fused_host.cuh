@@ -1,6 +1,7 @@
 // Host side of the fused V-cycle: per-level launch shapes, the split between
 // streamed levels and the block-resident coarse levels, and the launches.
 #pragma once
+#include <algorithm>
 #include <cmath>
 #include <cstring>
 #include <type_traits>
@@ -118,7 +119,9 @@ struct FusedPlan {
 // the slowest axis, enough blocks to fill every SM with the blocks that fit
 // its shared memory plus `extra` (then a block's chunk is shorter).  Small
 // levels are latency-bound: short chunks (more blocks, shorter serial plane
-// chains) beat the extra halo planes they load.
+// chains) beat the extra halo planes they load.  The column kernel takes
+// exactly that many blocks (no partial last wave) and cuts each tile's planes
+// into chunks of nearly equal length itself.
 inline void level_grid(FusedPlan* F, const Geom& g, int l, int extra) {
   const int nx = F->dim == 3 ? g.n[2] : g.n[1];
   const int ny = F->dim == 3 ? g.n[1] : 1;
@@ -129,6 +132,16 @@ inline void level_grid(FusedPlan* F, const Geom& g, int l, int extra) {
   F->tiles_y[l] = F->dim == 3 ? (ny + ty - 1) / ty : 1;
   const long long tiles = (long long)F->tiles_x[l] * F->tiles_y[l];
   const long long target = (long long)(per_sm + extra) * F->num_sms;
+  if (c) {
+    // k_colsweep: exactly `target` blocks (whole waves), each tile cut into
+    // chunks of nearly equal even length (at least 2 planes)
+    long long nb = std::min(target, tiles * (g.n[0] / 2));
+    nb = std::max(nb, tiles);
+    F->blocks[l] = (int)nb;
+    F->chunk[l] = (int)((g.n[0] * tiles + nb - 1) / nb);  // the mean chunk
+    F->grid_extra[l] = (unsigned char)extra;
+    return;
+  }
   long long chunk = (long long)g.n[0] * tiles / target;
   if (chunk < 2) chunk = 2;
   chunk &= ~1LL;
@@ -511,13 +524,15 @@ inline bool tensor_map_3d(CUtensorMap* m, const void* base, int es, const Geom& 
 }
 
 // The column kernel runs streamed level l of a 3D label-uniform plan with
-// pre_post 2 whose rows are whole 16-byte units of every array and whose
-// extents halve evenly (pairs of rows, pairs of planes).
+// pre_post 2 whose rows are whole 16-byte units of every array, whose
+// extents halve evenly (pairs of rows, pairs of planes) and whose cells have
+// 32-bit indices.
 inline bool col_ok(const FusedPlan& F, const Level* lv, int l) {
   if (!F.valid || F.sto || F.dim != 3 || F.ns != 4 || l >= F.lc || F.split[l]) return false;
   const Geom& g = lv[l].g;
   const int es = F.storage == MG_STORE_F32 ? 4 : 2;
-  return g.n[2] % (16 / es) == 0 && g.n[1] % 2 == 0 && g.n[0] % 2 == 0 && encode_tiled() != nullptr;
+  return g.n[2] % (16 / es) == 0 && g.n[1] % 2 == 0 && g.n[0] % 2 == 0 &&
+         (long long)g.n[0] * g.n[1] * g.n[2] < (1LL << 31) && encode_tiled() != nullptr;
 }
 
 template <typename ST, int NS, int TX, int TY, bool PRE, int MINB>
