@@ -136,7 +136,7 @@ __device__ void coarse_smooth(const CoarseArgs& A, int l, int phase, float* zm, 
     const int p = g.at(c0, c1, c2);
     const float a = sa[p];
     if (a == 0.0f) continue;
-    zm[p] = __fdiv_rn(__fsub_rn(sr[p], csum_t<STO>(zm, sx, A.total, p, g, A.dim, ms)), a);
+    zm[p] = div_pos(__fsub_rn(sr[p], csum_t<STO>(zm, sx, A.total, p, g, A.dim, ms)), a);
   }
 }
 
@@ -254,7 +254,7 @@ __device__ __forceinline__ void coarse_vcycle(const CoarseArgs& A, unsigned char
               const int ps = p >= 0 ? p : g.at(0, 0, 0);     // an in-range cell for empty slots
               const float r_ = ph ? rr[1][k] : rr[0][k];
               const float a_ = ph ? aa[1][k] : aa[0][k];
-              v[k] = __fdiv_rn(__fsub_rn(r_, csum_t<STO>(zm, sx, A.total, ps, g, dim, ms)), a_);
+              v[k] = div_pos(__fsub_rn(r_, csum_t<STO>(zm, sx, A.total, ps, g, dim, ms)), a_);
             }
 #pragma unroll
             for (int k = 0; k < kBottomPerThread; ++k) {   // then the stores

@@ -81,6 +81,20 @@ __device__ __forceinline__ void tma_load_3d(void* dst, const CUtensorMap* map, u
       : "memory");
 }
 
+// A shared-memory load the compiler may schedule freely within a plane step
+// (no memory clobber).  Its address comes from launder() after the step's
+// barrier, so it is never hoisted above that barrier; it is used only for
+// cells no thread writes during the step.
+__device__ __forceinline__ float lds_free(uint32_t addr) {
+  float v;
+  asm("ld.shared.f32 %0, [%1];" : "=f"(v) : "r"(addr));
+  return v;
+}
+__device__ __forceinline__ uint32_t launder(uint32_t a) {
+  asm volatile("" : "+r"(a));
+  return a;
+}
+
 // ---- shape of one instantiation -------------------------------------------------------
 template <typename ST, int NS, int TX, int TY>
 struct ColGeom {
@@ -126,11 +140,11 @@ __device__ __forceinline__ float smooth_cell(float ms, float s, float r, float a
     const float sum = __fadd_rn(__fadd_rn(__fadd_rn(z0m, z0p), __fadd_rn(z1m, z1p)), __fadd_rn(z2m, z2p));
     return __fdividef(fmaf(s, sum, r), a);
   } else {
-    float ret = 0.0f;
-    ret = __fadd_rn(ret, __fadd_rn(__fmul_rn(ms, z0m), __fmul_rn(ms, z0p)));
+    // (the reference's sum starts from 0; 0 + x == x up to the sign of a zero)
+    float ret = __fadd_rn(__fmul_rn(ms, z0m), __fmul_rn(ms, z0p));
     ret = __fadd_rn(ret, __fadd_rn(__fmul_rn(ms, z1m), __fmul_rn(ms, z1p)));
     ret = __fadd_rn(ret, __fadd_rn(__fmul_rn(ms, z2m), __fmul_rn(ms, z2p)));
-    return __fdiv_rn(__fsub_rn(r, ret), a);
+    return div_pos(__fsub_rn(r, ret), a);
   }
 }
 
@@ -142,8 +156,7 @@ __device__ __forceinline__ float residual_cell(float ms, float s, float r, float
     const float sum = __fadd_rn(__fadd_rn(__fadd_rn(z0m, z0p), __fadd_rn(z1m, z1p)), __fadd_rn(z2m, z2p));
     return fmaf(-a, z, fmaf(s, sum, r));
   } else {
-    float ret = 0.0f;
-    ret = __fadd_rn(ret, __fadd_rn(__fmul_rn(ms, z0m), __fmul_rn(ms, z0p)));
+    float ret = __fadd_rn(__fmul_rn(ms, z0m), __fmul_rn(ms, z0p));
     ret = __fadd_rn(ret, __fadd_rn(__fmul_rn(ms, z1m), __fmul_rn(ms, z1p)));
     ret = __fadd_rn(ret, __fadd_rn(__fmul_rn(ms, z2m), __fmul_rn(ms, z2p)));
     return __fsub_rn(r, __fadd_rn(__fmul_rn(a, z), ret));
@@ -256,6 +269,8 @@ __global__ void __launch_bounds__(ColGeom<ST, NS, TX, TY>::NT, MINB)
   float* const pB = zs + (rowB + 1) * ZX + rx + 1;
   const float* const qA = zs + (outA + 1) * ZX + rx + 1;  // the out-of-pair row neighbours
   const float* const qB = zs + (outB + 1) * ZX + rx + 1;
+  const uint32_t aPA = smem_addr(pA), aPB = smem_addr(pB), aQA = smem_addr(qA), aQB = smem_addr(qB);
+  constexpr uint32_t PLB4 = ZPL * 4;  // bytes between shared z planes
   const int kA = rowA * RXB + rx + XOFF, kB = rowB * RXB + rx + XOFF;  // in a TMA slot
   const int dxr = max(max(HX - rx, rx - (HX + TX - 1)), 0);
   const int ringA = max(dxr, max(max(NS - rowA, rowA - (NS + TY - 1)), 0));
@@ -316,6 +331,8 @@ __global__ void __launch_bounds__(ColGeom<ST, NS, TX, TY>::NT, MINB)
       const int P = P0 + u;
       if (P > p_last) break;
       const int q = P - p_first;
+      // this step's in-plane neighbour reads (planes written before the last barrier)
+      const uint32_t sPA = launder(aPA), sPB = launder(aPB), sQA = launder(aQA), sQB = launder(aQB);
       // plane P + W - 1 into the slot of plane P - 1 (read before the last barrier)
       if (t == 0 && P + W - 1 <= p_last) issue(P + W - 1, (u + W - 1) % W);
 
@@ -338,10 +355,10 @@ __global__ void __launch_bounds__(ColGeom<ST, NS, TX, TY>::NT, MINB)
           // the first half sweep is pointwise (z = 0 before it): z = r / Adiag on
           // the colour-0 cell, the one active in this step (A: even P)
           if ((u & 1) == 0) {
-            zA[u] = aA[u] != 0.0f ? (FAST ? __fdividef(rA[u], aA[u]) : __fdiv_rn(rA[u], aA[u])) : 0.0f;
+            zA[u] = aA[u] != 0.0f ? (FAST ? __fdividef(rA[u], aA[u]) : div_pos(rA[u], aA[u])) : 0.0f;
             zB[u] = 0.0f;
           } else {
-            zB[u] = aB[u] != 0.0f ? (FAST ? __fdividef(rB[u], aB[u]) : __fdiv_rn(rB[u], aB[u])) : 0.0f;
+            zB[u] = aB[u] != 0.0f ? (FAST ? __fdividef(rB[u], aB[u]) : div_pos(rB[u], aB[u])) : 0.0f;
             zA[u] = 0.0f;
           }
         } else {
@@ -376,15 +393,15 @@ __global__ void __launch_bounds__(ColGeom<ST, NS, TX, TY>::NT, MINB)
         // (a branch: most warps of a scene's air or solid skip the division)
         if ((u & 1) == 0) {
           if (ringA <= NS - s && aA[j] != 0.0f) {
-            const float v = smooth_cell<FAST>(ms, s_pos, rA[j], aA[j], zA[jm], zA[jp], qA[j * ZPL], zB[j],
-                                              pA[j * ZPL - 1], pA[j * ZPL + 1]);
+            const float v = smooth_cell<FAST>(ms, s_pos, rA[j], aA[j], zA[jm], zA[jp], lds_free(sQA + j * PLB4),
+                                              zB[j], lds_free(sPA + j * PLB4 - 4), lds_free(sPA + j * PLB4 + 4));
             zA[j] = v;
             pA[j * ZPL] = v;
           }
         } else {
           if (ringB <= NS - s && aB[j] != 0.0f) {
-            const float v = smooth_cell<FAST>(ms, s_pos, rB[j], aB[j], zB[jm], zB[jp], qB[j * ZPL], zA[j],
-                                              pB[j * ZPL - 1], pB[j * ZPL + 1]);
+            const float v = smooth_cell<FAST>(ms, s_pos, rB[j], aB[j], zB[jm], zB[jp], lds_free(sQB + j * PLB4),
+                                              zA[j], lds_free(sPB + j * PLB4 - 4), lds_free(sPB + j * PLB4 + 4));
             zB[j] = v;
             pB[j * ZPL] = v;
           }
@@ -420,11 +437,11 @@ __global__ void __launch_bounds__(ColGeom<ST, NS, TX, TY>::NT, MINB)
           const bool fA = in_grid && aA[jr] != 0.0f, fB = in_grid && aB[jr] != 0.0f;
           float vA = 0.0f, vB = 0.0f;
           if (fA)
-            vA = residual_cell<FAST>(ms, s_pos, rA[jr], aA[jr], zA[jr], zA[jrm], zA[jrp], qA[jr * ZPL], zB[jr],
-                                     pA[jr * ZPL - 1], pA[jr * ZPL + 1]);
+            vA = residual_cell<FAST>(ms, s_pos, rA[jr], aA[jr], zA[jr], zA[jrm], zA[jrp], lds_free(sQA + jr * PLB4),
+                                     zB[jr], lds_free(sPA + jr * PLB4 - 4), lds_free(sPA + jr * PLB4 + 4));
           if (fB)
-            vB = residual_cell<FAST>(ms, s_pos, rB[jr], aB[jr], zB[jr], zB[jrm], zB[jrp], qB[jr * ZPL], zA[jr],
-                                     pB[jr * ZPL - 1], pB[jr * ZPL + 1]);
+            vB = residual_cell<FAST>(ms, s_pos, rB[jr], aB[jr], zB[jr], zB[jrm], zB[jrp], lds_free(sQB + jr * PLB4),
+                                     zA[jr], lds_free(sPB + jr * PLB4 - 4), lds_free(sPB + jr * PLB4 + 4));
           // rows y0 (even) and y1 of this column; the x + 1 column is the next lane
           const float v0 = odd ? vB : vA, v1 = odd ? vA : vB;
           const bool f0 = odd ? fB : fA, f1 = odd ? fA : fB;

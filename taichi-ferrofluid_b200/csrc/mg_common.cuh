@@ -72,6 +72,15 @@ struct Control {
   double zAp;                 // z.Ap of the mixed form's flexible beta
 };
 
+// x / a in IEEE float32 for a > 0 (Adiag of a FLUID cell).  A zero dividend
+// would take the division's slow path (a subroutine call for the whole warp);
+// it is returned as is, which is x / a bit for bit (a zero of x's sign).
+__device__ __forceinline__ float div_pos(float x, float a) {
+  const bool z = x == 0.0f;
+  const float q = __fdiv_rn(z ? 1.0f : x, a);
+  return z ? x : q;
+}
+
 template <typename T> __device__ __forceinline__ float to_f(T v);
 template <> __device__ __forceinline__ float to_f<float>(float v) { return v; }
 template <> __device__ __forceinline__ float to_f<__half>(__half v) { return __half2float(v); }

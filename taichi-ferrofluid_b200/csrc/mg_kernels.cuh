@@ -261,7 +261,7 @@ __global__ void k_smooth_w4(Level L, int phase) {
 #pragma unroll
       for (int ee = 0; ee < 2; ++ee) {  // unrolled over both values of e0
         const int e = ee + 2 * h;
-        if (ee == e0) v = __fdiv_rn(__fsub_rn(g.R[e], group4_nsum(g, e)), g.D[e]);
+        if (ee == e0) v = div_pos(__fsub_rn(g.R[e], group4_nsum(g, e)), g.D[e]);
       }
       out[h] = v;
     }
@@ -293,7 +293,7 @@ __global__ void k_smooth_first_w4(Level L) {
     float v[4] = {0.0f, 0.0f, 0.0f, 0.0f};
 #pragma unroll
     for (int e = 0; e < 4; ++e)
-      if (((e - e0) & 1) == 0) v[e] = __fdiv_rn(__fsub_rn(R[e], 0.0f), D[e]);
+      if (((e - e0) & 1) == 0) v[e] = div_pos(__fsub_rn(R[e], 0.0f), D[e]);
     reinterpret_cast<float4*>(z)[q] = make_float4(v[0], v[1], v[2], v[3]);
   }
 }

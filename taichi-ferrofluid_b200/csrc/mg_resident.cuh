@@ -156,7 +156,7 @@ __device__ __forceinline__ void res_smooth(const RB& b, int col) {
       const float a = b.ad(c0, c1, c2);
       if (a != 0.0f) {
         const int p = b.zp(c0, c1, c2);
-        b.zs[p] = __fdiv_rn(__fsub_rn(b.rs[b.ri(c0, c1, c2)], res_nsum(b, p)), a);
+        b.zs[p] = div_pos(__fsub_rn(b.rs[b.ri(c0, c1, c2)], res_nsum(b, p)), a);
       }
     }
     return;
@@ -173,7 +173,7 @@ __device__ __forceinline__ void res_smooth(const RB& b, int col) {
       pz[u] = b.zp(c0, c1, c2);
       const float a = b.ad(c0, c1, c2);
       ok[u] = j0 + u * (int)blockDim.x < cnt && a != 0.0f;
-      val[u] = ok[u] ? __fdiv_rn(__fsub_rn(b.rs[b.ri(c0, c1, c2)], res_nsum(b, pz[u])), a) : 0.0f;
+      val[u] = ok[u] ? div_pos(__fsub_rn(b.rs[b.ri(c0, c1, c2)], res_nsum(b, pz[u])), a) : 0.0f;
     }
 #pragma unroll
     for (int u = 0; u < 2; ++u)
@@ -269,7 +269,7 @@ __global__ void __launch_bounds__(kResThreads, 1) k_resident(ResArgs A) {
       int c0, c1, c2;
       res_colour_cell(b, j, 0, c0, c1, c2);
       const float a = b.ad(c0, c1, c2);
-      if (a != 0.0f) b.zs[b.zp(c0, c1, c2)] = __fdiv_rn(b.rs[b.ri(c0, c1, c2)], a);
+      if (a != 0.0f) b.zs[b.zp(c0, c1, c2)] = div_pos(b.rs[b.ri(c0, c1, c2)], a);
     }
     for (int m = 2; m <= A.ns; ++m) {
       res_exchange(b, A, rank, 1 << ((m - 2) & 1));  // the colour of half sweep m - 1

@@ -214,7 +214,7 @@ __device__ __forceinline__ void sweep_body(const SweepArgs<ST>& A, int bid_, int
     for (int e = 0; e < 4; ++e) {
       if (PRE) {
         const bool c0 = ((p + gy + gx + e) & 1) == 0;
-        zv[e] = (c0 && a[e] != 0.0f) ? (FAST ? __fdividef(r[e], a[e]) : __fdiv_rn(r[e], a[e])) : 0.0f;
+        zv[e] = (c0 && a[e] != 0.0f) ? (FAST ? __fdividef(r[e], a[e]) : div_pos(r[e], a[e])) : 0.0f;
       } else {
         zv[e] = a[e] != 0.0f ? z[e] : 0.0f;
       }
@@ -293,7 +293,7 @@ __device__ __forceinline__ void sweep_body(const SweepArgs<ST>& A, int bid_, int
   // smooth (mgpcg.py:104-109) of the FLUID cell c with diagonal a and residual r
   auto upd = [&](float r, int sb, int sc, int sa_, int c, float a) -> float {
     if constexpr (FAST) return __fdividef(fmaf(spos, zsum(sb, sc, sa_, c), r), a);
-    else return __fdiv_rn(__fsub_rn(r, nsum(sb, sc, sa_, c)), a);
+    else return div_pos(__fsub_rn(r, nsum(sb, sc, sa_, c)), a);
   };
 
   float acc = 0.0f;                               // restriction accumulator (PRE)
