@@ -44,7 +44,7 @@ extern "C" {
 #define MG_SOLVE_CONVERGED 0
 #define MG_SOLVE_MAX_ITERS 1   /* stopped at max_iters (the reference is silent) */
 #define MG_SOLVE_NONFINITE 2   /* a reduction produced NaN/Inf (H3: zero Adiag) */
-#define MG_SOLVE_BAD_OPERATOR 3 /* mg_plan_prepare_declared's declaration was wrong */
+#define MG_SOLVE_BAD_OPERATOR 3 /* a declared operator form (mg_plan_prepare_declared*) was wrong */
 #define MG_SOLVE_TIMEOUT 4      /* a bounded wait on a TMA copy ran out (the sweep left its chunk) */
 
 /* V-cycle grid storage type */
@@ -381,6 +381,13 @@ MG_API int mg_plan_prepare(mg_plan_t* plan, void* stream);
  * MG_SOLVE_BAD_OPERATOR.  No reference counterpart (the reference has no
  * operator forms). */
 MG_API int mg_plan_prepare_declared(mg_plan_t* plan, const float* offdiag, void* stream);
+/* Prepare without synchronizing for a whole-domain operator: the caller
+ * declares that every cell of every level is FLUID with a nonzero diagonal
+ * and the couplings are stored (what the potential Strategies build with
+ * full_reinitialize, mgpcg.py:89-94, potential_function.py:6-60).  Verified
+ * on the device like mg_plan_prepare_declared; a wrong declaration ends the
+ * solve with MG_SOLVE_BAD_OPERATOR. */
+MG_API int mg_plan_prepare_declared_whole(mg_plan_t* plan, void* stream);
 
 /* The whole per-request pressure path in one call, enqueued on `stream` with
  * no host synchronization: initialize, cell_type, PressureProjectStrategy

@@ -64,7 +64,7 @@ struct Control {
   double scale_r;             // r (stored, level 0 input of the V-cycle) = scale_r * r
   double kappa;               // coefficient scale of 16-bit grids
   double n_fluid;             // FLUID cells of level 0
-  int bad_operator;           // set when a declared label-uniform form is wrong
+  int bad_operator;           // declared operator form: bit 0 wrong, bit 1 a FLUID cell with Adiag 0
   int wait_timeout;           // set when a bounded wait in a kernel ran out
   unsigned int counter[8];    // arrival counters of the last-block reductions
   double scratch[8];          // single-value results of mg_reduce
@@ -72,9 +72,10 @@ struct Control {
   double zAp;                 // z.Ap of the mixed form's flexible beta
 };
 
-// x / a in IEEE float32 for a > 0 (Adiag of a FLUID cell).  A zero dividend
+// x / a in IEEE float32 for a != 0 (Adiag of a FLUID cell).  A zero dividend
 // would take the division's slow path (a subroutine call for the whole warp);
-// it is returned as is, which is x / a bit for bit (a zero of x's sign).
+// it is returned as is: x / a bit for bit when a > 0, equal in value (a zero
+// of the other sign) when a < 0.
 __device__ __forceinline__ float div_pos(float x, float a) {
   const bool z = x == 0.0f;
   const float q = __fdiv_rn(z ? 1.0f : x, a);

@@ -19,21 +19,38 @@ __global__ void k_set_kappa(Control* ctl, double kappa) {
 }
 
 // Checks a declared label-uniform level: Adiag != 0 exactly on FLUID cells
-// and Ax = -s between two FLUID cells, 0 elsewhere.  Flags a mismatch.
+// and Ax = -s between two FLUID cells, 0 elsewhere.  Flags a mismatch (bit
+// 0), or a FLUID cell with a zero diagonal (bit 1: the reference's smoothing
+// divides by zero there, a non-finite solve).
 __global__ void k_verify_uniform(Level L, float s, Control* ctl) {
-  bool bad = false;
+  int bad = 0;
   for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < L.g.count;
        i += (long long)gridDim.x * blockDim.x) {
     int c[3];
     L.g.coords(i, c);
     const bool fl = L.type[i] == FLUID;
-    if (fl != (L.Adiag[i] != 0.0f)) bad = true;
+    if (fl && L.Adiag[i] == 0.0f) bad |= 2;
+    else if (!fl && L.Adiag[i] != 0.0f) bad |= 1;
     for (int k = 0; k < L.g.dim; ++k) {
       const bool coupled = fl && (c[k] + 1 < L.g.n[k]) && L.type[i + L.g.stride(k)] == FLUID;
-      if (L.Ax[k][i] != (coupled ? -s : 0.0f)) bad = true;
+      if (L.Ax[k][i] != (coupled ? -s : 0.0f)) bad |= 1;
     }
   }
-  if (__any_sync(0xffffffffu, bad) && (threadIdx.x & 31) == 0) atomicOr(&ctl->bad_operator, 1);
+  bad = __reduce_or_sync(0xffffffffu, bad);
+  if (bad && (threadIdx.x & 31) == 0) atomicOr(&ctl->bad_operator, bad);
+}
+
+// Checks a declared whole-domain level: every cell FLUID (bit 0) with
+// Adiag != 0 (bit 1, as k_verify_uniform).
+__global__ void k_verify_whole(Level L, Control* ctl) {
+  int bad = 0;
+  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < L.g.count;
+       i += (long long)gridDim.x * blockDim.x) {
+    if (L.type[i] != FLUID) bad |= 1;
+    if (L.Adiag[i] == 0.0f) bad |= 2;
+  }
+  bad = __reduce_or_sync(0xffffffffu, bad);
+  if (bad && (threadIdx.x & 31) == 0) atomicOr(&ctl->bad_operator, bad);
 }
 
 // Copies one solve's parameters into the control block.
@@ -93,8 +110,9 @@ __device__ __forceinline__ void pcg_begin_body(int bid_, int nb_, Level L, const
     ctl->run = 1;
     ctl->since_refresh = 0;
     if (warm) ctl->beta = 0.0f;  // p is rebuilt from z only
-    if (ctl->bad_operator) {     // the declared operator form did not hold
-      ctl->status = MG_SOLVE_BAD_OPERATOR;
+    if (ctl->bad_operator) {     // the declared operator form did not hold,
+      // or a FLUID cell has a zero diagonal (the reference divides by it)
+      ctl->status = (ctl->bad_operator & 1) ? MG_SOLVE_BAD_OPERATOR : MG_SOLVE_NONFINITE;
       ctl->run = 0;
     }
     ctl->wait_timeout = 0;

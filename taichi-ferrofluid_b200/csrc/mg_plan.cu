@@ -850,7 +850,7 @@ int solve_direct(mg_plan* P, const mg_solve_params_t* prm, cudaStream_t s) {
 // Lets the library's other translation units record an error message.
 void mg_internal_set_error(const char* msg) { snprintf(g_err, sizeof(g_err), "%s", msg); }
 
-static int finish_prepare(mg_plan_t* P, cudaStream_t s, bool declared);
+static int finish_prepare(mg_plan_t* P, cudaStream_t s, int declared);
 
 // ============================================================================
 // C ABI
@@ -1478,7 +1478,7 @@ int mg_plan_prepare(mg_plan_t* P, void* stream) {
     P->offdiag[l] = uniform && !none ? (float)(-h[0]) : 0.0f;
     P->whole[l] = h[3] == 0.0 ? 1 : 0;  // every cell FLUID with a nonzero diagonal
   }
-  return finish_prepare(P, s, false);
+  return finish_prepare(P, s, 0);
 }
 
 int mg_plan_prepare_declared(mg_plan_t* P, const float* offdiag, void* stream) {
@@ -1489,14 +1489,25 @@ int mg_plan_prepare_declared(mg_plan_t* P, const float* offdiag, void* stream) {
     P->offdiag[l] = offdiag[l];
     P->whole[l] = 0;
   }
-  return finish_prepare(P, S(stream), true);
+  return finish_prepare(P, S(stream), 1);
+}
+
+int mg_plan_prepare_declared_whole(mg_plan_t* P, void* stream) {
+  NEED_BOUND(P);
+  for (int l = 0; l < P->L; ++l) {
+    P->op_form[l] = 0;
+    P->offdiag[l] = 0.0f;
+    P->whole[l] = 1;
+  }
+  return finish_prepare(P, S(stream), 2);
 }
 
 }  // extern "C"
 
 // Launch shapes, 16-bit coefficient copies, FLUID count, scale factors and
-// (declared forms) the asynchronous verification; no host synchronization.
-static int finish_prepare(mg_plan_t* P, cudaStream_t s, bool declared) {
+// (declared forms: 1 label-uniform, 2 whole-domain) the asynchronous
+// verification; no host synchronization.
+static int finish_prepare(mg_plan_t* P, cudaStream_t s, int declared) {
   // 2. launch shapes of the fused V-cycle
   P->fp.valid = false;
   if (!(P->d.flags & MG_PLAN_STORED))
@@ -1524,10 +1535,15 @@ static int finish_prepare(mg_plan_t* P, cudaStream_t s, bool declared) {
   if (int rc = tune_split(P, s)) return rc;
   if (int rc = tune_stream(P, s)) return rc;
   if (int rc = tune_resident(P, s)) return rc;
-  if (declared) {
+  if (declared == 1) {
     for (int l = 0; l < P->L; ++l) {
       k_verify_uniform<<<P->ew_blocks[l], 256, 0, s>>>(P->lv[l], P->offdiag[l], P->ctl);
       CKL("k_verify_uniform");
+    }
+  } else if (declared == 2) {
+    for (int l = 0; l < P->L; ++l) {
+      k_verify_whole<<<P->ew_blocks[l], 256, 0, s>>>(P->lv[l], P->ctl);
+      CKL("k_verify_whole");
     }
   }
   // 4. the solve graph captured kernel arguments (shapes, s_l, kappa): rebuild

@@ -25,15 +25,15 @@
 // Adiag tells FLUID cells (nonzero on exactly the FLUID cells of a
 // label-uniform level).
 //
-// Ring reads and the barrier: after a half sweep of colour c every CTA
-// arrives at the cluster barrier (release) and waits (acquire), then copies
-// the colour-c cells of its ring from its neighbours' faces.  Meanwhile a
-// neighbour may already smooth the other colour, which writes no colour-c
-// cell; colour-c cells change again only after the next barrier, which the
-// reader reaches after its copy.  The copies before a restriction and after a
-// prolongation take both colours: a cell of the colour being smoothed that is
-// read early is copied again before it is used.  A final barrier keeps every
-// CTA's shared memory alive until its neighbours' last reads.
+// Rings and the barrier: whenever a CTA gives a FLUID cell on a face of its
+// brick a new z (a half sweep, the prolongation), it also stores the value
+// into the ring of the neighbour that reads it (distributed shared memory),
+// and one cluster barrier (arrive.release, wait.acquire) then publishes every
+// CTA's stores.  During a half sweep of colour c the CTAs store colour-c
+// values and read colour 1 - c ring cells only, so stores and reads of a ring
+// never meet between two barriers.  A barrier after the initial zeroing keeps
+// early stores from being overwritten, and a final one keeps every CTA's
+// shared memory alive until its neighbours' last stores.
 #pragma once
 #include <cooperative_groups.h>
 
@@ -144,9 +144,40 @@ __device__ __forceinline__ void res_colour_cell(const RB& b, int j, int col, int
   c2 = 2 * k + ((col - b.o0 - b.o1 - b.o2 - c0 - c1) & 1);
 }
 
+// The six neighbouring bricks' zs of a brick level (axis 0 lower, upper, axis
+// 1 lower, upper, axis 2 lower, upper) in their shared memory; null where the
+// level ends.
+struct RNb {
+  float* z[6];
+};
+__device__ __forceinline__ RNb res_nbrs(const RB& b, const ResArgs& A, int rank) {
+  cgx::cluster_group cl = cgx::this_cluster();
+  const int st1 = A.nb[2], st0 = A.nb[1] * A.nb[2];
+  RNb n;
+  n.z[0] = b.o0 > 0 ? cl.map_shared_rank(b.zs, rank - st0) : nullptr;
+  n.z[1] = b.o0 + b.B0 < b.n0 ? cl.map_shared_rank(b.zs, rank + st0) : nullptr;
+  n.z[2] = b.o1 > 0 ? cl.map_shared_rank(b.zs, rank - st1) : nullptr;
+  n.z[3] = b.o1 + b.B1 < b.n1 ? cl.map_shared_rank(b.zs, rank + st1) : nullptr;
+  n.z[4] = b.o2 > 0 ? cl.map_shared_rank(b.zs, rank - 1) : nullptr;
+  n.z[5] = b.o2 + b.B2 < b.n2 ? cl.map_shared_rank(b.zs, rank + 1) : nullptr;
+  return n;
+}
+
+// v, the new z of brick cell (c0, c1, c2), into the rings of the neighbours
+// whose cells are its face neighbours.
+__device__ __forceinline__ void res_push(const RB& b, const RNb& n, int c0, int c1, int c2, float v) {
+  if (c0 == 0 && n.z[0]) n.z[0][b.zp(b.B0, c1, c2)] = v;
+  if (c0 == b.B0 - 1 && n.z[1]) n.z[1][b.zp(-1, c1, c2)] = v;
+  if (c1 == 0 && n.z[2]) n.z[2][b.zp(c0, b.B1, c2)] = v;
+  if (c1 == b.B1 - 1 && n.z[3]) n.z[3][b.zp(c0, -1, c2)] = v;
+  if (c2 == 0 && n.z[4]) n.z[4][b.zp(c0, c1, b.B2)] = v;
+  if (c2 == b.B2 - 1 && n.z[5]) n.z[5][b.zp(c0, c1, -1)] = v;
+}
+
 // One red-black half sweep (mgpcg.py:104-109) of colour `col` over the brick,
-// two cells per thread and iteration, both computed before either is stored.
-__device__ __forceinline__ void res_smooth(const RB& b, int col) {
+// two cells per thread and iteration, both computed before either is stored;
+// face cells also go to the neighbours' rings.
+__device__ __forceinline__ void res_smooth(const RB& b, const RNb& n, int col) {
   const int cnt = (b.B0 * b.B1 * b.B2) >> 1;
   if (cnt <= (int)blockDim.x) {  // one cell per thread, no empty second item
     const int j = threadIdx.x;
@@ -156,77 +187,35 @@ __device__ __forceinline__ void res_smooth(const RB& b, int col) {
       const float a = b.ad(c0, c1, c2);
       if (a != 0.0f) {
         const int p = b.zp(c0, c1, c2);
-        b.zs[p] = div_pos(__fsub_rn(b.rs[b.ri(c0, c1, c2)], res_nsum(b, p)), a);
+        const float v = div_pos(__fsub_rn(b.rs[b.ri(c0, c1, c2)], res_nsum(b, p)), a);
+        b.zs[p] = v;
+        res_push(b, n, c0, c1, c2, v);
       }
     }
     return;
   }
   for (int j0 = threadIdx.x; j0 < cnt; j0 += 2 * blockDim.x) {
-    int pz[2];
+    int cc[2][3];
     float val[2];
     bool ok[2];
 #pragma unroll
     for (int u = 0; u < 2; ++u) {
       const int j = min(j0 + u * (int)blockDim.x, cnt - 1);
-      int c0, c1, c2;
-      res_colour_cell(b, j, col, c0, c1, c2);
-      pz[u] = b.zp(c0, c1, c2);
-      const float a = b.ad(c0, c1, c2);
+      res_colour_cell(b, j, col, cc[u][0], cc[u][1], cc[u][2]);
+      const float a = b.ad(cc[u][0], cc[u][1], cc[u][2]);
       ok[u] = j0 + u * (int)blockDim.x < cnt && a != 0.0f;
-      val[u] = ok[u] ? div_pos(__fsub_rn(b.rs[b.ri(c0, c1, c2)], res_nsum(b, pz[u])), a) : 0.0f;
+      val[u] = ok[u] ? div_pos(__fsub_rn(b.rs[b.ri(cc[u][0], cc[u][1], cc[u][2])],
+                                         res_nsum(b, b.zp(cc[u][0], cc[u][1], cc[u][2]))),
+                               a)
+                     : 0.0f;
     }
 #pragma unroll
     for (int u = 0; u < 2; ++u)
-      if (ok[u]) b.zs[pz[u]] = val[u];
+      if (ok[u]) {
+        b.zs[b.zp(cc[u][0], cc[u][1], cc[u][2])] = val[u];
+        res_push(b, n, cc[u][0], cc[u][1], cc[u][2], val[u]);
+      }
   }
-}
-
-// Cluster barrier, then the ring cells of the colours in cmask (bit c: colour
-// c) that lie inside the level, copied from the neighbours' face cells.  Ring
-// cells are enumerated face by face (axis 0, 1, 2; lower side, upper side).
-__device__ __forceinline__ void res_exchange(const RB& b, const ResArgs& A, int rank, int cmask) {
-  cgx::cluster_group cl = cgx::this_cluster();
-  cl.sync();
-  const int a0 = b.B1 * b.B2, a1 = b.B0 * b.B2, a2 = b.B0 * b.B1;
-  const int nf = 2 * (a0 + a1 + a2);
-  const int par = b.o0 + b.o1 + b.o2;
-  const int st1 = A.nb[2], st0 = A.nb[1] * A.nb[2];
-  for (int f = threadIdx.x; f < nf; f += blockDim.x) {
-    int c0, c1, c2, q0, q1, q2, nbr, side, u, g = f;
-    if (g < 2 * a0) {
-      side = g >= a0;
-      u = g - side * a0;
-      c1 = q1 = u >> b.l2;
-      c2 = q2 = u & (b.B2 - 1);
-      c0 = side ? b.B0 : -1;
-      q0 = side ? 0 : b.B0 - 1;
-      nbr = rank + (side ? st0 : -st0);
-      if (side ? b.o0 + b.B0 >= b.n0 : b.o0 == 0) continue;
-    } else if ((g -= 2 * a0) < 2 * a1) {
-      side = g >= a1;
-      u = g - side * a1;
-      c0 = q0 = u >> b.l2;
-      c2 = q2 = u & (b.B2 - 1);
-      c1 = side ? b.B1 : -1;
-      q1 = side ? 0 : b.B1 - 1;
-      nbr = rank + (side ? st1 : -st1);
-      if (side ? b.o1 + b.B1 >= b.n1 : b.o1 == 0) continue;
-    } else {
-      g -= 2 * a1;
-      side = g >= a2;
-      u = g - side * a2;
-      c0 = q0 = u >> b.l1;
-      c1 = q1 = u & (b.B1 - 1);
-      c2 = side ? b.B2 : -1;
-      q2 = side ? 0 : b.B2 - 1;
-      nbr = rank + (side ? 1 : -1);
-      if (side ? b.o2 + b.B2 >= b.n2 : b.o2 == 0) continue;
-    }
-    if (!((cmask >> ((par + c0 + c1 + c2) & 1)) & 1)) continue;
-    const float* rz = cl.map_shared_rank(b.zs, nbr);  // the neighbour's zs of this level
-    b.zs[b.zp(c0, c1, c2)] = rz[b.zp(q0, q1, q2)];
-  }
-  __syncthreads();
 }
 
 __global__ void __launch_bounds__(kResThreads, 1) k_resident(ResArgs A) {
@@ -237,7 +226,7 @@ __global__ void __launch_bounds__(kResThreads, 1) k_resident(ResArgs A) {
   const int nlev = A.nlev;
 
   for (int i = threadIdx.x; i < A.coff; i += blockDim.x) sm[i] = 0.0f;
-  __syncthreads();
+  cl.sync();  // every CTA's rings are zero before any neighbour stores into them
   for (int i = 0; i < nlev; ++i) {  // the bricks' Adiag, where it has room
     const RB b = res_brick(A, i, sm, rank);
     if (!b.sa) continue;
@@ -254,6 +243,7 @@ __global__ void __launch_bounds__(kResThreads, 1) k_resident(ResArgs A) {
   // ---- pre-smoothing and restriction, finest to coarsest ----------------------
   for (int i = 0; i < nlev; ++i) {
     const RB b = res_brick(A, i, sm, rank);
+    const RNb nb = res_nbrs(b, A, rank);
     const int cells = b.B0 * b.B1 * b.B2;
     if (i == 0) {  // r of level lp (FLUID cells; the others hold z = 0)
 #pragma unroll 4
@@ -269,13 +259,17 @@ __global__ void __launch_bounds__(kResThreads, 1) k_resident(ResArgs A) {
       int c0, c1, c2;
       res_colour_cell(b, j, 0, c0, c1, c2);
       const float a = b.ad(c0, c1, c2);
-      if (a != 0.0f) b.zs[b.zp(c0, c1, c2)] = div_pos(b.rs[b.ri(c0, c1, c2)], a);
+      if (a != 0.0f) {
+        const float v = div_pos(b.rs[b.ri(c0, c1, c2)], a);
+        b.zs[b.zp(c0, c1, c2)] = v;
+        res_push(b, nb, c0, c1, c2, v);
+      }
     }
     for (int m = 2; m <= A.ns; ++m) {
-      res_exchange(b, A, rank, 1 << ((m - 2) & 1));  // the colour of half sweep m - 1
-      res_smooth(b, (m - 1) & 1);
+      cl.sync();  // the rings of half sweep m - 1's colour
+      res_smooth(b, nb, (m - 1) & 1);
     }
-    res_exchange(b, A, rank, 1 << ((A.ns - 1) & 1));
+    cl.sync();  // both colours of the rings for the restriction
     // restriction (mgpcg.py:111-118): coarse r = rho * sum over the FLUID
     // children (lexicographic order) of r - A z; a coarse cell of the brick
     // has all 8 children in the brick
@@ -322,6 +316,7 @@ __global__ void __launch_bounds__(kResThreads, 1) k_resident(ResArgs A) {
   // ---- prolongation and post-smoothing, coarsest to finest -----------------------
   for (int i = nlev - 1; i >= 0; --i) {
     const RB b = res_brick(A, i, sm, rank);
+    const RNb nb = res_nbrs(b, A, rank);
     const int cells = b.B0 * b.B1 * b.B2;
     const bool last = i + 1 == nlev;
     RB c;
@@ -342,17 +337,18 @@ __global__ void __launch_bounds__(kResThreads, 1) k_resident(ResArgs A) {
       const float v = __fmul_rn(A.pi, zc);
       if (b.ad(c0, c1, c2) != 0.0f) {
         const int p = b.zp(c0, c1, c2);
-        b.zs[p] = __fadd_rn(b.zs[p], v);
+        const float w = __fadd_rn(b.zs[p], v);
+        b.zs[p] = w;
+        res_push(b, nb, c0, c1, c2, w);
       } else {
         b.rs[j] = __fadd_rn(b.rs[j], v);
       }
     }
-    __syncthreads();
     // post-smoothing: colours 1, 0, 1, 0 ... (mgpcg.py:144-147), each after
-    // the ring of the colour smoothed last (both after the prolongation)
+    // the rings of the colour smoothed last (both after the prolongation)
     for (int m = 1; m <= A.ns; ++m) {
-      res_exchange(b, A, rank, m == 1 ? 3 : 1 << ((m - 1) & 1));
-      res_smooth(b, m & 1);
+      cl.sync();
+      res_smooth(b, nb, m & 1);
     }
     __syncthreads();
   }

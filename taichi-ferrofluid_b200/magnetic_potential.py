@@ -80,3 +80,10 @@ class MagneticPotentialStrategy:
             p = self.pin
             check(solver.lib.mg_build_psi_A_level(solver.plan, int(level), fine.data_ptr(), out.data_ptr(), self.dx,
                                                   p[0], p[1], p[2], solver._s()), "mg_build_psi_A_level")
+
+    def declared_operator(self, solver):
+        """The form of the A this Strategy builds with full_reinitialize:
+        every cell FLUID with stored couplings and a positive diagonal, on
+        every level.  The solver then prepares without the detection pass and
+        its host synchronization; a device kernel still checks it."""
+        return "whole", None

@@ -106,6 +106,7 @@ _SIGS = {
                                                _vp]),
     "mg_plan_prepare": (ctypes.c_int, [_vp, _vp]),
     "mg_plan_prepare_declared": (ctypes.c_int, [_vp, ctypes.POINTER(_f32), _vp]),
+    "mg_plan_prepare_declared_whole": (ctypes.c_int, [_vp, _vp]),
     "mg_pressure_solve_async": (ctypes.c_int, [_vp, _vp, _vp, _vp, _vp, _vp, _f32, _f32, _f32, _i32, _f32,
                                                ctypes.c_void_p, _vp]),
     "mg_pressure_setup_async": (ctypes.c_int, [_vp, _vp, _vp, _vp, _vp, _vp, _f32, _f32, _f32, _i32, _f32, _i32,

@@ -165,9 +165,23 @@ class MGPCGPoissonSolver:
         ct = ct.to(torch.int32).contiguous()
         check(self.lib.mg_set_cell_type(self.plan, ct.data_ptr(), self._s()), "mg_set_cell_type")
 
-    def prepare(self):
-        """Chooses the V-cycle operator form for the A just built."""
-        check(self.lib.mg_plan_prepare(self.plan, self._s()), "mg_plan_prepare")
+    def prepare(self, strategy=None):
+        """Chooses the V-cycle operator form for the A just built: the form a
+        Strategy declares (``strategy.declared_operator(solver)`` returning
+        ("uniform", off-diagonal magnitude per level) or ("whole", None)),
+        checked on the device during the solve, else detected (one host
+        synchronization)."""
+        decl = getattr(strategy, "declared_operator", None) if strategy is not None else None
+        form = decl(self) if decl is not None else None
+        if form is None:
+            check(self.lib.mg_plan_prepare(self.plan, self._s()), "mg_plan_prepare")
+        elif form[0] == "uniform":
+            od = (mg_lib.ctypes.c_float * self.n_mg_levels)(*[float(v) for v in form[1]])
+            check(self.lib.mg_plan_prepare_declared(self.plan, od, self._s()), "mg_plan_prepare_declared")
+        elif form[0] == "whole":
+            check(self.lib.mg_plan_prepare_declared_whole(self.plan, self._s()), "mg_plan_prepare_declared_whole")
+        else:
+            raise ValueError(f"unknown declared operator form {form[0]!r}")
 
     def split_levels(self, bits=None):
         """(bits, streamed levels): the autotuner's per-level choice (bit l: level
@@ -233,7 +247,7 @@ class MGPCGPoissonSolver:
         for l in range(1, self.n_mg_levels):
             self.init_gridtype(self.grid_type[l - 1], self.grid_type[l])
             strategy.build_A(self, l)
-        self.prepare()
+        self.prepare(strategy)
 
     def full_reinitialize(self, strategy):
         """mgpcg.py:89-94."""
@@ -242,7 +256,7 @@ class MGPCGPoissonSolver:
         check(self.lib.mg_fill_fluid(self.plan, self._s()), "mg_fill_fluid")
         for l in range(self.n_mg_levels):
             strategy.build_A(self, l)
-        self.prepare()
+        self.prepare(strategy)
 
     def smooth(self, l, phase):
         """mgpcg.py:104-109."""

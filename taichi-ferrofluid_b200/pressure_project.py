@@ -73,3 +73,11 @@ class PressureProjectStrategy:
                                              int(bool(self.ghost_fluid_method)), float(self.gfm_clamp),
                                              solver._s()), "mg_build_pressure_A")
         self._keep_A = phi
+
+    def declared_operator(self, solver):
+        """The form of the A this Strategy builds: label-uniform, off-diagonal
+        -scale_A between FLUID cells on every level (pressure_project.py:56-58).
+        The solver then prepares without the detection pass and its host
+        synchronization; a device kernel still checks the declaration."""
+        sA, _ = self._scales()
+        return "uniform", [sA] * solver.n_mg_levels

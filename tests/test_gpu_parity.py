@@ -233,3 +233,45 @@ def test_warm_start_from_solution():
     g.reinitialize(torch.from_numpy(sc.cell_type).cuda(), st)
     it = g.solve(500, x0=x)
     assert it <= 1
+
+
+def test_declared_operator_form_is_checked():
+    """The pressure Strategy declares its operator form (label-uniform, off-
+    diagonal -scale_A) so the solver skips the detection pass; a device
+    kernel checks the declaration: a wrong one ends the solve with status
+    bad_operator, and without a declaration the same scene is detected and
+    solved to the same x."""
+    import torch
+    from pressure_project import PressureProjectStrategy
+    sc = SCENES["drop3d_32"]()
+    g, st = gpu_for(sc)
+    it = g.solve(500)
+    assert g.last_status == "converged"
+    x = _np(g.x)
+    dev = g.x.device
+    ct = torch.from_numpy(sc.cell_type).to(dev)
+
+    def strat(cls):
+        s = cls(sc.dim, [torch.from_numpy(v).to(dev) for v in sc.velocity], True,
+                torch.from_numpy(sc.phi).to(dev), sc.p0, gfm_clamp=sc.gfm_clamp)
+        s.scale_A, s.scale_b = sc.scale_A, sc.scale_b
+        return s
+
+    class WrongScale(PressureProjectStrategy):
+        def declared_operator(self, solver):
+            return "uniform", [2.0 * float(self.scale_A)] * solver.n_mg_levels
+
+    class WrongWhole(PressureProjectStrategy):
+        def declared_operator(self, solver):
+            return "whole", None
+
+    class Undeclared(PressureProjectStrategy):
+        declared_operator = None
+
+    for cls in (WrongScale, WrongWhole):
+        g.reinitialize(ct, strat(cls))
+        g.solve(500)
+        assert g.last_status == "bad_operator", cls.__name__
+    g.reinitialize(ct, strat(Undeclared))
+    assert g.solve(500) == it and g.last_status == "converged"
+    np.testing.assert_array_equal(_np(g.x), x)
