@@ -80,7 +80,7 @@ NCU_DRAM_BYTES = {
     ("pressure128", "pre_l0"): 16.83e6, ("pressure128", "post_l0"): 26.29e6,
     ("substep128", "Ap_alpha"): 11.70e6, ("pressure128", "Ap_alpha"): 11.70e6,
     ("substep128", "xr"): 24.33e6, ("pressure128", "xr"): 24.33e6,
-    ("precision256", "pre_l0"): 189.5e6, ("precision256", "post_l0"): 271.8e6,
+    ("precision256", "pre_l0"): 191.3e6, ("precision256", "post_l0"): 268.9e6,
 }
 
 
