@@ -140,12 +140,20 @@ __device__ __forceinline__ void smooth_cell(const Level& L, long long j, int pha
   // x = 2k + ((phase - rowsum) & 1); a row is (i0, i1) in 3D or (i0) in 2D.
   const int nl = g.dim == 3 ? g.n[2] : g.n[1];
   const int half = (nl + 1) >> 1;
-  long long row = j / half;
-  int k = (int)(j - row * half);
+  long long row;
+  int k;
+  if (g.count < (1LL << 31)) {  // 32-bit division (a 64-bit one is a long emulated sequence)
+    const unsigned ur = (unsigned)j / (unsigned)half;
+    row = ur;
+    k = (int)((unsigned)j - ur * (unsigned)half);
+  } else {
+    row = j / half;
+    k = (int)(j - row * half);
+  }
   int c[3];
   int rowsum;
   if (g.dim == 3) {
-    c[0] = (int)(row / g.n[1]);
+    c[0] = g.count < (1LL << 31) ? (int)((unsigned)row / (unsigned)g.n[1]) : (int)(row / g.n[1]);
     c[1] = (int)(row - (long long)c[0] * g.n[1]);
     rowsum = c[0] + c[1];
     c[2] = 2 * k + ((phase - rowsum) & 1);
@@ -234,6 +242,25 @@ __device__ __forceinline__ float group4_nsum(const Group4& g, int e) {
   return __fadd_rn(ret, __fadd_rn(lo, hi));
 }
 
+// Row (axis 0 and 1) and first column of 4-cell group q of a 3D level with
+// q2 groups a row: 32-bit division where the level has fewer than 2^31
+// groups (a 64-bit integer division is a long emulated sequence).
+__device__ __forceinline__ void group4_coords(long long q, int q2, int n1, long long groups, long long& row, int& x,
+                                              int& i1, int& i0) {
+  if (groups < (1LL << 31)) {
+    const unsigned uq = (unsigned)q, ur = uq / (unsigned)q2, u0 = ur / (unsigned)n1;
+    row = ur;
+    x = (int)(uq - ur * (unsigned)q2) * 4;
+    i1 = (int)(ur - u0 * (unsigned)n1);
+    i0 = (int)u0;
+    return;
+  }
+  row = q / q2;
+  x = (int)(q - row * q2) * 4;
+  i1 = (int)(row % n1);
+  i0 = (int)(row / n1);
+}
+
 // smooth(l, phase) on a whole-domain level (every cell FLUID with a nonzero
 // diagonal: the stored form's levels), 3D with the fastest extent a multiple
 // of 4: one thread per 4-cell group, which holds two cells of the colour.
@@ -248,9 +275,9 @@ __global__ void k_smooth_w4(Level L, int phase) {
   const long long groups = L.g.count >> 2;
   float* z = (float*)L.z;
   for (long long q = gtid(); q < groups; q += gstride()) {
-    const long long row = q / q2;
-    const int x = (int)(q - row * q2) * 4;
-    const int i1 = (int)(row % n1), i0 = (int)(row / n1);
+    long long row;
+    int x, i1, i0;
+    group4_coords(q, q2, n1, groups, row, x, i1, i0);
     const int e0 = (phase - i0 - i1 - x) & 1;  // first cell of the colour in the group
     Group4 g;
     load_group4(L, z, i0, i1, x, g);
@@ -283,9 +310,9 @@ __global__ void k_smooth_first_w4(Level L) {
   const long long groups = L.g.count >> 2;
   float* z = (float*)L.z;
   for (long long q = gtid(); q < groups; q += gstride()) {
-    const long long row = q / q2;
-    const int x = (int)(q - row * q2) * 4;
-    const int i1 = (int)(row % n1), i0 = (int)(row / n1);
+    long long row;
+    int x, i1, i0;
+    group4_coords(q, q2, n1, groups, row, x, i1, i0);
     const int e0 = (0 - i0 - i1 - x) & 1;  // first colour-0 cell of the group
     float R[4], D[4];
     unpack4(__ldg(reinterpret_cast<const float4*>((const float*)L.r) + q), R);
@@ -310,9 +337,10 @@ __global__ void k_restrict_w4(Level F, Level C) {
   const int pr = cn2 >> 1;  // coarse pairs per coarse row
   const long long pairs = C.g.count >> 1;
   for (long long t = gtid(); t < pairs; t += gstride()) {
-    const long long crow = t / pr;
-    const int cx = (int)(t - crow * pr) * 2;
-    const int c1 = (int)(crow % cn1), c0 = (int)(crow / cn1);
+    long long crow;
+    int cx, c1, c0;
+    group4_coords(t, pr, cn1, pairs, crow, cx, c1, c0);
+    cx >>= 1;  // pairs, not groups of 4: the first coarse column of the pair is 2 (t mod pr)
     float acc[2] = {0.0f, 0.0f};
 #pragma unroll
     for (int o0 = 0; o0 < 2; ++o0)
@@ -344,9 +372,9 @@ __global__ void k_prolongate4(Level F, Level C) {
   const int n1 = F.g.n[1], n2 = F.g.n[2], q2 = n2 >> 2;
   const long long groups = F.g.count >> 2;
   for (long long q = gtid(); q < groups; q += gstride()) {
-    const long long row = q / q2;
-    const int x = (int)(q - row * q2) * 4;
-    const int i1 = (int)(row % n1), i0 = (int)(row / n1);
+    long long row;
+    int x, i1, i0;
+    group4_coords(q, q2, n1, groups, row, x, i1, i0);
     const long long ic = C.g.index(i0 >> 1, i1 >> 1, x >> 1);
     const float a = zc[ic], b = zc[ic + 1];
     float4 v = reinterpret_cast<float4*>(zf)[q];

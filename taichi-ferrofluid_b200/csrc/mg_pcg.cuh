@@ -375,18 +375,14 @@ __global__ void __launch_bounds__(kRedThreads) k_Ap_alpha4(Level L, const float*
   const int groups = (int)(L.g.count >> 2);
   const float4 z4 = make_float4(0.f, 0.f, 0.f, 0.f);
   double acc = 0.0;
-  for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < groups; q += gridDim.x * blockDim.x) {
+  const int q0 = blockIdx.x * blockDim.x + threadIdx.x, S = gridDim.x * blockDim.x;
+  GroupWalk w(L.g, q0, S);
+  for (int q = q0; q < groups; q += S, w.advance()) {
     const int i = q << 2;
     const uint32_t t4 = __ldg(reinterpret_cast<const uint32_t*>(L.type) + q);
     if (t4 == 0x02020202u || t4 == 0x01010101u) continue;
-    const int x = i % nx, t = i / nx;
-    int c[2];
-    if (dim == 3) {
-      c[0] = t / L.g.n[1];
-      c[1] = t - c[0] * L.g.n[1];
-    } else {
-      c[0] = t;
-    }
+    const int x = w.x;
+    const int c[2] = {w.c0, w.c1};  // coordinates of the slower axes
     const float4 pc = __ldg(reinterpret_cast<const float4*>(p + i));
     const float4 ad = __ldg(reinterpret_cast<const float4*>(L.Adiag + i));
     const float* axx = L.Ax[dim - 1];
@@ -406,6 +402,7 @@ __global__ void __launch_bounds__(kRedThreads) k_Ap_alpha4(Level L, const float*
     }
     const float pv[4] = {pc.x, pc.y, pc.z, pc.w}, av[4] = {ad.x, ad.y, ad.z, ad.w};
     const float xv[4] = {xc.x, xc.y, xc.z, xc.w};
+    float out[4] = {0.f, 0.f, 0.f, 0.f};
 #pragma unroll
     for (int e = 0; e < 4; ++e) {
       if (!fluid_lane(t4, e)) continue;
@@ -423,8 +420,15 @@ __global__ void __launch_bounds__(kRedThreads) k_Ap_alpha4(Level L, const float*
       const float hi = x + e + 1 < nx ? __fmul_rn(xv[e], e == 3 ? pxr : pv[e + 1]) : 0.0f;
       ret = __fadd_rn(ret, __fadd_rn(lo, hi));
       const float v = __fadd_rn(__fmul_rn(av[e], pv[e]), ret);
-      Ap[i + e] = v;
+      out[e] = v;
       acc += (double)pv[e] * (double)v;
+    }
+    if (t4 == 0x01010101u * (uint32_t)(uint8_t)FLUID) {  // every lane FLUID (the whole-domain form): one 16-byte store
+      *reinterpret_cast<float4*>(Ap + i) = make_float4(out[0], out[1], out[2], out[3]);
+    } else {
+#pragma unroll
+      for (int e = 0; e < 4; ++e)
+        if (fluid_lane(t4, e)) Ap[i + e] = out[e];
     }
   }
   double tot;
