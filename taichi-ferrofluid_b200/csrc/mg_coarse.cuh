@@ -221,9 +221,11 @@ __device__ __forceinline__ void coarse_vcycle(const CoarseArgs& A, unsigned char
     if (pt > (int)blockDim.x || (cntb + pt - 1) / pt > kBottomPerThread) pt = blockDim.x;
     if (cntb <= kBottomPerThread * pt) {
       if ((int)threadIdx.x < pt) {
-        // each owned cell's padded index, r and Adiag in registers
+        // each owned cell's padded index, r and Adiag in registers (and, for
+        // STO, its six couplings: constant through the bottom sweeps)
         int gi[2][kBottomPerThread];
         float rr[2][kBottomPerThread], aa[2][kBottomPerThread];
+        float cx[2][kBottomPerThread][STO ? 6 : 1];
 #pragma unroll
         for (int ph = 0; ph < 2; ++ph) {
 #pragma unroll
@@ -233,12 +235,22 @@ __device__ __forceinline__ void coarse_vcycle(const CoarseArgs& A, unsigned char
             gi[ph][k] = -1;
             rr[ph][k] = 0.0f;
             aa[ph][k] = 1.0f;
+#pragma unroll
+            for (int e = 0; e < (STO ? 6 : 1); ++e) cx[ph][k][e] = 0.0f;
             if (j < cntb && colour_cell(g, dim, j, ph, c0, c1, c2)) {
               const int p = g.at(c0, c1, c2);
               if (sa[p] != 0.0f) {
                 gi[ph][k] = p;
                 rr[ph][k] = sr[p];
                 aa[ph][k] = sa[p];
+                if constexpr (STO) {  // the couplings csum_t reads, in its order
+                  cx[ph][k][0] = sx[p - g.s0];
+                  cx[ph][k][1] = sx[p];
+                  cx[ph][k][2] = sx[A.total + p - g.s1];
+                  cx[ph][k][3] = sx[A.total + p];
+                  cx[ph][k][4] = dim == 3 ? sx[2 * A.total + p - 1] : 0.0f;
+                  cx[ph][k][5] = dim == 3 ? sx[2 * A.total + p] : 0.0f;
+                }
               }
             }
           }
@@ -254,7 +266,17 @@ __device__ __forceinline__ void coarse_vcycle(const CoarseArgs& A, unsigned char
               const int ps = p >= 0 ? p : g.at(0, 0, 0);     // an in-range cell for empty slots
               const float r_ = ph ? rr[1][k] : rr[0][k];
               const float a_ = ph ? aa[1][k] : aa[0][k];
-              v[k] = div_pos(__fsub_rn(r_, csum_t<STO>(zm, sx, A.total, ps, g, dim, ms)), a_);
+              float sum;
+              if constexpr (STO) {  // csum_t with the couplings from registers
+                const float* x6 = ph ? cx[1][k] : cx[0][k];
+                sum = __fadd_rn(__fmul_rn(x6[0], zm[ps - g.s0]), __fmul_rn(x6[1], zm[ps + g.s0]));
+                sum = __fadd_rn(0.0f, sum);
+                sum = __fadd_rn(sum, __fadd_rn(__fmul_rn(x6[2], zm[ps - g.s1]), __fmul_rn(x6[3], zm[ps + g.s1])));
+                if (dim == 3) sum = __fadd_rn(sum, __fadd_rn(__fmul_rn(x6[4], zm[ps - 1]), __fmul_rn(x6[5], zm[ps + 1])));
+              } else {
+                sum = csum_t<STO>(zm, sx, A.total, ps, g, dim, ms);
+              }
+              v[k] = div_pos(__fsub_rn(r_, sum), a_);
             }
 #pragma unroll
             for (int k = 0; k < kBottomPerThread; ++k) {   // then the stores
