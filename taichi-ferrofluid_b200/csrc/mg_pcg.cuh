@@ -7,6 +7,7 @@
 // sets the condition of the CUDA graph while node that repeats the body.
 #pragma once
 #include "mg_common.cuh"
+#include "mg_kernels.cuh"
 
 namespace mg {
 
@@ -245,6 +246,63 @@ __device__ __forceinline__ void update_p4_body(int bid_, int nb_, Level L, float
     for (int e = 0; e < 4; ++e)
       if (fluid_lane(t4, e)) pp[e] = __fadd_rn(zv[e], __fmul_rn(beta, pp[e]));
     reinterpret_cast<float4*>(p)[q] = pv;
+  }
+}
+
+// The last post-smoothing half sweep of level 0 (colour 0, k_smooth_w4) of a
+// whole-domain level split into per-kernel passes, fused with the z.r that
+// k_zr4 would compute after it (mgpcg.py:161-166, 197-202): every thread has
+// its group's four final z values (two it computes, two of the other colour,
+// final since the half sweep before) and r, so the sum costs no extra pass;
+// the last block runs k_zr4's epilogue.  At most kMaxPartials / 2 blocks.
+__global__ void __launch_bounds__(kRedThreads) k_smooth_zr_w4(Level L, int phase, Control* ctl, double* partials,
+                                                              int mode) {
+  pdl_enter();
+  __shared__ double sh[32];
+  const int n1 = L.g.n[1], n2 = L.g.n[2];
+  const int q2 = n2 >> 2;
+  const long long groups = L.g.count >> 2;
+  float* z = (float*)L.z;
+  double acc = 0.0;
+  for (long long q = gtid(); q < groups; q += gstride()) {
+    long long row;
+    int x, i1, i0;
+    group4_coords(q, q2, n1, groups, row, x, i1, i0);
+    const int e0 = (phase - i0 - i1 - x) & 1;  // first cell of the colour in the group
+    Group4 g;
+    load_group4(L, z, i0, i1, x, g);
+    float out[2];
+#pragma unroll
+    for (int h = 0; h < 2; ++h) {
+      float v = 0.0f;
+#pragma unroll
+      for (int ee = 0; ee < 2; ++ee) {  // unrolled over both values of e0
+        const int e = ee + 2 * h;
+        if (ee == e0) v = div_pos(__fsub_rn(g.R[e], group4_nsum(g, e)), g.D[e]);
+      }
+      out[h] = v;
+    }
+    const long long idx = row * n2 + x;
+    z[idx + e0] = out[0];
+    z[idx + e0 + 2] = out[1];
+#pragma unroll
+    for (int e = 0; e < 4; ++e) {  // every cell FLUID (whole-domain level)
+      const float ze = ((e - e0) & 1) ? g.Z[e] : out[e >> 1];
+      acc += (double)ze * (double)g.R[e];
+    }
+  }
+  double tot;
+  if (last_block_total<kRedThreads>(acc, partials, &ctl->counter[1], sh, &tot) && threadIdx.x == 0) {
+    if (mode == 0) {
+      ctl->old_zTr = tot;
+      if (ctl->max_iters == 0) ctl->run = 0;
+    } else {
+      ctl->new_zTr = tot;
+      ctl->beta = (float)(tot / (ctl->old_zTr + ctl->eps));
+      ctl->old_zTr = tot;
+      ctl->iter += 1;
+      if (ctl->max_iters != -1 && ctl->iter >= ctl->max_iters) ctl->run = 0;
+    }
   }
 }
 

@@ -280,7 +280,13 @@ int launch_level(mg_plan* P, int l, bool pre, cudaStream_t s) {
   if (int rc = launch_prolongate(P, l, s)) return rc;
   for (int i = 0; i < P->d.pre_post; ++i) {
     if (int rc = launch_smooth(P, l, 1, s)) return rc;
-    if (int rc = launch_smooth(P, l, 0, s)) return rc;
+    if (l == 0 && i + 1 == P->d.pre_post && P->fp.zr_mode >= 0) {  // the last half sweep with z.r
+      const int nb = std::min(grid_for(P, level_cells(P, 0) / 4), kMaxPartials / 2);
+      CK(launch_k(k_smooth_zr_w4, nb, kRedThreads, 0, s, P->lv[0], 0, P->fp.zr_ctl, P->fp.zr_partials,
+                  P->fp.zr_mode));
+    } else if (int rc = launch_smooth(P, l, 0, s)) {
+      return rc;
+    }
   }
   return MG_OK;
 }
@@ -651,8 +657,16 @@ int tune_resident(mg_plan* P, cudaStream_t s) {
 // cluster launch) and a grid within the partials buffer.
 bool zr_fusable(const mg_plan* P) {
   const FusedPlan& F = P->fp;
-  return F.valid && !F.sto && P->d.storage == MG_STORE_F32 && F.lc > 0 && !F.split[0] &&
-         !(F.res && F.res_lp == 0) && F.blocks[0] <= kMaxPartials / 2;
+  const bool col = F.valid && !F.sto && P->d.storage == MG_STORE_F32 && F.lc > 0 && !F.split[0] &&
+                   !(F.res && F.res_lp == 0) && F.blocks[0] <= kMaxPartials / 2;
+  // or: level 0 split into per-kernel passes on a whole-domain float32 level
+  // of 4-cell groups, whose last post-smoothing half sweep takes z.r
+  // (k_smooth_zr_w4)
+  const bool split = F.valid && P->d.storage == MG_STORE_F32 && F.lc > 0 && F.split[0] && P->whole[0] &&
+                     !(F.res && F.res_lp == 0) &&
+                     P->d.dim == 3 && P->geom[0].n[2] % 4 == 0 && P->geom[0].count % 4 == 0 &&
+                     P->d.pre_post >= 1;
+  return col || split;
 }
 
 template <typename ST>
