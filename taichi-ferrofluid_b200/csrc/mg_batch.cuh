@@ -14,6 +14,7 @@
 // graph while-node whose condition k_bt_cond sets: any instance still running.
 #pragma once
 #include "mg_sweep.cuh"
+#include "mg_colsweep.cuh"
 #include "mg_coarse.cuh"
 #include "mg_pcg.cuh"
 
@@ -72,6 +73,24 @@ __global__ void __launch_bounds__(NT) k_bt_sweep(const BatchBlock* tab, const Sw
   const SweepArgs<ST>& A = args[e.inst];
   if (A.ctl->done) return;
   sweep_body<DIM, ST, NS, TX, TY, PRE, NT, K, false>(A, e.bid, e.nb);
+}
+
+// One column-kernel sweep stage (k_colsweep) over every instance in the
+// table whose level runs it with this tile: each instance's three tensor maps
+// (r, Adiag, the pre-smoothed z) sit at maps[3 * inst] in global memory,
+// written by the host before the launch.
+template <typename ST, int NS, int TX, int TY, bool PRE, int MINB>
+__global__ void __launch_bounds__(ColGeom<ST, NS, TX, TY>::NT, MINB)
+    k_bt_colsweep(const BatchBlock* tab, const SweepArgs<ST>* args, const CUtensorMap* maps) {
+  pdl_enter();
+  const BatchBlock e = tab[blockIdx.x];
+  const SweepArgs<ST>& A = args[e.inst];
+  if (A.ctl->done) return;
+  const CUtensorMap* m = maps + 3 * e.inst;
+  if (threadIdx.x == 0)  // the maps are read through the tensor-map proxy
+    for (int k = 0; k < 3; ++k)
+      asm volatile("fence.proxy.tensormap::generic.acquire.gpu [%0], 128;" ::"l"(m + k) : "memory");
+  colsweep_body<ST, NS, TX, TY, PRE>(A, const_cast<Control*>(A.ctl), m, m + 1, m + 2, e.bid, e.nb);
 }
 
 // The coarse block of every instance: block i solves instance i's coarse levels.

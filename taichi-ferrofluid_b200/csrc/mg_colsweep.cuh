@@ -175,10 +175,14 @@ __device__ __forceinline__ float residual_cell(float ms, float s, float r, float
 // planes), and one thread that waits for the next plane's loads before the
 // step's block barrier.
 // ---------------------------------------------------------------------------
-template <typename ST, int NS, int TX, int TY, bool PRE, int MINB>
-__global__ void __launch_bounds__(ColGeom<ST, NS, TX, TY>::NT, MINB)
-    k_colsweep(SweepArgs<ST> A, Control* flag, const __grid_constant__ CUtensorMap tm_r,
-               const __grid_constant__ CUtensorMap tm_ad, const __grid_constant__ CUtensorMap tm_zin) {
+//
+// colsweep_body is one block's work: block `bid` of the `nb` blocks of a
+// level's launch (k_colsweep: the launch itself; k_bt_colsweep: one
+// instance's blocks inside a batched launch).
+template <typename ST, int NS, int TX, int TY, bool PRE>
+__device__ __forceinline__ void colsweep_body(const SweepArgs<ST>& A, Control* flag, const CUtensorMap* tm_r,
+                                              const CUtensorMap* tm_ad, const CUtensorMap* tm_zin, int bid,
+                                              int nb) {
   using G = ColGeom<ST, NS, TX, TY>;
   constexpr int HX = G::HX, RX = G::RX, W = G::W, NT = G::NT, ZPL = G::ZPL, ZX = G::ZX;
   constexpr int RXB = G::RXB, XOFF = G::HB - G::HX;  // box columns; box column of region column 0
@@ -189,7 +193,6 @@ __global__ void __launch_bounds__(ColGeom<ST, NS, TX, TY>::NT, MINB)
   constexpr int SLOT = G::slot_bytes(PRE);
   constexpr int D = PRE ? NS - 1 : NS;  // steps from a plane's load to its final z
   constexpr int NI = TX * (TY / 2), NB = (NS / 2) * RX;
-  pdl_enter();
 
   extern __shared__ __align__(128) unsigned char smem_raw[];
   // 128-byte aligned by pointer arithmetic on the shared array (the compiler
@@ -204,16 +207,16 @@ __global__ void __launch_bounds__(ColGeom<ST, NS, TX, TY>::NT, MINB)
   const int n0 = F.n[0], n1 = F.n[1], n2 = F.n[2];
   // one wave of blocks: tile t is cut into q or q + 1 chunks of nearly equal
   // even length (the first r tiles get q + 1; the host launches
-  // ntile <= gridDim.x <= ntile * n0 / 2 blocks)
+  // ntile <= nb <= ntile * n0 / 2 blocks)
   const int ntile = A.tiles_x * A.tiles_y;
-  const int nq = (int)gridDim.x / ntile, nr = (int)gridDim.x % ntile;
+  const int nq = nb / ntile, nr = nb % ntile;
   int tile, cid, nch;
-  if ((int)blockIdx.x < nr * (nq + 1)) {
-    tile = blockIdx.x / (nq + 1);
-    cid = blockIdx.x % (nq + 1);
+  if (bid < nr * (nq + 1)) {
+    tile = bid / (nq + 1);
+    cid = bid % (nq + 1);
     nch = nq + 1;
   } else {
-    const int b2 = blockIdx.x - nr * (nq + 1);
+    const int b2 = bid - nr * (nq + 1);
     tile = nr + b2 / nq;
     cid = b2 % nq;
     nch = nq;
@@ -301,9 +304,9 @@ __global__ void __launch_bounds__(ColGeom<ST, NS, TX, TY>::NT, MINB)
   auto issue = [&](int p, int slot) {  // TMA loads of plane p into a ring slot (thread 0)
     unsigned char* sl = slots + slot * SLOT;
     mbar_expect_tx(&bar[slot], tx_bytes);
-    tma_load_3d(sl, &tm_r, &bar[slot], bx, oy, p);
-    tma_load_3d(sl + G::SLOT_R, &tm_ad, &bar[slot], bx, oy, p);
-    if (!PRE) tma_load_3d(sl + G::SLOT_R + G::SLOT_S, &tm_zin, &bar[slot], bx, oy, p);
+    tma_load_3d(sl, tm_r, &bar[slot], bx, oy, p);
+    tma_load_3d(sl + G::SLOT_R, tm_ad, &bar[slot], bx, oy, p);
+    if (!PRE) tma_load_3d(sl + G::SLOT_R + G::SLOT_S, tm_zin, &bar[slot], bx, oy, p);
   };
 
   if (t == 0) {
@@ -492,7 +495,8 @@ __global__ void __launch_bounds__(ColGeom<ST, NS, TX, TY>::NT, MINB)
       __shared__ double sh[32];
       double tot;
       Control* ctl = A.zr_ctl;
-      if (last_block_total<NT>(zr_acc, A.zr_partials, &ctl->counter[1], sh, &tot) && threadIdx.x == 0) {
+      if (last_block_total_at<NT>(zr_acc, A.zr_partials, &ctl->counter[1], sh, &tot, bid, nb) &&
+          threadIdx.x == 0) {
         if (A.zr == 0) {
           ctl->old_zTr = tot;
           if (ctl->max_iters == 0) ctl->run = 0;
@@ -506,6 +510,14 @@ __global__ void __launch_bounds__(ColGeom<ST, NS, TX, TY>::NT, MINB)
       }
     }
   }
+}
+
+template <typename ST, int NS, int TX, int TY, bool PRE, int MINB>
+__global__ void __launch_bounds__(ColGeom<ST, NS, TX, TY>::NT, MINB)
+    k_colsweep(SweepArgs<ST> A, Control* flag, const __grid_constant__ CUtensorMap tm_r,
+               const __grid_constant__ CUtensorMap tm_ad, const __grid_constant__ CUtensorMap tm_zin) {
+  pdl_enter();
+  colsweep_body<ST, NS, TX, TY, PRE>(A, flag, &tm_r, &tm_ad, &tm_zin, (int)blockIdx.x, (int)gridDim.x);
 }
 
 }  // namespace mg

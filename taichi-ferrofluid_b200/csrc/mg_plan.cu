@@ -1907,7 +1907,8 @@ struct mg_batch {
   // one sweep launch: instances of one kernel form at one level depth
   struct Group {
     int dim, one, pre, depth, blocks, ninst;
-    int64_t tab_off, args_off;
+    int col;  // 0: the ring sweep; k: the column kernel with kColShapes[k]
+    int64_t tab_off, args_off, maps_off;
   };
   std::vector<Group> groups;
   std::vector<unsigned char> blob;  // every table, laid out as in the workspace
@@ -1940,10 +1941,11 @@ int64_t put_blob(std::vector<unsigned char>& blob, const void* src, size_t bytes
 #define MG_BATCH_MIN_CHUNK 32
 #endif
 
-// The fused plan of an instance as the batch runs it: the tiled ring kernel on
-// every streamed level (no column kernel, two planes a step), chunks of at
-// least MG_BATCH_MIN_CHUNK planes, the coarse block for the levels from lc
-// (no cluster launch).  Every grid gives the same values.
+// The fused plan of an instance as the batch runs it: on every streamed level
+// the kernel the instance's own plan chose (the column kernel with its tile,
+// or the tiled ring kernel with two planes a step), chunks of at least
+// MG_BATCH_MIN_CHUNK planes, the coarse block for the levels from lc (no
+// cluster launch).  Every grid gives the same values.
 FusedPlan batch_plan(const mg_plan* P) {
   FusedPlan F = P->fp;
   F.res = false;
@@ -1951,11 +1953,14 @@ FusedPlan batch_plan(const mg_plan* P) {
   int min_chunk = MG_BATCH_MIN_CHUNK;  // MGPCG_BATCH_CHUNK=<planes> overrides (even, >= 2)
   if (const char* ov = std::getenv("MGPCG_BATCH_CHUNK")) min_chunk = std::max(2, (int)std::strtol(ov, nullptr, 0) & ~1);
   for (int l = 0; l < F.lc; ++l) {
-    F.col[l] = 0;
     F.step1[l] = 0;
     level_grid(&F, P->lv[l].g, l, F.grid_extra[l]);
     const int n0 = P->lv[l].g.n[0];
-    if (F.chunk[l] < min_chunk) {
+    if (F.col[l]) {  // each tile cut into k chunks of at least min_chunk planes
+      const int k = std::max(1, n0 / std::max(min_chunk, 2));
+      F.blocks[l] = F.tiles_x[l] * F.tiles_y[l] * k;
+      F.chunk[l] = n0 / k;
+    } else if (F.chunk[l] < min_chunk) {
       F.chunk[l] = std::min(n0, min_chunk);
       F.blocks[l] = F.tiles_x[l] * F.tiles_y[l] * ((n0 + F.chunk[l] - 1) / F.chunk[l]);
     }
@@ -1963,35 +1968,71 @@ FusedPlan batch_plan(const mg_plan* P) {
   return F;
 }
 
+// The column kernel's tensor maps of streamed level l of a plan (r, Adiag,
+// the pre-smoothed z; PRE takes the Adiag map in the third place, unused).
+template <typename ST, int TX, int TY, bool PRE>
+bool col_maps_t(const Level* lv, int l, CUtensorMap* m) {
+  using G = ColGeom<ST, 4, TX, TY>;
+  const Level& f = lv[l];
+  if (!tensor_map_3d(&m[0], f.r, l == 0 ? 4 : (int)sizeof(ST), f.g, G::RXB, G::RY) ||
+      !tensor_map_3d(&m[1], f.Adiag_s, (int)sizeof(ST), f.g, G::RXB, G::RY))
+    return false;
+  if (PRE) {
+    m[2] = m[1];
+    return true;
+  }
+  return tensor_map_3d(&m[2], f.zt, (int)sizeof(ST), f.g, G::RXB, G::RY);
+}
+
 template <typename ST, bool PRE>
-void batch_sweep_args(mg_batch* B, const std::vector<FusedPlan>& fps, int depth, int dim, int one) {
+bool col_maps(int c, const Level* lv, int l, CUtensorMap* m) {
+  switch (c) {
+    case 1: return col_maps_t<ST, 32, 16, PRE>(lv, l, m);
+    case 2: return col_maps_t<ST, 32, 32, PRE>(lv, l, m);
+    case 3: return col_maps_t<ST, 64, 16, PRE>(lv, l, m);
+  }
+  return false;
+}
+
+template <typename ST, bool PRE>
+int batch_sweep_args(mg_batch* B, const std::vector<FusedPlan>& fps, int depth, int dim, int one, int col) {
   std::vector<SweepArgs<ST>> args;
   std::vector<BatchBlock> tab;
+  std::vector<CUtensorMap> maps;
   for (int i = 0; i < B->n; ++i) {
     const mg_plan* P = B->plans[i];
     const FusedPlan& F = fps[i];
     if (depth >= F.lc || P->d.dim != dim) continue;
-    const int is_one = dim == 3 && F.chunk[depth] == 2;
+    if (F.col[depth] != col) continue;
+    const int is_one = !col && dim == 3 && F.chunk[depth] == 2;
     if (is_one != one) continue;
     const int k = (int)args.size();
     args.push_back(sweep_args<ST, PRE>(F, P->lv, depth, P->ctl));
+    if (col) {
+      CUtensorMap m[3];
+      if (!col_maps<ST, PRE>(col, P->lv, depth, m)) return bad("batch: a column-kernel tensor map");
+      maps.insert(maps.end(), m, m + 3);
+    }
     for (int b = 0; b < F.blocks[depth]; ++b) tab.push_back({k, b, F.blocks[depth]});
   }
-  if (args.empty()) return;
+  if (args.empty()) return MG_OK;
   mg_batch::Group g;
   g.dim = dim;
   g.one = one;
   g.pre = PRE;
   g.depth = depth;
+  g.col = col;
   g.blocks = (int)tab.size();
   g.ninst = (int)args.size();
   g.args_off = put_blob(B->blob, args.data(), args.size() * sizeof(SweepArgs<ST>));
   g.tab_off = put_blob(B->blob, tab.data(), tab.size() * sizeof(BatchBlock));
+  g.maps_off = col ? put_blob(B->blob, maps.data(), maps.size() * sizeof(CUtensorMap)) : 0;
   B->groups.push_back(g);
+  return MG_OK;
 }
 
 template <typename ST>
-void batch_tables(mg_batch* B) {
+int batch_tables(mg_batch* B) {
   std::vector<FusedPlan> fps;
   for (auto* P : B->plans) fps.push_back(batch_plan(P));
   B->maxlc = 0;
@@ -1999,10 +2040,14 @@ void batch_tables(mg_batch* B) {
   // sweeps in V-cycle order: PRE by depth, (coarse), POST by depth upward
   for (int d = 0; d < B->maxlc; ++d)
     for (int dim = 3; dim >= 2; --dim)
-      for (int one = 0; one <= 1; ++one) batch_sweep_args<ST, true>(B, fps, d, dim, one);
+      for (int col = 0; col < kColShapeCount; ++col)
+        for (int one = 0; one <= (col ? 0 : 1); ++one)
+          if (int rc = batch_sweep_args<ST, true>(B, fps, d, dim, one, col)) return rc;
   for (int d = B->maxlc - 1; d >= 0; --d)
     for (int dim = 3; dim >= 2; --dim)
-      for (int one = 0; one <= 1; ++one) batch_sweep_args<ST, false>(B, fps, d, dim, one);
+      for (int col = 0; col < kColShapeCount; ++col)
+        for (int one = 0; one <= (col ? 0 : 1); ++one)
+          if (int rc = batch_sweep_args<ST, false>(B, fps, d, dim, one, col)) return rc;
   std::vector<CoarseArgs> coarse;
   B->coarse_smem = 0;
   for (int i = 0; i < B->n; ++i) {
@@ -2043,16 +2088,33 @@ void batch_tables(mg_batch* B) {
   const int zero = 0;
   B->off_any = put_blob(B->blob, &zero, sizeof(int));
   B->ws_bytes = align256((int64_t)B->blob.size());
+  return MG_OK;
 }
 
 template <typename T>
 const T* bptr(const mg_batch* B, int64_t off) { return (const T*)(B->base + off); }
+
+template <typename ST, int TX, int TY, bool PRE, int MINB>
+cudaError_t launch_bt_col_t(const mg_batch* B, const mg_batch::Group& g, cudaStream_t s) {
+  using G = ColGeom<ST, 4, TX, TY>;
+  auto kern = k_bt_colsweep<ST, 4, TX, TY, PRE, MINB>;
+  const size_t smem = G::smem(PRE);
+  cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (e != cudaSuccess) return e;
+  return launch_k(kern, g.blocks, G::NT, smem, s, bptr<BatchBlock>(B, g.tab_off),
+                  bptr<SweepArgs<ST>>(B, g.args_off), bptr<CUtensorMap>(B, g.maps_off));
+}
 
 template <typename ST, bool PRE>
 cudaError_t launch_bt_group(const mg_batch* B, const mg_batch::Group& g, cudaStream_t s) {
   const BatchBlock* tab = bptr<BatchBlock>(B, g.tab_off);
   const SweepArgs<ST>* args = bptr<SweepArgs<ST>>(B, g.args_off);
   constexpr int NS = 4;
+  switch (g.col) {  // the column kernel (shapes as launch_col_st)
+    case 1: return launch_bt_col_t<ST, 32, 16, PRE, 2>(B, g, s);
+    case 2: return launch_bt_col_t<ST, 32, 32, PRE, 1>(B, g, s);
+    case 3: return launch_bt_col_t<ST, 64, 16, PRE, 1>(B, g, s);
+  }
   if (g.dim == 3) {
     constexpr TileShape T = kTile3;
     if (g.one) {
@@ -2213,10 +2275,15 @@ int mg_batch_create(mg_plan_t* const* plans, int32_t n, mg_batch_t** out) {
   B->storage = plans[0]->d.storage;
   B->refresh = plans[0]->d.refresh_every > 0;
   for (auto* P : B->plans) B->refresh = B->refresh || P->d.refresh_every > 0;
+  int rc = MG_OK;
   switch (B->storage) {
-    case MG_STORE_F16: batch_tables<__half>(B); break;
-    case MG_STORE_BF16: batch_tables<__nv_bfloat16>(B); break;
-    default: batch_tables<float>(B);
+    case MG_STORE_F16: rc = batch_tables<__half>(B); break;
+    case MG_STORE_BF16: rc = batch_tables<__nv_bfloat16>(B); break;
+    default: rc = batch_tables<float>(B);
+  }
+  if (rc != MG_OK) {
+    delete B;
+    return rc;
   }
   *out = B;
   return MG_OK;
