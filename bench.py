@@ -580,7 +580,8 @@ def batched_variant(dev, reps=3):
                                             "iters_max": max(s.iters for s in st),
                                             "launches_per_pass": body,
                                             "form": "one launch per V-cycle stage / CG step for all instances "
-                                                    "(tables of blocks), one CUDA graph"}
+                                                    "of a sub-batch (tables of blocks), one CUDA graph each, "
+                                                    f"{b.batch_groups} sub-batches on their own streams"}
         if storage == "f32":
             b.solve_one_at_a_time()
             ms1 = min(b.solve_one_at_a_time()[0] for _ in range(2))

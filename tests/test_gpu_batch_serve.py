@@ -81,8 +81,13 @@ def test_batched_kernels_match_alone(storage):
     assert all(st.status == 0 for st in stats), [st.status for st in stats]
     xs = [inst.solver.x.clone() for inst in batch.instances]
     its = [st.iters for st in stats]
+    batch.solve_batched(groups=1)
     pro, body = batch.batch_launch_counts()
     assert body < 4 * len(scenes)  # one launch per stage, not per instance
+    _, one = batch.solve_batched(groups=1)  # one graph for all: the same solves
+    assert [st.iters for st in one] == its
+    for inst, x in zip(batch.instances, xs):
+        assert torch.equal(inst.solver.x, x)
     _, again = batch.solve_batched()
     assert [st.iters for st in again] == its
     for inst, x in zip(batch.instances, xs):
