@@ -1,6 +1,8 @@
 // The coarse V-cycle of the fused path: every level from lc down in ONE
 // thread block with all grids in shared memory.
 #pragma once
+#include <type_traits>
+
 #include "mg_fused.cuh"
 
 namespace mg {
@@ -124,6 +126,25 @@ __device__ __forceinline__ float csum_t(const float* zm, const float* sx, int to
   }
 }
 
+// A half sweep of colour `phase` over the calling thread's own cells of
+// level l, listed by padded index (-1: none, or not FLUID): the list form of
+// coarse_smooth for a level whose colours have at most 2 * blockDim.x cells.
+template <bool STO>
+__device__ __forceinline__ void coarse_smooth_list(const CoarseArgs& A, int l, const int (&li)[2], float* zm,
+                                                   const float* sr, const float* sa, const float* sx) {
+  const PGeom g = pgeom(A, l);
+  const float ms = -A.s[l];
+  float v[2];
+#pragma unroll
+  for (int k = 0; k < 2; ++k) {
+    const int p = li[k] >= 0 ? li[k] : g.at(0, 0, 0);
+    v[k] = div_pos(__fsub_rn(sr[p], csum_t<STO>(zm, sx, A.total, p, g, A.dim, ms)), sa[p]);
+  }
+#pragma unroll
+  for (int k = 0; k < 2; ++k)
+    if (li[k] >= 0) zm[li[k]] = v[k];
+}
+
 template <bool STO>
 __device__ void coarse_smooth(const CoarseArgs& A, int l, int phase, float* zm, const float* sr, const float* sa,
                               const float* sx) {
@@ -175,11 +196,32 @@ __device__ __forceinline__ void coarse_vcycle(const CoarseArgs& A, unsigned char
   }
   __syncthreads();
   const int L = A.nlev;
+  // the finest level's cells of each colour, at most 2 per thread: listed once
+  // (padded index, -1 for none or not FLUID) for its pre- and post-smoothing
+  int li[2][2] = {{-1, -1}, {-1, -1}};
+  const bool listed = L > 1 && colour_count(pgeom(A, 0), dim) <= 2 * (int)blockDim.x;
+  if (listed) {
+    const PGeom g = pgeom(A, 0);
+    const int cnt = colour_count(g, dim);
+#pragma unroll
+    for (int ph = 0; ph < 2; ++ph)
+#pragma unroll
+      for (int k = 0; k < 2; ++k) {
+        const int j = threadIdx.x + k * blockDim.x;
+        int c0, c1, c2;
+        if (j < cnt && colour_cell(g, dim, j, ph, c0, c1, c2)) {
+          const int p = g.at(c0, c1, c2);
+          if (sa[p] != 0.0f) li[ph][k] = p;
+        }
+      }
+  }
   for (int l = 0; l < L - 1; ++l) {
     for (int i = 0; i < A.pre_post; ++i) {
-      coarse_smooth<STO>(A, l, 0, zm, sr, sa, sx);
+      if (l == 0 && listed) coarse_smooth_list<STO>(A, 0, li[0], zm, sr, sa, sx);
+      else coarse_smooth<STO>(A, l, 0, zm, sr, sa, sx);
       __syncthreads();
-      coarse_smooth<STO>(A, l, 1, zm, sr, sa, sx);
+      if (l == 0 && listed) coarse_smooth_list<STO>(A, 0, li[1], zm, sr, sa, sx);
+      else coarse_smooth<STO>(A, l, 1, zm, sr, sa, sx);
       __syncthreads();
     }
     // restrict: coarse r = rho * sum over FLUID children (lexicographic order);
@@ -187,6 +229,42 @@ __device__ __forceinline__ void coarse_vcycle(const CoarseArgs& A, unsigned char
     const PGeom gf = pgeom(A, l), gc = pgeom(A, l + 1);
     const float ms = -A.s[l];
     const int cnt = gc.n0 * gc.n1 * gc.n2;
+    if (dim == 3) {
+      // a lane per child: 8 consecutive lanes hold one coarse cell's children
+      // (o0, o1, o2 lexicographic), and the first sums their r - A z in that
+      // order (blockDim.x is a multiple of 32: every lane of a warp takes the
+      // same iterations)
+      for (int b = 0; b < 8 * cnt; b += blockDim.x) {
+        const int i = b + threadIdx.x;
+        const int q = i >> 3, o = i & 7;
+        bool use = false;
+        float val = 0.0f;
+        int pc = -1;
+        if (i < 8 * cnt) {
+          const int c2 = q % gc.n2, t = q / gc.n2;
+          const int c1 = t % gc.n1, c0 = t / gc.n1;
+          pc = gc.at(c0, c1, c2);
+          const int p = gf.at(2 * c0 + (o >> 2), 2 * c1 + ((o >> 1) & 1), 2 * c2 + (o & 1));
+          const float a = sa[p];
+          if (a != 0.0f && sa[pc] != 0.0f) {
+            const float Az = __fadd_rn(__fmul_rn(a, zm[p]), csum_t<STO>(zm, sx, A.total, p, gf, dim, ms));
+            val = __fsub_rn(sr[p], Az);
+            use = true;
+          }
+        }
+        const int lead = (int)(threadIdx.x & 31u) & ~7;
+        float acc = 0.0f;
+#pragma unroll
+        for (int k = 0; k < 8; ++k) {
+          const float vk = __shfl_sync(0xffffffffu, val, lead + k);
+          const int uk = __shfl_sync(0xffffffffu, (int)use, lead + k);
+          if (uk) acc = __fadd_rn(acc, vk);
+        }
+        if (o == 0 && pc >= 0 && sa[pc] != 0.0f) sr[pc] = __fmul_rn(A.rho, acc);
+      }
+      __syncthreads();
+      continue;
+    }
     for (int i = threadIdx.x; i < cnt; i += blockDim.x) {
       const int c2 = dim == 3 ? i % gc.n2 : 0;
       const int t = dim == 3 ? i / gc.n2 : i;
@@ -221,10 +299,11 @@ __device__ __forceinline__ void coarse_vcycle(const CoarseArgs& A, unsigned char
     if (pt > (int)blockDim.x || (cntb + pt - 1) / pt > kBottomPerThread) pt = blockDim.x;
     if (cntb <= kBottomPerThread * pt) {
       if ((int)threadIdx.x < pt) {
-        // each owned cell's padded index, r and Adiag in registers (and, for
+        // each owned cell's padded index, r and 1 / Adiag in registers (and, for
         // STO, its six couplings: constant through the bottom sweeps)
         int gi[2][kBottomPerThread];
-        float rr[2][kBottomPerThread], aa[2][kBottomPerThread];
+        float rr[2][kBottomPerThread];
+        double yd[2][kBottomPerThread];  // 1 / Adiag (div_recip64)
         float cx[2][kBottomPerThread][STO ? 6 : 1];
 #pragma unroll
         for (int ph = 0; ph < 2; ++ph) {
@@ -234,7 +313,7 @@ __device__ __forceinline__ void coarse_vcycle(const CoarseArgs& A, unsigned char
             int c0, c1, c2;
             gi[ph][k] = -1;
             rr[ph][k] = 0.0f;
-            aa[ph][k] = 1.0f;
+            yd[ph][k] = 1.0;
 #pragma unroll
             for (int e = 0; e < (STO ? 6 : 1); ++e) cx[ph][k][e] = 0.0f;
             if (j < cntb && colour_cell(g, dim, j, ph, c0, c1, c2)) {
@@ -242,7 +321,7 @@ __device__ __forceinline__ void coarse_vcycle(const CoarseArgs& A, unsigned char
               if (sa[p] != 0.0f) {
                 gi[ph][k] = p;
                 rr[ph][k] = sr[p];
-                aa[ph][k] = sa[p];
+                yd[ph][k] = 1.0 / (double)sa[p];
                 if constexpr (STO) {  // the couplings csum_t reads, in its order
                   cx[ph][k][0] = sx[p - g.s0];
                   cx[ph][k][1] = sx[p];
@@ -255,36 +334,43 @@ __device__ __forceinline__ void coarse_vcycle(const CoarseArgs& A, unsigned char
             }
           }
         }
-        for (int i = 0; i < 2 * nh; ++i) {
+        // one half sweep of colour PH (a compile-time constant: the owned
+        // cells' registers are named directly, no selects between colours)
+        auto half = [&](auto PH) {
+          constexpr int ph = decltype(PH)::value;
+          float v[kBottomPerThread];
 #pragma unroll
-          for (int h = 0; h < 2; ++h) {
-            const int ph = i < nh ? h : 1 - h;
-            float v[kBottomPerThread];
-#pragma unroll
-            for (int k = 0; k < kBottomPerThread; ++k) {   // all loads first
-              const int p = ph ? gi[1][k] : gi[0][k];
-              const int ps = p >= 0 ? p : g.at(0, 0, 0);     // an in-range cell for empty slots
-              const float r_ = ph ? rr[1][k] : rr[0][k];
-              const float a_ = ph ? aa[1][k] : aa[0][k];
-              float sum;
-              if constexpr (STO) {  // csum_t with the couplings from registers
-                const float* x6 = ph ? cx[1][k] : cx[0][k];
-                sum = __fadd_rn(__fmul_rn(x6[0], zm[ps - g.s0]), __fmul_rn(x6[1], zm[ps + g.s0]));
-                sum = __fadd_rn(0.0f, sum);
-                sum = __fadd_rn(sum, __fadd_rn(__fmul_rn(x6[2], zm[ps - g.s1]), __fmul_rn(x6[3], zm[ps + g.s1])));
-                if (dim == 3) sum = __fadd_rn(sum, __fadd_rn(__fmul_rn(x6[4], zm[ps - 1]), __fmul_rn(x6[5], zm[ps + 1])));
-              } else {
-                sum = csum_t<STO>(zm, sx, A.total, ps, g, dim, ms);
-              }
-              v[k] = div_pos(__fsub_rn(r_, sum), a_);
+          for (int k = 0; k < kBottomPerThread; ++k) {   // all loads first
+            const int p = gi[ph][k];
+            const int ps = p >= 0 ? p : g.at(0, 0, 0);     // an in-range cell for empty slots
+            float sum;
+            if constexpr (STO) {  // csum_t with the couplings from registers
+              const float* x6 = cx[ph][k];
+              sum = __fadd_rn(__fmul_rn(x6[0], zm[ps - g.s0]), __fmul_rn(x6[1], zm[ps + g.s0]));
+              sum = __fadd_rn(0.0f, sum);
+              sum = __fadd_rn(sum, __fadd_rn(__fmul_rn(x6[2], zm[ps - g.s1]), __fmul_rn(x6[3], zm[ps + g.s1])));
+              if (dim == 3) sum = __fadd_rn(sum, __fadd_rn(__fmul_rn(x6[4], zm[ps - 1]), __fmul_rn(x6[5], zm[ps + 1])));
+            } else {
+              sum = csum_t<STO>(zm, sx, A.total, ps, g, dim, ms);
             }
-#pragma unroll
-            for (int k = 0; k < kBottomPerThread; ++k) {   // then the stores
-              const int p = ph ? gi[1][k] : gi[0][k];
-              if (p >= 0) zm[p] = v[k];
-            }
-            asm volatile("bar.sync 1, %0;" ::"r"(pt) : "memory");
+            v[k] = div_recip64(__fsub_rn(rr[ph][k], sum), yd[ph][k]);
           }
+#pragma unroll
+          for (int k = 0; k < kBottomPerThread; ++k) {   // then the stores
+            const int p = gi[ph][k];
+            if (p >= 0) zm[p] = v[k];
+          }
+          asm volatile("bar.sync 1, %0;" ::"r"(pt) : "memory");
+        };
+        using C0 = std::integral_constant<int, 0>;
+        using C1 = std::integral_constant<int, 1>;
+        for (int i = 0; i < nh; ++i) {  // colours 0, 1 (mgpcg.py:136-138)
+          half(C0{});
+          half(C1{});
+        }
+        for (int i = 0; i < nh; ++i) {  // then 1, 0 (mgpcg.py:139-141)
+          half(C1{});
+          half(C0{});
         }
       }
       __syncthreads();
@@ -313,9 +399,11 @@ __device__ __forceinline__ void coarse_vcycle(const CoarseArgs& A, unsigned char
     }
     __syncthreads();
     for (int i = 0; i < A.pre_post; ++i) {
-      coarse_smooth<STO>(A, l, 1, zm, sr, sa, sx);
+      if (l == 0 && listed) coarse_smooth_list<STO>(A, 0, li[1], zm, sr, sa, sx);
+      else coarse_smooth<STO>(A, l, 1, zm, sr, sa, sx);
       __syncthreads();
-      coarse_smooth<STO>(A, l, 0, zm, sr, sa, sx);
+      if (l == 0 && listed) coarse_smooth_list<STO>(A, 0, li[0], zm, sr, sa, sx);
+      else coarse_smooth<STO>(A, l, 0, zm, sr, sa, sx);
       __syncthreads();
     }
   }

@@ -82,6 +82,18 @@ __device__ __forceinline__ float div_pos(float x, float a) {
   return z ? x : q;
 }
 
+// x / a in IEEE float32 (round to nearest even) from yd = 1 / (double)a, for
+// a divisor used many times.  The double product x * yd is within 2^-52
+// (relative) of x / a, while a quotient of two floats that is not a float
+// lies at least 2^-49 (relative) from every float32 rounding boundary (a
+// boundary has an odd 25-bit significand, which a 24-bit divisor times it
+// cannot bring back to a 24-bit dividend; the same holds for the subnormal
+// grid and the overflow threshold), so the product rounds to the correctly
+// rounded quotient (rounding twice, first to 53 bits, is innocuous here).
+// For a > 0 it is x / a bit for bit, zeros keeping the dividend's sign as in
+// div_pos.
+__device__ __forceinline__ float div_recip64(float x, double yd) { return __double2float_rn((double)x * yd); }
+
 template <typename T> __device__ __forceinline__ float to_f(T v);
 template <> __device__ __forceinline__ float to_f<float>(float v) { return v; }
 template <> __device__ __forceinline__ float to_f<__half>(__half v) { return __half2float(v); }
