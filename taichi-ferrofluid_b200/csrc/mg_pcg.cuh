@@ -371,6 +371,12 @@ __global__ void __launch_bounds__(kRedThreads) k_Ap_alpha(Level L, const float* 
   }
 }
 
+// Component e (a compile-time constant after unrolling) of a float4, without
+// taking its address (which would keep the vector in local memory).
+__device__ __forceinline__ float f4at(const float4& v, int e) {
+  return e == 0 ? v.x : (e == 1 ? v.y : (e == 2 ? v.z : v.w));
+}
+
 // k_Ap_alpha over groups of 4 consecutive cells along the fastest axis (its
 // extent a multiple of 4): 16-byte loads of labels, Adiag, p, the stored
 // couplings and the neighbour rows; the neighbour sum of nbr_sum_f32 per
@@ -382,10 +388,14 @@ struct GroupWalk {
   int x, c0, c1;     // coordinates of the current group's first cell
   int dx, dc0, dc1;  // the loop's stride in cells, split the same way
   int nx, n1, dim;
-  __device__ __forceinline__ GroupWalk(const Geom& g, int q, int stride_groups) {
-    dim = g.dim;
-    nx = g.n[dim - 1];
-    n1 = g.n[1];
+  __device__ __forceinline__ GroupWalk(const Geom& g, int q, int stride_groups)
+      : GroupWalk(g.dim, g.n[g.dim - 1], g.n[1], q, stride_groups) {}
+  // the extents given directly (no runtime index into a Geom, which would
+  // keep the kernel parameter in local memory)
+  __device__ __forceinline__ GroupWalk(int dim_, int nx_, int n1_, int q, int stride_groups) {
+    dim = dim_;
+    nx = nx_;
+    n1 = n1_;
     const long long i = 4LL * q, di = 4LL * stride_groups;
     const long long t = i / nx, dt = di / nx;
     x = (int)(i % nx);
@@ -422,22 +432,25 @@ struct GroupWalk {
   }
 };
 
-__global__ void __launch_bounds__(kRedThreads) k_Ap_alpha4(Level L, const float* __restrict__ p,
-                                                           float* __restrict__ Ap, Control* ctl, double* partials,
-                                                           int force = 0) {
-  pdl_enter();
-  if (!ctl->run && !force) return;
-  __shared__ double sh[32];
-  const int dim = L.g.dim;
+// The grid-stride loop of k_Ap_alpha4 for a compile-time dim (the per-axis
+// neighbour rows and couplings stay in registers); returns this thread's p.Ap.
+template <int DIM>
+__device__ __forceinline__ double Ap4_loop(Level L, const float* __restrict__ p, float* __restrict__ Ap) {
+  constexpr int dim = DIM;
   const int nx = L.g.n[dim - 1];
   const int groups = (int)(L.g.count >> 2);
   const float4 z4 = make_float4(0.f, 0.f, 0.f, 0.f);
   double acc = 0.0;
   const int q0 = blockIdx.x * blockDim.x + threadIdx.x, S = gridDim.x * blockDim.x;
-  GroupWalk w(L.g, q0, S);
+  GroupWalk w(dim, nx, L.g.n[1], q0, S);
+  // the next group's labels are loaded one iteration ahead: the loads of a
+  // group wait on one round trip, not two
+  const uint32_t* t4p = reinterpret_cast<const uint32_t*>(L.type);
+  uint32_t t4n = q0 < groups ? __ldg(t4p + q0) : 0x01010101u;
   for (int q = q0; q < groups; q += S, w.advance()) {
     const int i = q << 2;
-    const uint32_t t4 = __ldg(reinterpret_cast<const uint32_t*>(L.type) + q);
+    const uint32_t t4 = t4n;
+    t4n = q + S < groups ? __ldg(t4p + q + S) : 0x01010101u;
     if (t4 == 0x02020202u || t4 == 0x01010101u) continue;
     const int x = w.x;
     const int c[2] = {w.c0, w.c1};  // coordinates of the slower axes
@@ -449,6 +462,7 @@ __global__ void __launch_bounds__(kRedThreads) k_Ap_alpha4(Level L, const float*
     const float pxr = x + 4 < nx ? __ldg(p + i + 4) : 0.0f;
     float4 plo[2], phi_[2], alo[2], ahi[2];
     bool has_lo[2], has_hi[2];
+#pragma unroll
     for (int k = 0; k < dim - 1; ++k) {
       const int st = k == 0 ? (dim == 3 ? L.g.n[1] * nx : nx) : nx;
       has_lo[k] = c[k] > 0;
@@ -458,28 +472,24 @@ __global__ void __launch_bounds__(kRedThreads) k_Ap_alpha4(Level L, const float*
       phi_[k] = has_hi[k] ? __ldg(reinterpret_cast<const float4*>(p + i + st)) : z4;
       ahi[k] = __ldg(reinterpret_cast<const float4*>(L.Ax[k] + i));
     }
-    const float pv[4] = {pc.x, pc.y, pc.z, pc.w}, av[4] = {ad.x, ad.y, ad.z, ad.w};
-    const float xv[4] = {xc.x, xc.y, xc.z, xc.w};
+    // components through f4at (see Ap_uniform4_loop)
     float out[4] = {0.f, 0.f, 0.f, 0.f};
 #pragma unroll
     for (int e = 0; e < 4; ++e) {
       if (!fluid_lane(t4, e)) continue;
       float ret = 0.0f;
-      for (int k = 0; k < dim - 1; ++k) {
-        const float* pl4 = reinterpret_cast<const float*>(&plo[k]);
-        const float* ph4 = reinterpret_cast<const float*>(&phi_[k]);
-        const float* al4 = reinterpret_cast<const float*>(&alo[k]);
-        const float* ah4 = reinterpret_cast<const float*>(&ahi[k]);
-        const float lo = has_lo[k] ? __fmul_rn(al4[e], pl4[e]) : 0.0f;
-        const float hi = has_hi[k] ? __fmul_rn(ah4[e], ph4[e]) : 0.0f;
+  #pragma unroll
+    for (int k = 0; k < dim - 1; ++k) {
+        const float lo = has_lo[k] ? __fmul_rn(f4at(alo[k], e), f4at(plo[k], e)) : 0.0f;
+        const float hi = has_hi[k] ? __fmul_rn(f4at(ahi[k], e), f4at(phi_[k], e)) : 0.0f;
         ret = __fadd_rn(ret, __fadd_rn(lo, hi));
       }
-      const float lo = x + e > 0 ? __fmul_rn(e == 0 ? axl : xv[e - 1], e == 0 ? pxl : pv[e - 1]) : 0.0f;
-      const float hi = x + e + 1 < nx ? __fmul_rn(xv[e], e == 3 ? pxr : pv[e + 1]) : 0.0f;
+      const float lo = x + e > 0 ? __fmul_rn(e == 0 ? axl : f4at(xc, e - 1), e == 0 ? pxl : f4at(pc, e - 1)) : 0.0f;
+      const float hi = x + e + 1 < nx ? __fmul_rn(f4at(xc, e), e == 3 ? pxr : f4at(pc, e + 1)) : 0.0f;
       ret = __fadd_rn(ret, __fadd_rn(lo, hi));
-      const float v = __fadd_rn(__fmul_rn(av[e], pv[e]), ret);
+      const float v = __fadd_rn(__fmul_rn(f4at(ad, e), f4at(pc, e)), ret);
       out[e] = v;
-      acc += (double)pv[e] * (double)v;
+      acc += (double)f4at(pc, e) * (double)v;
     }
     if (t4 == 0x01010101u * (uint32_t)(uint8_t)FLUID) {  // every lane FLUID (the whole-domain form): one 16-byte store
       *reinterpret_cast<float4*>(Ap + i) = make_float4(out[0], out[1], out[2], out[3]);
@@ -489,6 +499,16 @@ __global__ void __launch_bounds__(kRedThreads) k_Ap_alpha4(Level L, const float*
         if (fluid_lane(t4, e)) Ap[i + e] = out[e];
     }
   }
+  return acc;
+}
+
+__global__ void __launch_bounds__(kRedThreads, 4) k_Ap_alpha4(Level L, const float* __restrict__ p,
+                                                           float* __restrict__ Ap, Control* ctl, double* partials,
+                                                           int force = 0) {
+  pdl_enter();
+  if (!ctl->run && !force) return;
+  __shared__ double sh[32];
+  const double acc = L.g.dim == 3 ? Ap4_loop<3>(L, p, Ap) : Ap4_loop<2>(L, p, Ap);
   double tot;
   if (last_block_total<kRedThreads>(acc, partials, &ctl->counter[2], sh, &tot) && threadIdx.x == 0) {
     ctl->pAp = tot;
@@ -550,22 +570,25 @@ __global__ void __launch_bounds__(kRedThreads) k_Ap_alpha_uniform(Level L, const
 // the x neighbours, 32-bit indices, several groups in flight per thread.  The
 // same float32 operations per cell in the same axis order; non-FLUID cells
 // keep their Ap (written only where Adiag != 0).
-__device__ __forceinline__ void Ap_alpha_uniform4_body(int bid_, int nb_, Level L, const float* __restrict__ p,
-                                                                   float* __restrict__ Ap, float s, Control* ctl,
-                                                                   double* partials, int force) {
-
-  if (!ctl->run && !force) return;
-  __shared__ double sh[32];
-  const float ms = -s;
-  const int dim = L.g.dim;
+// The grid-stride loop of Ap_alpha_uniform4_body for a compile-time dim (the
+// per-axis neighbour rows stay in registers); returns this thread's p.Ap.
+template <int DIM>
+__device__ __forceinline__ double Ap_uniform4_loop(int bid_, int nb_, Level L, const float* __restrict__ p,
+                                                   float* __restrict__ Ap, float ms) {
+  constexpr int dim = DIM;
   const int nx = L.g.n[dim - 1];
   const int groups = (int)(L.g.count >> 2);
   double acc = 0.0;
   const int q0 = bid_ * blockDim.x + threadIdx.x, S = nb_ * blockDim.x;
-  GroupWalk w(L.g, q0, S);
+  GroupWalk w(dim, nx, L.g.n[1], q0, S);
+  // the next group's Adiag is loaded one iteration ahead: a group's p loads
+  // wait on one round trip, not two
+  const float4 z4 = make_float4(0.f, 0.f, 0.f, 0.f);
+  float4 an = q0 < groups ? __ldg(reinterpret_cast<const float4*>(L.Adiag) + q0) : z4;
   for (int q = q0; q < groups; q += S, w.advance()) {
     const int i = q << 2;
-    const float4 a = __ldg(reinterpret_cast<const float4*>(L.Adiag + i));
+    const float4 a = an;
+    an = q + S < groups ? __ldg(reinterpret_cast<const float4*>(L.Adiag) + q + S) : z4;
     // a group without a FLUID cell loads nothing more (large AIR regions at
     // sizes beyond L2)
     if (a.x == 0.0f && a.y == 0.0f && a.z == 0.0f && a.w == 0.0f) continue;
@@ -576,42 +599,54 @@ __device__ __forceinline__ void Ap_alpha_uniform4_body(int bid_, int nb_, Level 
     const float pxr = x + 4 < nx ? __ldg(p + i + 4) : 0.0f;
     float4 lo4[2], hi4[2];
     bool has_lo[2], has_hi[2];
+#pragma unroll
     for (int k = 0; k < dim - 1; ++k) {
       const int st = k == 0 ? (dim == 3 ? L.g.n[1] * nx : nx) : nx;
       has_lo[k] = c[k] > 0;
       has_hi[k] = c[k] + 1 < L.g.n[k];
-      lo4[k] = has_lo[k] ? __ldg(reinterpret_cast<const float4*>(p + i - st)) : make_float4(0.f, 0.f, 0.f, 0.f);
-      hi4[k] = has_hi[k] ? __ldg(reinterpret_cast<const float4*>(p + i + st)) : make_float4(0.f, 0.f, 0.f, 0.f);
+      lo4[k] = has_lo[k] ? __ldg(reinterpret_cast<const float4*>(p + i - st)) : z4;
+      hi4[k] = has_hi[k] ? __ldg(reinterpret_cast<const float4*>(p + i + st)) : z4;
     }
-    const float av[4] = {a.x, a.y, a.z, a.w};
-    const float pv[4] = {pc.x, pc.y, pc.z, pc.w};
+    // components through f4at (the neighbours e - 1, e + 1 of the end cells
+    // are never selected; an array indexed there would live in local memory)
     float out[4];
 #pragma unroll
     for (int e = 0; e < 4; ++e) {
       float ret = 0.0f;
+#pragma unroll
       for (int k = 0; k < dim - 1; ++k) {
-        const float* l4 = reinterpret_cast<const float*>(&lo4[k]);
-        const float* h4 = reinterpret_cast<const float*>(&hi4[k]);
-        const float lo = has_lo[k] ? __fmul_rn(ms, l4[e]) : 0.0f;
-        const float hi = has_hi[k] ? __fmul_rn(ms, h4[e]) : 0.0f;
+        const float lo = has_lo[k] ? __fmul_rn(ms, f4at(lo4[k], e)) : 0.0f;
+        const float hi = has_hi[k] ? __fmul_rn(ms, f4at(hi4[k], e)) : 0.0f;
         ret = __fadd_rn(ret, __fadd_rn(lo, hi));
       }
-      const float pl = e == 0 ? pxl : pv[e - 1];
-      const float pr = e == 3 ? pxr : pv[e + 1];
+      const float pl = e == 0 ? pxl : f4at(pc, e - 1);
+      const float pr = e == 3 ? pxr : f4at(pc, e + 1);
       const float lo = x + e > 0 ? __fmul_rn(ms, pl) : 0.0f;
       const float hi = x + e + 1 < nx ? __fmul_rn(ms, pr) : 0.0f;
       ret = __fadd_rn(ret, __fadd_rn(lo, hi));
-      out[e] = __fadd_rn(__fmul_rn(av[e], pv[e]), ret);
-      if (av[e] != 0.0f) acc += (double)pv[e] * (double)out[e];
+      const float pe = f4at(pc, e), ae = f4at(a, e);
+      out[e] = __fadd_rn(__fmul_rn(ae, pe), ret);
+      if (ae != 0.0f) acc += (double)pe * (double)out[e];
     }
     if (a.x != 0.0f && a.y != 0.0f && a.z != 0.0f && a.w != 0.0f) {
       *reinterpret_cast<float4*>(Ap + i) = make_float4(out[0], out[1], out[2], out[3]);
     } else {
 #pragma unroll
       for (int e = 0; e < 4; ++e)
-        if (av[e] != 0.0f) Ap[i + e] = out[e];
+        if (f4at(a, e) != 0.0f) Ap[i + e] = out[e];
     }
   }
+  return acc;
+}
+
+__device__ __forceinline__ void Ap_alpha_uniform4_body(int bid_, int nb_, Level L, const float* __restrict__ p,
+                                                                   float* __restrict__ Ap, float s, Control* ctl,
+                                                                   double* partials, int force) {
+
+  if (!ctl->run && !force) return;
+  __shared__ double sh[32];
+  const double acc = L.g.dim == 3 ? Ap_uniform4_loop<3>(bid_, nb_, L, p, Ap, -s)
+                                  : Ap_uniform4_loop<2>(bid_, nb_, L, p, Ap, -s);
   double tot;
   if (last_block_total_at<kRedThreads>(acc, partials, &ctl->counter[2], sh, &tot, bid_, nb_) && threadIdx.x == 0) {
     ctl->pAp = tot;
@@ -703,38 +738,54 @@ __device__ __forceinline__ void xr4_body(int bid_, int nb_, Level L, float* __re
   float* r = (float*)L.r;
   const int groups = (int)(L.g.count >> 2);
   double acc = 0.0;
-  for (int q = bid_ * blockDim.x + threadIdx.x; q < groups; q += nb_ * blockDim.x) {
-    const uint32_t t4 = __ldg(reinterpret_cast<const uint32_t*>(L.type) + q);
-    float4 xv = reinterpret_cast<float4*>(x)[q];
-    const float4 pv = __ldg(reinterpret_cast<const float4*>(p) + q);
-    float4 rv = reinterpret_cast<float4*>(r)[q];
-    const float4 av = __ldg(reinterpret_cast<const float4*>(Ap) + q);
-    if (t4 == 0x02020202u || t4 == 0x01010101u) continue;  // no FLUID lane
-    float* xs = reinterpret_cast<float*>(&xv);
-    float* rs = reinterpret_cast<float*>(&rv);
-    const float ps[4] = {pv.x, pv.y, pv.z, pv.w}, as[4] = {av.x, av.y, av.z, av.w};
-    if (xh) {  // mixed form: x accumulates in FP64, x (float32) is its rounding
-      double2* xh2 = reinterpret_cast<double2*>(xh) + 2 * q;
-      double2 h0 = xh2[0], h1 = xh2[1];
-      double hv[4] = {h0.x, h0.y, h1.x, h1.y};
+  const int S = nb_ * blockDim.x;
+  // two groups per iteration (q and q + S, the grid-stride order), every load
+  // of both issued before either is used: twice the bytes in flight
+  for (int q = bid_ * blockDim.x + threadIdx.x; q < groups; q += 2 * S) {
+    uint32_t t4[2];
+    float4 xv[2], pv[2], rv[2], av[2];
+#pragma unroll
+    for (int u = 0; u < 2; ++u) {
+      const int qq = q + u * S;
+      t4[u] = 0x01010101u;
+      if (qq < groups) {
+        t4[u] = __ldg(reinterpret_cast<const uint32_t*>(L.type) + qq);
+        xv[u] = reinterpret_cast<float4*>(x)[qq];
+        pv[u] = __ldg(reinterpret_cast<const float4*>(p) + qq);
+        rv[u] = reinterpret_cast<float4*>(r)[qq];
+        av[u] = __ldg(reinterpret_cast<const float4*>(Ap) + qq);
+      }
+    }
+#pragma unroll
+    for (int u = 0; u < 2; ++u) {
+      const int qq = q + u * S;
+      if (t4[u] == 0x02020202u || t4[u] == 0x01010101u) continue;  // no FLUID lane (or past the end)
+      float* xs = reinterpret_cast<float*>(&xv[u]);
+      float* rs = reinterpret_cast<float*>(&rv[u]);
+      const float ps[4] = {pv[u].x, pv[u].y, pv[u].z, pv[u].w}, as[4] = {av[u].x, av[u].y, av[u].z, av[u].w};
+      if (xh) {  // mixed form: x accumulates in FP64, x (float32) is its rounding
+        double2* xh2 = reinterpret_cast<double2*>(xh) + 2 * qq;
+        double2 h0 = xh2[0], h1 = xh2[1];
+        double hv[4] = {h0.x, h0.y, h1.x, h1.y};
+#pragma unroll
+        for (int e = 0; e < 4; ++e) {
+          if (!fluid_lane(t4[u], e)) continue;
+          hv[e] += (double)alpha * (double)ps[e];
+          xs[e] = (float)hv[e];
+        }
+        xh2[0] = make_double2(hv[0], hv[1]);
+        xh2[1] = make_double2(hv[2], hv[3]);
+      }
 #pragma unroll
       for (int e = 0; e < 4; ++e) {
-        if (!fluid_lane(t4, e)) continue;
-        hv[e] += (double)alpha * (double)ps[e];
-        xs[e] = (float)hv[e];
+        if (!fluid_lane(t4[u], e)) continue;
+        if (!xh) xs[e] = __fadd_rn(xs[e], __fmul_rn(alpha, ps[e]));
+        rs[e] = __fsub_rn(rs[e], __fmul_rn(alpha, as[e]));
+        acc += (double)rs[e] * (double)rs[e];
       }
-      xh2[0] = make_double2(hv[0], hv[1]);
-      xh2[1] = make_double2(hv[2], hv[3]);
+      reinterpret_cast<float4*>(x)[qq] = xv[u];
+      reinterpret_cast<float4*>(r)[qq] = rv[u];
     }
-#pragma unroll
-    for (int e = 0; e < 4; ++e) {
-      if (!fluid_lane(t4, e)) continue;
-      if (!xh) xs[e] = __fadd_rn(xs[e], __fmul_rn(alpha, ps[e]));
-      rs[e] = __fsub_rn(rs[e], __fmul_rn(alpha, as[e]));
-      acc += (double)rs[e] * (double)rs[e];
-    }
-    reinterpret_cast<float4*>(x)[q] = xv;
-    reinterpret_cast<float4*>(r)[q] = rv;
   }
   double tot;
   if (last_block_total_at<kRedThreads>(acc, partials, &ctl->counter[3], sh, &tot, bid_, nb_) && threadIdx.x == 0) {
