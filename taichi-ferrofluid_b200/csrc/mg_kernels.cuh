@@ -47,10 +47,10 @@ __device__ __forceinline__ float vel_at(const float* v, const Geom& g, int k, in
   return v[((long long)c0 * n1 + c1) * n2 + c2];
 }
 
-// PressureProjectStrategy.build_b_kernel (pressure_project.py:15-39).  The two
-// passes of the reference touch only b[I] of the cell itself, so one thread
-// runs pass 1 then pass 2 for its cell with the same operation order.
-__global__ void k_build_pressure_b(Level L, const float* __restrict__ v0, const float* __restrict__ v1,
+// k_build_pressure_b for a compile-time dim (its per-axis arrays and the level's
+// extents indexed by constants, so nothing is kept in local memory).
+template <int DIM>
+__device__ __forceinline__ void k_build_pressure_b_dim(Level L, const float* __restrict__ v0, const float* __restrict__ v1,
                                    const float* __restrict__ v2, const float* __restrict__ phi,
                                    float p0, float sA, float sB, int ghost, float clamp, float* b) {
   const float* vel[3] = {v0, v1, v2};
@@ -59,7 +59,8 @@ __global__ void k_build_pressure_b(Level L, const float* __restrict__ v0, const 
     int c[3];
     L.g.coords(i, c);
     float bi = b[i];
-    for (int k = 0; k < L.g.dim; ++k) {
+#pragma unroll
+    for (int k = 0; k < DIM; ++k) {
       int cp[3] = {c[0], c[1], c[2]};
       cp[k] += 1;
       float a = vel_at(vel[k], L.g, k, c[0], c[1], c[2]);
@@ -67,7 +68,9 @@ __global__ void k_build_pressure_b(Level L, const float* __restrict__ v0, const 
       bi = __fadd_rn(bi, __fsub_rn(a, bb));
     }
     bi = __fmul_rn(bi, sB);
-    for (int k = 0; k < L.g.dim; ++k) {
+#pragma unroll
+    for (int k = 0; k < DIM; ++k) {
+#pragma unroll
       for (int s = -1; s <= 1; s += 2) {
         int8_t nt = nb_type(L, i, c, k, s);
         if (nt == SOLID) {
@@ -93,15 +96,29 @@ __global__ void k_build_pressure_b(Level L, const float* __restrict__ v0, const 
   }
 }
 
-// PressureProjectStrategy.build_A_kernel (pressure_project.py:45-64).
-__global__ void k_build_pressure_A(Level L, int level, const float* __restrict__ phi, float sA,
+// PressureProjectStrategy.build_b_kernel (pressure_project.py:15-39).  The two
+// passes of the reference touch only b[I] of the cell itself, so one thread
+// runs pass 1 then pass 2 for its cell with the same operation order.
+__global__ void k_build_pressure_b(Level L, const float* __restrict__ v0, const float* __restrict__ v1,
+                                   const float* __restrict__ v2, const float* __restrict__ phi,
+                                   float p0, float sA, float sB, int ghost, float clamp, float* b) {
+  if (L.g.dim == 3) k_build_pressure_b_dim<3>(L, v0, v1, v2, phi, p0, sA, sB, ghost, clamp, b);
+  else k_build_pressure_b_dim<2>(L, v0, v1, v2, phi, p0, sA, sB, ghost, clamp, b);
+}
+
+// k_build_pressure_A for a compile-time dim (its per-axis arrays and the level's
+// extents indexed by constants, so nothing is kept in local memory).
+template <int DIM>
+__device__ __forceinline__ void k_build_pressure_A_dim(Level L, int level, const float* __restrict__ phi, float sA,
                                    int ghost, float clamp) {
   for (long long i = gtid(); i < L.g.count; i += gstride()) {
     if (L.type[i] != FLUID) continue;
     int c[3];
     L.g.coords(i, c);
     float d = L.Adiag[i];
-    for (int k = 0; k < L.g.dim; ++k) {
+#pragma unroll
+    for (int k = 0; k < DIM; ++k) {
+#pragma unroll
       for (int s = -1; s <= 1; s += 2) {
         int8_t nt = nb_type(L, i, c, k, s);
         if (nt == FLUID) {
@@ -120,6 +137,13 @@ __global__ void k_build_pressure_A(Level L, int level, const float* __restrict__
     }
     L.Adiag[i] = d;
   }
+}
+
+// PressureProjectStrategy.build_A_kernel (pressure_project.py:45-64).
+__global__ void k_build_pressure_A(Level L, int level, const float* __restrict__ phi, float sA,
+                                   int ghost, float clamp) {
+  if (L.g.dim == 3) k_build_pressure_A_dim<3>(L, level, phi, sA, ghost, clamp);
+  else k_build_pressure_A_dim<2>(L, level, phi, sA, ghost, clamp);
 }
 
 // b += c * src (or += c) on FLUID cells (volume_control.py:33-37).

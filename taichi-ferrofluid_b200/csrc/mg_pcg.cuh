@@ -19,11 +19,10 @@ __global__ void k_set_kappa(Control* ctl, double kappa) {
   ctl->bad_operator = 0;
 }
 
-// Checks a declared label-uniform level: Adiag != 0 exactly on FLUID cells
-// and Ax = -s between two FLUID cells, 0 elsewhere.  Flags a mismatch (bit
-// 0), or a FLUID cell with a zero diagonal (bit 1: the reference's smoothing
-// divides by zero there, a non-finite solve).
-__global__ void k_verify_uniform(Level L, float s, Control* ctl) {
+// k_verify_uniform for a compile-time dim (its per-axis arrays and the level's
+// extents indexed by constants, so nothing is kept in local memory).
+template <int DIM>
+__device__ __forceinline__ void k_verify_uniform_dim(Level L, float s, Control* ctl) {
   int bad = 0;
   for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < L.g.count;
        i += (long long)gridDim.x * blockDim.x) {
@@ -32,13 +31,23 @@ __global__ void k_verify_uniform(Level L, float s, Control* ctl) {
     const bool fl = L.type[i] == FLUID;
     if (fl && L.Adiag[i] == 0.0f) bad |= 2;
     else if (!fl && L.Adiag[i] != 0.0f) bad |= 1;
-    for (int k = 0; k < L.g.dim; ++k) {
+#pragma unroll
+    for (int k = 0; k < DIM; ++k) {
       const bool coupled = fl && (c[k] + 1 < L.g.n[k]) && L.type[i + L.g.stride(k)] == FLUID;
       if (L.Ax[k][i] != (coupled ? -s : 0.0f)) bad |= 1;
     }
   }
   bad = __reduce_or_sync(0xffffffffu, bad);
   if (bad && (threadIdx.x & 31) == 0) atomicOr(&ctl->bad_operator, bad);
+}
+
+// Checks a declared label-uniform level: Adiag != 0 exactly on FLUID cells
+// and Ax = -s between two FLUID cells, 0 elsewhere.  Flags a mismatch (bit
+// 0), or a FLUID cell with a zero diagonal (bit 1: the reference's smoothing
+// divides by zero there, a non-finite solve).
+__global__ void k_verify_uniform(Level L, float s, Control* ctl) {
+  if (L.g.dim == 3) k_verify_uniform_dim<3>(L, s, ctl);
+  else k_verify_uniform_dim<2>(L, s, ctl);
 }
 
 // Checks a declared whole-domain level: every cell FLUID (bit 0) with
@@ -478,7 +487,7 @@ __device__ __forceinline__ double Ap4_loop(Level L, const float* __restrict__ p,
     for (int e = 0; e < 4; ++e) {
       if (!fluid_lane(t4, e)) continue;
       float ret = 0.0f;
-  #pragma unroll
+#pragma unroll
     for (int k = 0; k < dim - 1; ++k) {
         const float lo = has_lo[k] ? __fmul_rn(f4at(alo[k], e), f4at(plo[k], e)) : 0.0f;
         const float hi = has_hi[k] ? __fmul_rn(f4at(ahi[k], e), f4at(phi_[k], e)) : 0.0f;

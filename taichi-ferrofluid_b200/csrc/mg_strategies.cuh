@@ -16,11 +16,10 @@ __device__ __forceinline__ float mu_face(float chi_a, float chi_b) {
   return __fdiv_rn(__fmul_rn(2.0f, __fmul_rn(ma, mb)), __fadd_rn(ma, mb));
 }
 
-// Magnetic potential right-hand side on level 0:
-//   b_I = -(1/dx) sum_k H_k (mu(I, I+e_k) - mu(I-e_k, I))
-// over faces inside the domain (no flux through the boundary), b = 0 at the
-// pinned cell.  H is constant (the external field).
-__global__ void k_build_psi_b(Level L, float* b, const float* __restrict__ chi, float H0, float H1, float H2,
+// k_build_psi_b for a compile-time dim (its per-axis arrays and the level's
+// extents indexed by constants, so nothing is kept in local memory).
+template <int DIM>
+__device__ __forceinline__ void k_build_psi_b_dim(Level L, float* b, const float* __restrict__ chi, float H0, float H1, float H2,
                               float dx, int p0, int p1, int p2) {
   const float Hk[3] = {H0, H1, H2};
   const int pin[3] = {p0, p1, p2};
@@ -28,12 +27,13 @@ __global__ void k_build_psi_b(Level L, float* b, const float* __restrict__ chi, 
        i += (long long)gridDim.x * blockDim.x) {
     int c[3];
     L.g.coords(i, c);
-    if (is_pin(c, pin, L.g.dim)) {
+    if (is_pin(c, pin, DIM)) {
       b[i] = 0.0f;
       continue;
     }
     float acc = 0.0f;
-    for (int k = 0; k < L.g.dim; ++k) {
+#pragma unroll
+    for (int k = 0; k < DIM; ++k) {
       const long long s = L.g.stride(k);
       if (c[k] + 1 < L.g.n[k]) acc = __fadd_rn(acc, __fmul_rn(Hk[k], mu_face(chi[i], chi[i + s])));
       if (c[k] > 0) acc = __fsub_rn(acc, __fmul_rn(Hk[k], mu_face(chi[i - s], chi[i])));
@@ -42,24 +42,35 @@ __global__ void k_build_psi_b(Level L, float* b, const float* __restrict__ chi, 
   }
 }
 
-// Magnetic potential operator on level 0: face coefficient mu(I, J) / dx^2
-// (symmetric positive definite), Neumann at the domain boundary, Dirichlet
-// psi = 0 at the pinned cell (its couplings removed, its row the identity
-// times 1/dx^2).
-__global__ void k_build_psi_A(Level L, const float* __restrict__ chi, float dx, int p0, int p1, int p2) {
+// Magnetic potential right-hand side on level 0:
+//   b_I = -(1/dx) sum_k H_k (mu(I, I+e_k) - mu(I-e_k, I))
+// over faces inside the domain (no flux through the boundary), b = 0 at the
+// pinned cell.  H is constant (the external field).
+__global__ void k_build_psi_b(Level L, float* b, const float* __restrict__ chi, float H0, float H1, float H2,
+                              float dx, int p0, int p1, int p2) {
+  if (L.g.dim == 3) k_build_psi_b_dim<3>(L, b, chi, H0, H1, H2, dx, p0, p1, p2);
+  else k_build_psi_b_dim<2>(L, b, chi, H0, H1, H2, dx, p0, p1, p2);
+}
+
+// k_build_psi_A for a compile-time dim (its per-axis arrays and the level's
+// extents indexed by constants, so nothing is kept in local memory).
+template <int DIM>
+__device__ __forceinline__ void k_build_psi_A_dim(Level L, const float* __restrict__ chi, float dx, int p0, int p1, int p2) {
   const int pin[3] = {p0, p1, p2};
   const float dx2 = __fmul_rn(dx, dx);
   for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < L.g.count;
        i += (long long)gridDim.x * blockDim.x) {
     int c[3];
     L.g.coords(i, c);
-    if (is_pin(c, pin, L.g.dim)) {
+    if (is_pin(c, pin, DIM)) {
       L.Adiag[i] = __fdiv_rn(1.0f, dx2);
-      for (int k = 0; k < L.g.dim; ++k) L.Ax[k][i] = 0.0f;
+#pragma unroll
+      for (int k = 0; k < DIM; ++k) L.Ax[k][i] = 0.0f;
       continue;
     }
     float d = 0.0f;
-    for (int k = 0; k < L.g.dim; ++k) {
+#pragma unroll
+    for (int k = 0; k < DIM; ++k) {
       const long long s = L.g.stride(k);
       float up = 0.0f;
       if (c[k] > 0) d = __fadd_rn(d, __fdiv_rn(mu_face(chi[i - s], chi[i]), dx2));
@@ -68,12 +79,21 @@ __global__ void k_build_psi_A(Level L, const float* __restrict__ chi, float dx, 
         d = __fadd_rn(d, cf);
         int cn[3] = {c[0], c[1], c[2]};
         cn[k] += 1;
-        up = is_pin(cn, pin, L.g.dim) ? 0.0f : -cf;
+        up = is_pin(cn, pin, DIM) ? 0.0f : -cf;
       }
       L.Ax[k][i] = up;
     }
     L.Adiag[i] = d;
   }
+}
+
+// Magnetic potential operator on level 0: face coefficient mu(I, J) / dx^2
+// (symmetric positive definite), Neumann at the domain boundary, Dirichlet
+// psi = 0 at the pinned cell (its couplings removed, its row the identity
+// times 1/dx^2).
+__global__ void k_build_psi_A(Level L, const float* __restrict__ chi, float dx, int p0, int p1, int p2) {
+  if (L.g.dim == 3) k_build_psi_A_dim<3>(L, chi, dx, p0, p1, p2);
+  else k_build_psi_A_dim<2>(L, chi, dx, p0, p1, p2);
 }
 
 // chi of a coarse level: the mean of the 2^dim children of the finer level,
@@ -94,6 +114,35 @@ __global__ void k_mean_children(Geom gf, const float* __restrict__ fine, Geom gc
   }
 }
 
+// k_galerkin for a compile-time dim (its per-axis arrays and the level's
+// extents indexed by constants, so nothing is kept in local memory).
+template <int DIM>
+__device__ __forceinline__ void k_galerkin_dim(Level F, Level C, float scale) {
+  for (long long ic = (long long)blockIdx.x * blockDim.x + threadIdx.x; ic < C.g.count;
+       ic += (long long)gridDim.x * blockDim.x) {
+    int cc[3];
+    C.g.coords(ic, cc);
+    constexpr int dim = DIM;
+    float d = 0.0f, ax[3] = {0.0f, 0.0f, 0.0f};
+    for (int o0 = 0; o0 < 2; ++o0)
+      for (int o1 = 0; o1 < 2; ++o1)
+        for (int o2 = 0; o2 < (dim == 3 ? 2 : 1); ++o2) {
+          const int o[3] = {o0, o1, o2};
+          const long long i = F.g.index(2 * cc[0] + o0, 2 * cc[1] + o1, dim == 3 ? 2 * cc[2] + o2 : 0);
+          d = __fadd_rn(d, F.Adiag[i]);
+#pragma unroll
+          for (int k = 0; k < dim; ++k) {
+            const float a = F.Ax[k][i];
+            if (o[k] == 0) d = __fadd_rn(d, __fmul_rn(2.0f, a));  // internal face
+            else ax[k] = __fadd_rn(ax[k], a);                       // face to the next block
+          }
+        }
+    C.Adiag[ic] = __fmul_rn(scale, d);
+#pragma unroll
+    for (int k = 0; k < dim; ++k) C.Ax[k][ic] = (cc[k] + 1 < C.g.n[k]) ? __fmul_rn(scale, ax[k]) : 0.0f;
+  }
+}
+
 // Galerkin coarse operator A_c = P^T A P for the reference's transfer pair
 // (prolongation: piecewise constant, mgpcg.py:120-123; restriction: the
 // unweighted sum of the 2^d children, mgpcg.py:111-118):
@@ -104,27 +153,8 @@ __global__ void k_mean_children(Geom gf, const float* __restrict__ fine, Geom gc
 // by `scale` (a power of two, so the product is exact): 1 gives P^T A P, 1/2
 // the over-corrected coarse operator of the magnetic potential Strategy.
 __global__ void k_galerkin(Level F, Level C, float scale) {
-  for (long long ic = (long long)blockIdx.x * blockDim.x + threadIdx.x; ic < C.g.count;
-       ic += (long long)gridDim.x * blockDim.x) {
-    int cc[3];
-    C.g.coords(ic, cc);
-    const int dim = C.g.dim;
-    float d = 0.0f, ax[3] = {0.0f, 0.0f, 0.0f};
-    for (int o0 = 0; o0 < 2; ++o0)
-      for (int o1 = 0; o1 < 2; ++o1)
-        for (int o2 = 0; o2 < (dim == 3 ? 2 : 1); ++o2) {
-          const int o[3] = {o0, o1, o2};
-          const long long i = F.g.index(2 * cc[0] + o0, 2 * cc[1] + o1, dim == 3 ? 2 * cc[2] + o2 : 0);
-          d = __fadd_rn(d, F.Adiag[i]);
-          for (int k = 0; k < dim; ++k) {
-            const float a = F.Ax[k][i];
-            if (o[k] == 0) d = __fadd_rn(d, __fmul_rn(2.0f, a));  // internal face
-            else ax[k] = __fadd_rn(ax[k], a);                       // face to the next block
-          }
-        }
-    C.Adiag[ic] = __fmul_rn(scale, d);
-    for (int k = 0; k < dim; ++k) C.Ax[k][ic] = (cc[k] + 1 < C.g.n[k]) ? __fmul_rn(scale, ax[k]) : 0.0f;
-  }
+  if (C.g.dim == 3) k_galerkin_dim<3>(F, C, scale);
+  else k_galerkin_dim<2>(F, C, scale);
 }
 
 // ---------------------------------------------------------------------------
@@ -191,21 +221,16 @@ __device__ __forceinline__ float h2_at(const float* const Hs[3], const Geom& g, 
   return hh;
 }
 
-// FluidSimulator.apply_pressure (fluid_simulator.py:193-214) and, with H given,
-// FerrofluidSimulator.apply_magnetic_force (ferrofluid_simulator.py:115-137)
-// for axis k: the pressure-gradient update of the MAC velocity u_k on face I
-// (between cells I - e_k and I) of every cell I.  Out-of-range cells are SOLID
-// (fluid_simulator.py:123-136).  With H the AIR side pressure is
-// p0 + coef |H(air cell + 0.5)|^2 and no ghost-fluid factor applies.
-// Cell labels come from ct32 (the simulator's int32 field) or, when it is
-// null, from the plan's level-0 labels.  scale = dt / (rho dx).
-__global__ void k_apply_pressure(Level L, int k, float* __restrict__ u, const float* __restrict__ pr,
+// k_apply_pressure for a compile-time dim (its per-axis arrays and the level's
+// extents indexed by constants, so nothing is kept in local memory).
+template <int DIM>
+__device__ __forceinline__ void k_apply_pressure_dim(Level L, int k, float* __restrict__ u, const float* __restrict__ pr,
                                  const int32_t* __restrict__ ct32, const float* __restrict__ phi, float scale,
                                  float p0, int ghost, float clamp, const float* H0, const float* H1,
                                  const float* H2, float coef) {
   const Geom& g = L.g;
   const float* const Hs[3] = {H0, H1, H2};
-  const int nu1 = g.n[1] + (k == 1), nu2 = g.dim == 3 ? g.n[2] + (k == 2) : 1;
+  const int nu1 = g.n[1] + (k == 1), nu2 = DIM == 3 ? g.n[2] + (k == 2) : 1;
   for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < g.count;
        i += (long long)gridDim.x * blockDim.x) {
     int c[3];
@@ -244,6 +269,22 @@ __global__ void k_apply_pressure(Level L, int k, float* __restrict__ u, const fl
       u[f] = __fsub_rn(u[f], __fmul_rn(scale, __fsub_rn(pr[i], pr[i1])));
     }
   }
+}
+
+// FluidSimulator.apply_pressure (fluid_simulator.py:193-214) and, with H given,
+// FerrofluidSimulator.apply_magnetic_force (ferrofluid_simulator.py:115-137)
+// for axis k: the pressure-gradient update of the MAC velocity u_k on face I
+// (between cells I - e_k and I) of every cell I.  Out-of-range cells are SOLID
+// (fluid_simulator.py:123-136).  With H the AIR side pressure is
+// p0 + coef |H(air cell + 0.5)|^2 and no ghost-fluid factor applies.
+// Cell labels come from ct32 (the simulator's int32 field) or, when it is
+// null, from the plan's level-0 labels.  scale = dt / (rho dx).
+__global__ void k_apply_pressure(Level L, int k, float* __restrict__ u, const float* __restrict__ pr,
+                                 const int32_t* __restrict__ ct32, const float* __restrict__ phi, float scale,
+                                 float p0, int ghost, float clamp, const float* H0, const float* H1,
+                                 const float* H2, float coef) {
+  if (L.g.dim == 3) k_apply_pressure_dim<3>(L, k, u, pr, ct32, phi, scale, p0, ghost, clamp, H0, H1, H2, coef);
+  else k_apply_pressure_dim<2>(L, k, u, pr, ct32, phi, scale, p0, ghost, clamp, H0, H1, H2, coef);
 }
 
 // LevelSet.theta (level_set.py:24-30): smoothed Heaviside of half width eps.
@@ -325,12 +366,10 @@ __global__ void k_add_c(Level L, float* b, const double* __restrict__ state) {
     if (L.type[i] == FLUID) b[i] = __fadd_rn(b[i], c);
 }
 
-// MagneticForceStrategy.build_b_kernel (magnetic_force.py:17-38): the pressure
-// right-hand side whose AIR faces carry the magnetic pressure
-// p0 + (k mu0 / 2) |H|^2, H sampled from the MAC field H at the face
-// (FerrofluidSimulator.H_interp, ferrofluid_simulator.py:64-69); no ghost
-// fluid factor in b.  coef = 0.5 * k * mu0.
-__global__ void k_build_magnetic_b(Level L, const float* __restrict__ v0, const float* __restrict__ v1,
+// k_build_magnetic_b for a compile-time dim (its per-axis arrays and the level's
+// extents indexed by constants, so nothing is kept in local memory).
+template <int DIM>
+__device__ __forceinline__ void k_build_magnetic_b_dim(Level L, const float* __restrict__ v0, const float* __restrict__ v1,
                                    const float* __restrict__ v2, const float* __restrict__ H0,
                                    const float* __restrict__ H1, const float* __restrict__ H2, float p0, float sA,
                                    float sB, float coef, float* b) {
@@ -342,13 +381,16 @@ __global__ void k_build_magnetic_b(Level L, const float* __restrict__ v0, const 
     int c[3];
     L.g.coords(i, c);
     float bi = b[i];
-    for (int k = 0; k < L.g.dim; ++k) {
+#pragma unroll
+    for (int k = 0; k < DIM; ++k) {
       int cp[3] = {c[0], c[1], c[2]};
       cp[k] += 1;
       bi = __fadd_rn(bi, __fsub_rn(vel_at(vel[k], L.g, k, c[0], c[1], c[2]), vel_at(vel[k], L.g, k, cp[0], cp[1], cp[2])));
     }
     bi = __fmul_rn(bi, sB);
-    for (int k = 0; k < L.g.dim; ++k) {
+#pragma unroll
+    for (int k = 0; k < DIM; ++k) {
+#pragma unroll
       for (int s = -1; s <= 1; s += 2) {
         const int8_t nt = nb_type(L, i, c, k, s);
         if (nt == SOLID) {
@@ -370,6 +412,19 @@ __global__ void k_build_magnetic_b(Level L, const float* __restrict__ v0, const 
   }
 }
 
+// MagneticForceStrategy.build_b_kernel (magnetic_force.py:17-38): the pressure
+// right-hand side whose AIR faces carry the magnetic pressure
+// p0 + (k mu0 / 2) |H|^2, H sampled from the MAC field H at the face
+// (FerrofluidSimulator.H_interp, ferrofluid_simulator.py:64-69); no ghost
+// fluid factor in b.  coef = 0.5 * k * mu0.
+__global__ void k_build_magnetic_b(Level L, const float* __restrict__ v0, const float* __restrict__ v1,
+                                   const float* __restrict__ v2, const float* __restrict__ H0,
+                                   const float* __restrict__ H1, const float* __restrict__ H2, float p0, float sA,
+                                   float sB, float coef, float* b) {
+  if (L.g.dim == 3) k_build_magnetic_b_dim<3>(L, v0, v1, v2, H0, H1, H2, p0, sA, sB, coef, b);
+  else k_build_magnetic_b_dim<2>(L, v0, v1, v2, H0, H1, H2, p0, sA, sB, coef, b);
+}
+
 // PotentialFunctionStrategy (potential_function.py:19-55), the reference's
 // form: whole domain, A negative definite, cell 0 pinned, in_domain tested
 // against the FINE resolution on every level, chi sampled at the faces.
@@ -379,14 +434,17 @@ __device__ __forceinline__ bool in_domain(const int c[3], const int res[3], int 
   return true;
 }
 
-__global__ void k_build_potential_b(Level L, float* b, const float* __restrict__ chi, const float* __restrict__ Hx0,
+// k_build_potential_b for a compile-time dim (its per-axis arrays and the level's
+// extents indexed by constants, so nothing is kept in local memory).
+template <int DIM>
+__device__ __forceinline__ void k_build_potential_b_dim(Level L, float* b, const float* __restrict__ chi, const float* __restrict__ Hx0,
                                     const float* __restrict__ Hx1, const float* __restrict__ Hx2, int r0, int r1,
                                     int r2) {
   const int res[3] = {r0, r1, r2};
   const float* Hx[3] = {Hx0, Hx1, Hx2};
   Field fc;
   fc.v = chi;
-  fc.dim = L.g.dim;
+  fc.dim = DIM;
   fc.n[0] = L.g.n[0];
   fc.n[1] = L.g.n[1];
   fc.n[2] = L.g.n[2];
@@ -394,23 +452,24 @@ __global__ void k_build_potential_b(Level L, float* b, const float* __restrict__
        i += (long long)gridDim.x * blockDim.x) {
     int c[3];
     L.g.coords(i, c);
-    const bool origin = c[0] == 0 && c[1] == 0 && (L.g.dim == 2 || c[2] == 0);
+    const bool origin = c[0] == 0 && c[1] == 0 && (DIM == 2 || c[2] == 0);
     if (origin) {
       b[i] = 0.0f;
       continue;
     }
-    if (!in_domain(c, res, L.g.dim)) continue;
+    if (!in_domain(c, res, DIM)) continue;
     float bi = b[i];
-    for (int k = 0; k < L.g.dim; ++k) {
+#pragma unroll
+    for (int k = 0; k < DIM; ++k) {
       int up[3] = {c[0], c[1], c[2]}, dn[3] = {c[0], c[1], c[2]};
       up[k] += 1;
       dn[k] -= 1;
-      if (in_domain(up, res, L.g.dim)) {
+      if (in_domain(up, res, DIM)) {
         float pos[3];
         for (int a = 0; a < 3; ++a) pos[a] = __fadd_rn((float)up[a], a == k ? 0.0f : 0.5f);
         bi = __fadd_rn(bi, __fmul_rn(sample(fc, pos), vel_at(Hx[k], L.g, k, up[0], up[1], up[2])));
       }
-      if (in_domain(dn, res, L.g.dim)) {
+      if (in_domain(dn, res, DIM)) {
         float pos[3];
         for (int a = 0; a < 3; ++a) pos[a] = __fadd_rn((float)c[a], a == k ? 0.0f : 0.5f);
         bi = __fsub_rn(bi, __fmul_rn(sample(fc, pos), vel_at(Hx[k], L.g, k, c[0], c[1], c[2])));
@@ -420,9 +479,17 @@ __global__ void k_build_potential_b(Level L, float* b, const float* __restrict__
   }
 }
 
-// dx_l = dx 2^level and inv_dx_l = 1 / dx_l are folded on the host (the
-// reference computes both in double before they meet f32 values).
-__global__ void k_build_potential_A(Level L, int level, const float* __restrict__ chi, Geom fine, float dx_l,
+__global__ void k_build_potential_b(Level L, float* b, const float* __restrict__ chi, const float* __restrict__ Hx0,
+                                    const float* __restrict__ Hx1, const float* __restrict__ Hx2, int r0, int r1,
+                                    int r2) {
+  if (L.g.dim == 3) k_build_potential_b_dim<3>(L, b, chi, Hx0, Hx1, Hx2, r0, r1, r2);
+  else k_build_potential_b_dim<2>(L, b, chi, Hx0, Hx1, Hx2, r0, r1, r2);
+}
+
+// k_build_potential_A for a compile-time dim (its per-axis arrays and the level's
+// extents indexed by constants, so nothing is kept in local memory).
+template <int DIM>
+__device__ __forceinline__ void k_build_potential_A_dim(Level L, int level, const float* __restrict__ chi, Geom fine, float dx_l,
                                     float inv_dx_l, int r0, int r1, int r2) {
   const int res[3] = {r0, r1, r2};
   Field fc;
@@ -436,18 +503,20 @@ __global__ void k_build_potential_A(Level L, int level, const float* __restrict_
        i += (long long)gridDim.x * blockDim.x) {
     int c[3];
     L.g.coords(i, c);
-    const bool origin = c[0] == 0 && c[1] == 0 && (L.g.dim == 2 || c[2] == 0);
+    const bool origin = c[0] == 0 && c[1] == 0 && (DIM == 2 || c[2] == 0);
     if (origin) {
       L.Adiag[i] = inv_dx_l;
       continue;
     }
-    if (!in_domain(c, res, L.g.dim)) continue;
+    if (!in_domain(c, res, DIM)) continue;
     float d = L.Adiag[i];
-    for (int k = 0; k < L.g.dim; ++k) {
+#pragma unroll
+    for (int k = 0; k < DIM; ++k) {
+#pragma unroll
       for (int s = -1; s <= 1; s += 2) {
         int nb[3] = {c[0], c[1], c[2]};
         nb[k] += s;
-        if (!in_domain(nb, res, L.g.dim)) continue;
+        if (!in_domain(nb, res, DIM)) continue;
         float pos[3];
         for (int a = 0; a < 3; ++a)
           pos[a] = __fmul_rn(__fadd_rn((float)c[a], a == k ? 0.5f * (float)s : 0.0f), sc);
@@ -458,6 +527,14 @@ __global__ void k_build_potential_A(Level L, int level, const float* __restrict_
     }
     L.Adiag[i] = d;
   }
+}
+
+// dx_l = dx 2^level and inv_dx_l = 1 / dx_l are folded on the host (the
+// reference computes both in double before they meet f32 values).
+__global__ void k_build_potential_A(Level L, int level, const float* __restrict__ chi, Geom fine, float dx_l,
+                                    float inv_dx_l, int r0, int r1, int r2) {
+  if (L.g.dim == 3) k_build_potential_A_dim<3>(L, level, chi, fine, dx_l, inv_dx_l, r0, r1, r2);
+  else k_build_potential_A_dim<2>(L, level, chi, fine, dx_l, inv_dx_l, r0, r1, r2);
 }
 
 // FerrofluidSimulator.update_magnetic_susceptibility (ferrofluid_simulator.py:
@@ -518,30 +595,40 @@ __device__ __forceinline__ void face_pos(const int c[3], const int h[3], int d, 
   }
 }
 
-// SurfaceTension.calc_n (surface_tension.py:108-121): n = grad phi / |grad phi|
-// at I + 0.5 (1 - e_d) by central differences of sampled phi; |n| = 0 leaves
-// the unnormalised gradient.  n is stored as dim planes of the cell grid.
-__global__ void k_calc_n(Geom g, int d, const float* __restrict__ phi, float dx, float* __restrict__ n) {
+// k_calc_n for a compile-time dim (its per-axis arrays and the level's
+// extents indexed by constants, so nothing is kept in local memory).
+template <int DIM>
+__device__ __forceinline__ void k_calc_n_dim(Geom g, int d, const float* __restrict__ phi, float dx, float* __restrict__ n) {
   const Field fp = cell_field(phi, g);
   for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < g.count;
        i += (long long)gridDim.x * blockDim.x) {
     int c[3];
     g.coords(i, c);
     float v[3] = {0.0f, 0.0f, 0.0f};
-    for (int k = 0; k < g.dim; ++k) {
+#pragma unroll
+    for (int k = 0; k < DIM; ++k) {
       int hp[3] = {0, 0, 0}, hm[3] = {0, 0, 0};
       hp[k] = 1;
       hm[k] = -1;
       float pp[3], pm[3];
-      face_pos(c, hp, d, g.dim, 1.0f, pp);
-      face_pos(c, hm, d, g.dim, 1.0f, pm);
+      face_pos(c, hp, d, DIM, 1.0f, pp);
+      face_pos(c, hm, d, DIM, 1.0f, pm);
       v[k] = __fdiv_rn(__fsub_rn(sample(fp, pp), sample(fp, pm)), dx);
     }
     float nn = __fmul_rn(v[0], v[0]);
-    for (int k = 1; k < g.dim; ++k) nn = __fadd_rn(nn, __fmul_rn(v[k], v[k]));
+    for (int k = 1; k < DIM; ++k) nn = __fadd_rn(nn, __fmul_rn(v[k], v[k]));
     const float norm = __fsqrt_rn(nn);
-    for (int k = 0; k < g.dim; ++k) n[k * g.count + i] = norm > 0.0f ? __fdiv_rn(v[k], norm) : v[k];
+#pragma unroll
+    for (int k = 0; k < DIM; ++k) n[k * g.count + i] = norm > 0.0f ? __fdiv_rn(v[k], norm) : v[k];
   }
+}
+
+// SurfaceTension.calc_n (surface_tension.py:108-121): n = grad phi / |grad phi|
+// at I + 0.5 (1 - e_d) by central differences of sampled phi; |n| = 0 leaves
+// the unnormalised gradient.  n is stored as dim planes of the cell grid.
+__global__ void k_calc_n(Geom g, int d, const float* __restrict__ phi, float dx, float* __restrict__ n) {
+  if (g.dim == 3) k_calc_n_dim<3>(g, d, phi, dx, n);
+  else k_calc_n_dim<2>(g, d, phi, dx, n);
 }
 
 // SurfaceTension.calc_kappa (surface_tension.py:123-129): kappa = div n by
@@ -565,11 +652,10 @@ __global__ void k_calc_kappa(Geom g, const float* __restrict__ n, float dx, floa
   }
 }
 
-// SurfaceTensionStrategy.build_b_kernel (surface_tension.py:23-71) for axis d:
-// b = u_d / dt - sigma delta(phi) (kappa n_d + dt (n^T D2 n + kappa grad u . n))
-// with grad u and the Hessian D2 of u_d from samples of the face field at
-// half-cell offsets.  dx2 = dx^2 folded on the host.  Whole domain.
-__global__ void k_build_st_b(Geom g, int d, const float* __restrict__ u, const float* __restrict__ phi,
+// k_build_st_b for a compile-time dim (its per-axis arrays and the level's
+// extents indexed by constants, so nothing is kept in local memory).
+template <int DIM>
+__device__ __forceinline__ void k_build_st_b_dim(Geom g, int d, const float* __restrict__ u, const float* __restrict__ phi,
                              const float* __restrict__ n, const float* __restrict__ kappa, float sigma, float dt,
                              float dx, float dx2, ThetaK th, float* __restrict__ b) {
   const Field fp = cell_field(phi, g);
@@ -581,13 +667,15 @@ __global__ void k_build_st_b(Geom g, int d, const float* __restrict__ u, const f
     float bi = __fdiv_rn(vel_at(u, g, d, c[0], c[1], c[2]), dt);
     float pos[3];
     const int h0[3] = {0, 0, 0};
-    face_pos(c, h0, d, g.dim, 1.0f, pos);
+    face_pos(c, h0, d, DIM, 1.0f, pos);
     const float scale = __fmul_rn(sigma, delta_h(sample(fp, pos), th));
     float nv[3];
-    for (int k = 0; k < g.dim; ++k) nv[k] = n[k * g.count + i];
+#pragma unroll
+    for (int k = 0; k < DIM; ++k) nv[k] = n[k * g.count + i];
     // Du/Dn
     float du = 0.0f;
-    for (int k = 0; k < g.dim; ++k) {
+#pragma unroll
+    for (int k = 0; k < DIM; ++k) {
       float pp[3], pm[3];
       for (int a = 0; a < 3; ++a) {
         pp[a] = __fadd_rn((float)c[a], a == k ? 0.5f : 0.0f);
@@ -598,8 +686,8 @@ __global__ void k_build_st_b(Geom g, int d, const float* __restrict__ u, const f
     }
     // D2u/Dn2 = (n^T D2) n, accumulated in index order
     float D2[3][3];
-    for (int k1 = 0; k1 < g.dim; ++k1)
-      for (int k2 = 0; k2 < g.dim; ++k2) {
+    for (int k1 = 0; k1 < DIM; ++k1)
+      for (int k2 = 0; k2 < DIM; ++k2) {
         float p00[3], p10[3], p01[3], p11[3];
         for (int a = 0; a < 3; ++a) {
           const float h1 = a == k1 ? 0.5f : 0.0f, h2 = a == k2 ? 0.5f : 0.0f;
@@ -613,14 +701,60 @@ __global__ void k_build_st_b(Geom g, int d, const float* __restrict__ u, const f
         D2[k1][k2] = __fdiv_rn(__fsub_rn(__fsub_rn(__fadd_rn(v11, v00), v10), v01), dx2);
       }
     float d2 = 0.0f;
-    for (int j = 0; j < g.dim; ++j) {
+    for (int j = 0; j < DIM; ++j) {
       float t = __fmul_rn(nv[0], D2[0][j]);
-      for (int k = 1; k < g.dim; ++k) t = __fadd_rn(t, __fmul_rn(nv[k], D2[k][j]));
+      for (int k = 1; k < DIM; ++k) t = __fadd_rn(t, __fmul_rn(nv[k], D2[k][j]));
       d2 = j == 0 ? __fmul_rn(t, nv[0]) : __fadd_rn(d2, __fmul_rn(t, nv[j]));
     }
     const float kap = kappa[i];
     const float inner = __fadd_rn(__fmul_rn(kap, nv[d]), __fmul_rn(dt, __fadd_rn(d2, __fmul_rn(kap, du))));
     b[i] = __fsub_rn(bi, __fmul_rn(scale, inner));
+  }
+}
+
+// SurfaceTensionStrategy.build_b_kernel (surface_tension.py:23-71) for axis d:
+// b = u_d / dt - sigma delta(phi) (kappa n_d + dt (n^T D2 n + kappa grad u . n))
+// with grad u and the Hessian D2 of u_d from samples of the face field at
+// half-cell offsets.  dx2 = dx^2 folded on the host.  Whole domain.
+__global__ void k_build_st_b(Geom g, int d, const float* __restrict__ u, const float* __restrict__ phi,
+                             const float* __restrict__ n, const float* __restrict__ kappa, float sigma, float dt,
+                             float dx, float dx2, ThetaK th, float* __restrict__ b) {
+  if (g.dim == 3) k_build_st_b_dim<3>(g, d, u, phi, n, kappa, sigma, dt, dx, dx2, th, b);
+  else k_build_st_b_dim<2>(g, d, u, phi, n, kappa, sigma, dt, dx, dx2, th, b);
+}
+
+// k_build_st_A for a compile-time dim (its per-axis arrays and the level's
+// extents indexed by constants, so nothing is kept in local memory).
+template <int DIM>
+__device__ __forceinline__ void k_build_st_A_dim(Level L, int level, Geom fine, int d, const float* __restrict__ phi, float inv_dt,
+                             float scale, ThetaK th) {
+  const Field fp = cell_field(phi, fine);
+  const float m = (float)(1 << level);
+  const float nscale = -scale;
+  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < L.g.count;
+       i += (long long)gridDim.x * blockDim.x) {
+    int c[3];
+    L.g.coords(i, c);
+    float ad = inv_dt;
+#pragma unroll
+    for (int k = 0; k < DIM; ++k) {
+      int hp[3] = {0, 0, 0}, hm[3] = {0, 0, 0};
+      hp[k] = 1;
+      hm[k] = -1;
+      if (c[k] + 1 < fine.n[k]) {
+        float pos[3];
+        face_pos(c, hp, d, DIM, m, pos);
+        const float dl = delta_h(sample(fp, pos), th);
+        L.Ax[k][i] = __fmul_rn(nscale, dl);
+        ad = __fadd_rn(ad, __fmul_rn(scale, dl));
+      }
+      if (c[k] - 1 >= 0) {
+        float pos[3];
+        face_pos(c, hm, d, DIM, m, pos);
+        ad = __fadd_rn(ad, __fmul_rn(scale, delta_h(sample(fp, pos), th)));
+      }
+    }
+    L.Adiag[i] = ad;
   }
 }
 
@@ -631,33 +765,8 @@ __global__ void k_build_st_b(Geom g, int d, const float* __restrict__ u, const f
 // scale = sigma dt / (dx 2^level)^2 are folded on the host.
 __global__ void k_build_st_A(Level L, int level, Geom fine, int d, const float* __restrict__ phi, float inv_dt,
                              float scale, ThetaK th) {
-  const Field fp = cell_field(phi, fine);
-  const float m = (float)(1 << level);
-  const float nscale = -scale;
-  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < L.g.count;
-       i += (long long)gridDim.x * blockDim.x) {
-    int c[3];
-    L.g.coords(i, c);
-    float ad = inv_dt;
-    for (int k = 0; k < L.g.dim; ++k) {
-      int hp[3] = {0, 0, 0}, hm[3] = {0, 0, 0};
-      hp[k] = 1;
-      hm[k] = -1;
-      if (c[k] + 1 < fine.n[k]) {
-        float pos[3];
-        face_pos(c, hp, d, L.g.dim, m, pos);
-        const float dl = delta_h(sample(fp, pos), th);
-        L.Ax[k][i] = __fmul_rn(nscale, dl);
-        ad = __fadd_rn(ad, __fmul_rn(scale, dl));
-      }
-      if (c[k] - 1 >= 0) {
-        float pos[3];
-        face_pos(c, hm, d, L.g.dim, m, pos);
-        ad = __fadd_rn(ad, __fmul_rn(scale, delta_h(sample(fp, pos), th)));
-      }
-    }
-    L.Adiag[i] = ad;
-  }
+  if (L.g.dim == 3) k_build_st_A_dim<3>(L, level, fine, d, phi, inv_dt, scale, th);
+  else k_build_st_A_dim<2>(L, level, fine, d, phi, inv_dt, scale, th);
 }
 
 }  // namespace mg
