@@ -107,6 +107,7 @@ struct FusedPlan {
   bool res_ok = false, res = false;
   int res_lp = 0, res_lb = 0, res_blocks = 0;
   size_t res_smem = 0;
+  int res_threads = kResThreads;  // k_resident's CTA size (kResThreads or 512)
   ResArgs res_args;
   // z.r of the PCG loop inside the level-0 POST sweep while the plan launches
   // a PCG part (-1: not now; 0 / 1: before / inside the loop)
@@ -382,7 +383,7 @@ inline cudaLaunchConfig_t resident_config(const FusedPlan& F, cudaStream_t s, cu
   at[0].val.clusterDim.z = 1;
   cudaLaunchConfig_t cfg = {};
   cfg.gridDim = dim3(F.res_blocks);
-  cfg.blockDim = dim3(kResThreads);
+  cfg.blockDim = dim3(F.res_threads);
   cfg.dynamicSmemBytes = F.res_smem;
   cfg.stream = s;
   cfg.attrs = at;
@@ -390,9 +391,14 @@ inline cudaLaunchConfig_t resident_config(const FusedPlan& F, cudaStream_t s, cu
   return cfg;
 }
 
+// The instantiation of k_resident for the plan's CTA size.
+inline void (*res_kernel(const FusedPlan& F))(ResArgs) {
+  return F.res_threads == 512 ? k_resident<512> : k_resident<kResThreads>;
+}
+
 inline cudaError_t resident_attributes(const FusedPlan& F) {
-  cudaError_t e = cudaFuncSetAttribute(k_resident, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)F.res_smem);
-  if (e == cudaSuccess) e = cudaFuncSetAttribute(k_resident, cudaFuncAttributeNonPortableClusterSizeAllowed, 1);
+  cudaError_t e = cudaFuncSetAttribute(res_kernel(F), cudaFuncAttributeMaxDynamicSharedMemorySize, (int)F.res_smem);
+  if (e == cudaSuccess) e = cudaFuncSetAttribute(res_kernel(F), cudaFuncAttributeNonPortableClusterSizeAllowed, 1);
   return e;
 }
 
@@ -401,7 +407,7 @@ inline cudaError_t launch_resident(const FusedPlan& F, cudaStream_t s) {
   if (e != cudaSuccess) return e;
   cudaLaunchAttribute at[1];
   const cudaLaunchConfig_t cfg = resident_config(F, s, at);
-  return cudaLaunchKernelEx(&cfg, k_resident, F.res_args);
+  return cudaLaunchKernelEx(&cfg, res_kernel(F), F.res_args);
 }
 
 template <typename ST, bool PRE>

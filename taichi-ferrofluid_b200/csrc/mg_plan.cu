@@ -550,15 +550,15 @@ int tune_stream(mg_plan* P, cudaStream_t s) {
 // MGPCG_RESIDENT=<level> (the cluster from the first feasible level from
 // there) or MGPCG_RESIDENT=off replaces the timing, e.g. for profilers, which
 // serialise the trial launches.
-std::map<std::array<int, 7>, int> g_tune_res;  // first brick level, -1: streamed
+std::map<std::array<int, 7>, int> g_tune_res;  // -1: streamed; else first brick level, + 256 for 512-thread CTAs
 
 // The cluster plan from the first feasible level in [lp_min, lp_max], checked
 // against what the device can hold; false (res_ok = false) when there is none.
 bool plan_resident(mg_plan* P, int lp_min, int lp_max, cudaStream_t s) {
   if (!make_resident_plan(&P->fp, P->lv, P->L, P->d.pre_post, P->d.bottom, lp_min, lp_max)) return false;
-  // whether the device holds the cluster, asked once per (device, CTAs, bytes)
-  static std::map<std::array<int64_t, 3>, bool> fits;
-  const std::array<int64_t, 3> key = {P->device, P->fp.res_blocks, (int64_t)P->fp.res_smem};
+  // whether the device holds the cluster, asked once per (device, CTAs, bytes, threads)
+  static std::map<std::array<int64_t, 4>, bool> fits;
+  const std::array<int64_t, 4> key = {P->device, P->fp.res_blocks, (int64_t)P->fp.res_smem, P->fp.res_threads};
   {
     std::lock_guard<std::mutex> lk(g_tune_mu);
     auto it = fits.find(key);
@@ -572,7 +572,7 @@ bool plan_resident(mg_plan* P, int lp_min, int lp_max, cudaStream_t s) {
     cudaLaunchAttribute at[1];
     const cudaLaunchConfig_t cfg = resident_config(P->fp, s, at);
     int clusters = 0;
-    ok = cudaOccupancyMaxActiveClusters(&clusters, k_resident, &cfg) == cudaSuccess && clusters >= 1;
+    ok = cudaOccupancyMaxActiveClusters(&clusters, res_kernel(P->fp), &cfg) == cudaSuccess && clusters >= 1;
   }
   if (!ok) cudaGetLastError();
   P->fp.res_ok = ok;
@@ -583,15 +583,30 @@ bool plan_resident(mg_plan* P, int lp_min, int lp_max, cudaStream_t s) {
 
 int tune_resident(mg_plan* P, cudaStream_t s) {
   P->fp.res = false;
+  P->fp.res_threads = kResThreads;
   if (!P->fp.valid) return MG_OK;
   if (!plan_resident(P, 0, P->L, s)) return MG_OK;
   const int lp_first = P->fp.res_lp;
+  // MGPCG_RES_THREADS=512|1024 pins the cluster's CTA size with MGPCG_RESIDENT
+  const char* ov_nt = std::getenv("MGPCG_RES_THREADS");
   if (const char* ov = std::getenv("MGPCG_RESIDENT")) {  // "off" / -1, or a start level
     const long v = std::strcmp(ov, "off") == 0 ? -1 : std::strtol(ov, nullptr, 0);
+    if (ov_nt && std::strtol(ov_nt, nullptr, 0) == 512) P->fp.res_threads = 512;
     if (v >= 0 && plan_resident(P, (int)v, P->L, s)) P->fp.res = true;
     else plan_resident(P, lp_first, lp_first, s);
     return MG_OK;
   }
+  // the choice: -1 streamed, else the first cluster level + 256 for 512 threads
+  auto apply = [&](int choice) {
+    P->fp.res_threads = choice >= 256 ? 512 : kResThreads;
+    const int lp = choice >= 0 ? (choice & 255) : -1;
+    if (lp >= 0 && plan_resident(P, lp, lp, s)) {
+      P->fp.res = true;
+    } else {
+      P->fp.res_threads = kResThreads;
+      plan_resident(P, lp_first, lp_first, s);
+    }
+  };
   const Geom& g = P->geom[0];
   const std::array<int, 7> key = {g.dim, g.n[0], g.n[1], g.n[2], P->L, P->d.pre_post, P->fp.lc};
   int cached = -2;  // -2: not timed yet
@@ -601,8 +616,7 @@ int tune_resident(mg_plan* P, cudaStream_t s) {
     if (it != g_tune_res.end()) cached = it->second;
   }
   if (cached != -2) {  // (plan_resident takes the lock itself)
-    if (cached >= 0 && plan_resident(P, cached, cached, s)) P->fp.res = true;
-    else plan_resident(P, lp_first, lp_first, s);
+    apply(cached);
     return MG_OK;
   }
   cudaEvent_t e0 = nullptr, e1 = nullptr;
@@ -625,30 +639,32 @@ int tune_resident(mg_plan* P, cudaStream_t s) {
     return e == cudaSuccess ? MG_OK : set_err("tune_resident", e);
   };
   float best = 0.0f;
-  int best_lp = -1;
+  int best_choice = -1;
   int rc = time_vcycle(&best);  // streamed (res = false)
   for (int lp = lp_first; rc == MG_OK && lp < P->L; ++lp) {
-    if (!plan_resident(P, lp, lp, s)) continue;
-    P->fp.res = true;
-    float t = 0.0f;
-    rc = time_vcycle(&t);
-    P->fp.res = false;
-    if (rc == MG_OK && t < best) {
-      best = t;
-      best_lp = lp;
+    for (int nt : {kResThreads, 512}) {
+      if (rc != MG_OK) break;
+      P->fp.res_threads = nt;
+      if (!plan_resident(P, lp, lp, s)) continue;
+      P->fp.res = true;
+      float t = 0.0f;
+      rc = time_vcycle(&t);
+      P->fp.res = false;
+      if (rc == MG_OK && t < best) {
+        best = t;
+        best_choice = lp + (nt == 512 ? 256 : 0);
+      }
     }
   }
   cudaEventDestroy(e0);
   cudaEventDestroy(e1);
-  if (rc != MG_OK) return rc;
-  if (best_lp >= 0) {
-    plan_resident(P, best_lp, best_lp, s);
-    P->fp.res = true;
-  } else {
-    plan_resident(P, lp_first, lp_first, s);
+  if (rc != MG_OK) {
+    P->fp.res_threads = kResThreads;
+    return rc;
   }
+  apply(best_choice);
   std::lock_guard<std::mutex> lk(g_tune_mu);
-  g_tune_res[key] = best_lp;
+  g_tune_res[key] = best_choice;
   return MG_OK;
 }
 

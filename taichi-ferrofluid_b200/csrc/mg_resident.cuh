@@ -218,7 +218,11 @@ __device__ __forceinline__ void res_smooth(const RB& b, const RNb& n, int col) {
   }
 }
 
-__global__ void __launch_bounds__(kResThreads, 1) k_resident(ResArgs A) {
+// NT threads a CTA (1024 or 512, chosen by measurement per shape: at 512 a
+// thread has 128 registers instead of 64, and handles two cells per colour
+// of a 2048-cell brick).
+template <int NT>
+__global__ void __launch_bounds__(NT, 1) k_resident(ResArgs A) {
   extern __shared__ __align__(16) unsigned char smem[];
   float* sm = (float*)smem;
   cgx::cluster_group cl = cgx::this_cluster();
