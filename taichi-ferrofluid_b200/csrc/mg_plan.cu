@@ -28,6 +28,12 @@
 
 using namespace mg;
 
+// Blocks per SM of the reduction kernels' grids (a whole number of waves at
+// their register counts).
+#ifndef MG_RED_BLOCKS_PER_SM
+#define MG_RED_BLOCKS_PER_SM 4
+#endif
+
 namespace {
 
 thread_local char g_err[512] = "";
@@ -927,7 +933,7 @@ int mg_plan_create(const mg_plan_desc_t* desc, mg_plan_t** out) {
   cudaGetLastError();
   int64_t n0 = P->geom[0].count;
   int64_t rb = (n0 + kRedThreads * 8 - 1) / (kRedThreads * 8);
-  if (rb > P->num_sms * 4) rb = P->num_sms * 4;
+  if (rb > P->num_sms * MG_RED_BLOCKS_PER_SM) rb = P->num_sms * MG_RED_BLOCKS_PER_SM;
   if (rb > kMaxPartials / 2) rb = kMaxPartials / 2;  // two partial regions (b.b and r.r)
   if (rb < 1) rb = 1;
   P->red_blocks = (int)rb;
