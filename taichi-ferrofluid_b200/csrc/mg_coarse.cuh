@@ -52,6 +52,7 @@ struct CoarseArgs {
 // absent third axis).
 struct PGeom {
   int n0, n1, n2, P1, P2, o;   // sizes, padded strides, level offset
+  float r1, r2;                // 1 / n1, 1 / n2 (rounded; cell_coords)
   int s0, s1, s2;              // neighbour strides in the padded grid
   __device__ __forceinline__ int at(int c0, int c1, int c2) const {
     return o + ((c0 + 1) * P1 + (c1 + 1)) * P2 + c2 + (P2 > 1 ? 1 : 0);
@@ -69,7 +70,26 @@ __device__ __forceinline__ PGeom pgeom(const CoarseArgs& A, int l) {
   g.s0 = g.P1 * g.P2;
   g.s1 = g.P2;
   g.s2 = 1;
+  g.r1 = 1.0f / (float)g.n1;
+  g.r2 = 1.0f / (float)g.n2;
   return g;
+}
+
+// Cell i of a level as (c0, c1, c2) (2D: (c0, c1, 0)), the quotients taken
+// through float reciprocals: exact for i < 2^22, since the relative error of
+// (i + 0.5) * RN(1 / n), at most 2^-23, stays below the 0.5 / n that
+// separates (i + 0.5) / n from an integer.
+__device__ __forceinline__ void cell_coords(const PGeom& g, int dim, int i, int& c0, int& c1, int& c2) {
+  if (dim == 3) {
+    const int t = (int)(((float)i + 0.5f) * g.r2);
+    c2 = i - t * g.n2;
+    c0 = (int)(((float)t + 0.5f) * g.r1);
+    c1 = t - c0 * g.n1;
+  } else {
+    c2 = 0;
+    c0 = (int)(((float)i + 0.5f) * g.r1);
+    c1 = i - c0 * g.n1;
+  }
 }
 
 // j-th cell of colour `phase` (rows of the last axis, every other cell);
@@ -176,15 +196,19 @@ __device__ __forceinline__ void coarse_vcycle(const CoarseArgs& A, unsigned char
   const int narr = STO ? 3 + dim : 3;
   // zero everything (the rings stay 0), then load each level's Adiag (and
   // couplings) and level lc's r (FLUID cells) - z starts at 0
-  for (int i = threadIdx.x; i < narr * A.total; i += blockDim.x) zm[i] = 0.0f;
+  {  // 16-byte stores (the region starts 16-byte aligned), then the tail
+    const int nz = narr * A.total, n4 = nz >> 2;
+    float4* z4 = reinterpret_cast<float4*>(zm);
+    for (int i = threadIdx.x; i < n4; i += blockDim.x) z4[i] = make_float4(0.f, 0.f, 0.f, 0.f);
+    for (int i = 4 * n4 + threadIdx.x; i < nz; i += blockDim.x) zm[i] = 0.0f;
+  }
   __syncthreads();
   for (int l = 0; l < A.nlev; ++l) {
     const PGeom g = pgeom(A, l);
     const int cnt = g.n0 * g.n1 * g.n2;
     for (int i = threadIdx.x; i < cnt; i += blockDim.x) {
-      const int c2 = dim == 3 ? i % g.n2 : 0;
-      const int t = dim == 3 ? i / g.n2 : i;
-      const int c1 = t % g.n1, c0 = t / g.n1;
+      int c0, c1, c2;
+      cell_coords(g, dim, i, c0, c1, c2);
       const int p = g.at(c0, c1, c2);
       const float a = to_f<ST>(((const ST*)A.Ad[l])[i]);
       sa[p] = a;
@@ -241,8 +265,8 @@ __device__ __forceinline__ void coarse_vcycle(const CoarseArgs& A, unsigned char
         float val = 0.0f;
         int pc = -1;
         if (i < 8 * cnt) {
-          const int c2 = q % gc.n2, t = q / gc.n2;
-          const int c1 = t % gc.n1, c0 = t / gc.n1;
+          int c0, c1, c2;
+          cell_coords(gc, 3, q, c0, c1, c2);
           pc = gc.at(c0, c1, c2);
           const int p = gf.at(2 * c0 + (o >> 2), 2 * c1 + ((o >> 1) & 1), 2 * c2 + (o & 1));
           const float a = sa[p];
@@ -266,9 +290,8 @@ __device__ __forceinline__ void coarse_vcycle(const CoarseArgs& A, unsigned char
       continue;
     }
     for (int i = threadIdx.x; i < cnt; i += blockDim.x) {
-      const int c2 = dim == 3 ? i % gc.n2 : 0;
-      const int t = dim == 3 ? i / gc.n2 : i;
-      const int c1 = t % gc.n1, c0 = t / gc.n1;
+      int c0, c1, c2;
+      cell_coords(gc, dim, i, c0, c1, c2);
       const int pc = gc.at(c0, c1, c2);
       if (sa[pc] == 0.0f) continue;
       float acc = 0.0f;
@@ -388,9 +411,8 @@ __device__ __forceinline__ void coarse_vcycle(const CoarseArgs& A, unsigned char
     const PGeom gf = pgeom(A, l), gc = pgeom(A, l + 1);
     const int cnt = gf.n0 * gf.n1 * gf.n2;
     for (int i = threadIdx.x; i < cnt; i += blockDim.x) {
-      const int c2 = dim == 3 ? i % gf.n2 : 0;
-      const int t = dim == 3 ? i / gf.n2 : i;
-      const int c1 = t % gf.n1, c0 = t / gf.n1;
+      int c0, c1, c2;
+      cell_coords(gf, dim, i, c0, c1, c2);
       const int pc = gc.at(c0 >> 1, c1 >> 1, dim == 3 ? c2 >> 1 : 0);
       const float v = __fmul_rn(A.pi, sa[pc] != 0.0f ? zm[pc] : sr[pc]);
       const int p = gf.at(c0, c1, c2);
@@ -410,9 +432,8 @@ __device__ __forceinline__ void coarse_vcycle(const CoarseArgs& A, unsigned char
   const PGeom g0 = pgeom(A, 0);
   const int cnt0 = g0.n0 * g0.n1 * g0.n2;
   for (int i = threadIdx.x; i < cnt0; i += blockDim.x) {
-    const int c2 = dim == 3 ? i % g0.n2 : 0;
-    const int t = dim == 3 ? i / g0.n2 : i;
-    const int c1 = t % g0.n1, c0 = t / g0.n1;
+    int c0, c1, c2;
+    cell_coords(g0, dim, i, c0, c1, c2);
     const int p = g0.at(c0, c1, c2);
     ((ST*)A.z0)[i] = from_f<ST>(sa[p] != 0.0f ? zm[p] : sr[p]);
   }
