@@ -461,9 +461,10 @@ MG_API int mg_plan_sweep_kernel(mg_plan_t* plan, int32_t set, uint32_t* bits);
  * its brick of every level in shared memory and reading its neighbours'
  * through distributed shared memory; the levels above stay streamed.  When a
  * shape is first prepared the V-cycle is timed streamed and with the cluster
- * from each feasible level, and the fastest kept (cached per shape);
- * MGPCG_RESIDENT=<level> (the first feasible
- * start level from there) or MGPCG_RESIDENT=off replaces the timing.  set != 0 forces *on and, when
+ * from each feasible level in 1024- and in 512-thread CTAs, and the fastest
+ * kept (cached per shape); MGPCG_RESIDENT=<level> (the first feasible start
+ * level from there; MGPCG_RES_THREADS=512 for 512-thread CTAs) or
+ * MGPCG_RESIDENT=off replaces the timing.  set != 0 forces *on and, when
  * *on and first_level != NULL and *first_level >= 0, the level the cluster
  * starts at (after the plan is prepared; valid until the next prepare; fails
  * when that level, or any, allows no bricks); *on returns the choice and
