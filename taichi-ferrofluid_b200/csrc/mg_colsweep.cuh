@@ -23,7 +23,7 @@
 //   neighbours published in the previous step, so a step needs ONE block
 //   barrier, not one per half sweep.
 // * r, Adiag (and POST's input z) arrive by TMA (cp.async.bulk.tensor, 3D
-//   tile loads of the region plane, no multicast) into a ring of NS + 2
+//   tile loads of the region plane, each block its own) into a ring of NS + 2
 //   shared slots, NS + 1 planes ahead of the one being smoothed, completed on
 //   one mbarrier per slot.  Out-of-grid boxes are zero-filled, which makes
 //   those cells non-FLUID (Adiag 0) with z 0: rule H1 with no bounds checks.
