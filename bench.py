@@ -109,16 +109,23 @@ def parse():
 
 
 # ---------------------------------------------------------------- distributed
-def dist_init(n):
+def dist_init(n, group=True):
+    """Rank, world size and local rank from torchrun's environment.  With
+    `group` and more than one rank, joins the process group: NCCL with the
+    local GPU selected where CUDA is present, else gloo (the host-logic tests).
+    The reference arm passes group=False: rank 0 alone works, so its ranks
+    take no collective step."""
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
-    if world > 1:
+    if world > 1 and group:
         import torch
         import torch.distributed as dist
         import datetime
-        torch.cuda.set_device(local)
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+        backend = "nccl" if torch.cuda.is_available() else "gloo"
+        if backend == "nccl":
+            torch.cuda.set_device(local)
+        dist.init_process_group(backend, timeout=datetime.timedelta(seconds=120))
     return rank, world, local
 
 
@@ -127,7 +134,8 @@ def max_over_ranks(v, world):
         return v
     import torch
     import torch.distributed as dist
-    t = torch.tensor([float(v)], device="cuda")
+    dev = "cuda" if dist.get_backend() == "nccl" else "cpu"
+    t = torch.tensor([float(v)], dtype=torch.float64, device=dev)
     dist.all_reduce(t, op=dist.ReduceOp.MAX)
     return float(t.item())
 
@@ -869,7 +877,7 @@ def main():
     global DIRECT_LAUNCH
     args = parse()
     DIRECT_LAUNCH = args.direct
-    rank, world, local = dist_init(args.gpus)
+    rank, world, local = dist_init(args.gpus, group=args.impl != "reference")
     if args.impl == "reference":
         out = reference_arm(args, rank, world)
         if out is not None:
