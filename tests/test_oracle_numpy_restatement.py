@@ -231,3 +231,93 @@ def test_bit_identity_detects_a_changed_colour_order():
     bad.r[0] = r.copy()
     bad.v_cycle()
     assert not np.array_equal(bad.z[0], o.get("z", 0))
+
+
+# ---- the pressure Strategy's system (pressure_project.py:15-64) and the coarse
+# labels (mgpcg.py:46-60), restated in float32 numpy --------------------------------
+
+AIR, SOLID = mg_scenes.AIR, mg_scenes.SOLID
+
+
+def _nb(a, k, s, fill):
+    """a[I + s e_k] with `fill` outside the grid (labels: SOLID)."""
+    p = np.pad(a, 1, constant_values=fill)
+    sl = [slice(1, -1)] * a.ndim
+    sl[k] = slice(1 + s, p.shape[k] - 1 + s)
+    return p[tuple(sl)]
+
+
+def _vel_at(v, k, s):
+    """velocity[k][I] (s = 0) or velocity[k][I + e_k] (s = 1) on the cell grid."""
+    sl = [slice(None)] * v.ndim
+    sl[k] = slice(s, v.shape[k] - 1 + s)
+    return v[tuple(sl)]
+
+
+def numpy_build_b(sc, clamp):  # pressure_project.py:15-38 (ghost fluid method on)
+    ct = sc.cell_type
+    fl = ct == FLUID
+    sA, sB, p0 = F32(sc.scale_A), F32(sc.scale_b), F32(sc.p0)
+    phi = sc.phi.astype(F32)
+    vel = [v.astype(F32) for v in sc.velocity]
+    b = np.zeros(sc.res, F32)
+    for k in range(sc.dim):
+        b = np.where(fl, b + (_vel_at(vel[k], k, 0) - _vel_at(vel[k], k, 1)), b)
+    b = np.where(fl, b * sB, b)
+    with np.errstate(divide="ignore", invalid="ignore"):
+        for k in range(sc.dim):
+            for s in (-1, 1):
+                nt = _nb(ct, k, s, SOLID)
+                if s < 0:
+                    b = np.where(fl & (nt == SOLID), b - sB * (_vel_at(vel[k], k, 0) - F32(0)), b)
+                else:
+                    b = np.where(fl & (nt == SOLID), b + sB * (_vel_at(vel[k], k, 1) - F32(0)), b)
+                c = (phi - _nb(phi, k, s, F32(1))) / phi
+                b = np.where(fl & (nt == AIR), b + sA * np.minimum(c, F32(clamp)) * p0, b)
+    return b
+
+
+def numpy_build_A(sc, grid_type, level, clamp):  # pressure_project.py:43-64
+    fl = grid_type == FLUID
+    sA = F32(sc.scale_A)
+    phi = sc.phi.astype(F32)
+    Ad = np.zeros(grid_type.shape, F32)
+    Ax = np.zeros((sc.dim,) + grid_type.shape, F32)
+    with np.errstate(divide="ignore", invalid="ignore"):
+        for k in range(sc.dim):
+            for s in (-1, 1):
+                nt = _nb(grid_type, k, s, SOLID)
+                Ad = np.where(fl & (nt == FLUID), Ad + sA, Ad)
+                if s > 0:
+                    Ax[k] = np.where(fl & (nt == FLUID), -sA, Ax[k])
+                if level == 0:
+                    c = (phi - _nb(phi, k, s, F32(1))) / phi
+                    Ad = np.where(fl & (nt == AIR), Ad + sA * np.minimum(c, F32(clamp)), Ad)
+                else:
+                    Ad = np.where(fl & (nt == AIR), Ad + sA, Ad)
+    return Ad, Ax
+
+
+def numpy_init_gridtype(fine):  # mgpcg.py:46-60
+    kids = [fine[tuple(slice(o, None, 2) for o in off)] for off in np.ndindex(*((2,) * fine.ndim))]
+    any_air = np.any([k == AIR for k in kids], axis=0)
+    any_fluid = np.any([k == FLUID for k in kids], axis=0)
+    return np.where(any_air, AIR, np.where(any_fluid, FLUID, SOLID)).astype(np.int8)
+
+
+@pytest.mark.parametrize("name", list(SCENES))
+def test_pressure_system_bit_identical_to_oracle(name):
+    """b, and every level's labels, Adiag and Ax, restated in float32 numpy,
+    equal the float32 oracle's bit for bit."""
+    sc = SCENES[name]()
+    o = _oracle(sc)
+    b = numpy_build_b(sc, sc.gfm_clamp)
+    assert np.array_equal(b.view(np.uint32), o.get("b", 0).view(np.uint32)), int(np.sum(b != o.get("b", 0)))
+    gt = sc.cell_type.astype(np.int8)
+    for l in range(sc.levels):
+        if l > 0:
+            gt = numpy_init_gridtype(gt)
+        assert np.array_equal(gt, o.get("grid_type", l)), l
+        Ad, Ax = numpy_build_A(sc, gt, l, sc.gfm_clamp)
+        assert np.array_equal(Ad.view(np.uint32), o.get("Adiag", l).view(np.uint32)), (l, int(np.sum(Ad != o.get("Adiag", l))))
+        assert np.array_equal(Ax.view(np.uint32), o.get("Ax", l).view(np.uint32)), l
