@@ -128,3 +128,16 @@ def test_static_reduce_refuses_bad_arguments_before_any_cuda_call():
     assert "negative cell count" in mg_lib.last_error()
     assert lib.mg_reduce_static(p, p, p, 33_554_433, p, None) == mg_lib.MG_E_TOO_BIG
     assert "static scratch limit" in mg_lib.last_error()
+
+
+def test_missing_library_fails_loudly(monkeypatch, tmp_path):
+    """Without the built library the product path raises; nothing falls back
+    to a CPU or PyTorch implementation."""
+    import mg_lib
+    monkeypatch.setattr(mg_lib, "_lib", None)
+    monkeypatch.setattr(mg_lib, "LIB_PATH", str(tmp_path / "libmgpcg_b200.so"))
+    with pytest.raises(ImportError, match="no fallback"):
+        mg_lib.load()
+    from mgpcg import MGPCGPoissonSolver
+    with pytest.raises(ImportError, match="no fallback"):
+        MGPCGPoissonSolver(2, (64, 64), 3, 2, 50)
