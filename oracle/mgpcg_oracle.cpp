@@ -7,8 +7,12 @@
 // Python on the Taichi DSL and Taichi is not installable offline, so its own
 // MGPCG cannot be run.  It ships no tests and no golden vectors.  This
 // restatement is pinned instead by (1) scipy sparse direct solves of the same
-// assembled system, (2) an independent numpy assembly of A and b, and (3) the
-// symmetry and linearity of the V-cycle preconditioner (tests/test_oracle.py).
+// assembled system, (2) an independent numpy assembly of A and b, (3) the
+// symmetry and linearity of the V-cycle preconditioner (tests/test_oracle.py),
+// and (4) a second restatement in vectorised float32 numpy, written from the
+// reference's statements, whose system and V-cycle equal this file's bit for
+// bit and whose CG loop reaches the same solution
+// (tests/test_oracle_numpy_restatement.py).
 //
 // Followed statement by statement:
 //   mgpcg.py:46-60   init_gridtype     (coarse label from 2^d children)
